@@ -1,0 +1,640 @@
+"""CPU float64 oracle for the FEA hot path.
+
+TEST INFRASTRUCTURE ONLY.  Nothing in the product (``fea_b200``) may import or
+call this module; only ``tests/``, ``__graft_entry__.smoke()`` and the CPU
+baseline leg of ``bench.py`` use it, and only as the checker or the timed CPU
+baseline.
+
+It restates, in torch-on-CPU float64 code of its own, the algorithms of the
+reference package sssnnn7119/FEA for the path that the CUDA library replaces.
+Every function names the reference lines (``path:line`` inside that project)
+whose behaviour it follows.  The arithmetic is kept in the reference's own
+form (a materialised 81-entry material tangent, einsum contractions over
+``[gauss, element, ...]`` tensors, a sort-based COO pattern) so that it is an
+independent check of the factored formulas used by the kernels.
+
+Parity of this oracle is pinned against golden fixtures produced by running
+the reference package itself (``tests/golden/make_golden.py``).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+DT = torch.float64
+
+# ---------------------------------------------------------------------------
+# Reference elements: Gauss points, weights, shape functions and derivatives
+# ---------------------------------------------------------------------------
+
+
+def tet4_rule():
+    """C3D4: one Gauss point at (1/4, 1/4, 1/4), weight 1/6, linear N.
+
+    Follows FEA/assemble/elements/C3/tetrahedral.py:28-42 (shape table
+    N0 = 1-x-y-z, N1 = x, N2 = y, N3 = z; p0 and the 1/6 weight).
+    Returns (N [G,nn], dN/dxi [G,3,nn], weight [G]).
+    """
+    p = torch.tensor([[0.25, 0.25, 0.25]], dtype=DT)
+    x, y, z = p[:, 0], p[:, 1], p[:, 2]
+    N = torch.stack([1 - x - y - z, x, y, z], dim=1)
+    dN = torch.zeros(1, 3, 4, dtype=DT)
+    dN[:, :, 0] = -1.0
+    for m in range(3):
+        dN[:, m, m + 1] = 1.0
+    return N, dN, torch.tensor([1.0 / 6.0], dtype=DT)
+
+
+HEX_CORNERS = torch.tensor([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
+                            [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], dtype=DT)
+
+
+def hex8_rule():
+    """C3D8: 2x2x2 Gauss points at +-1/sqrt(3) (weight 1), trilinear N.
+
+    Follows FEA/assemble/elements/C3/brick.py:47-164: node ordering of the
+    Abaqus brick (the 8 corners listed at brick.py:15-25), Gauss point order
+    at brick.py:151-160, N_a = 1/8 (1+g g_a)(1+h h_a)(1+r r_a).
+    """
+    q = 1.0 / np.sqrt(3.0)
+    p = HEX_CORNERS * q
+    s = HEX_CORNERS
+    G = p.shape[0]
+    N = torch.zeros(G, 8, dtype=DT)
+    dN = torch.zeros(G, 3, 8, dtype=DT)
+    for g in range(G):
+        f = 1.0 + s * p[g]                      # [8,3] factors (1 + xi*xi_a)
+        N[g] = 0.125 * f.prod(dim=1)
+        for m in range(3):
+            others = [d for d in range(3) if d != m]
+            dN[g, m] = 0.125 * s[:, m] * f[:, others[0]] * f[:, others[1]]
+    return N, dN, torch.ones(G, dtype=DT)
+
+
+def rule(kind: str):
+    return {"C3D4": tet4_rule, "C3D8": hex8_rule}[kind]()
+
+
+def tri3_rule():
+    """T3 surface: 3-point rule (1/6,1/6),(2/3,1/6),(1/6,2/3), weights 1/6.
+
+    Follows FEA/assemble/elements/C3/surfaces/triangle.py (shape table and the
+    three-point rule of T3.initialize).  Returns (N [G,nn], dN [G,2,nn], w [G]).
+    """
+    p = torch.tensor([[1 / 6, 1 / 6], [2 / 3, 1 / 6], [1 / 6, 2 / 3]], dtype=DT)
+    N = torch.stack([1 - p[:, 0] - p[:, 1], p[:, 0], p[:, 1]], dim=1)
+    dN = torch.tensor([[-1.0, 1.0, 0.0], [-1.0, 0.0, 1.0]], dtype=DT).expand(3, 2, 3).clone()
+    return N, dN, torch.full((3,), 1.0 / 6.0, dtype=DT)
+
+
+def quad4_rule():
+    """Q4 surface: 2x2 Gauss at +-1/sqrt(3), weight 1, bilinear N.
+
+    Follows FEA/assemble/elements/C3/surfaces/quadrilateral.py (Q4 shape table,
+    Gauss points (-g,-g),(g,-g),(g,g),(-g,g)).
+    """
+    q = 1.0 / math.sqrt(3.0)
+    p = torch.tensor([[-q, -q], [q, -q], [q, q], [-q, q]], dtype=DT)
+    c = torch.tensor([[-1, -1], [1, -1], [1, 1], [-1, 1]], dtype=DT)
+    N = torch.zeros(4, 4, dtype=DT)
+    dN = torch.zeros(4, 2, 4, dtype=DT)
+    for g in range(4):
+        f = 1.0 + c * p[g]
+        N[g] = 0.25 * f[:, 0] * f[:, 1]
+        dN[g, 0] = 0.25 * c[:, 0] * f[:, 1]
+        dN[g, 1] = 0.25 * c[:, 1] * f[:, 0]
+    return N, dN, torch.ones(4, dtype=DT)
+
+
+# Face node lists per volume element (face id -> local nodes), outward ordering.
+# C3D4: tetrahedral.py:45-64.  C3D8: brick.py:166-201.
+FACES = {
+    "C3D4": {0: [0, 2, 1], 1: [0, 1, 3], 2: [1, 2, 3], 3: [0, 3, 2]},
+    "C3D8": {0: [0, 3, 2, 1], 1: [4, 5, 6, 7], 2: [0, 1, 5, 4], 3: [1, 2, 6, 5],
+             4: [2, 3, 7, 6], 5: [0, 4, 7, 3]},
+}
+
+
+# ---------------------------------------------------------------------------
+# Element geometry (reference configuration)
+# ---------------------------------------------------------------------------
+
+
+def preload_gaussian(kind: str, X: torch.Tensor, elems: torch.Tensor):
+    """dN/dX, N and w*detJ at every Gauss point of every element.
+
+    Follows Element_3D._pre_load_gaussian, FEA/assemble/elements/C3/C3base.py:
+    155-216: Jacobian J[g,e,i,m] = sum_a dN_a/dxi_m X_{a,i}; dN/dX =
+    J^{-T} dN/dxi; weight = detJ * w_g (the sign of detJ is kept).
+    Returns dNdX [G,E,3,nn], wdet [G,E], N [G,E,nn].
+    """
+    N, dN, w = rule(kind)
+    Xe = X[elems]                                        # [E,nn,3]
+    Jac = torch.einsum("gma,eai->geim", dN, Xe)          # [G,E,3(i),3(m)]
+    det = torch.linalg.det(Jac)
+    inv = torch.linalg.inv(Jac)                          # [G,E,m,i]
+    dNdX = torch.einsum("gemi,gma->geia", inv, dN)
+    G, E = Jac.shape[:2]
+    return dNdX, det * w[:, None], N[:, None, :].expand(G, E, N.shape[1])
+
+
+# ---------------------------------------------------------------------------
+# Element pattern (unreduced, per element group)
+# ---------------------------------------------------------------------------
+
+
+def element_pattern(elems: torch.Tensor):
+    """Unique sorted COO of the group's DOF pairs and the element-to-slot map.
+
+    Follows Element_3D.initialize, C3base.py:109-153: entries are enumerated in
+    (a, j, b, k, e) order with e fastest; the COO is the sorted set of distinct
+    (row, col) = (3 n_a + j, 3 n_b + k) pairs; the slot map gives, for every
+    enumerated entry, its position in that COO.  The force index is
+    3 n_a + j in (a, j, e) order.
+    Returns (indices_matrix int64 [2,nnz], slot_map int64 [(3nn)^2 E],
+             indices_force int64 [3 nn E]).
+    """
+    E, nn = elems.shape
+    el = elems.to(torch.int64).T                         # [nn,E]
+    j3 = torch.arange(3, dtype=torch.int64)
+    row = (3 * el[:, None, None, None, :] + j3[None, :, None, None, None]).expand(nn, 3, nn, 3, E)
+    col = (3 * el[None, None, :, None, :] + j3[None, None, None, :, None]).expand(nn, 3, nn, 3, E)
+    S = int(3 * int(elems.max()) + 3)
+    key = (row * S + col).reshape(-1)
+    uniq, inverse = torch.unique(key, sorted=True, return_inverse=True)
+    idx = torch.stack([uniq // S, uniq % S])
+    force = (3 * el[:, None, :] + j3[None, :, None]).reshape(-1)
+    return idx, inverse, force
+
+
+# ---------------------------------------------------------------------------
+# Kinematics and Neo-Hookean material
+# ---------------------------------------------------------------------------
+
+
+def deformation_gradient(U: torch.Tensor, elems: torch.Tensor, dNdX: torch.Tensor):
+    """F[g,e,I,i] = delta_Ii + sum_a U_{a,I} dN_a/dX_i.
+
+    Follows Element_3D.components_Solid, C3base.py:454-469 (and the same sum in
+    potential_Energy, C3base.py:387-400).
+    """
+    Ue = U[elems]                                        # [E,nn,3]
+    F = torch.einsum("geia,eaI->geIi", dNdX, Ue)
+    F = F + torch.eye(3, dtype=DT)
+    return F
+
+
+def neohookean_energy(F, mu, kappa):
+    """W = mu/2 (J^{-2/3} tr(F^T F) - 3) + kappa/2 (J-1)^2.
+
+    Follows NeoHookean.strain_energy_density_C3, hyperelastic.py:25-33.
+    """
+    J = torch.linalg.det(F)
+    I1 = (F ** 2).sum((-1, -2)) * J ** (-2.0 / 3.0)
+    return mu / 2 * (I1 - 3) + kappa / 2 * (J - 1) ** 2
+
+
+def neohookean_stress_tangent(F, mu, kappa):
+    """s = P^T and the full C_ijkl = ds_ij/dF_kl (materialised).
+
+    Follows NeoHookean.material_Constitutive_C3, hyperelastic.py:35-84 with
+    J, J^{-2/3}, I1 and F^{-1} as in C3base.py:466-469.
+    """
+    invF = torch.linalg.inv(F)
+    J = torch.linalg.det(F)[..., None, None]
+    Jm = J ** (-2.0 / 3.0)
+    I1 = (F ** 2).sum((-1, -2))[..., None, None] * Jm
+    muJ = mu * Jm
+    FtJ = F.transpose(-1, -2) * muJ
+    muI1inv = mu * I1 * invF
+    kJinv = kappa * J * invF
+    s = FtJ - muI1inv / 3.0 + kJinv * (J - 1)
+    T1 = -2.0 / 3.0 * FtJ + kJinv * (2 * J - 1) + 2.0 / 9.0 * muI1inv
+    T2 = -2.0 / 3.0 * muJ * invF
+    T3 = muI1inv / 3.0 - kJinv * (J - 1)
+    C = torch.einsum("geij,gelk->geijkl", T1, invF)
+    C = C + torch.einsum("geij,gekl->geijkl", T2, F)
+    C = C + torch.einsum("geik,gelj->geijkl", T3, invF)
+    d = torch.eye(3, dtype=DT)
+    C = C + muJ[..., None, None] * torch.einsum("il,jk->ijkl", d, d)
+    return s, C
+
+
+def element_residual_tangent(kind, X, elems, U, mu, kappa, want_K=True):
+    """Per-element residual R_e[a,j,e] and tangent K_e[a,j,b,k,e].
+
+    Follows Element_3D.structural_Force, C3base.py:413-452:
+    R_e = sum_g s_ij dN_ai w ('geij,geia,ge->aje'),
+    K_e = sum_g C_ijkl dN_ai dN_bl w ('geijkl,gelb,geia,ge->ajbke').
+    """
+    dNdX, w, _ = preload_gaussian(kind, X, elems)
+    F = deformation_gradient(U, elems, dNdX)
+    s, C = neohookean_stress_tangent(F, mu, kappa)
+    R = torch.einsum("geij,geia,ge->aje", s, dNdX, w)
+    if not want_K:
+        return R, None
+    K = torch.einsum("geijkl,gelb,geia,ge->ajbke", C, dNdX, dNdX, w)
+    return R, K
+
+
+def element_energy(kind, X, elems, U, mu, kappa):
+    """sum_{g,e} W(F) w.  Follows Element_3D.potential_Energy, C3base.py:387-411."""
+    dNdX, w, _ = preload_gaussian(kind, X, elems)
+    F = deformation_gradient(U, elems, dNdX)
+    return (neohookean_energy(F, mu, kappa) * w).sum()
+
+
+def element_mass(kind, X, elems, rho):
+    """Consistent element mass M_ab = sum_g rho N_a N_b w  [nn,nn,E].
+
+    Follows Element_3D.get_mass_matrix, C3base.py:348-384 (before the 3-DOF
+    expansion and the slot scatter).
+    """
+    _, w, N = preload_gaussian(kind, X, elems)
+    return torch.einsum("gea,geb,ge->abe", N, N, w * rho)
+
+
+# ---------------------------------------------------------------------------
+# Follower pressure (enclosed-volume potential) on T3 / Q4 faces
+# ---------------------------------------------------------------------------
+
+
+def _surface_rule(nn):
+    return tri3_rule() if nn == 3 else quad4_rule()
+
+
+def _surface_frames(x, faces):
+    N, dN, w = _surface_rule(faces.shape[1])
+    sfa = torch.cat([N[:, None, :], dN], dim=1)          # [G,3(m),nn]
+    xf = x[faces]                                        # [E,nn,3]
+    r = torch.einsum("gma,eai->geim", sfa, xf)           # columns: x, x_xi, x_eta
+    return sfa, r, w
+
+
+def pressure_force_tangent(x, faces, p, want_K=True):
+    """Follower pressure from the enclosed-volume potential.
+
+    Follows Pressure.get_stiffness, FEA/assemble/loads/pressure.py:80-132:
+    V = 1/3 sum_g w det[x, x_xi, x_eta]; the load's force values are
+    -p dV/dx in (e, i, a) order and its stiffness values -p d2V/dx2 in
+    (e, i, a, j, b) order.  Returns (f [E,3,nn], k [E,3,nn,3,nn] or None).
+    """
+    sfa, r, w = _surface_frames(x, faces)
+    det = torch.linalg.det(r)
+    inv = torch.linalg.inv(r)
+    cof = det[..., None, None] * inv.transpose(-1, -2)   # d det / d r[i,m]
+    Vdr = w[:, None, None, None] * cof / 3.0
+    f = torch.einsum("gma,geim->eia", sfa, Vdr)
+    if not want_K:
+        return -p * f, None
+    part1 = torch.einsum("geim,genj->geimjn", cof, inv)
+    part2 = part1.permute(0, 1, 2, 5, 4, 3)
+    V2 = (part1 - part2) * w[:, None, None, None, None, None] / 3.0
+    k = torch.einsum("gma,gnb,geimjn->eiajb", sfa, sfa, V2)
+    return -p * f, -p * k
+
+
+def pressure_volume(x, faces):
+    """Enclosed-volume functional; follows Pressure.get_potential_energy, pressure.py:134-159."""
+    _, r, w = _surface_frames(x, faces)
+    return (w[:, None] * torch.linalg.det(r)).sum() / 3.0
+
+
+# ---------------------------------------------------------------------------
+# A model in the reference's terms: one instance, element groups, pressure
+# loads on faces and Dirichlet node sets.
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class Group:
+    kind: str
+    elems: torch.Tensor          # [E,nn] int64 (part node ids)
+    mu: float
+    kappa: float
+    rho: float = 1.0
+
+
+@dataclass
+class PressureLoad:
+    faces: torch.Tensor          # [F,nf] int64 node ids (T3 or Q4)
+    p: float
+
+
+@dataclass
+class Model:
+    X: torch.Tensor                                      # [N,3]
+    groups: list = field(default_factory=list)
+    pressures: list = field(default_factory=list)
+    fixed: list = field(default_factory=list)            # list of (node ids, dofs)
+
+    def __post_init__(self):
+        self.X = self.X.to(DT)
+
+    # DOF bookkeeping: assembly.py:157-183 and boundary_condition.py:35-41
+    def free_mask(self):
+        N = self.X.shape[0]
+        m = torch.zeros(N, 3, dtype=torch.bool)
+        for g in self.groups:
+            m[torch.unique(g.elems)] = True
+        for pl in self.pressures:
+            m[torch.unique(pl.faces)] = True
+        for nodes, dofs in self.fixed:
+            for d in dofs:
+                m[torch.as_tensor(nodes, dtype=torch.int64), d] = False
+        return m.reshape(-1)
+
+    def initial_gc(self):
+        """GC0 with the 1e-5 seed on the last node (assembly.py:113)."""
+        N = self.X.shape[0]
+        rgc = torch.zeros(N, 3, dtype=DT)
+        rgc[-1] = 1e-5
+        for nodes, dofs in self.fixed:
+            for d in dofs:
+                rgc[torch.as_tensor(nodes, dtype=torch.int64), d] = 0.0
+        return rgc.reshape(-1)[self.free_mask()]
+
+    def gc_to_u(self, gc):
+        """_GC2RGC, assembly.py:470-492 (Dirichlet values are zero)."""
+        u = torch.zeros(self.X.shape[0] * 3, dtype=DT)
+        u[self.free_mask()] = gc
+        return u.reshape(-1, 3)
+
+    # assembly.py:311-387
+    def assemble(self, gc, want_K=True):
+        """Reduced (R, coalesced CSR (indptr, indices, values)).
+
+        Follows Assembly._assemble_generalized_Matrix and
+        _assemble_reduced_Matrix (assembly.py:311-387): element R and K plus
+        the loads' -f and -k, scattered over all DOFs, then rows/cols of
+        Dirichlet DOFs dropped and the rest relabelled in GC order.
+        """
+        u = self.gc_to_u(gc)
+        ndof = self.X.shape[0] * 3
+        R0 = torch.zeros(ndof, dtype=DT)
+        rows, cols, vals = [], [], []
+        for g in self.groups:
+            Re, Ke = element_residual_tangent(g.kind, self.X, g.elems, u, g.mu, g.kappa, want_K)
+            idx, slot, force = element_pattern(g.elems)
+            R0.scatter_add_(0, force, Re.reshape(-1))
+            if want_K:
+                v = torch.zeros(idx.shape[1], dtype=DT).scatter_add_(0, slot, Ke.reshape(-1))
+                rows.append(idx[0]); cols.append(idx[1]); vals.append(v)
+        x = self.X + u
+        for pl in self.pressures:
+            f, k = pressure_force_tangent(x, pl.faces, pl.p, want_K)
+            fi = torch.stack([3 * pl.faces, 3 * pl.faces + 1, 3 * pl.faces + 2], dim=1)
+            R0.scatter_add_(0, fi.reshape(-1), -f.reshape(-1))
+            if want_K:
+                E, nf = pl.faces.shape
+                ra = (3 * pl.faces[:, None, :, None, None] + torch.arange(3)[None, :, None, None, None])
+                cb = (3 * pl.faces[:, None, None, None, :] + torch.arange(3)[None, None, None, :, None])
+                rows.append(ra.expand(E, 3, nf, 3, nf).reshape(-1))
+                cols.append(cb.expand(E, 3, nf, 3, nf).reshape(-1))
+                vals.append(-k.reshape(-1))
+        free = self.free_mask()
+        R = R0[free]
+        if not want_K:
+            return R, None
+        rows = torch.cat(rows); cols = torch.cat(cols); vals = torch.cat(vals)
+        keep = free[rows] & free[cols]
+        rid = torch.cumsum(free.to(torch.int64), 0) - 1    # rank among free DOFs
+        n = int(free.sum())
+        A = torch.sparse_coo_tensor(torch.stack([rid[rows[keep]], rid[cols[keep]]]), vals[keep], (n, n)).coalesce()
+        Ac = A.to_sparse_csr()
+        return R, (Ac.crow_indices(), Ac.col_indices(), Ac.values())
+
+    def energy(self, gc):
+        """Assembly._total_Potential_Energy, assembly.py:389-415 (pressure.py:134-159)."""
+        u = self.gc_to_u(gc)
+        e = torch.zeros((), dtype=DT)
+        for g in self.groups:
+            e = e + element_energy(g.kind, self.X, g.elems, u, g.mu, g.kappa)
+        x = self.X + u
+        for pl in self.pressures:
+            e = e + pl.p * pressure_volume(x, pl.faces)
+        return e
+
+    def lumped_mass_inv(self):
+        """Row-sum lumped inverse mass over free DOFs.
+
+        Follows Element_3D.get_mass_matrix (C3base.py:348-384), the reduction
+        in Assembly.assemble_mass_matrix (assembly.py:421-443) and
+        DynamicExplicitSolver.get_lumped_mass_inv (dynamic_explicit.py:147-167).
+        """
+        free = self.free_mask()
+        ndof = self.X.shape[0] * 3
+        m = torch.zeros(ndof, dtype=DT)
+        for g in self.groups:
+            Me = element_mass(g.kind, self.X, g.elems, g.rho)      # [nn,nn,E]
+            for d in range(3):
+                ra = 3 * g.elems.T + d                             # [nn,E]
+                contrib = Me * free[(3 * g.elems.T + d)][None, :, :]   # drop fixed columns
+                m.scatter_add_(0, ra.reshape(-1), contrib.sum(1).reshape(-1))
+        m = m[free]
+        m[m.abs() < 1e-12] = 1.0
+        return 1.0 / m
+
+
+# ---------------------------------------------------------------------------
+# Solvers
+# ---------------------------------------------------------------------------
+
+
+def csr_matvec(indptr, indices, values, x):
+    A = torch.sparse_csr_tensor(indptr, indices, values, (x.shape[0], x.shape[0]))
+    return A @ x
+
+
+def conjugate_gradient(indptr, indices, values, b, x0=None, tol=1e-3, max_iter=1500):
+    """Plain CG with the squared-ratio stop test ||r||^2/||b||^2 < tol.
+
+    Follows _linear_solver.conjugate_gradient, FEA/solver/_linear_solver.py:6-42.
+    Returns (x, iterations).
+    """
+    x = torch.zeros_like(b) if x0 is None else x0.clone()
+    r_r0 = torch.dot(b, b)
+    r = b - csr_matvec(indptr, indices, values, x)
+    p = r.clone()
+    rs = torch.dot(r, r)
+    it = 0
+    for it in range(1, max_iter + 1):
+        Ap = csr_matvec(indptr, indices, values, p)
+        a = rs / torch.dot(p, Ap)
+        x = x + a * p
+        r = r - a * Ap
+        rsn = torch.dot(r, r)
+        if rsn / r_r0 < tol:
+            break
+        p = r + rsn / rs * p
+        rs = rsn
+    return x, it
+
+
+def jacobi_scaled_cg(indptr, indices, values, R, x0, tol=1e-5, max_iter=1500):
+    """Symmetric Jacobi scaling d = sqrt|diag K| then CG on D^-1 K D^-1.
+
+    Follows StaticImplicitSolver._solve_linear_equation, static_implicit.py:
+    352-405 (diag from the COO diagonal, zero diag -> 1, x0 = dGC0 * d, result
+    divided by d).
+    """
+    n = R.shape[0]
+    rows = torch.repeat_interleave(torch.arange(n), indptr[1:] - indptr[:-1])
+    diag = torch.zeros(n, dtype=DT).scatter_add_(0, rows[rows == indices], values[rows == indices]).abs().sqrt()
+    diag[diag == 0] = 1.0
+    vs = values / diag[rows] / diag[indices]
+    y, it = conjugate_gradient(indptr, indices, vs, R / diag, x0 * diag, tol, max_iter)
+    return y / diag, it
+
+
+def direct_solve(indptr, indices, values, b):
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    n = b.shape[0]
+    A = sp.csr_matrix((values.numpy(), indices.numpy(), indptr.numpy()), shape=(n, n))
+    return torch.from_numpy(spla.spsolve(A.tocsc(), b.numpy()))
+
+
+def newton_solve(model: Model, gc0, tol_error=1e-5, max_iter=100, rtol=None, linear="direct",
+                 cg_tol=1e-5, cg_max=6000):
+    """Newton with Armijo backtracking on the total potential.
+
+    Follows StaticImplicitSolver._solve_iteration and _line_search,
+    static_implicit.py:153-350 (c1 = 0.3, halving, alpha < 1e-12 -> 0; stop
+    when (max|dGC| < tol and max|R| < tol) or max|R| < 1e-6).  With ``rtol``
+    set, the stop test is instead ||R||/||R(gc0)|| <= rtol.
+    Returns (gc, iterations).
+    """
+    gc = gc0.clone()
+    energy = model.energy(gc)
+    dgc = torch.zeros_like(gc)
+    r_ref = None
+    it = 0
+    while it < max_iter:
+        R, (ip, ix, vv) = model.assemble(gc)
+        if r_ref is None:
+            r_ref = R.norm()
+        it += 1
+        if rtol is not None and R.norm() <= rtol * r_ref:
+            break
+        if linear == "direct":
+            dgc = direct_solve(ip, ix, vv, -R)
+        else:
+            dgc, _ = jacobi_scaled_cg(ip, ix, vv, -R, dgc, cg_tol, cg_max)
+        # line search (static_implicit.py:153-232)
+        alpha, c1 = 1.0, 0.3
+        dE = (dgc * R).sum()
+        if dE > 0:
+            dgc, dE = -dgc, -dE
+        while True:
+            trial = gc + alpha * dgc
+            e_new = model.energy(trial)
+            if torch.isnan(e_new) or torch.isinf(e_new) or e_new > energy + c1 * dE * alpha:
+                alpha *= 0.5
+                if alpha < 1e-12:
+                    alpha, trial, e_new = 0.0, gc.clone(), energy
+                    break
+            else:
+                break
+        if alpha == 0.0:
+            break
+        gc, energy = trial, e_new
+        if rtol is None and ((dgc.abs().max() < tol_error and R.abs().max() < tol_error)
+                             or R.abs().max() < 1e-6):
+            break
+    return gc, it
+
+
+def explicit_run(model: Model, gc0, gv0, dt, steps):
+    """Central difference with half-step velocity and lumped mass.
+
+    Follows DynamicExplicitSolver.solve, dynamic_explicit.py:66-145.
+    Returns (u, v, a) after ``steps`` steps (v is the averaged velocity).
+    """
+    minv = model.lumped_mass_inv()
+    a = minv * -model.assemble(gc0, want_K=False)[0]
+    vh_prev = gv0 - 0.5 * dt * a
+    u = gc0.clone()
+    v = gv0.clone()
+    for _ in range(steps):
+        vh = vh_prev + dt * a
+        u = u + dt * vh
+        a = minv * -model.assemble(u, want_K=False)[0]
+        v = 0.5 * (vh + vh_prev)
+        vh_prev = vh
+    return u, v, a
+
+
+# ---------------------------------------------------------------------------
+# Synthetic meshes of the benchmark configurations (seeded)
+# ---------------------------------------------------------------------------
+
+
+def grid_nodes(nx, ny, nz, lx=1.0, ly=1.0, lz=1.0):
+    gx = np.linspace(0, lx, nx + 1)
+    gy = np.linspace(0, ly, ny + 1)
+    gz = np.linspace(0, lz, nz + 1)
+    X, Y, Z = np.meshgrid(gx, gy, gz, indexing="ij")
+    return np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+
+
+def _nid(i, j, k, ny, nz):
+    return (i * (ny + 1) + j) * (nz + 1) + k
+
+
+def hex_block(n, jitter=0.0, seed=0, dims=None, lengths=(1.0, 1.0, 1.0)):
+    """Structured C3D8 block with optional seeded nodal jitter U(-j h, j h)."""
+    nx, ny, nz = dims if dims is not None else (n, n, n)
+    nodes = grid_nodes(nx, ny, nz, *lengths)
+    if jitter:
+        h = np.array([lengths[0] / nx, lengths[1] / ny, lengths[2] / nz])
+        nodes = nodes + np.random.default_rng(seed).uniform(-1, 1, nodes.shape) * jitter * h
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    f = lambda a, b, c: _nid(a, b, c, ny, nz)
+    el = np.stack([f(i, j, k), f(i + 1, j, k), f(i + 1, j + 1, k), f(i, j + 1, k),
+                   f(i, j, k + 1), f(i + 1, j, k + 1), f(i + 1, j + 1, k + 1), f(i, j + 1, k + 1)], 1)
+    return torch.tensor(nodes, dtype=DT), torch.tensor(el, dtype=torch.int64)
+
+
+def tet_block(n, dims=None, lengths=(1.0, 1.0, 1.0)):
+    """Hex grid with every cell Kuhn-split into 6 positively oriented C3D4.
+
+    The 6 tets follow the paths 0 -> x -> y -> z permutations along the cell's
+    0-6 diagonal; tets with negative volume get two nodes swapped.
+    """
+    nx, ny, nz = dims if dims is not None else (n, n, n)
+    nodes = grid_nodes(nx, ny, nz, *lengths)
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    off = {1: (1, 0, 0), 2: (0, 1, 0), 4: (0, 0, 1)}
+    paths = [(1, 2, 4), (1, 4, 2), (2, 1, 4), (2, 4, 1), (4, 1, 2), (4, 2, 1)]
+    tets = []
+    for pth in paths:
+        c = np.zeros(3, dtype=np.int64)
+        t = [_nid(i, j, k, ny, nz)]
+        for s in pth:
+            c = c + np.array(off[s])
+            t.append(_nid(i + c[0], j + c[1], k + c[2], ny, nz))
+        tets.append(np.stack(t, 1))
+    el = np.stack(tets, 1).reshape(-1, 4)               # cell-major, 6 tets per cell
+    x = nodes[el]
+    v = np.einsum("ei,ei->e", np.cross(x[:, 1] - x[:, 0], x[:, 2] - x[:, 0]), x[:, 3] - x[:, 0])
+    neg = v < 0
+    el[neg] = el[neg][:, [0, 2, 1, 3]]
+    return torch.tensor(nodes, dtype=DT), torch.tensor(el, dtype=torch.int64)
+
+
+def boundary_faces(kind, elems, X, axis, value, tol=1e-9):
+    """Faces (node lists in the element's outward face order) lying on a plane."""
+    res = []
+    on = (X[:, axis] - value).abs() < tol
+    for fid, loc in FACES[kind].items():
+        f = elems[:, loc]
+        m = on[f].all(dim=1)
+        if m.any():
+            res.append((torch.nonzero(m).flatten(), fid, f[m]))
+    return res

@@ -1,0 +1,145 @@
+"""The CPU oracle against fixtures produced by running the reference itself."""
+import numpy as np
+import torch
+
+from oracle import fea_oracle as O
+
+DT = torch.float64
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def tet_model(g):
+    X = torch.from_numpy(g["X"])
+    el = torch.from_numpy(g["elems"])
+    faces = torch.from_numpy(g["pressure_faces"])
+    return O.Model(X, [O.Group("C3D4", el, float(g["mu"]), float(g["kappa"]))],
+                   [O.PressureLoad(faces, float(g["p"]))], [(g["fixed"], (0, 1, 2))])
+
+
+def hex_model(g):
+    X = torch.from_numpy(g["X"])
+    el = torch.from_numpy(g["elems"])
+    faces = torch.from_numpy(g["pressure_faces"])
+    return O.Model(X, [O.Group("C3D8", el, float(g["mu"]), float(g["kappa"]))],
+                   [O.PressureLoad(faces, float(g["p"]))], [(g["fixed"], (0, 1, 2))])
+
+
+def test_pressure_faces_match_face_tables(golden):
+    """The load's face node lists equal the element face tables (tetrahedral.py:45-64)."""
+    g = golden("cfg1")
+    el = torch.from_numpy(g["elems"])
+    X = torch.from_numpy(g["X"])
+    mine = torch.cat([f for _, _, f in O.boundary_faces("C3D4", el, X, 2, 1.0)])
+    assert torch.equal(mine, torch.from_numpy(g["pressure_faces"]))
+
+
+def test_initial_gc_quirk(golden):
+    for name, mk in (("cfg1", tet_model), ("hex5", hex_model)):
+        g = golden(name)
+        m = mk(g)
+        np.testing.assert_array_equal(m.initial_gc().numpy(), g["gc0"])
+
+
+def test_element_pattern_bit_exact(golden):
+    for name in ("tet3", "hex5"):
+        g = golden(name)
+        idx, slot, force = O.element_pattern(torch.from_numpy(g["elems"]))
+        np.testing.assert_array_equal(idx.numpy(), g["elem_K_indices"])
+        np.testing.assert_array_equal(slot.numpy(), g["elem_slot"])
+        np.testing.assert_array_equal(force.numpy(), g["elem_force_index"])
+
+
+def test_element_residual_tangent_energy(golden):
+    for name, kind in (("tet3", "C3D4"), ("hex5", "C3D8")):
+        g = golden(name)
+        m = tet_model(g) if kind == "C3D4" else hex_model(g)
+        U = m.gc_to_u(torch.from_numpy(g["state"]))
+        Re, Ke = O.element_residual_tangent(kind, m.X, m.groups[0].elems, U, m.groups[0].mu, m.groups[0].kappa)
+        assert rel(Re.reshape(-1), g["elem_R"]) < 1e-13
+        idx, slot, _ = O.element_pattern(m.groups[0].elems)
+        vals = torch.zeros(idx.shape[1], dtype=DT).scatter_add_(0, slot, Ke.reshape(-1))
+        assert rel(vals, g["elem_K_values"]) < 1e-13
+        e = O.element_energy(kind, m.X, m.groups[0].elems, U, m.groups[0].mu, m.groups[0].kappa)
+        assert abs(float(e) - float(g["elem_energy"])) <= 1e-13 * abs(float(g["elem_energy"]))
+
+
+def test_element_mass(golden):
+    for name, kind in (("tet3", "C3D4"), ("hex5", "C3D8")):
+        g = golden(name)
+        el = torch.from_numpy(g["elems"])
+        Me = O.element_mass(kind, torch.from_numpy(g["X"]), el, 1.0)
+        full = torch.zeros(el.shape[1], 3, el.shape[1], 3, el.shape[0], dtype=DT)
+        for d in range(3):
+            full[:, d, :, d, :] = Me
+        idx, slot, _ = O.element_pattern(el)
+        vals = torch.zeros(idx.shape[1], dtype=DT).scatter_add_(0, slot, full.reshape(-1))
+        np.testing.assert_array_equal(idx.numpy(), g["mass_indices"])
+        assert rel(vals, g["mass_values"]) < 1e-14
+
+
+def test_pressure_load(golden):
+    g = golden("hex5")
+    m = hex_model(g)
+    x = m.X + m.gc_to_u(torch.from_numpy(g["state"]))
+    f, k = O.pressure_force_tangent(x, m.pressures[0].faces, m.pressures[0].p)
+    assert rel(f.reshape(-1), g["pressure_force"]) < 1e-13
+    assert rel(k.reshape(-1), g["pressure_K"]) < 1e-13
+    v = O.pressure_volume(x, m.pressures[0].faces)
+    assert abs(float(-m.pressures[0].p * v) - float(g["pressure_energy"])) < 1e-13 * abs(float(g["pressure_energy"]))
+
+
+def test_reduced_assembly_csr(golden):
+    for name, mk in (("cfg1", tet_model), ("tet3", tet_model), ("hex5", hex_model)):
+        g = golden(name)
+        m = mk(g)
+        state = torch.from_numpy(g["state"])
+        R, (ip, ix, vv) = m.assemble(state)
+        np.testing.assert_array_equal(ip.numpy(), g["indptr"])
+        np.testing.assert_array_equal(ix.numpy(), g["indices"])
+        assert rel(vv, g["values"]) < 1e-13
+        assert rel(R, g["R"]) < 1e-13
+        assert abs(float(m.energy(state)) - float(g["energy"])) <= 1e-13 * abs(float(g["energy"]))
+
+
+def test_newton_converged_displacements(golden):
+    """Oracle Newton (direct solve) lands on the reference's converged GC."""
+    g = golden("hex5")
+    m = hex_model(g)
+    gc, _ = O.newton_solve(m, m.initial_gc(), rtol=1e-13, max_iter=30)
+    assert rel(gc, g["gc_converged"]) < 1e-10
+    g = golden("cfg1")
+    m = tet_model(g)
+    gc = m.initial_gc()
+    for k in range(5):
+        m.pressures[0].p = float(g["p"]) * (k + 1) / 5
+        gc, _ = O.newton_solve(m, gc, rtol=1e-13, max_iter=30)
+        assert rel(gc, g["gc_increments"][k]) < 1e-10
+
+
+def test_explicit_run(golden):
+    g = golden("explicit_tet4")
+    X = torch.from_numpy(g["X"])
+    m = O.Model(X, [O.Group("C3D4", torch.from_numpy(g["elems"]), float(g["mu"]), float(g["kappa"]), float(g["rho"]))])
+    assert rel(m.lumped_mass_inv(), g["minv"]) < 1e-14
+    n = X.shape[0] * 3
+    u, v, a = O.explicit_run(m, torch.zeros(n, dtype=DT), torch.from_numpy(g["gv0"]), float(g["dt"]), int(g["steps"]))
+    assert rel(u, g["u_final"]) < 1e-12
+    assert rel(v, g["v_final"]) < 1e-12
+    assert rel(a, g["a_final"]) < 1e-12
+
+
+def test_cg_matches_reference_semantics(golden):
+    """Jacobi-scaled CG solves the reduced system of the reference."""
+    g = golden("hex5")
+    ip = torch.from_numpy(g["indptr"]); ix = torch.from_numpy(g["indices"]).long(); vv = torch.from_numpy(g["values"])
+    b = -torch.from_numpy(g["R"])
+    x, it = O.jacobi_scaled_cg(ip, ix, vv, b, torch.zeros_like(b), tol=1e-24, max_iter=5000)
+    r = b - O.csr_matvec(ip, ix, vv, x)
+    assert r.norm() / b.norm() < 1e-10
+    xd = O.direct_solve(ip, ix, vv, b)
+    assert rel(x, xd) < 1e-9
