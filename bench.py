@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Element residual + tangent + reduced-CSR assembly throughput (GElem/s).
+
+Workload (one GPU): a 64^3 C3D8 block on [0,1]^3, nodes jittered by
+U(-0.1h, 0.1h) (seed 0), compressible Neo-Hookean mu = 1, kappa = 50, the
+x = 0 face clamped, follower pressure p = -0.02 on the x = 1 face (Q4);
+262,144 elements, 274,625 nodes, 811,200 free DOFs, 63,695,790 nonzeros.
+One step = one full assembly of the reduced residual R and tangent K at a
+seeded displacement state (all element groups and the pressure load), i.e.
+what the Newton solver does per iteration.  The K values (510 MB) exceed the
+126 MB L2, so no flush is needed between steps.
+
+`value` is device-timed (inputs resident in HBM).  `e2e` goes through the
+public API ``Assembly.assemble_Stiffness_Matrix`` with the displacement
+copied from pinned host memory and the residual read back every step.
+Under torchrun (N > 1) every rank assembles its own block (weak scaling,
+no collective in the data path); times are the max over ranks.
+
+``--impl reference`` times the CPU restatement of the reference algorithm
+(oracle/) on a bounded slab of the same mesh with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "elem tangent+assembly GElem/s"
+UNIT = "GElem/s"
+
+
+def args_():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="fea_b200", choices=["fea_b200", "reference"])
+    ap.add_argument("--n", type=int, default=64, help="elements per side of the C3D8 block")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-clocks", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n):
+    """Mesh, clamp set, pressure surface and state of the benchmark."""
+    from fea_b200 import meshes
+    X, el = meshes.hex_block(n, jitter=0.1, seed=0)
+    E = el.shape[0]
+    i_el = np.arange(E) // (n * n)
+    end = np.nonzero(i_el == n - 1)[0]
+    clamp = np.arange((n + 1) * (n + 1))           # node plane i = 0
+    faces = el[end][:, [1, 2, 6, 5]]                # face 3 (x = max) of the end elements
+    return X, el, clamp, end, faces
+
+
+def algorithmic_bytes(E, nn, nnz, N, n):
+    """Per-assembly algorithmic bytes: connectivity, the reference's int32
+    element-to-slot map, K values, coordinates + displacement, residual."""
+    return E * 4 * nn + E * 4 * (3 * nn) ** 2 + 8 * nnz + 48 * N + 8 * n
+
+
+def sample_clocks(stop, out, dev):
+    cmd = ["nvidia-smi", "-i", str(dev), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+           "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+           "--format=csv,noheader,nounits", "-lms", "100"]
+    try:
+        p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except OSError:
+        return
+    def reader():
+        for line in p.stdout:
+            out.append(line.strip())
+    t = threading.Thread(target=reader, daemon=True)
+    t.start()
+    stop.wait()
+    p.terminate()
+    try:
+        p.wait(timeout=5)
+    except subprocess.TimeoutExpired:
+        p.kill()
+    t.join(timeout=2)
+
+
+def summarize_clocks(lines):
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for ln in lines:
+        f = [x.strip() for x in ln.split(",")]
+        if len(f) < 8:
+            continue
+        try:
+            sm.append(float(f[0]))
+            mx = float(f[1])
+        except ValueError:
+            continue
+        for nm, v in zip(names, f[4:8]):
+            if v.lower().startswith("active"):
+                reasons.add(nm)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(n, seconds):
+    """Oracle (CPU restatement of the reference) on a slab of the same mesh."""
+    import torch
+    from oracle import fea_oracle as O
+    torch.set_num_threads(os.cpu_count() or 1)
+    X, el, clamp, end, faces = workload(n)
+    slab = max(1, min(n, 4))                        # elements i < slab
+    E = el.shape[0]
+    keep = np.nonzero(np.arange(E) // (n * n) < slab)[0]
+    els = torch.from_numpy(el[keep])
+    m = O.Model(torch.from_numpy(X), [O.Group("C3D8", els, 1.0, 50.0)], [], [(clamp, (0, 1, 2))])
+    free = m.free_mask()
+    gc = 1e-3 * torch.randn(int(free.sum()), generator=torch.Generator().manual_seed(0), dtype=torch.float64)
+    m.assemble(gc)                                   # warm-up (pattern build excluded below)
+    pat = O.element_pattern(els)
+    t0, reps = time.perf_counter(), 0
+    while True:
+        # R + K + slot scatter + Dirichlet reduction, pattern precomputed
+        u = m.gc_to_u(gc)
+        Re, Ke = O.element_residual_tangent("C3D8", m.X, els, u, 1.0, 50.0)
+        idx, slot, force = pat
+        R0 = torch.zeros(m.X.shape[0] * 3, dtype=torch.float64).scatter_add_(0, force, Re.reshape(-1))
+        v = torch.zeros(idx.shape[1], dtype=torch.float64).scatter_add_(0, slot, Ke.reshape(-1))
+        keepk = free[idx[0]] & free[idx[1]]
+        _ = (R0[free], v[keepk])
+        reps += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = (time.perf_counter() - t0) / reps
+    return {"value": len(keep) / dt / 1e9, "unit": UNIT, "cores": torch.get_num_threads(), "kind": "port",
+            "sample": "%d-element slab (%d x %d x %d C3D8) of the same mesh, R+K+slot scatter+reduction, "
+                      "%d reps in %.1f s" % (len(keep), slab, n, n, reps, reps * dt)}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = []
+    cb = None
+    for k in range(a.warmup + a.steps):
+        cb = cpu_baseline(a.n, max(1.0, a.cpu_seconds / max(1, a.steps)))
+        if k >= a.warmup:
+            steps.append(cb["value"])
+    v = statistics.median(steps)
+    cb["value"] = v
+    X, el, *_ = workload(a.n)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": el.shape[0] / (v * 1e9) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "c3d8_%dcube_jitter_neohookean_assembly" % a.n, "elements": int(el.shape[0])},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = args_()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    import torch
+    import torch.distributed as dist
+    import fea_b200 as F
+    from fea_b200 import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    X, el, clamp, end, faces = workload(a.n)
+    n = a.n
+    part = F.Part(X)
+    e = F.elements.C3D8(elems=el, elems_index=np.arange(el.shape[0]), part=part)
+    e.set_materials(F.materials.NeoHookean(1.0, 50.0))
+    part.add_element(e)
+    part.set_nodes["clamp"] = clamp
+    part.add_surface_set("end", [(end, 3)])
+    asm = F.Assembly()
+    asm.add_part(part, "block")
+    asm.add_instance(F.Instance(part), "block")
+    asm.add_load(F.loads.Pressure("block", "end", -0.02), "traction")
+    asm.add_boundary(F.boundarys.Boundary_Condition("block", "clamp"), "clamp")
+    asm.initialize()
+    P = asm.plan
+    E, N, ndof, nnz = el.shape[0], X.shape[0], P.ndof, P.nnz
+    gc = (1e-3 * torch.randn(ndof, generator=torch.Generator().manual_seed(0), dtype=torch.float64)).cuda()
+    K = torch.empty(nnz, dtype=torch.float64, device="cuda")
+    R = torch.empty(ndof, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t)
+
+    # element kernel timed live: events around the volume kernel of every step
+    mu, kappa = 1.0, 50.0
+
+    def step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        P.assemble_volume(0, mu, kappa, gc, K=K, R=R)
+        if ev is not None:
+            ev[1].record(stream)
+        P.assemble_pressure(0, -0.02, asm._Xinst, gc, K=K, R=R)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    clocks_lines, stop = [], threading.Event()
+    th = None
+    if not a.no_clocks:
+        th = threading.Thread(target=sample_clocks, args=(stop, clocks_lines, local), daemon=True)
+        th.start()
+        time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    l0 = _lib.fea_launch_count()
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(a.steps):
+        step(evs[k])
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    launches = _lib.fea_launch_count() - l0
+    barrier()
+    stop.set()
+    if th is not None:
+        th.join(timeout=10)
+    ms = max_over_ranks(t_start.elapsed_time(t_end) / a.steps)
+    kern_ms = statistics.mean(s.elapsed_time(t) for s, t in evs)
+    value = world * E / (ms * 1e-3) / 1e9
+
+    # end to end through the public API, host buffers
+    gc_h = gc.cpu().pin_memory()
+    r_h = torch.empty(ndof, dtype=torch.float64).pin_memory()
+    gc_d = torch.empty_like(gc)
+    for _ in range(2):
+        gc_d.copy_(gc_h, non_blocking=True)
+        Rr, Ki, Kv = asm.assemble_Stiffness_Matrix(GC=gc_d)
+        r_h.copy_(Rr, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        gc_d.copy_(gc_h, non_blocking=True)
+        Rr, Ki, Kv = asm.assemble_Stiffness_Matrix(GC=gc_d)
+        r_h.copy_(Rr, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / a.steps)
+    barrier()
+
+    B = algorithmic_bytes(E, 8, nnz, N, ndof)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = B / (kern_ms * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "c3d8_rk_traffic.json")
+    if os.path.exists(tf):
+        try:
+            t = json.load(open(tf))
+            traffic = float(t["bytes_per_element"]) * E
+        except (OSError, KeyError, ValueError):
+            traffic = None
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "c3d8_%dcube_jitter_neohookean_assembly" % n, "elements": E, "nodes": N,
+                   "ndof": ndof, "nnz": nnz, "parallelism": "replica per GPU" if world > 1 else "single GPU",
+                   "l2": "K values %.0f MB > 126 MB L2, no flush" % (8 * nnz / 1e6)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic, "algorithmic_bytes": B, "kernel_ms": kern_ms,
+                     "kernel": "k_vol_rk<8> (C3D8 R+K gather)",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650"},
+        "e2e": {"value": world * E / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": 8 * ndof, "d2h_bytes_per_step": 8 * ndof,
+                "api": "Assembly.assemble_Stiffness_Matrix"},
+        "gpu_launches": int(launches),
+        "clocks": summarize_clocks(clocks_lines),
+    }
+    if world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(n, a.cpu_seconds)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

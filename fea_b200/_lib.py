@@ -1,0 +1,103 @@
+"""ctypes binding of libfea_b200.so (the C ABI declared in include/fea_b200.h).
+
+The library is built in-tree (``python -m fea_b200._build``).  Importing this
+module loads it; a missing library raises ImportError — there is no fallback
+implementation of any kernel.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfea_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError("fea_b200: native library %s is missing; build it with "
+                      "`python -m fea_b200._build` (nvcc, sm_100a)" % LIB_PATH)
+lib = C.CDLL(LIB_PATH)
+
+FEA_OK = 0
+ERRORS = {-1: "invalid argument", -2: "index out of range", -3: "a node does not fit one gather chunk",
+          -4: "shared memory request exceeds the device limit", -5: "work buffer too small",
+          -6: "iteration cap reached", -7: "PCG breakdown (p.Ap <= 0 or non-finite)"}
+FEA_ENOTCONV = -6
+FEA_EBREAKDOWN = -7
+
+FEA_C3D4, FEA_C3D8, FEA_T3, FEA_Q4 = 4, 8, 3, 40
+
+(FEA_S_NDOF, FEA_S_NNZ, FEA_S_NNZB) = (0, 1, 2)
+(FEA_A_RDOF, FEA_A_MASK, FEA_A_DBASE, FEA_A_VBASE, FEA_A_ROWLEN, FEA_A_INDPTR, FEA_A_INDICES,
+ FEA_A_ADJPTR, FEA_A_ADJCOL, FEA_A_ADJOFF) = range(10, 20)
+G_BASE, F_BASE = 30, 50
+(A_INC, A_BOFF, A_NODEINC, A_CHUNKNODE, A_CHUNKINC, S_NCHUNK, S_MAXVAL, S_THREADS, S_SMEM) = range(9)
+
+
+class FeaError(RuntimeError):
+    def __init__(self, what, status):
+        self.status = status
+        msg = ERRORS.get(status, "CUDA error %d" % status if status > 0 else "status %d" % status)
+        super().__init__("%s failed: %s" % (what, msg))
+
+
+def check(status, what):
+    if status != FEA_OK:
+        raise FeaError(what, status)
+    return status
+
+
+class Nodes(C.Structure):
+    _fields_ = [("n_nodes", C.c_int64), ("ndof", C.c_int64), ("nnz", C.c_int64),
+                ("X_dev", C.c_void_p), ("rdof_dev", C.c_void_p), ("mask_dev", C.c_void_p),
+                ("vbase_dev", C.c_void_p), ("rowlen_dev", C.c_void_p), ("dbase_dev", C.c_void_p)]
+
+
+class Group(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("nn", C.c_int32), ("ne", C.c_int64),
+                ("conn_dev", C.c_void_p), ("inc_dev", C.c_void_p), ("boff_dev", C.c_void_p),
+                ("nodeinc_dev", C.c_void_p), ("chunknode_dev", C.c_void_p), ("chunkinc_dev", C.c_void_p),
+                ("nchunk", C.c_int64), ("maxval", C.c_int32), ("threads", C.c_int32),
+                ("smem_doubles", C.c_int64)]
+
+
+P = C.c_void_p
+I32, I64, D = C.c_int32, C.c_int64, C.c_double
+NP, GP = C.POINTER(Nodes), C.POINTER(Group)
+
+
+def _sig(name, res, *args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+fea_plan_build = _sig("fea_plan_build", I32, I64, P, I32, P, P, P, I32, P, P, P, I32, I64, C.POINTER(P))
+fea_plan_free = _sig("fea_plan_free", None, P)
+fea_plan_get = _sig("fea_plan_get", I32, P, I32, I32, P, C.POINTER(I64))
+fea_assemble_volume = _sig("fea_assemble_volume", I32, NP, GP, D, D, P, P, P, P, I32, P)
+fea_assemble_pressure = _sig("fea_assemble_pressure", I32, NP, GP, D, P, P, P, P, P)
+fea_reduce_scratch_len = _sig("fea_reduce_scratch_len", I64, I64)
+fea_energy_volume = _sig("fea_energy_volume", I32, NP, GP, D, D, P, P, P, I64, P)
+fea_energy_pressure = _sig("fea_energy_pressure", I32, NP, GP, P, P, P, P, I64, P)
+fea_lumped_mass = _sig("fea_lumped_mass", I32, NP, GP, D, P, P)
+fea_invert_mass = _sig("fea_invert_mass", I32, I64, P, P)
+fea_pcg_work_len = _sig("fea_pcg_work_len", I64, I64)
+fea_pcg_solve = _sig("fea_pcg_solve", I32, I64, P, P, P, P, P, D, I32, I32, I32, P, I64,
+                     C.POINTER(I32), C.POINTER(D), P)
+fea_pcg_mixed_work_len = _sig("fea_pcg_mixed_work_len", I64, I64)
+fea_pcg_solve_mixed = _sig("fea_pcg_solve_mixed", I32, I64, P, P, P, P, P, P, D, D, I32, I32, P, I64,
+                           C.POINTER(I32), C.POINTER(I32), C.POINTER(D), P)
+fea_spmv = _sig("fea_spmv", I32, I64, P, P, P, P, P, P)
+fea_convert_f32 = _sig("fea_convert_f32", I32, I64, P, P, P)
+fea_explicit_work_len = _sig("fea_explicit_work_len", I64, I64)
+fea_explicit_run = _sig("fea_explicit_run", I32, NP, GP, D, D, P, D, I64, I32, I32, P, P, P, P, P, I64, P)
+fea_version = _sig("fea_version", I32)
+fea_launch_count = _sig("fea_launch_count", I64)
+
+# every symbol the header declares (checked by the CPU test suite)
+EXPORTED = ["fea_plan_build", "fea_plan_free", "fea_plan_get", "fea_assemble_volume", "fea_assemble_pressure",
+            "fea_reduce_scratch_len", "fea_energy_volume", "fea_energy_pressure", "fea_lumped_mass",
+            "fea_invert_mass", "fea_pcg_work_len", "fea_pcg_solve", "fea_pcg_mixed_work_len",
+            "fea_pcg_solve_mixed", "fea_spmv", "fea_convert_f32", "fea_explicit_work_len", "fea_explicit_run",
+            "fea_version", "fea_launch_count"]

@@ -1,0 +1,794 @@
+// Element residual / tangent assembly, follower pressure, energy and lumped
+// mass for C3D4 / C3D8 Neo-Hookean groups (sm_100a, FP64).
+//
+// Assembly is a per-node-row GATHER: every (row node n, incident element e)
+// pair ("incidence") gets one thread, which evaluates the element at all its
+// Gauss points and accumulates the 3 x (3 nn) strip K_e[a(n), :] in
+// registers.  The strips of one node are summed in shared memory in a fixed
+// order (incidence rank), and the chunk's rows — a contiguous range of the
+// reduced CSR values — are written to HBM exactly once.  No atomics, no
+// colouring, bitwise-deterministic results.
+//
+// Reference behaviour reproduced (FEA = sssnnn7119/FEA):
+//   F, J, J^-2/3, I1          Element_3D.components_Solid   C3base.py:454-480
+//   s = P^T, C_ijkl           NeoHookean.material_Constitutive_C3
+//                                                   materials/hyperelastic.py:35-84
+//   R_e, K_e, slot scatter    Element_3D.structural_Force   C3base.py:413-452
+//   reduced R, K              Assembly._assemble_*_Matrix   assembly.py:311-387
+// The kernel never forms the 81-entry C: with alpha = -2/3 mu J^-2/3,
+// beta = kappa J (2J-1) + 2/9 mu I1, gamma = mu I1/3 - kappa J (J-1),
+// f_b = F g_b and q_b = F^-T g_b (g_b = dN_b/dX), the reference's
+// contraction sum_il C_ijkl g_ai g_bl equals
+//   (alpha f_a + beta q_a)_j q_bk + alpha q_aj f_bk + gamma q_ak q_bj
+//   + mu J^-2/3 (g_a . g_b) delta_jk.
+#include <cmath>
+#include <cstdio>
+
+#include "common.cuh"
+
+namespace fea {
+
+struct VolParams {
+  const double* __restrict__ X;
+  const int32_t* __restrict__ rdof;
+  const uint8_t* __restrict__ mask;
+  const int64_t* __restrict__ vbase;
+  const int32_t* __restrict__ rowlen;
+  const int32_t* __restrict__ dbase;
+  const int32_t* __restrict__ conn;
+  const int32_t* __restrict__ inc;
+  const uint16_t* __restrict__ boff;
+  const int32_t* __restrict__ nodeinc;
+  const int32_t* __restrict__ chunknode;
+  const int32_t* __restrict__ chunkinc;
+  const double* __restrict__ gc;
+  double* K;
+  double* R;
+  double* elemR;
+  double mu, kappa;
+  int64_t ne;
+  int32_t maxval;
+  int32_t n_nodes;
+};
+
+// Kinematics of one element at one Gauss point: w, F, F^-1, J and the two
+// gradient maps Mq = J0^-1 F^-1, Mf = J0^-1 F^T (so that q_b = Mq^T dxi_b,
+// f_b = Mf^T dxi_b) plus iJ = J0^-1 (g_b = iJ^T dxi_b).
+template <int NN>
+__device__ __forceinline__ void gauss_kin(const VolParams& P, const int32_t* cn, const unsigned* mk,
+                                          const int32_t* rd, int g, double& w, double F[9], double iF[9],
+                                          double& J, double iJ[9]) {
+  double J0[9], Ju[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) J0[i] = Ju[i] = 0.0;
+#pragma unroll
+  for (int b = 0; b < NN; ++b) {
+    const double* xb = P.X + 3 * (int64_t)cn[b];
+    double x0 = __ldg(xb), x1 = __ldg(xb + 1), x2 = __ldg(xb + 2);
+    double u0 = node_u(P.gc, rd[b], mk[b], 0), u1 = node_u(P.gc, rd[b], mk[b], 1),
+           u2 = node_u(P.gc, rd[b], mk[b], 2);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      double d = Elem<NN>::dxi(g, b, m);
+      J0[m] += x0 * d; J0[3 + m] += x1 * d; J0[6 + m] += x2 * d;
+      Ju[m] += u0 * d; Ju[3 + m] += u1 * d; Ju[6 + m] += u2 * d;
+    }
+  }
+  double det0 = inv3(J0, iJ);
+  w = det0 * Elem<NN>::wq(g);
+#pragma unroll
+  for (int I = 0; I < 3; ++I)
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      F[3 * I + i] = (I == i ? 1.0 : 0.0) + Ju[3 * I] * iJ[i] + Ju[3 * I + 1] * iJ[3 + i] + Ju[3 * I + 2] * iJ[6 + i];
+  J = inv3(F, iF);
+}
+
+// Residual strip (3) and, if WK, tangent strip (NN x 9) of local node a.
+template <int NN, bool WK>
+__device__ __forceinline__ void element_strip(const VolParams& P, const int32_t* cn, int a,
+                                              double (*acc)[9], double racc[3]) {
+  unsigned mk[NN];
+  int32_t rd[NN];
+#pragma unroll
+  for (int b = 0; b < NN; ++b) {
+    mk[b] = P.mask[cn[b]];
+    rd[b] = P.rdof[cn[b]];
+  }
+  racc[0] = racc[1] = racc[2] = 0.0;
+  if (WK) {
+#pragma unroll
+    for (int b = 0; b < NN; ++b)
+#pragma unroll
+      for (int i = 0; i < 9; ++i) acc[b][i] = 0.0;
+  }
+  const double mu = P.mu, kappa = P.kappa;
+#pragma unroll
+  for (int g = 0; g < Elem<NN>::NG; ++g) {
+    double w, F[9], iF[9], J, iJ[9];
+    gauss_kin<NN>(P, cn, mk, rd, g, w, F, iF, J, iJ);
+    double Jm = pow(J, -2.0 / 3.0);
+    double sF2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];
+    double I1 = Jm * sF2;
+    double muJm = mu * Jm;
+    double c2 = kappa * J * (J - 1.0) - mu * I1 / 3.0;
+    // Mq[m][k] = sum_i iJ[m][i] iF[i][k];  Mf[m][k] = sum_i iJ[m][i] F[k][i]
+    double Mq[9], Mf[9];
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        Mq[3 * m + k] = iJ[3 * m] * iF[k] + iJ[3 * m + 1] * iF[3 + k] + iJ[3 * m + 2] * iF[6 + k];
+        Mf[3 * m + k] = iJ[3 * m] * F[3 * k] + iJ[3 * m + 1] * F[3 * k + 1] + iJ[3 * m + 2] * F[3 * k + 2];
+      }
+    double da0 = Elem<NN>::dxi(g, a, 0), da1 = Elem<NN>::dxi(g, a, 1), da2 = Elem<NN>::dxi(g, a, 2);
+    double qa[3], fa[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      qa[k] = da0 * Mq[k] + da1 * Mq[3 + k] + da2 * Mq[6 + k];
+      fa[k] = da0 * Mf[k] + da1 * Mf[3 + k] + da2 * Mf[6 + k];
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) racc[j] += w * (muJm * fa[j] + c2 * qa[j]);
+    if (WK) {
+      double alpha = -2.0 / 3.0 * muJm;
+      double beta = kappa * J * (2.0 * J - 1.0) + 2.0 / 9.0 * mu * I1;
+      double gamma = mu * I1 / 3.0 - kappa * J * (J - 1.0);
+      double va[3], ua[3], ga[3], gm[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        va[j] = w * (alpha * fa[j] + beta * qa[j]);
+        ua[j] = w * alpha * qa[j];
+        ga[j] = w * gamma * qa[j];
+      }
+      // g_a = iJ^T dxi_a ; gm = iJ g_a (so that g_a . g_b = gm . dxi_b)
+      double gav[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) gav[i] = da0 * iJ[i] + da1 * iJ[3 + i] + da2 * iJ[6 + i];
+      double wc = w * muJm;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) gm[m] = wc * (iJ[3 * m] * gav[0] + iJ[3 * m + 1] * gav[1] + iJ[3 * m + 2] * gav[2]);
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          double h[3];
+#pragma unroll
+          for (int m = 0; m < 3; ++m)
+            h[m] = va[j] * Mq[3 * m + k] + ua[j] * Mf[3 * m + k] + ga[k] * Mq[3 * m + j] + (j == k ? gm[m] : 0.0);
+#pragma unroll
+          for (int b = 0; b < NN; ++b)
+            acc[b][3 * j + k] += Elem<NN>::dxi(g, b, 0) * h[0] + Elem<NN>::dxi(g, b, 1) * h[1] +
+                                 Elem<NN>::dxi(g, b, 2) * h[2];
+        }
+    }
+  }
+}
+
+template <int NN>
+struct VolTPB { static constexpr int v = NN == 8 ? 128 : 256; };
+
+// R + K gather kernel: one CTA per chunk of consecutive node rows.
+template <int NN, bool WR, bool ACC, bool ER>
+__global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
+  extern __shared__ double sm[];
+  const int ch = blockIdx.x;
+  const int n0 = P.chunknode[ch], n1 = P.chunknode[ch + 1];
+  const int i0 = P.chunkinc[ch], i1 = P.chunkinc[ch + 1];
+  const int64_t v0 = P.vbase[n0];
+  const int nv = (int)(P.vbase[n1] - v0);
+  const int d0 = P.dbase[n0];
+  const int nr = WR ? P.dbase[n1] - d0 : 0;
+  for (int i = threadIdx.x; i < nv + nr; i += blockDim.x) sm[i] = 0.0;
+  __syncthreads();
+
+  const int q = i0 + threadIdx.x;
+  const bool act = q < i1;
+  double acc[NN][9];
+  double racc[3];
+  int32_t cn[NN];
+  int rank = -1, a = 0, n = 0;
+  if (act) {
+    const int ea = P.inc[q];
+    const int64_t e = ea >> 4;
+    a = ea & 15;
+#pragma unroll
+    for (int b = 0; b < NN; ++b) cn[b] = P.conn[e * NN + b];
+    n = cn[a];
+    rank = q - P.nodeinc[n];
+    element_strip<NN, true>(P, cn, a, acc, racc);
+    if (ER) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) P.elemR[(int64_t)(3 * a + j) * P.ne + e] = racc[j];
+    }
+  }
+  // per-node sums in incidence order (one thread per node per round)
+  unsigned mn = 0;
+  int rowoff = 0, L = 0, dr = 0;
+  if (act) {
+    mn = P.mask[n];
+    rowoff = (int)(P.vbase[n] - v0);
+    L = P.rowlen[n];
+    dr = P.dbase[n] - d0;
+  }
+  for (int k = 0; k < P.maxval; ++k) {
+    if (rank == k) {
+#pragma unroll
+      for (int b = 0; b < NN; ++b) {
+        const unsigned bo = P.boff[(int64_t)q * NN + b];
+        if (bo == 0xFFFFu) continue;
+        const unsigned mc = P.mask[cn[b]];
+        int rj = 0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          if (!(mn >> j & 1u)) continue;
+          double* row = sm + rowoff + rj * L + bo;
+          int rk = 0;
+#pragma unroll
+          for (int kk = 0; kk < 3; ++kk) {
+            if (!(mc >> kk & 1u)) continue;
+            row[rk] += acc[b][3 * j + kk];
+            ++rk;
+          }
+          ++rj;
+        }
+      }
+      if (WR) {
+        int rj = 0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          if (mn >> j & 1u) sm[nv + dr + rj++] += racc[j];
+      }
+    }
+    __syncthreads();
+  }
+  double* Kout = P.K + v0;
+  for (int i = threadIdx.x; i < nv; i += blockDim.x) {
+    if (ACC) Kout[i] += sm[i];
+    else Kout[i] = sm[i];
+  }
+  if (WR) {
+    double* Rout = P.R + d0;
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+      if (ACC) Rout[i] += sm[nv + i];
+      else Rout[i] = sm[nv + i];
+    }
+  }
+}
+
+// R-only kernel: one thread per node, sequential over its incidences.
+template <int NN, bool ACC, bool ER>
+__global__ void __launch_bounds__(128) k_vol_r(VolParams P) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= P.n_nodes) return;
+  const unsigned mn = P.mask[n];
+  if (!mn) return;
+  double r[3] = {0.0, 0.0, 0.0};
+  for (int q = P.nodeinc[n]; q < P.nodeinc[n + 1]; ++q) {
+    const int ea = P.inc[q];
+    const int64_t e = ea >> 4;
+    const int a = ea & 15;
+    int32_t cn[NN];
+#pragma unroll
+    for (int b = 0; b < NN; ++b) cn[b] = P.conn[e * NN + b];
+    double racc[3];
+    element_strip<NN, false>(P, cn, a, nullptr, racc);
+    if (ER) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) P.elemR[(int64_t)(3 * a + j) * P.ne + e] = racc[j];
+    }
+    r[0] += racc[0]; r[1] += racc[1]; r[2] += racc[2];
+  }
+  double* Rout = P.R + P.rdof[n];
+  int rj = 0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+    if (mn >> j & 1u) {
+      if (ACC) Rout[rj] += r[j];
+      else Rout[rj] = r[j];
+      ++rj;
+    }
+}
+
+// ---- element energy: thread per element, deterministic two-stage sum ----
+template <int NN>
+__global__ void __launch_bounds__(256) k_vol_energy(VolParams P, double* partial) {
+  __shared__ double sh[256];
+  const int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  double acc = 0.0;
+  if (e < P.ne) {
+    int32_t cn[NN];
+    unsigned mk[NN];
+    int32_t rd[NN];
+#pragma unroll
+    for (int b = 0; b < NN; ++b) {
+      cn[b] = P.conn[e * NN + b];
+      mk[b] = P.mask[cn[b]];
+      rd[b] = P.rdof[cn[b]];
+    }
+#pragma unroll
+    for (int g = 0; g < Elem<NN>::NG; ++g) {
+      double w, F[9], iF[9], J, iJ[9];
+      gauss_kin<NN>(P, cn, mk, rd, g, w, F, iF, J, iJ);
+      double sF2 = 0.0;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];
+      double I1 = sF2 * pow(J, -2.0 / 3.0);
+      double W = P.mu / 2.0 * (I1 - 3.0) + P.kappa / 2.0 * (J - 1.0) * (J - 1.0);
+      acc += W * w;
+    }
+  }
+  double s = block_sum<256>(acc, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(256) k_sum_partials(const double* __restrict__ partial, int64_t n, double* out,
+                                                      int accumulate) {
+  __shared__ double sh[256];
+  double acc = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += 256) acc += partial[i];
+  double s = block_sum<256>(acc, sh);
+  if (threadIdx.x == 0) out[0] = accumulate ? out[0] + s : s;
+}
+
+// ---- follower pressure (enclosed volume) ---------------------------------
+struct FaceParams {
+  const double* __restrict__ Xi;   // instance coordinates
+  const int32_t* __restrict__ rdof;
+  const uint8_t* __restrict__ mask;
+  const int64_t* __restrict__ vbase;
+  const int32_t* __restrict__ rowlen;
+  const int32_t* __restrict__ dbase;
+  const int32_t* __restrict__ conn;
+  const int32_t* __restrict__ inc;
+  const uint16_t* __restrict__ boff;
+  const int32_t* __restrict__ nodeinc;
+  const int32_t* __restrict__ chunknode;
+  const int32_t* __restrict__ chunkinc;
+  const double* __restrict__ gc;
+  double* K;
+  double* R;
+  double p;
+  int64_t nf;
+  int32_t maxval;
+};
+
+template <int NF>
+struct Face;
+template <>
+struct Face<3> {
+  static constexpr int NG = 3;
+  __device__ static __forceinline__ double sf(int g, int m, int a) { return c_sf_t3[g][m][a]; }
+  __device__ static __forceinline__ double w(int g) { return c_w_t3[g]; }
+};
+template <>
+struct Face<4> {
+  static constexpr int NG = 4;
+  __device__ static __forceinline__ double sf(int g, int m, int a) { return c_sf_q4[g][m][a]; }
+  __device__ static __forceinline__ double w(int g) { return c_w_q4[g]; }
+};
+
+// Frame r[i][m] = sum_b sf[m][b] x_b[i] (columns: x, x_xi, x_eta) at Gauss point g.
+template <int NF>
+__device__ __forceinline__ void face_frame(const double (*x)[3], int g, double r[9]) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      double s = 0.0;
+#pragma unroll
+      for (int b = 0; b < NF; ++b) s += Face<NF>::sf(g, m, b) * x[b][i];
+      r[3 * i + m] = s;
+    }
+}
+
+template <int NF>
+__device__ __forceinline__ void face_nodes(const FaceParams& P, const int32_t* cn, double (*x)[3]) {
+#pragma unroll
+  for (int b = 0; b < NF; ++b) {
+    unsigned m = P.mask[cn[b]];
+    int32_t rd = P.rdof[cn[b]];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) x[b][i] = P.Xi[3 * (int64_t)cn[b] + i] + node_u(P.gc, rd, m, i);
+  }
+}
+
+// Pressure.get_stiffness (pressure.py:80-132) for row node a of one face:
+//   dV/dx_a[i]       = sum_g w/3 A_i,            A_i = sum_m sf[m][a] cof[i][m]
+//   d2V/dx_a,i dx_b,j = sum_g w/3 (A_i C_j(b) - D_i(b) B_j),
+//   B_j = sum_m sf[m][a] inv[m][j], C_j(b) = sum_n sf[n][b] inv[n][j],
+//   D_i(b) = sum_n sf[n][b] cof[i][n], cof = det * inv^T.
+// The assembly adds +p dV/dx to R and +p d2V/dx2 to K (assembly.py:336-341).
+template <int NF>
+__global__ void __launch_bounds__(128) k_face_rk(FaceParams P) {
+  extern __shared__ double sm[];
+  const int ch = blockIdx.x;
+  const int n0 = P.chunknode[ch], n1 = P.chunknode[ch + 1];
+  const int i0 = P.chunkinc[ch], i1 = P.chunkinc[ch + 1];
+  const int64_t v0 = P.vbase[n0];
+  const int nv = P.K ? (int)(P.vbase[n1] - v0) : 0;
+  const int d0 = P.dbase[n0];
+  const int nr = P.R ? P.dbase[n1] - d0 : 0;
+  for (int i = threadIdx.x; i < nv + nr; i += blockDim.x) sm[i] = 0.0;
+  __syncthreads();
+  const int q = i0 + threadIdx.x;
+  const bool act = q < i1;
+  double kacc[NF][9];
+  double racc[3] = {0.0, 0.0, 0.0};
+  int32_t cn[NF];
+  int rank = -1, n = 0;
+  if (act) {
+    const int ea = P.inc[q];
+    const int64_t f = ea >> 4;
+    const int a = ea & 15;
+#pragma unroll
+    for (int b = 0; b < NF; ++b) cn[b] = P.conn[f * NF + b];
+    n = cn[a];
+    rank = q - P.nodeinc[n];
+    double x[NF][3];
+    face_nodes<NF>(P, cn, x);
+#pragma unroll
+    for (int b = 0; b < NF; ++b)
+#pragma unroll
+      for (int i = 0; i < 9; ++i) kacc[b][i] = 0.0;
+#pragma unroll
+    for (int g = 0; g < Face<NF>::NG; ++g) {
+      double r[9], inv[9];
+      face_frame<NF>(x, g, r);
+      double det = inv3(r, inv);
+      double w3 = Face<NF>::w(g) / 3.0 * P.p;
+      double A[3], B[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        double sa = 0.0, sb = 0.0;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          sa += Face<NF>::sf(g, m, a) * det * inv[3 * m + i];   // cof[i][m] = det inv[m][i]
+          sb += Face<NF>::sf(g, m, a) * inv[3 * m + i];         // B_i
+        }
+        A[i] = sa;
+        B[i] = sb;
+      }
+#pragma unroll
+      for (int i = 0; i < 3; ++i) racc[i] += w3 * A[i];
+#pragma unroll
+      for (int b = 0; b < NF; ++b) {
+        double C[3], D[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          double sc = 0.0;
+#pragma unroll
+          for (int m = 0; m < 3; ++m) sc += Face<NF>::sf(g, m, b) * inv[3 * m + j];
+          C[j] = sc;
+          D[j] = det * sc;   // D_i(b) = sum_n sf[n][b] det inv[n][i]
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) kacc[b][3 * i + j] += w3 * (A[i] * C[j] - D[i] * B[j]);
+      }
+    }
+  }
+  unsigned mn = 0;
+  int rowoff = 0, L = 0, dr = 0;
+  if (act) {
+    mn = P.mask[n];
+    rowoff = (int)(P.vbase[n] - v0);
+    L = P.rowlen[n];
+    dr = P.dbase[n] - d0;
+  }
+  for (int k = 0; k < P.maxval; ++k) {
+    if (rank == k) {
+      if (nv) {
+#pragma unroll
+        for (int b = 0; b < NF; ++b) {
+          const unsigned bo = P.boff[(int64_t)q * NF + b];
+          if (bo == 0xFFFFu) continue;
+          const unsigned mc = P.mask[cn[b]];
+          int rj = 0;
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            if (!(mn >> j & 1u)) continue;
+            double* row = sm + rowoff + rj * L + bo;
+            int rk = 0;
+#pragma unroll
+            for (int kk = 0; kk < 3; ++kk) {
+              if (!(mc >> kk & 1u)) continue;
+              row[rk] += kacc[b][3 * j + kk];
+              ++rk;
+            }
+            ++rj;
+          }
+        }
+      }
+      if (nr) {
+        int rj = 0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          if (mn >> j & 1u) sm[nv + dr + rj++] += racc[j];
+      }
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < nv; i += blockDim.x) P.K[v0 + i] += sm[i];
+  for (int i = threadIdx.x; i < nr; i += blockDim.x) P.R[d0 + i] += sm[nv + i];
+}
+
+template <int NF>
+__global__ void __launch_bounds__(256) k_face_volume(FaceParams P, double* partial) {
+  __shared__ double sh[256];
+  const int64_t f = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  double acc = 0.0;
+  if (f < P.nf) {
+    int32_t cn[NF];
+#pragma unroll
+    for (int b = 0; b < NF; ++b) cn[b] = P.conn[f * NF + b];
+    double x[NF][3];
+    face_nodes<NF>(P, cn, x);
+#pragma unroll
+    for (int g = 0; g < Face<NF>::NG; ++g) {
+      double r[9];
+      face_frame<NF>(x, g, r);
+      acc += Face<NF>::w(g) * det3(r) / 3.0;
+    }
+  }
+  double s = block_sum<256>(acc, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+// ---- lumped mass: thread per node ------------------------------------------
+// m[(n,d)] += sum_{e,b} rho w N_a N_b over free (conn[e][b], d), the row sum
+// of the reduced consistent mass (C3base.py:348-384, assembly.py:421-443,
+// dynamic_explicit.py:147-167).
+template <int NN>
+__global__ void __launch_bounds__(128) k_lumped_mass(VolParams P, double rho, double* m) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= P.n_nodes) return;
+  const unsigned mn = P.mask[n];
+  if (!mn) return;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int q = P.nodeinc[n]; q < P.nodeinc[n + 1]; ++q) {
+    const int ea = P.inc[q];
+    const int64_t e = ea >> 4;
+    const int a = ea & 15;
+    int32_t cn[NN];
+    unsigned mk[NN];
+#pragma unroll
+    for (int b = 0; b < NN; ++b) {
+      cn[b] = P.conn[e * NN + b];
+      mk[b] = P.mask[cn[b]];
+    }
+#pragma unroll
+    for (int g = 0; g < Elem<NN>::NG; ++g) {
+      double J0[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) J0[i] = 0.0;
+#pragma unroll
+      for (int b = 0; b < NN; ++b)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          double d = Elem<NN>::dxi(g, b, m);
+#pragma unroll
+          for (int i = 0; i < 3; ++i) J0[3 * i + m] += P.X[3 * (int64_t)cn[b] + i] * d;
+        }
+      double w = det3(J0) * Elem<NN>::wq(g) * rho * Elem<NN>::N(g, a);
+#pragma unroll
+      for (int b = 0; b < NN; ++b) {
+        double t = w * Elem<NN>::N(g, b);
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          if (mk[b] >> d & 1u) acc[d] += t;
+      }
+    }
+  }
+  double* out = m + P.rdof[n];
+  int rj = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    if (mn >> d & 1u) out[rj++] += acc[d];
+}
+
+__global__ void k_invert_mass(int64_t n, double* m) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    double v = m[i];
+    m[i] = 1.0 / (fabs(v) < 1e-12 ? 1.0 : v);
+  }
+}
+
+// ---- host side ---------------------------------------------------------------
+static VolParams vol_params(const fea_nodes_t* N, const fea_group_t* G, double mu, double kappa,
+                            const double* gc) {
+  VolParams P;
+  P.X = N->X_dev;
+  P.rdof = N->rdof_dev;
+  P.mask = N->mask_dev;
+  P.vbase = N->vbase_dev;
+  P.rowlen = N->rowlen_dev;
+  P.dbase = N->dbase_dev;
+  P.conn = G->conn_dev;
+  P.inc = G->inc_dev;
+  P.boff = G->boff_dev;
+  P.nodeinc = G->nodeinc_dev;
+  P.chunknode = G->chunknode_dev;
+  P.chunkinc = G->chunkinc_dev;
+  P.gc = gc;
+  P.K = P.R = P.elemR = nullptr;
+  P.mu = mu;
+  P.kappa = kappa;
+  P.ne = G->ne;
+  P.maxval = G->maxval;
+  P.n_nodes = (int32_t)N->n_nodes;
+  return P;
+}
+
+static int smem_limit() {
+  int dev = 0, v = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return v;
+}
+
+template <class Prm>
+static int launch_chunked(void (*kern)(Prm), int64_t nchunk, int threads, int64_t smem_doubles, cudaStream_t st,
+                          const Prm& p) {
+  size_t bytes = (size_t)smem_doubles * sizeof(double);
+  if (bytes > (size_t)smem_limit()) return FEA_ESMEM;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (err != cudaSuccess) return (int)err;
+  if (nchunk <= 0) return 0;
+  kern<<<(unsigned)nchunk, threads, bytes, st>>>(p);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+}  // namespace fea
+
+using namespace fea;
+
+extern "C" int64_t fea_reduce_scratch_len(int64_t n_items) { return (n_items + 255) / 256 + 1; }
+
+extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, double mu, double kappa,
+                                   const double* gc, double* K, double* R, double* elemR, int32_t accumulate,
+                                   cudaStream_t st) {
+  if (!N || !G || !gc || (G->kind != FEA_C3D4 && G->kind != FEA_C3D8)) return FEA_EINVAL;
+  if (G->nn != (G->kind == FEA_C3D8 ? 8 : 4)) return FEA_EINVAL;
+  if (int r = ensure_tables()) return r;
+  VolParams P = vol_params(N, G, mu, kappa, gc);
+  P.K = K;
+  P.R = R;
+  P.elemR = elemR;
+  const bool hex = G->kind == FEA_C3D8;
+  const int tpb = hex ? VolTPB<8>::v : VolTPB<4>::v;
+  if (G->threads != tpb) return FEA_ECHUNK;
+  if (K) {
+    int64_t smem = G->smem_doubles;
+    const bool acc = accumulate != 0, wr = R != nullptr, er = elemR != nullptr;
+#define FEA_RK(NN_, WR_, ACC_, ER_)                                                                    \
+  if (wr == WR_ && acc == ACC_ && er == ER_)                                                           \
+    return launch_chunked(k_vol_rk<NN_, WR_, ACC_, ER_>, G->nchunk, tpb, smem, st, P);
+    if (hex) {
+      FEA_RK(8, true, false, false) FEA_RK(8, true, true, false) FEA_RK(8, false, false, false)
+      FEA_RK(8, false, true, false) FEA_RK(8, true, false, true) FEA_RK(8, true, true, true)
+      FEA_RK(8, false, false, true) FEA_RK(8, false, true, true)
+    } else {
+      FEA_RK(4, true, false, false) FEA_RK(4, true, true, false) FEA_RK(4, false, false, false)
+      FEA_RK(4, false, true, false) FEA_RK(4, true, false, true) FEA_RK(4, true, true, true)
+      FEA_RK(4, false, false, true) FEA_RK(4, false, true, true)
+    }
+#undef FEA_RK
+    return FEA_EINVAL;
+  }
+  if (!R && !elemR) return FEA_OK;
+  double* Rtmp = R;
+  if (!R) return FEA_EINVAL;  // the residual-only path writes R
+  P.R = Rtmp;
+  const int grid = grid_for(N->n_nodes, 128);
+  if (N->n_nodes == 0) return FEA_OK;
+  if (hex) {
+    if (accumulate) elemR ? k_vol_r<8, true, true><<<grid, 128, 0, st>>>(P) : k_vol_r<8, true, false><<<grid, 128, 0, st>>>(P);
+    else elemR ? k_vol_r<8, false, true><<<grid, 128, 0, st>>>(P) : k_vol_r<8, false, false><<<grid, 128, 0, st>>>(P);
+  } else {
+    if (accumulate) elemR ? k_vol_r<4, true, true><<<grid, 128, 0, st>>>(P) : k_vol_r<4, true, false><<<grid, 128, 0, st>>>(P);
+    else elemR ? k_vol_r<4, false, true><<<grid, 128, 0, st>>>(P) : k_vol_r<4, false, false><<<grid, 128, 0, st>>>(P);
+  }
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+static FaceParams face_params(const fea_nodes_t* N, const fea_group_t* G, double p, const double* Xi,
+                              const double* gc) {
+  FaceParams P;
+  P.Xi = Xi;
+  P.rdof = N->rdof_dev;
+  P.mask = N->mask_dev;
+  P.vbase = N->vbase_dev;
+  P.rowlen = N->rowlen_dev;
+  P.dbase = N->dbase_dev;
+  P.conn = G->conn_dev;
+  P.inc = G->inc_dev;
+  P.boff = G->boff_dev;
+  P.nodeinc = G->nodeinc_dev;
+  P.chunknode = G->chunknode_dev;
+  P.chunkinc = G->chunkinc_dev;
+  P.gc = gc;
+  P.K = P.R = nullptr;
+  P.p = p;
+  P.nf = G->ne;
+  P.maxval = G->maxval;
+  return P;
+}
+
+extern "C" int fea_assemble_pressure(const fea_nodes_t* N, const fea_group_t* G, double p, const double* Xi,
+                                     const double* gc, double* K, double* R, cudaStream_t st) {
+  if (!N || !G || !Xi || !gc || (G->kind != FEA_T3 && G->kind != FEA_Q4)) return FEA_EINVAL;
+  if (G->nn != (G->kind == FEA_T3 ? 3 : 4) || G->threads != 128) return FEA_EINVAL;
+  if (int r = ensure_tables()) return r;
+  if (!K && !R) return FEA_OK;
+  FaceParams P = face_params(N, G, p, Xi, gc);
+  P.K = K;
+  P.R = R;
+  if (G->kind == FEA_T3) return launch_chunked(k_face_rk<3>, G->nchunk, 128, G->smem_doubles, st, P);
+  return launch_chunked(k_face_rk<4>, G->nchunk, 128, G->smem_doubles, st, P);
+}
+
+extern "C" int fea_energy_volume(const fea_nodes_t* N, const fea_group_t* G, double mu, double kappa,
+                                 const double* gc, double* out, double* scratch, int64_t scratch_len,
+                                 cudaStream_t st) {
+  if (!N || !G || !gc || !out || !scratch) return FEA_EINVAL;
+  if (G->kind != FEA_C3D4 && G->kind != FEA_C3D8) return FEA_EINVAL;
+  if (scratch_len < fea_reduce_scratch_len(G->ne)) return FEA_EWORK;
+  if (int r = ensure_tables()) return r;
+  VolParams P = vol_params(N, G, mu, kappa, gc);
+  const int64_t nb = (G->ne + 255) / 256;
+  if (nb > 0) {
+    if (G->kind == FEA_C3D8) k_vol_energy<8><<<(unsigned)nb, 256, 0, st>>>(P, scratch);
+    else k_vol_energy<4><<<(unsigned)nb, 256, 0, st>>>(P, scratch);
+    count_launch();
+  }
+  k_sum_partials<<<1, 256, 0, st>>>(scratch, nb, out, 0);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+extern "C" int fea_energy_pressure(const fea_nodes_t* N, const fea_group_t* G, const double* Xi,
+                                   const double* gc, double* out, double* scratch, int64_t scratch_len,
+                                   cudaStream_t st) {
+  if (!N || !G || !Xi || !gc || !out || !scratch) return FEA_EINVAL;
+  if (G->kind != FEA_T3 && G->kind != FEA_Q4) return FEA_EINVAL;
+  if (scratch_len < fea_reduce_scratch_len(G->ne)) return FEA_EWORK;
+  if (int r = ensure_tables()) return r;
+  FaceParams P = face_params(N, G, 0.0, Xi, gc);
+  const int64_t nb = (G->ne + 255) / 256;
+  if (nb > 0) {
+    if (G->kind == FEA_T3) k_face_volume<3><<<(unsigned)nb, 256, 0, st>>>(P, scratch);
+    else k_face_volume<4><<<(unsigned)nb, 256, 0, st>>>(P, scratch);
+    count_launch();
+  }
+  k_sum_partials<<<1, 256, 0, st>>>(scratch, nb, out, 0);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+extern "C" int fea_lumped_mass(const fea_nodes_t* N, const fea_group_t* G, double rho, double* m,
+                               cudaStream_t st) {
+  if (!N || !G || !m || (G->kind != FEA_C3D4 && G->kind != FEA_C3D8)) return FEA_EINVAL;
+  if (int r = ensure_tables()) return r;
+  if (N->n_nodes == 0) return FEA_OK;
+  VolParams P = vol_params(N, G, 0.0, 0.0, nullptr);
+  const int grid = grid_for(N->n_nodes, 128);
+  if (G->kind == FEA_C3D8) k_lumped_mass<8><<<grid, 128, 0, st>>>(P, rho, m);
+  else k_lumped_mass<4><<<grid, 128, 0, st>>>(P, rho, m);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+extern "C" int fea_invert_mass(int64_t n, double* m, cudaStream_t st) {
+  if (!m || n < 0) return FEA_EINVAL;
+  if (n == 0) return FEA_OK;
+  k_invert_mass<<<grid_for(n, 256), 256, 0, st>>>(n, m);
+  count_launch();
+  return (int)cudaGetLastError();
+}

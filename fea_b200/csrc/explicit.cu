@@ -1,0 +1,213 @@
+// Explicit central difference with lumped mass, one fused kernel per step
+// (sm_100a).
+//
+// Replaces the time loop of DynamicExplicitSolver.solve (FEA =
+// sssnnn7119/FEA, FEA/solver/dynamic_explicit.py:97-140):
+//     vh_{k+1/2} = vh_{k-1/2} + dt a_k
+//     u_{k+1}    = u_k + dt vh_{k+1/2}
+//     a_{k+1}    = minv * (-f_int(u_{k+1}))          (assemble_force, R0 = -R)
+//     v_{k+1}    = (vh_{k+1/2} + vh_{k-1/2}) / 2
+// One thread per node evaluates the internal force of the node from its
+// incident elements (gather, no atomics) and immediately advances that node's
+// state; u is double-buffered so every thread reads a consistent u_k.  The
+// element math runs in T (double, or float for the FP32 variant) and the
+// nodal sums in double.
+#include <cmath>
+
+#include "common.cuh"
+
+namespace fea {
+
+struct ExParams {
+  const double* __restrict__ X;
+  const int32_t* __restrict__ rdof;
+  const uint8_t* __restrict__ mask;
+  const int32_t* __restrict__ conn;
+  const int32_t* __restrict__ inc;
+  const int32_t* __restrict__ nodeinc;
+  const double* __restrict__ minv;
+  const double* __restrict__ u;   // u_k (read by all threads)
+  double* unext;                  // u_{k+1}
+  double* vh;                     // in: vh_{k-1/2} (or v0 when init), out: vh_{k+1/2}
+  double* v;                      // out: v_{k+1}
+  double* a;                      // in/out
+  double mu, kappa, dt;
+  int32_t n_nodes;
+};
+
+// residual contribution of local node a of one element, computed in T
+template <int NN, class T>
+__device__ __forceinline__ void elem_force(const ExParams& P, const int32_t* cn, int a, double r[3]) {
+  unsigned mk[NN];
+  int32_t rd[NN];
+#pragma unroll
+  for (int b = 0; b < NN; ++b) {
+    mk[b] = P.mask[cn[b]];
+    rd[b] = P.rdof[cn[b]];
+  }
+  const T mu = (T)P.mu, kappa = (T)P.kappa;
+#pragma unroll
+  for (int g = 0; g < Elem<NN>::NG; ++g) {
+    T J0[9], Ju[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) J0[i] = Ju[i] = T(0);
+#pragma unroll
+    for (int b = 0; b < NN; ++b) {
+      const double* xb = P.X + 3 * (int64_t)cn[b];
+      T x[3], uu[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        x[i] = (T)__ldg(xb + i);
+        uu[i] = (T)node_u(P.u, rd[b], mk[b], i);
+      }
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        T d = (T)Elem<NN>::dxi(g, b, m);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          J0[3 * i + m] += x[i] * d;
+          Ju[3 * i + m] += uu[i] * d;
+        }
+      }
+    }
+    T iJ[9], F[9], iF[9];
+    T det0 = inv3(J0, iJ);
+    T w = det0 * (T)Elem<NN>::wq(g);
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        F[3 * I + i] = (I == i ? T(1) : T(0)) + Ju[3 * I] * iJ[i] + Ju[3 * I + 1] * iJ[3 + i] + Ju[3 * I + 2] * iJ[6 + i];
+    T J = inv3(F, iF);
+    T Jm = (T)pow((double)J, -2.0 / 3.0);
+    T sF2 = T(0);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];
+    T I1 = Jm * sF2;
+    T muJm = mu * Jm;
+    T c2 = kappa * J * (J - T(1)) - mu * I1 / T(3);
+    // g_a = iJ^T dxi_a ; f_a = F g_a ; q_a = F^-T g_a
+    T ga[3];
+    const T d0 = (T)Elem<NN>::dxi(g, a, 0), d1 = (T)Elem<NN>::dxi(g, a, 1), d2 = (T)Elem<NN>::dxi(g, a, 2);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) ga[i] = d0 * iJ[i] + d1 * iJ[3 + i] + d2 * iJ[6 + i];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      T fa = F[3 * j] * ga[0] + F[3 * j + 1] * ga[1] + F[3 * j + 2] * ga[2];
+      T qa = iF[j] * ga[0] + iF[3 + j] * ga[1] + iF[6 + j] * ga[2];
+      r[j] += (double)(w * (muJm * fa + c2 * qa));
+    }
+  }
+}
+
+// flags: bit0 compute the force (else use a), bit1 init (vh = v0 - dt/2 a),
+//        bit2 advance (vh, v, u_next)
+template <int NN, class T>
+__global__ void __launch_bounds__(128) k_explicit(ExParams P, int flags) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= P.n_nodes) return;
+  const unsigned mn = P.mask[n];
+  if (!mn) return;
+  double r[3] = {0.0, 0.0, 0.0};
+  if (flags & 1) {
+    for (int q = P.nodeinc[n]; q < P.nodeinc[n + 1]; ++q) {
+      const int ea = P.inc[q];
+      const int64_t e = ea >> 4;
+      int32_t cn[NN];
+#pragma unroll
+      for (int b = 0; b < NN; ++b) cn[b] = P.conn[e * NN + b];
+      elem_force<NN, T>(P, cn, ea & 15, r);
+    }
+  }
+  const int32_t base = P.rdof[n];
+  int rj = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (!(mn >> d & 1u)) continue;
+    const int32_t i = base + rj++;
+    double acc = (flags & 1) ? -P.minv[i] * r[d] : P.a[i];
+    if (flags & 1) P.a[i] = acc;
+    if (flags & 4) {
+      double vh = (flags & 2) ? P.vh[i] - 0.5 * P.dt * acc : P.vh[i];
+      double vhn = vh + P.dt * acc;
+      P.v[i] = 0.5 * (vhn + vh);
+      P.vh[i] = vhn;
+      P.unext[i] = P.u[i] + P.dt * vhn;
+    } else if (flags & 2) {
+      P.vh[i] = P.vh[i] - 0.5 * P.dt * acc;
+    }
+  }
+}
+
+}  // namespace fea
+
+using namespace fea;
+
+extern "C" int64_t fea_explicit_work_len(int64_t ndof) { return ndof; }
+
+// state on entry: u = u_k, vh = vh_{k-1/2}, a = a_k   (init == 0), or
+//                 u = u_0, v = v_0 (a, vh are outputs)  (init != 0)
+extern "C" int fea_explicit_run(const fea_nodes_t* N, const fea_group_t* G, double mu, double kappa,
+                                   const double* minv, double dt, int64_t steps, int32_t fp32, int32_t init,
+                                   double* u, double* vh, double* a, double* v, double* work, int64_t work_len,
+                                   cudaStream_t st) {
+  if (!N || !G || !minv || !u || !vh || !a || !v || !work || steps < 0) return FEA_EINVAL;
+  if (G->kind != FEA_C3D4 && G->kind != FEA_C3D8) return FEA_EINVAL;
+  if (work_len < fea_explicit_work_len(N->ndof)) return FEA_EWORK;
+  if (int r = ensure_tables()) return r;
+  if (N->n_nodes == 0 || N->ndof == 0) return FEA_OK;
+  ExParams P;
+  P.X = N->X_dev;
+  P.rdof = N->rdof_dev;
+  P.mask = N->mask_dev;
+  P.conn = G->conn_dev;
+  P.inc = G->inc_dev;
+  P.nodeinc = G->nodeinc_dev;
+  P.minv = minv;
+  P.vh = vh;
+  P.v = v;
+  P.a = a;
+  P.mu = mu;
+  P.kappa = kappa;
+  P.dt = dt;
+  P.n_nodes = (int32_t)N->n_nodes;
+  const int grid = grid_for(N->n_nodes, 128);
+  const bool hex = G->kind == FEA_C3D8;
+  auto launch = [&](const double* ucur, double* unext, int flags) {
+    P.u = ucur;
+    P.unext = unext;
+    if (hex) {
+      if (fp32) k_explicit<8, float><<<grid, 128, 0, st>>>(P, flags);
+      else k_explicit<8, double><<<grid, 128, 0, st>>>(P, flags);
+    } else {
+      if (fp32) k_explicit<4, float><<<grid, 128, 0, st>>>(P, flags);
+      else k_explicit<4, double><<<grid, 128, 0, st>>>(P, flags);
+    }
+    count_launch();
+  };
+  double* buf[2] = {u, work};
+  int cur = 0;
+  if (init) {
+    // v = v0 on entry; v is overwritten with v_1 only when advancing
+    if (steps == 0) {
+      // a_0 = minv (-f(u_0)); vh_{-1/2} = v0 - dt/2 a_0 ; v stays v0
+      cudaMemcpyAsync(vh, v, sizeof(double) * N->ndof, cudaMemcpyDeviceToDevice, st);
+      launch(u, work, 1 | 2);
+      return (int)cudaGetLastError();
+    }
+    cudaMemcpyAsync(vh, v, sizeof(double) * N->ndof, cudaMemcpyDeviceToDevice, st);
+    launch(buf[cur], buf[1 - cur], 1 | 2 | 4);
+  } else {
+    if (steps == 0) return FEA_OK;
+    launch(buf[cur], buf[1 - cur], 4);   // advance with the given a_k
+  }
+  cur = 1 - cur;
+  for (int64_t k = 1; k < steps; ++k) {
+    launch(buf[cur], buf[1 - cur], 1 | 4);
+    cur = 1 - cur;
+  }
+  launch(buf[cur], nullptr, 1);            // a at the final state
+  if (cur == 1) cudaMemcpyAsync(u, work, sizeof(double) * N->ndof, cudaMemcpyDeviceToDevice, st);
+  return (int)cudaGetLastError();
+}
+

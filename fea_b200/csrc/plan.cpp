@@ -1,0 +1,355 @@
+// Host-side assembly plan: reduced DOF numbering, node adjacency, reduced CSR
+// pattern and the per-node gather lists used by the element kernels.
+//
+// Replaces, once per mesh, the reference's sort-based COO pattern and
+// element-to-slot map (FEA/assemble/elements/C3/C3base.py:109-153) and the
+// per-Newton-iteration Dirichlet masking + unique() relabelling
+// (FEA/assemble/assembly.py:357-387).  The resulting CSR (indptr, indices)
+// is, by construction, the coalesced reduced pattern of the reference:
+// rows/cols are free DOFs in node-major order (GC order, assembly.py:170-183)
+// and a row (n, j) holds every free DOF (c, k) of every node c sharing an
+// element or a pressure face with n, sorted by column.
+//
+// The element-to-slot map is kept at node level: for every (row node n,
+// incident element e) pair the plan stores, per element node b, the offset
+// of node conn[e][b]'s column block inside row n (uint16).  The value of
+// K[(n,j),(c,k)] lives at vbase[n] + rank(j)*rowlen[n] + boff + rank(k).
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <thread>
+#include <vector>
+
+#include "../../include/fea_b200.h"
+
+namespace {
+
+inline int popc3(uint8_t m) { return (m & 1) + ((m >> 1) & 1) + ((m >> 2) & 1); }
+
+int nodes_per(int kind) {
+  switch (kind) {
+    case FEA_C3D4: return 4;
+    case FEA_C3D8: return 8;
+    case FEA_T3: return 3;
+    case FEA_Q4: return 4;
+    default: return -1;
+  }
+}
+
+struct GatherList {            // one element group or one face group
+  int kind = 0, nn = 0;
+  int64_t ne = 0;
+  std::vector<int32_t> inc;      // e*16 + a
+  std::vector<uint16_t> boff;    // [ninc, nn]
+  std::vector<int32_t> nodeinc;  // [N+1]
+  std::vector<int32_t> chunknode, chunkinc;
+  int64_t maxval = 0, threads = 0, smem = 0;
+};
+
+template <class F>
+void parallel_for(int64_t n, F f) {
+  unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  if (n < 4096 || hw == 1) { f(0, n); return; }
+  std::vector<std::thread> th;
+  int64_t step = (n + hw - 1) / hw;
+  for (unsigned t = 0; t < hw; ++t) {
+    int64_t a = t * step, b = std::min<int64_t>(n, a + step);
+    if (a >= b) break;
+    th.emplace_back([=, &f] { f(a, b); });
+  }
+  for (auto& t : th) t.join();
+}
+
+}  // namespace
+
+struct fea_plan {
+  int64_t N = 0, ndof = 0, nnz = 0, nnzb = 0;
+  std::vector<int32_t> rdof, dbase, rowlen;
+  std::vector<uint8_t> mask;
+  std::vector<int64_t> vbase, indptr, adjptr;
+  std::vector<int32_t> indices, adjcol, adjoff;
+  std::vector<GatherList> groups, faces;
+};
+
+namespace {
+
+// node -> incident (element, local index) lists, element order ascending
+struct Incidence {
+  std::vector<int64_t> ptr;   // [N+1]
+  std::vector<int64_t> ent;   // e*16 + a
+};
+
+int build_incidence(int64_t N, int nn, int64_t ne, const int32_t* conn, Incidence& inc) {
+  inc.ptr.assign(N + 1, 0);
+  for (int64_t i = 0; i < ne * nn; ++i) {
+    int32_t v = conn[i];
+    if (v < 0 || v >= N) return FEA_ERANGE;
+    inc.ptr[v + 1]++;
+  }
+  for (int64_t n = 0; n < N; ++n) inc.ptr[n + 1] += inc.ptr[n];
+  inc.ent.resize(inc.ptr[N]);
+  std::vector<int64_t> fill(inc.ptr.begin(), inc.ptr.end() - 1);
+  for (int64_t e = 0; e < ne; ++e)
+    for (int a = 0; a < nn; ++a) inc.ent[fill[conn[e * nn + a]]++] = e * 16 + a;
+  return FEA_OK;
+}
+
+int build_gather(const fea_plan& P, int kind, int64_t ne, const int32_t* conn, const Incidence& I,
+                 int threads, int64_t smem_budget, GatherList& G) {
+  G.kind = kind;
+  G.nn = nodes_per(kind);
+  G.ne = ne;
+  const int nn = G.nn;
+  const int64_t N = P.N;
+  G.nodeinc.assign(N + 1, 0);
+  for (int64_t n = 0; n < N; ++n) {
+    int64_t c = P.mask[n] ? (I.ptr[n + 1] - I.ptr[n]) : 0;
+    G.nodeinc[n + 1] = (int32_t)(G.nodeinc[n] + c);
+    G.maxval = std::max<int64_t>(G.maxval, c);
+  }
+  int64_t ninc = G.nodeinc[N];
+  if (ninc >= INT32_MAX) return FEA_ERANGE;
+  G.inc.resize(ninc);
+  G.boff.resize(ninc * nn);
+  int err = FEA_OK;
+  parallel_for(N, [&](int64_t a0, int64_t a1) {
+    for (int64_t n = a0; n < a1; ++n) {
+      if (!P.mask[n]) continue;
+      int64_t o = G.nodeinc[n];
+      const int32_t* col = P.adjcol.data() + P.adjptr[n];
+      int64_t ncol = P.adjptr[n + 1] - P.adjptr[n];
+      for (int64_t q = I.ptr[n]; q < I.ptr[n + 1]; ++q, ++o) {
+        int64_t e = I.ent[q] >> 4;
+        G.inc[o] = (int32_t)I.ent[q];
+        for (int b = 0; b < nn; ++b) {
+          int32_t c = conn[e * nn + b];
+          uint16_t bo = 0xFFFF;
+          if (P.mask[c]) {
+            const int32_t* it = std::lower_bound(col, col + ncol, c);
+            if (it == col + ncol || *it != c) { err = FEA_ERANGE; continue; }
+            int32_t off = P.adjoff[P.adjptr[n] + (it - col)];
+            if (off >= 0xFFFF) { err = FEA_ECHUNK; continue; }
+            bo = (uint16_t)off;
+          }
+          G.boff[o * nn + b] = bo;
+        }
+      }
+    }
+  });
+  if (err) return err;
+  // chunks of consecutive nodes: incidences <= threads, shared doubles <= budget
+  G.threads = threads;
+  G.chunknode.push_back(0);
+  G.chunkinc.push_back(0);
+  int64_t cur_inc = 0, cur_sm = 0;
+  for (int64_t n = 0; n < N; ++n) {
+    int64_t ni = G.nodeinc[n + 1] - G.nodeinc[n];
+    int64_t f = popc3(P.mask[n]);
+    int64_t sm = f * (int64_t)P.rowlen[n] + f;
+    if (ni > threads || sm > smem_budget) return FEA_ECHUNK;
+    if (cur_inc + ni > threads || cur_sm + sm > smem_budget) {
+      G.chunknode.push_back((int32_t)n);
+      G.chunkinc.push_back(G.nodeinc[n]);
+      G.smem = std::max(G.smem, cur_sm);
+      cur_inc = 0;
+      cur_sm = 0;
+    }
+    cur_inc += ni;
+    cur_sm += sm;
+  }
+  G.smem = std::max(G.smem, cur_sm);
+  if (G.chunknode.back() != N) {
+    G.chunknode.push_back((int32_t)N);
+    G.chunkinc.push_back(G.nodeinc[N]);
+  }
+  return FEA_OK;
+}
+
+}  // namespace
+
+extern "C" int fea_plan_build(int64_t n_nodes, const uint8_t* free_mask, int32_t n_groups,
+                              const int32_t* group_kind, const int64_t* group_ne,
+                              const int32_t* const* group_conn, int32_t n_faces, const int32_t* face_kind,
+                              const int64_t* face_nf, const int32_t* const* face_conn, int32_t vol_threads,
+                              int64_t smem_doubles, fea_plan** out) {
+  if (!out || n_nodes < 0 || n_nodes >= INT32_MAX || (n_nodes > 0 && !free_mask) || n_groups < 0 ||
+      n_faces < 0)
+    return FEA_EINVAL;
+  *out = nullptr;
+  for (int g = 0; g < n_groups; ++g) {
+    int k = group_kind[g];
+    if ((k != FEA_C3D4 && k != FEA_C3D8) || group_ne[g] < 0 || (group_ne[g] > 0 && !group_conn[g]))
+      return FEA_EINVAL;
+  }
+  for (int g = 0; g < n_faces; ++g) {
+    int k = face_kind[g];
+    if ((k != FEA_T3 && k != FEA_Q4) || face_nf[g] < 0 || (face_nf[g] > 0 && !face_conn[g])) return FEA_EINVAL;
+  }
+  std::unique_ptr<fea_plan> P(new fea_plan);
+  const int64_t N = n_nodes;
+  P->N = N;
+  P->mask.assign(free_mask, free_mask + N);
+  for (auto& m : P->mask) m &= 7;
+  // free-DOF numbering (node-major)
+  P->dbase.assign(N + 1, 0);
+  P->rdof.assign(N, -1);
+  for (int64_t n = 0; n < N; ++n) {
+    int f = popc3(P->mask[n]);
+    if (f) P->rdof[n] = P->dbase[n];
+    if ((int64_t)P->dbase[n] + f >= INT32_MAX) return FEA_ERANGE;
+    P->dbase[n + 1] = P->dbase[n] + f;
+  }
+  P->ndof = P->dbase[N];
+  // incidences
+  std::vector<Incidence> ginc(n_groups), finc(n_faces);
+  for (int g = 0; g < n_groups; ++g) {
+    int r = build_incidence(N, nodes_per(group_kind[g]), group_ne[g], group_conn[g], ginc[g]);
+    if (r) return r;
+  }
+  for (int g = 0; g < n_faces; ++g) {
+    int r = build_incidence(N, nodes_per(face_kind[g]), face_nf[g], face_conn[g], finc[g]);
+    if (r) return r;
+  }
+  // node adjacency over active nodes (sorted neighbour lists)
+  std::vector<std::vector<int32_t>> adj(N);
+  parallel_for(N, [&](int64_t a0, int64_t a1) {
+    std::vector<int32_t> tmp;
+    for (int64_t n = a0; n < a1; ++n) {
+      if (!P->mask[n]) continue;
+      tmp.clear();
+      auto add = [&](const Incidence& I, int nn, const int32_t* conn) {
+        for (int64_t q = I.ptr[n]; q < I.ptr[n + 1]; ++q) {
+          int64_t e = I.ent[q] >> 4;
+          for (int b = 0; b < nn; ++b) {
+            int32_t c = conn[e * nn + b];
+            if (P->mask[c]) tmp.push_back(c);
+          }
+        }
+      };
+      for (int g = 0; g < n_groups; ++g) add(ginc[g], nodes_per(group_kind[g]), group_conn[g]);
+      for (int g = 0; g < n_faces; ++g) add(finc[g], nodes_per(face_kind[g]), face_conn[g]);
+      std::sort(tmp.begin(), tmp.end());
+      tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+      adj[n] = tmp;
+    }
+  });
+  P->adjptr.assign(N + 1, 0);
+  P->rowlen.assign(N, 0);
+  P->vbase.assign(N + 1, 0);
+  for (int64_t n = 0; n < N; ++n) {
+    int64_t L = 0;
+    for (int32_t c : adj[n]) L += popc3(P->mask[c]);
+    if (L >= INT32_MAX) return FEA_ERANGE;
+    P->rowlen[n] = (int32_t)L;
+    P->adjptr[n + 1] = P->adjptr[n] + (int64_t)adj[n].size();
+    P->vbase[n + 1] = P->vbase[n] + popc3(P->mask[n]) * L;
+  }
+  P->nnzb = P->adjptr[N];
+  P->nnz = P->vbase[N];
+  P->adjcol.resize(P->nnzb);
+  P->adjoff.resize(P->nnzb);
+  P->indptr.assign(P->ndof + 1, 0);
+  P->indices.resize(P->nnz);
+  parallel_for(N, [&](int64_t a0, int64_t a1) {
+    for (int64_t n = a0; n < a1; ++n) {
+      int64_t o = P->adjptr[n];
+      int32_t off = 0;
+      for (int32_t c : adj[n]) {
+        P->adjcol[o] = c;
+        P->adjoff[o] = off;
+        off += popc3(P->mask[c]);
+        ++o;
+      }
+      int f = popc3(P->mask[n]);
+      int64_t L = P->rowlen[n];
+      for (int r = 0; r < f; ++r) {
+        int64_t row = P->dbase[n] + r;
+        int64_t v = P->vbase[n] + r * L;
+        P->indptr[row] = v;
+        for (int32_t c : adj[n]) {
+          int32_t d = P->dbase[c];
+          for (int k = 0; k < 3; ++k)
+            if (P->mask[c] >> k & 1) P->indices[v++] = d++;
+        }
+      }
+    }
+  });
+  P->indptr[P->ndof] = P->nnz;
+  { std::vector<std::vector<int32_t>>().swap(adj); }
+  // gather lists
+  P->groups.resize(n_groups);
+  P->faces.resize(n_faces);
+  const int64_t budget = smem_doubles > 0 ? smem_doubles : 12288;
+  for (int g = 0; g < n_groups; ++g) {
+    int th = vol_threads > 0 ? vol_threads : (group_kind[g] == FEA_C3D8 ? 128 : 256);
+    int r = build_gather(*P, group_kind[g], group_ne[g], group_conn[g], ginc[g], th, budget, P->groups[g]);
+    if (r) return r;
+  }
+  for (int g = 0; g < n_faces; ++g) {
+    int r = build_gather(*P, face_kind[g], face_nf[g], face_conn[g], finc[g], 128, budget, P->faces[g]);
+    if (r) return r;
+  }
+  *out = P.release();
+  return FEA_OK;
+}
+
+extern "C" void fea_plan_free(fea_plan* plan) { delete plan; }
+
+namespace {
+template <class T>
+int put(const std::vector<T>& v, void* dst, int64_t* count) {
+  if (count) *count = (int64_t)v.size();
+  if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(T));
+  return FEA_OK;
+}
+int scalar(int64_t s, int64_t* count) {
+  if (!count) return FEA_EINVAL;
+  *count = s;
+  return FEA_OK;
+}
+}  // namespace
+
+extern "C" int fea_plan_get(const fea_plan* P, int32_t id, int32_t group, void* dst, int64_t* count) {
+  if (!P) return FEA_EINVAL;
+  const GatherList* G = nullptr;
+  if (id >= 30 && id < 50) {
+    if (group < 0 || group >= (int)P->groups.size()) return FEA_EINVAL;
+    G = &P->groups[group];
+    id -= 30;
+  } else if (id >= 50 && id < 70) {
+    if (group < 0 || group >= (int)P->faces.size()) return FEA_EINVAL;
+    G = &P->faces[group];
+    id -= 50;
+  }
+  if (G) {
+    switch (id) {
+      case 0: return put(G->inc, dst, count);
+      case 1: return put(G->boff, dst, count);
+      case 2: return put(G->nodeinc, dst, count);
+      case 3: return put(G->chunknode, dst, count);
+      case 4: return put(G->chunkinc, dst, count);
+      case 5: return scalar((int64_t)G->chunknode.size() - 1, count);
+      case 6: return scalar(G->maxval, count);
+      case 7: return scalar(G->threads, count);
+      case 8: return scalar(G->smem, count);
+      default: return FEA_EINVAL;
+    }
+  }
+  switch (id) {
+    case FEA_S_NDOF: return scalar(P->ndof, count);
+    case FEA_S_NNZ: return scalar(P->nnz, count);
+    case FEA_S_NNZB: return scalar(P->nnzb, count);
+    case FEA_A_RDOF: return put(P->rdof, dst, count);
+    case FEA_A_MASK: return put(P->mask, dst, count);
+    case FEA_A_DBASE: return put(P->dbase, dst, count);
+    case FEA_A_VBASE: return put(P->vbase, dst, count);
+    case FEA_A_ROWLEN: return put(P->rowlen, dst, count);
+    case FEA_A_INDPTR: return put(P->indptr, dst, count);
+    case FEA_A_INDICES: return put(P->indices, dst, count);
+    case FEA_A_ADJPTR: return put(P->adjptr, dst, count);
+    case FEA_A_ADJCOL: return put(P->adjcol, dst, count);
+    case FEA_A_ADJOFF: return put(P->adjoff, dst, count);
+    default: return FEA_EINVAL;
+  }
+}

@@ -1,0 +1,232 @@
+"""Device-resident assembly plan: the mesh, the reduced CSR pattern and the
+per-node gather lists, plus typed wrappers of every library entry point.
+
+One ``DevicePlan`` serves one reduced system (all element groups and pressure
+face groups of an assembly, Dirichlet DOFs removed).  The plan is built once
+per mesh on the host (C++ ``fea_plan_build``) and uploaded; every later call
+only launches kernels on the current torch stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+KIND = {"C3D4": L.FEA_C3D4, "C3D8": L.FEA_C3D8, "T3": L.FEA_T3, "Q4": L.FEA_Q4}
+NODES_PER = {L.FEA_C3D4: 4, L.FEA_C3D8: 8, L.FEA_T3: 3, L.FEA_Q4: 4}
+
+
+def vptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class HostPlan:
+    """Result of ``fea_plan_build`` (host memory)."""
+
+    _DT = {L.FEA_A_RDOF: np.int32, L.FEA_A_MASK: np.uint8, L.FEA_A_DBASE: np.int32, L.FEA_A_VBASE: np.int64,
+           L.FEA_A_ROWLEN: np.int32, L.FEA_A_INDPTR: np.int64, L.FEA_A_INDICES: np.int32,
+           L.FEA_A_ADJPTR: np.int64, L.FEA_A_ADJCOL: np.int32, L.FEA_A_ADJOFF: np.int32}
+    _GDT = {L.A_INC: np.int32, L.A_BOFF: np.uint16, L.A_NODEINC: np.int32, L.A_CHUNKNODE: np.int32,
+            L.A_CHUNKINC: np.int32}
+
+    def __init__(self, n_nodes, free_mask, groups, faces, vol_threads=0, smem_doubles=0):
+        self._h = None
+        mask = np.ascontiguousarray(free_mask, dtype=np.uint8)
+        gconn = [np.ascontiguousarray(c, dtype=np.int32) for _, c in groups]
+        fconn = [np.ascontiguousarray(c, dtype=np.int32) for _, c in faces]
+        self._keep = (mask, gconn, fconn)
+        gk = (C.c_int32 * max(1, len(groups)))(*[k for k, _ in groups])
+        gn = (C.c_int64 * max(1, len(groups)))(*[c.shape[0] for c in gconn])
+        gp = (C.c_void_p * max(1, len(groups)))(*[c.ctypes.data for c in gconn])
+        fk = (C.c_int32 * max(1, len(faces)))(*[k for k, _ in faces])
+        fn = (C.c_int64 * max(1, len(faces)))(*[c.shape[0] for c in fconn])
+        fp = (C.c_void_p * max(1, len(faces)))(*[c.ctypes.data for c in fconn])
+        h = C.c_void_p()
+        L.check(L.fea_plan_build(int(n_nodes), mask.ctypes.data, len(groups), gk, gn, gp, len(faces), fk, fn, fp,
+                                 int(vol_threads), int(smem_doubles), C.byref(h)), "fea_plan_build")
+        self._h = h
+        self.n_groups, self.n_faces = len(groups), len(faces)
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h and L is not None and getattr(L, "fea_plan_free", None) is not None:
+            L.fea_plan_free(h)
+
+    def scalar(self, sid, group=0):
+        v = C.c_int64(0)
+        L.check(L.fea_plan_get(self._h, sid, group, None, C.byref(v)), "fea_plan_get")
+        return int(v.value)
+
+    def array(self, aid, group=0):
+        if aid >= L.F_BASE:
+            dt = self._GDT[aid - L.F_BASE]
+        elif aid >= L.G_BASE:
+            dt = self._GDT[aid - L.G_BASE]
+        else:
+            dt = self._DT[aid]
+        n = C.c_int64(0)
+        L.check(L.fea_plan_get(self._h, aid, group, None, C.byref(n)), "fea_plan_get")
+        out = np.empty(n.value, dtype=dt)
+        L.check(L.fea_plan_get(self._h, aid, group, out.ctypes.data if n.value else None, C.byref(n)),
+                "fea_plan_get")
+        return out
+
+
+class GatherGroup:
+    """Device arrays of one element or face group and its ctypes descriptor."""
+
+    def __init__(self, hp: HostPlan, base, index, kind, conn, device):
+        dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)
+        self.kind = kind
+        self.nn = NODES_PER[kind]
+        self.conn = dev(np.asarray(conn, dtype=np.int32))
+        self.inc = dev(hp.array(base + L.A_INC, index))
+        self.boff = dev(hp.array(base + L.A_BOFF, index).view(np.int16))
+        self.nodeinc = dev(hp.array(base + L.A_NODEINC, index))
+        self.chunknode = dev(hp.array(base + L.A_CHUNKNODE, index))
+        self.chunkinc = dev(hp.array(base + L.A_CHUNKINC, index))
+        self.ne = int(self.conn.shape[0])
+        self.desc = L.Group(kind, self.nn, self.ne, self.conn.data_ptr(), self.inc.data_ptr(), self.boff.data_ptr(),
+                            self.nodeinc.data_ptr(), self.chunknode.data_ptr(), self.chunkinc.data_ptr(),
+                            hp.scalar(base + L.S_NCHUNK, index), hp.scalar(base + L.S_MAXVAL, index),
+                            hp.scalar(base + L.S_THREADS, index), hp.scalar(base + L.S_SMEM, index))
+        self.nchunk = int(self.desc.nchunk)
+
+
+class DevicePlan:
+    """Reduced system of one assembly on one CUDA device.
+
+    X: [N,3] float64 reference coordinates (elements); free_mask: uint8 [N]
+    (bit k = DOF k free); groups: [(kind name, conn [E,nn])]; faces:
+    [(kind name, conn [F,nf])].
+    """
+
+    def __init__(self, X, free_mask, groups, faces=(), device=None, vol_threads=0, smem_doubles=0):
+        if not torch.cuda.is_available():
+            raise RuntimeError("fea_b200 needs a CUDA device (sm_100a); none is available")
+        self.device = torch.device(device if device is not None else "cuda")
+        Xn = np.ascontiguousarray(torch.as_tensor(X).detach().cpu().numpy(), dtype=np.float64)
+        self.n_nodes = Xn.shape[0]
+        gl = [(KIND[k], np.asarray(c)) for k, c in groups]
+        fl = [(KIND[k], np.asarray(c)) for k, c in faces]
+        with torch.cuda.device(self.device):
+            self.host = hp = HostPlan(self.n_nodes, free_mask, gl, fl, vol_threads, smem_doubles)
+            dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
+            self.ndof = hp.scalar(L.FEA_S_NDOF)
+            self.nnz = hp.scalar(L.FEA_S_NNZ)
+            self.X = dev(Xn)
+            self.rdof = dev(hp.array(L.FEA_A_RDOF))
+            self.mask = dev(hp.array(L.FEA_A_MASK))
+            self.dbase = dev(hp.array(L.FEA_A_DBASE))
+            self.vbase = dev(hp.array(L.FEA_A_VBASE))
+            self.rowlen = dev(hp.array(L.FEA_A_ROWLEN))
+            self.indptr = dev(hp.array(L.FEA_A_INDPTR))
+            self.indices = dev(hp.array(L.FEA_A_INDICES))
+            self.nodes = L.Nodes(self.n_nodes, self.ndof, self.nnz, self.X.data_ptr(), self.rdof.data_ptr(),
+                                 self.mask.data_ptr(), self.vbase.data_ptr(), self.rowlen.data_ptr(),
+                                 self.dbase.data_ptr())
+            self.groups = [GatherGroup(hp, L.G_BASE, i, k, c, self.device) for i, (k, c) in enumerate(gl)]
+            self.faces = [GatherGroup(hp, L.F_BASE, i, k, c, self.device) for i, (k, c) in enumerate(fl)]
+        self._scratch = None
+        self._coo = None
+
+    # -- buffers ------------------------------------------------------------
+    def zeros(self, n, dtype=torch.float64):
+        return torch.zeros(n, dtype=dtype, device=self.device)
+
+    def scratch(self, n):
+        if self._scratch is None or self._scratch.numel() < n:
+            self._scratch = torch.empty(max(n, 1024), dtype=torch.float64, device=self.device)
+        return self._scratch
+
+    def coo_indices(self):
+        """int64 [2, nnz] (row, col) of the reduced CSR pattern (cached)."""
+        if self._coo is None:
+            counts = self.indptr[1:] - self.indptr[:-1]
+            rows = torch.repeat_interleave(torch.arange(self.ndof, device=self.device), counts)
+            self._coo = torch.stack([rows, self.indices.to(torch.int64)])
+        return self._coo
+
+    # -- element / load kernels ---------------------------------------------
+    def assemble_volume(self, gi, mu, kappa, gc, K=None, R=None, elemR=None, accumulate=False):
+        g = self.groups[gi]
+        L.check(L.fea_assemble_volume(C.byref(self.nodes), C.byref(g.desc), float(mu), float(kappa), vptr(gc),
+                                      vptr(K), vptr(R), vptr(elemR), int(bool(accumulate)), stream()),
+                "fea_assemble_volume")
+
+    def assemble_pressure(self, fi, p, Xinst, gc, K=None, R=None):
+        f = self.faces[fi]
+        L.check(L.fea_assemble_pressure(C.byref(self.nodes), C.byref(f.desc), float(p), vptr(Xinst), vptr(gc),
+                                        vptr(K), vptr(R), stream()), "fea_assemble_pressure")
+
+    def energy_volume(self, gi, mu, kappa, gc, out):
+        g = self.groups[gi]
+        n = L.fea_reduce_scratch_len(g.ne)
+        s = self.scratch(n)
+        L.check(L.fea_energy_volume(C.byref(self.nodes), C.byref(g.desc), float(mu), float(kappa), vptr(gc),
+                                    vptr(out), vptr(s), s.numel(), stream()), "fea_energy_volume")
+
+    def pressure_volume(self, fi, Xinst, gc, out):
+        f = self.faces[fi]
+        n = L.fea_reduce_scratch_len(f.ne)
+        s = self.scratch(n)
+        L.check(L.fea_energy_pressure(C.byref(self.nodes), C.byref(f.desc), vptr(Xinst), vptr(gc), vptr(out),
+                                      vptr(s), s.numel(), stream()), "fea_energy_pressure")
+
+    def lumped_mass_inv(self, rhos):
+        m = self.zeros(self.ndof)
+        for gi, rho in enumerate(rhos):
+            L.check(L.fea_lumped_mass(C.byref(self.nodes), C.byref(self.groups[gi].desc), float(rho), vptr(m),
+                                      stream()), "fea_lumped_mass")
+        L.check(L.fea_invert_mass(self.ndof, vptr(m), stream()), "fea_invert_mass")
+        return m
+
+    # -- linear algebra --------------------------------------------------------
+    def spmv(self, values, x, y=None):
+        y = self.zeros(self.ndof) if y is None else y
+        L.check(L.fea_spmv(self.ndof, vptr(self.indptr), vptr(self.indices), vptr(values), vptr(x), vptr(y),
+                           stream()), "fea_spmv")
+        return y
+
+    def pcg(self, values, b, x, tol, max_iter, check_every=20, jacobi=True, raise_on_cap=False):
+        """Jacobi-PCG, in place on x. Returns (iterations, relres, status)."""
+        n = self.ndof
+        wl = L.fea_pcg_work_len(n)
+        w = self.scratch(wl)
+        it, rr = C.c_int32(0), C.c_double(0.0)
+        st = L.fea_pcg_solve(n, vptr(self.indptr), vptr(self.indices), vptr(values), vptr(b), vptr(x), float(tol),
+                             int(max_iter), int(check_every), int(bool(jacobi)), vptr(w), w.numel(), C.byref(it),
+                             C.byref(rr), stream())
+        if st not in (L.FEA_OK, L.FEA_ENOTCONV) or (raise_on_cap and st == L.FEA_ENOTCONV):
+            L.check(st, "fea_pcg_solve")
+        return int(it.value), float(rr.value), st
+
+    def pcg_mixed(self, values, values32, b, x, tol, inner_tol, max_iter, check_every=20):
+        n = self.ndof
+        wl = L.fea_pcg_mixed_work_len(n)
+        w = self.scratch(wl)
+        it, outer, rr = C.c_int32(0), C.c_int32(0), C.c_double(0.0)
+        st = L.fea_pcg_solve_mixed(n, vptr(self.indptr), vptr(self.indices), vptr(values), vptr(values32), vptr(b),
+                                   vptr(x), float(tol), float(inner_tol), int(max_iter), int(check_every), vptr(w),
+                                   w.numel(), C.byref(it), C.byref(outer), C.byref(rr), stream())
+        if st not in (L.FEA_OK, L.FEA_ENOTCONV):
+            L.check(st, "fea_pcg_solve_mixed")
+        return int(it.value), int(outer.value), float(rr.value), st
+
+    def to_f32(self, values, out=None):
+        out = torch.empty(values.numel(), dtype=torch.float32, device=self.device) if out is None else out
+        L.check(L.fea_convert_f32(values.numel(), vptr(values), vptr(out), stream()), "fea_convert_f32")
+        return out
+
+    def explicit_run(self, gi, mu, kappa, minv, dt, steps, u, vh, a, v, fp32=False, init=False):
+        w = self.scratch(L.fea_explicit_work_len(self.ndof))
+        L.check(L.fea_explicit_run(C.byref(self.nodes), C.byref(self.groups[gi].desc), float(mu), float(kappa),
+                                   vptr(minv), float(dt), int(steps), int(bool(fp32)), int(bool(init)), vptr(u),
+                                   vptr(vh), vptr(a), vptr(v), vptr(w), w.numel(), stream()), "fea_explicit_run")

@@ -1,0 +1,302 @@
+"""Solvers on the B200 kernels (mirrors FEA/solver of sssnnn7119/FEA).
+
+StaticImplicitSolver keeps the reference's Newton control flow — Armijo
+backtracking on the total potential, low-alpha bookkeeping, the absolute
+stop test (static_implicit.py:153-350) — and replaces the linear solve by
+the device Jacobi-PCG (static_implicit.py:352-405: symmetric Jacobi scaling
++ CG is Jacobi-PCG).  Where the reference switches to its CPU direct solver
+(scaled residual below 1e-3, or repeated small steps, static_implicit.py:
+384-388) this solver runs the PCG to a tight tolerance instead.  ``rtol``
+adds a relative stop test ||R|| / ||R_first|| <= rtol.
+
+DynamicExplicitSolver keeps the reference's time and storage bookkeeping
+(dynamic_explicit.py:66-145) and advances the state with the fused
+explicit kernel between storage points.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import torch
+
+from . import _lib as L
+
+
+class BaseSolver:
+    def __init__(self) -> None:
+        self.assembly = None
+        self.GC = None
+
+    def initialize(self, assembly, *args, **kwargs):
+        self.assembly = assembly
+
+    def solve(self, GC0=None, *args, **kwargs):
+        raise NotImplementedError
+
+
+class StaticImplicitSolver(BaseSolver):
+    def __init__(self, maximum_iteration: int = 10000, tol_error: float = 1e-5, rtol: float = None,
+                 pcg_tol: float = 1e-5, pcg_max_iter: int = 1500, tight_pcg_tol: float = 1e-22,
+                 tight_pcg_max_iter: int = 20000, precision: str = "fp64", verbose: bool = False) -> None:
+        super().__init__()
+        self.maximum_iteration = maximum_iteration
+        self.tol_error = tol_error
+        self.rtol = rtol
+        self.pcg_tol = pcg_tol
+        self.pcg_max_iter = pcg_max_iter
+        self.tight_pcg_tol = tight_pcg_tol
+        self.tight_pcg_max_iter = tight_pcg_max_iter
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.precision = precision
+        self.verbose = verbose
+        self._iter_now = 0
+        self._maximum_step_length = 1e10
+        self._low_alpha_count = 0
+        self.history = []
+
+    def solve(self, GC0=None, *args, **kwargs):
+        t0 = time.time()
+        if GC0 is None:
+            GC0 = self.assembly.GC
+        result = self._solve_iteration(GC=self.assembly._gc(GC=GC0), tol_error=self.tol_error)
+        if isinstance(result, bool):
+            return result
+        self.GC = result
+        self.assembly.GC = result
+        self.assembly.RGC = self.assembly._GC2RGC(result)
+        if self.verbose:
+            print("total_iter:%d, total_time:%.2f" % (self._iter_now, time.time() - t0))
+        return self.GC
+
+    def get_total_energy(self, GC_now):
+        return self.assembly._total_Potential_Energy(GC=GC_now)
+
+    def get_stiffness_matrix(self, GC_now):
+        return self.assembly.assemble_Stiffness_Matrix(GC=GC_now)
+
+    def _line_search(self, GC0, dGC, R, energy0):
+        """Armijo backtracking, c1 = 0.3, halving, alpha < 1e-12 -> 0 (static_implicit.py:153-232)."""
+        alpha, c1 = 1.0, 0.3
+        deltaE = float((dGC * R).sum())
+        if deltaE > 0:
+            dGC, deltaE = -dGC, -deltaE
+        if not bool(torch.isfinite(dGC).all()):
+            raise ValueError("dGC has nan or inf")
+        e0 = float(energy0)
+        step_max = float(dGC.abs().max())
+        while True:
+            GCnew = GC0 + alpha * dGC
+            e_new = float(self.get_total_energy(GCnew))
+            if (not math.isfinite(e_new)) or e_new > e0 + c1 * deltaE * alpha or \
+                    alpha * step_max > self._maximum_step_length:
+                alpha *= 0.5
+                if alpha < 1e-12:
+                    return 0.0, GC0.clone(), energy0
+            else:
+                return alpha, GCnew, torch.tensor(e_new, dtype=torch.float64)
+
+    def _solve_iteration(self, GC, tol_error):
+        """Newton loop (static_implicit.py:234-350); returns GC or False."""
+        self._iter_now = 0
+        energy = self.get_total_energy(GC)
+        dGC = torch.zeros_like(GC)
+        low_alpha, alpha = 0, 0.0
+        r_first = None
+        self.history = []
+        while True:
+            if self._iter_now > self.maximum_iteration:
+                return False
+            R, Kv = self.assembly.assemble_csr(GC)
+            self._iter_now += 1
+            rmax = float(R.abs().max()) if R.numel() else 0.0
+            rnorm = float(R.norm())
+            if r_first is None:
+                r_first = rnorm
+            self.history.append(dict(iter=self._iter_now, rmax=rmax, rnorm=rnorm))
+            if self.rtol is not None and rnorm <= self.rtol * max(r_first, 1e-300):
+                break
+            dGC = self._solve_linear_equation(Kv, -R, self._iter_now, alpha, dGC)
+            alpha, GCnew, energynew = self._line_search(GC, dGC, R, energy)
+            self.history[-1].update(alpha=alpha)
+            if alpha == 0 and rmax > tol_error and self.rtol is None:
+                return False
+            if alpha == 0:
+                break
+            if alpha < 0.01:
+                low_alpha += 1
+            else:
+                low_alpha = max(0, low_alpha - 5)
+            if low_alpha > 10:
+                return False
+            GC = GCnew
+            energy = self.get_total_energy(GC)
+            if self.verbose:
+                print("iter %3d  alpha %.2f  energy %.10e  max|R| %.4e" % (self._iter_now, alpha, float(energy), rmax))
+            if self.rtol is None and ((float(dGC.abs().max()) < tol_error and rmax < tol_error) or rmax < 1e-6):
+                break
+        return GC
+
+    def _solve_linear_equation(self, K_values, R, iter_now=0, alpha0=None, dGC0=None, tol_error=None):
+        """K dGC = R by device PCG, warm-started from the previous step (static_implicit.py:352-405)."""
+        P = self.assembly.plan
+        x = (torch.zeros_like(R) if dGC0 is None else dGC0.clone()).contiguous()
+        alpha0 = 1e-10 if alpha0 is None else alpha0
+        self._low_alpha_count = self._low_alpha_count + 1 if alpha0 < 1e-1 else 0
+        # scaled residual max|R/sqrt|diag K||, the reference's switch to an exact solve
+        tight = self._low_alpha_count > 3 or self._scaled_rmax(K_values, R) < 1e-3
+        if tight:
+            tol, cap = self.tight_pcg_tol, self.tight_pcg_max_iter
+            self._low_alpha_count = 0
+        else:
+            tol = self.pcg_tol
+            cap = 6000 if (iter_now % 20 == 0 or self._low_alpha_count > 0) else self.pcg_max_iter
+        if self.precision == "mixed":
+            v32 = P.to_f32(K_values)
+            it, outer, rr, st = P.pcg_mixed(K_values, v32, R.contiguous(), x, tol, 1e-4, cap)
+        else:
+            it, rr, st = P.pcg(K_values, R.contiguous(), x, tol, cap)
+        self.history[-1].update(pcg_iters=it, pcg_relres=rr, pcg_tight=tight)
+        return x
+
+    def _scaled_rmax(self, K_values, R):
+        P = self.assembly.plan
+        diag = self._diag(K_values)
+        return float((R / diag.abs().sqrt().clamp_min(1e-300)).abs().max()) if R.numel() else 0.0
+
+    def _diag(self, K_values):
+        P = self.assembly.plan
+        if not hasattr(self, "_diag_pos") or self._diag_pos.numel() != P.ndof:
+            rows = P.coo_indices()
+            self._diag_pos = torch.nonzero(rows[0] == rows[1]).flatten()
+        d = K_values[self._diag_pos]
+        return torch.where(d == 0, torch.ones_like(d), d)
+
+
+class DynamicExplicitSolver(BaseSolver):
+    """Central difference with lumped mass (dynamic_explicit.py:10-167).
+
+    The reference advances each step from the last *stored* displacement
+    (dynamic_explicit.py:100), which only follows the central-difference
+    recurrence when a state is stored at every step; this solver always
+    advances from the previous step.
+    """
+
+    def __init__(self, time_end: float = 1.0, time_per_storage: float = 1e-4, fp32: bool = False) -> None:
+        super().__init__()
+        self._time_end = time_end
+        self._time_per_storage = time_per_storage
+        self._next_storage_time = 0.0
+        self._GC_list = None
+        self._GV_list = None
+        self._GA_list = None
+        self._time_list = []
+        self._deltaT = 0.0
+        self.fp32 = fp32
+
+    def initialize(self, assembly, *args, **kwargs):
+        super().initialize(assembly)
+        self.assembly.initialize_dynamic()
+        self._deltaT = self.estimate_critical_timestep()
+        if self._deltaT <= 0:
+            raise ValueError("Critical timestep must be positive.")
+        self._GC_list, self._GV_list, self._GA_list, self._time_list = [], [], [], []
+
+    def estimate_critical_timestep(self, safety_factor=0.8) -> float:
+        """The reference's placeholder (dynamic_explicit.py:54-64); see cfl_timestep."""
+        return safety_factor * 5e-6
+
+    def cfl_timestep(self, factor=0.5) -> float:
+        """factor * min_e(l_e / c): l_e = smallest tet altitude 3V/max face area,
+        c = sqrt((kappa + 4 mu / 3) / rho) (one C3D4 group)."""
+        P = self.assembly.plan
+        es = self.assembly._mat_elems
+        if len(es) != 1 or es[0].kind != "C3D4":
+            raise NotImplementedError("cfl_timestep covers one C3D4 group")
+        e = es[0]
+        x = P.X[e._elems.to(P.device)]
+        v = torch.einsum("ei,ei->e", torch.cross(x[:, 1] - x[:, 0], x[:, 2] - x[:, 0], dim=1), x[:, 3] - x[:, 0]).abs() / 6
+        fa = []
+        for tri in ([0, 1, 2], [0, 1, 3], [0, 2, 3], [1, 2, 3]):
+            a = x[:, tri]
+            fa.append(0.5 * torch.cross(a[:, 1] - a[:, 0], a[:, 2] - a[:, 0], dim=1).norm(dim=1))
+        hmin = float((3 * v / torch.stack(fa, 1).max(1).values).min())
+        mu, kappa = e.materials.parameters()
+        c = math.sqrt((kappa + 4 * mu / 3) / float(e.density))
+        return factor * hmin / c
+
+    def _group(self):
+        es = self.assembly._mat_elems
+        if len(es) != 1 or self.assembly._face_loads:
+            raise NotImplementedError("the fused explicit kernel covers one element group without loads")
+        return 0, es[0].materials.parameters()
+
+    def solve(self, GC0=None, GV0=None, *args, **kwargs):
+        A = self.assembly
+        P = A.plan
+        gi, (mu, kappa) = self._group()
+        dt = float(self._deltaT)
+        u = (A.GC.clone() if GC0 is None else A._gc(GC=GC0).clone()).contiguous()
+        v = (torch.zeros_like(u) if GV0 is None else A._gc(GC=GV0).clone()).contiguous()
+        vh = torch.empty_like(u)
+        a = torch.empty_like(u)
+        minv = A.lumped_mass_inv()
+        # a_0 and vh_{-1/2} (dynamic_explicit.py:80-91)
+        P.explicit_run(gi, mu, kappa, minv, dt, 0, u, vh, a, v, fp32=self.fp32, init=True)
+        self._GC_list.append(u.clone())
+        self._GV_list.append(v.clone())
+        self._GA_list.append(a.clone())
+        self._time_list.append(0.0)
+        # the reference's time / storage bookkeeping (dynamic_explicit.py:97-134)
+        current_time, pending = 0.0, 0
+        while current_time < self._time_end:
+            current_time += dt
+            pending += 1
+            if current_time >= self._next_storage_time or current_time >= self._time_end:
+                P.explicit_run(gi, mu, kappa, minv, dt, pending, u, vh, a, v, fp32=self.fp32, init=False)
+                pending = 0
+                self._GC_list.append(u.clone())
+                self._GV_list.append(v.clone())
+                self._GA_list.append(a.clone())
+                self._time_list.append(current_time)
+                self._next_storage_time += self._time_per_storage
+        if pending:
+            P.explicit_run(gi, mu, kappa, minv, dt, pending, u, vh, a, v, fp32=self.fp32, init=False)
+        self.GC = u
+        self.GV, self.GA, self.GV_half = v, a, vh
+        return True
+
+    def get_lumped_mass_inv(self, GC=None):
+        return self.assembly.lumped_mass_inv()
+
+
+class _LinearSolverModule:
+    """``_linear_solver`` namespace (FEA/solver/_linear_solver.py)."""
+
+    @staticmethod
+    def conjugate_gradient(A_indices, A_values, b, x0=None, tol: float = 1e-3, max_iter: int = 1500):
+        """Plain CG on a COO matrix with the reference's stop test ||r||^2/||b||^2 < tol
+        (_linear_solver.py:6-42), run by the device PCG kernels without preconditioner."""
+        from .plan import vptr, stream
+        import ctypes as C
+        b = torch.as_tensor(b, dtype=torch.float64)
+        dev = b.device if b.is_cuda else torch.device("cuda")
+        b = b.to(dev).contiguous()
+        n = b.shape[0]
+        A = torch.sparse_coo_tensor(A_indices.to(dev), A_values.to(dev, torch.float64), (n, n)).coalesce()
+        Ac = A.to_sparse_csr()
+        ip = Ac.crow_indices().to(torch.int64).contiguous()
+        ix = Ac.col_indices().to(torch.int32).contiguous()
+        vv = Ac.values().contiguous()
+        x = torch.zeros_like(b) if (x0 is None or x0.numel() == 0) else x0.to(dev, torch.float64).clone().contiguous()
+        w = torch.empty(L.fea_pcg_work_len(n), dtype=torch.float64, device=dev)
+        it, rr = C.c_int32(0), C.c_double(0.0)
+        st = L.fea_pcg_solve(n, vptr(ip), vptr(ix), vptr(vv), vptr(b), vptr(x), float(tol), int(max_iter), 20, 0,
+                             vptr(w), w.numel(), C.byref(it), C.byref(rr), stream())
+        if st not in (L.FEA_OK, L.FEA_ENOTCONV):
+            L.check(st, "conjugate_gradient")
+        return x
+
+
+_linear_solver = _LinearSolverModule()

@@ -1,0 +1,249 @@
+/*
+ * fea_b200 — C ABI of the B200 (sm_100a) element / assembly / solver library.
+ *
+ * Plain C: integers, raw pointers and sizes, no framework types.  Every entry
+ * point returns an int status: 0 = ok, negative = bad argument / size /
+ * plan (see FEA_E*), positive = a CUDA error code from the launch.  Device
+ * entry points are asynchronous on the given stream unless stated; pointers
+ * named *_dev are device memory, the others host memory.
+ *
+ * The library replaces the hot path of the reference package sssnnn7119/FEA:
+ *   - Element_3D.initialize COO pattern + element-to-slot map
+ *       (FEA/assemble/elements/C3/C3base.py:109-153) and the Dirichlet
+ *       reduction/relabelling (FEA/assemble/assembly.py:357-387)
+ *         -> fea_plan_build / fea_plan_get  (host, once per mesh)
+ *   - Element_3D.structural_Force R + K + slot scatter (C3base.py:413-452),
+ *       NeoHookean.material_Constitutive_C3 (materials/hyperelastic.py:35-84),
+ *       Assembly._assemble_generalized_Matrix (assembly.py:311-355)
+ *         -> fea_assemble_volume
+ *   - Pressure.get_stiffness (FEA/assemble/loads/pressure.py:80-132)
+ *         -> fea_assemble_pressure
+ *   - Element_3D.potential_Energy (C3base.py:387-411) and
+ *       Pressure.get_potential_energy (pressure.py:134-159)
+ *         -> fea_energy_volume / fea_energy_pressure
+ *   - Element_3D.get_mass_matrix + row-sum lumping (C3base.py:348-384,
+ *       FEA/solver/dynamic_explicit.py:147-167) -> fea_lumped_mass
+ *   - _linear_solver.conjugate_gradient with the symmetric Jacobi scaling of
+ *       StaticImplicitSolver._solve_linear_equation
+ *       (FEA/solver/_linear_solver.py:6-42, FEA/solver/static_implicit.py:352-405)
+ *         -> fea_pcg_solve / fea_pcg_solve_mixed
+ *   - DynamicExplicitSolver.solve time loop (dynamic_explicit.py:97-140)
+ *         -> fea_explicit_run
+ */
+#ifndef FEA_B200_H
+#define FEA_B200_H
+
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FEA_OK 0
+#define FEA_EINVAL -1      /* bad argument (null pointer, negative size, bad kind) */
+#define FEA_ERANGE -2      /* index out of range in the inputs (node id >= n_nodes) */
+#define FEA_ECHUNK -3      /* one node needs more threads / shared memory than a chunk holds */
+#define FEA_ESMEM -4       /* requested shared memory exceeds the device limit */
+#define FEA_EWORK -5       /* caller-provided work buffer too small */
+#define FEA_ENOTCONV -6    /* iterative solver hit its iteration cap */
+#define FEA_EBREAKDOWN -7  /* PCG breakdown (p.Ap <= 0 or non-finite) */
+
+/* element kinds (reference class names) */
+#define FEA_C3D4 4
+#define FEA_C3D8 8
+/* surface kinds for the follower pressure */
+#define FEA_T3 3
+#define FEA_Q4 40
+
+/* ---------------------------------------------------------------------------
+ * Host-side plan: reduced pattern, node adjacency and per-node gather lists.
+ * ------------------------------------------------------------------------- */
+typedef struct fea_plan fea_plan;
+
+/* Build the plan for one assembly.
+ *   n_nodes          nodes of the (single) instance
+ *   free_mask[n]     bit k set <=> DOF (n, k) is free (not Dirichlet, and the
+ *                    node belongs to an element); 0 = node has no rows
+ *   groups           n_groups element groups: kind (FEA_C3D4 / FEA_C3D8),
+ *                    element count, connectivity int32 [ne, nn] (host)
+ *   faces            n_faces pressure face groups: kind (FEA_T3 / FEA_Q4),
+ *                    face count, node lists int32 [nf, 3|4] (host)
+ *   vol_threads      threads per gather chunk for the element kernels
+ *                    (0 = default: 128 for C3D8, 256 for C3D4)
+ *   smem_doubles     per-chunk shared-memory budget in doubles (0 = default)
+ * The reduced DOF numbering is node-major over free DOFs, as GC in the
+ * reference (assembly.py:170-183); the CSR pattern equals the reference's
+ * coalesced reduced K pattern. */
+int fea_plan_build(int64_t n_nodes, const uint8_t* free_mask,
+                   int32_t n_groups, const int32_t* group_kind, const int64_t* group_ne,
+                   const int32_t* const* group_conn,
+                   int32_t n_faces, const int32_t* face_kind, const int64_t* face_nf,
+                   const int32_t* const* face_conn,
+                   int32_t vol_threads, int64_t smem_doubles, fea_plan** out);
+void fea_plan_free(fea_plan* plan);
+
+/* Array / scalar ids for fea_plan_get. "group" selects the element group
+ * (FEA_A_G_*) or the face group (FEA_A_F_*); ignored otherwise. */
+enum {
+  FEA_S_NDOF = 0,        /* int64 scalar: reduced DOF count n            */
+  FEA_S_NNZ = 1,         /* int64 scalar: nonzeros of the reduced K       */
+  FEA_S_NNZB = 2,        /* int64 scalar: node-level adjacency entries    */
+  FEA_A_RDOF = 10,       /* int32 [N]   first reduced DOF of node, -1 none */
+  FEA_A_MASK = 11,       /* uint8 [N]   free-DOF bits                      */
+  FEA_A_DBASE = 12,      /* int32 [N+1] prefix of free-DOF counts          */
+  FEA_A_VBASE = 13,      /* int64 [N+1] first K value of the node's rows   */
+  FEA_A_ROWLEN = 14,     /* int32 [N]   scalar row length of the node      */
+  FEA_A_INDPTR = 15,     /* int64 [n+1] CSR row pointer                    */
+  FEA_A_INDICES = 16,    /* int32 [nnz] CSR column indices                 */
+  FEA_A_ADJPTR = 17,     /* int64 [N+1] node adjacency row pointer         */
+  FEA_A_ADJCOL = 18,     /* int32 [nnzb] neighbour node                    */
+  FEA_A_ADJOFF = 19,     /* int32 [nnzb] value offset of neighbour in row  */
+  FEA_A_G_INC = 30,      /* int32 [ninc] element*16 + local node           */
+  FEA_A_G_BOFF = 31,     /* uint16 [ninc, nn] row offset per element node  */
+  FEA_A_G_NODEINC = 32,  /* int32 [N+1] first incidence of each node       */
+  FEA_A_G_CHUNKNODE = 33,/* int32 [nchunk+1] first node of each chunk      */
+  FEA_A_G_CHUNKINC = 34, /* int32 [nchunk+1] first incidence of each chunk */
+  FEA_S_G_NCHUNK = 35,   /* int64 scalar */
+  FEA_S_G_MAXVAL = 36,   /* int64 scalar: max incidences of one node       */
+  FEA_S_G_THREADS = 37,  /* int64 scalar: threads per chunk                */
+  FEA_S_G_SMEM = 38,     /* int64 scalar: max shared doubles of a chunk    */
+  FEA_A_F_INC = 50,      /* same five arrays / four scalars for face groups */
+  FEA_A_F_BOFF = 51,
+  FEA_A_F_NODEINC = 52,
+  FEA_A_F_CHUNKNODE = 53,
+  FEA_A_F_CHUNKINC = 54,
+  FEA_S_F_NCHUNK = 55,
+  FEA_S_F_MAXVAL = 56,
+  FEA_S_F_THREADS = 57,
+  FEA_S_F_SMEM = 58
+};
+
+/* Copy array `id` (of element/face group `group`) into dst (host memory),
+ * or, for FEA_S_* ids, write the scalar to *count.  With dst == NULL only
+ * *count (number of entries) is set. */
+int fea_plan_get(const fea_plan* plan, int32_t id, int32_t group, void* dst, int64_t* count);
+
+/* ---------------------------------------------------------------------------
+ * Device-side descriptors (device pointers; filled from the plan's arrays).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int64_t n_nodes;
+  int64_t ndof;
+  int64_t nnz;
+  const double* X_dev;        /* [N,3] reference coordinates of the part     */
+  const int32_t* rdof_dev;    /* FEA_A_RDOF   */
+  const uint8_t* mask_dev;    /* FEA_A_MASK   */
+  const int64_t* vbase_dev;   /* FEA_A_VBASE  */
+  const int32_t* rowlen_dev;  /* FEA_A_ROWLEN */
+  const int32_t* dbase_dev;   /* FEA_A_DBASE  */
+} fea_nodes_t;
+
+typedef struct {
+  int32_t kind;               /* FEA_C3D4 / FEA_C3D8, or FEA_T3 / FEA_Q4      */
+  int32_t nn;                 /* nodes per element / face                     */
+  int64_t ne;                 /* elements / faces                             */
+  const int32_t* conn_dev;    /* [ne, nn]                                     */
+  const int32_t* inc_dev;     /* FEA_A_*_INC                                  */
+  const uint16_t* boff_dev;   /* FEA_A_*_BOFF                                 */
+  const int32_t* nodeinc_dev; /* FEA_A_*_NODEINC                              */
+  const int32_t* chunknode_dev;
+  const int32_t* chunkinc_dev;
+  int64_t nchunk;
+  int32_t maxval;
+  int32_t threads;
+  int64_t smem_doubles;
+} fea_group_t;
+
+/* Element residual and tangent of one Neo-Hookean group, gathered per node
+ * row and written once into the reduced CSR values (store mode) or added to
+ * them (accumulate != 0).  gc_dev: reduced displacement [ndof].  Any of
+ * K_dev / R_dev / elemR_dev may be NULL.  elemR_dev receives the unassembled
+ * element residual in the reference's (a, j, e) order [nn*3*ne]; it is only
+ * meaningful for a plan whose every element node is active. */
+int fea_assemble_volume(const fea_nodes_t* nodes, const fea_group_t* group, double mu, double kappa,
+                        const double* gc_dev, double* K_dev, double* R_dev, double* elemR_dev,
+                        int32_t accumulate, cudaStream_t stream);
+
+/* Follower pressure p on a face group: adds -p dV/dx to R and -p d2V/dx2 to
+ * K (always accumulate).  Xinst_dev: instance node coordinates [N,3]. */
+int fea_assemble_pressure(const fea_nodes_t* nodes, const fea_group_t* faces, double p,
+                          const double* Xinst_dev, const double* gc_dev,
+                          double* K_dev, double* R_dev, cudaStream_t stream);
+
+/* Strain energy sum_{g,e} W(F) w of a group, written to out_dev[0]
+ * (deterministic two-stage reduction; scratch_dev needs
+ * fea_reduce_scratch_len(ne) doubles). */
+int64_t fea_reduce_scratch_len(int64_t n_items);
+int fea_energy_volume(const fea_nodes_t* nodes, const fea_group_t* group, double mu, double kappa,
+                      const double* gc_dev, double* out_dev, double* scratch_dev, int64_t scratch_len,
+                      cudaStream_t stream);
+/* Enclosed-volume functional V of a face group -> out_dev[0]. */
+int fea_energy_pressure(const fea_nodes_t* nodes, const fea_group_t* faces, const double* Xinst_dev,
+                        const double* gc_dev, double* out_dev, double* scratch_dev, int64_t scratch_len,
+                        cudaStream_t stream);
+
+/* Row-sum lumped mass over free DOFs, added into m_dev [ndof] (call once per
+ * group on a zeroed vector, then fea_invert_mass). */
+int fea_lumped_mass(const fea_nodes_t* nodes, const fea_group_t* group, double rho,
+                    double* m_dev, cudaStream_t stream);
+int fea_invert_mass(int64_t ndof, double* m_dev, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Jacobi-preconditioned CG on the reduced CSR matrix.
+ *   stop test: (r.D^-1 r) / (b.D^-1 b) < tol  — the reference's
+ *   ||r~||^2/||b~||^2 < tol on the symmetrically scaled system.
+ *   x_dev holds the initial guess on entry (warm start) and the solution on
+ *   exit.  work_dev: fea_pcg_work_len(n) doubles.  iters / relres: host outs.
+ *   check_every: iterations between host-side convergence checks.
+ *   jacobi: 1 = Jacobi preconditioner (the solver's scaled CG), 0 = plain CG
+ *   (the reference's conjugate_gradient on an unscaled matrix).
+ * Returns FEA_OK, FEA_ENOTCONV (cap reached) or FEA_EBREAKDOWN.
+ * ------------------------------------------------------------------------- */
+int64_t fea_pcg_work_len(int64_t n);
+int fea_pcg_solve(int64_t n, const int64_t* indptr_dev, const int32_t* indices_dev, const double* values_dev,
+                  const double* b_dev, double* x_dev, double tol, int32_t max_iter, int32_t check_every,
+                  int32_t jacobi, double* work_dev, int64_t work_len, int32_t* iters, double* relres,
+                  cudaStream_t stream);
+/* FP32 SpMV inner CG with FP64 iterative refinement of the residual.
+ * values32_dev: float copy of values.  inner_tol: squared-ratio reduction
+ * asked of each inner solve.  work: fea_pcg_mixed_work_len(n) doubles. */
+int64_t fea_pcg_mixed_work_len(int64_t n);
+int fea_pcg_solve_mixed(int64_t n, const int64_t* indptr_dev, const int32_t* indices_dev,
+                        const double* values_dev, const float* values32_dev,
+                        const double* b_dev, double* x_dev, double tol, double inner_tol,
+                        int32_t max_iter, int32_t check_every,
+                        double* work_dev, int64_t work_len, int32_t* iters, int32_t* outer,
+                        double* relres, cudaStream_t stream);
+/* y = K x (FP64) */
+int fea_spmv(int64_t n, const int64_t* indptr_dev, const int32_t* indices_dev, const double* values_dev,
+             const double* x_dev, double* y_dev, cudaStream_t stream);
+/* values32 = (float) values */
+int fea_convert_f32(int64_t nnz, const double* values_dev, float* values32_dev, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Explicit central difference (lumped mass), one element group, no loads.
+ * One reference time step (dynamic_explicit.py:103-117) is
+ *   vh += dt a;  u += dt vh;  a = minv * (-f_int(u));  v = (vh_new + vh_old)/2.
+ * init != 0: on entry u = u_0 and v = v_0; a_0 and vh_{-1/2} = v_0 - dt/2 a_0
+ *            are computed first (dynamic_explicit.py:80-91).
+ * init == 0: on entry u = u_k, vh = vh_{k-1/2}, a = a_k.
+ * Runs `steps` steps and leaves u, vh, a, v at the final step.
+ * fp32 != 0 evaluates the element force in FP32 with FP64 nodal sums.
+ * work_dev: fea_explicit_work_len(ndof) doubles (second u buffer).
+ * ------------------------------------------------------------------------- */
+int64_t fea_explicit_work_len(int64_t ndof);
+int fea_explicit_run(const fea_nodes_t* nodes, const fea_group_t* group, double mu, double kappa,
+                     const double* minv_dev, double dt, int64_t steps, int32_t fp32, int32_t init,
+                     double* u_dev, double* vh_dev, double* a_dev, double* v_dev,
+                     double* work_dev, int64_t work_len, cudaStream_t stream);
+
+/* Library version and the number of kernels this library has launched
+ * (a host-side counter, for instrumentation). */
+int32_t fea_version(void);
+int64_t fea_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FEA_B200_H */

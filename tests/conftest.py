@@ -14,6 +14,12 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
     config.addinivalue_line("markers", "slow: long-running CPU test")
+    # the native library is built in-tree; (re)build it when missing or stale
+    try:
+        from fea_b200 import _build
+        _build.build()
+    except Exception as e:  # the tests that load the library report the failure
+        sys.stderr.write("fea_b200 build failed: %s\n" % e)
 
 
 def load_golden(name):

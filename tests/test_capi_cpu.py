@@ -1,0 +1,143 @@
+"""CPU checks of the C ABI: the library loads, exports every declared symbol,
+and its host-side plan reproduces the reference's reduced pattern."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import fea_oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "fea_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(fea_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    from fea_b200 import _lib
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    names = declared_functions()
+    assert len(names) >= 18
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(_lib.EXPORTED) == names
+    assert _lib.fea_version() == 1
+
+
+def _plan(N, mask, groups, faces=()):
+    from fea_b200.plan import HostPlan, KIND
+    return HostPlan(N, mask, [(KIND[k], c) for k, c in groups], [(KIND[k], c) for k, c in faces])
+
+
+@pytest.mark.parametrize("name,kind", [("cfg1", "C3D4"), ("tet3", "C3D4"), ("hex5", "C3D8")])
+def test_host_plan_csr_bit_exact(golden, name, kind):
+    from fea_b200 import _lib as L
+    g = golden(name)
+    N = g["X"].shape[0]
+    mask = np.zeros(N, np.uint8)
+    mask[np.unique(g["elems"])] = 7
+    mask[g["fixed"]] = 0
+    faces = g["pressure_faces"]
+    hp = _plan(N, mask, [(kind, g["elems"])], [("T3" if faces.shape[1] == 3 else "Q4", faces)])
+    np.testing.assert_array_equal(hp.array(L.FEA_A_INDPTR), g["indptr"])
+    np.testing.assert_array_equal(hp.array(L.FEA_A_INDICES), g["indices"])
+    assert hp.scalar(L.FEA_S_NDOF) == g["R"].shape[0]
+
+
+@pytest.mark.parametrize("dofs", [(0,), (1, 2), (0, 2)])
+def test_host_plan_partial_dirichlet_vs_oracle(dofs):
+    from fea_b200 import _lib as L
+    X, el = O.hex_block(3, jitter=0.1, seed=3)
+    fixed = torch.nonzero(X[:, 0] < 1e-9).flatten().numpy()
+    m = O.Model(X, [O.Group("C3D8", el, 1.0, 10.0)], [], [(fixed, dofs)])
+    R, (ip, ix, vv) = m.assemble(torch.zeros(int(m.free_mask().sum()), dtype=torch.float64))
+    mask = np.full(X.shape[0], 7, np.uint8)
+    for d in dofs:
+        mask[fixed] &= ~np.uint8(1 << d)
+    hp = _plan(X.shape[0], mask, [("C3D8", el.numpy())])
+    np.testing.assert_array_equal(hp.array(L.FEA_A_INDPTR), ip.numpy())
+    np.testing.assert_array_equal(hp.array(L.FEA_A_INDICES), ix.numpy())
+
+
+def test_host_plan_mixed_groups_and_shared_nodes():
+    """A tet block glued to a hex block: one pattern over both groups."""
+    from fea_b200 import _lib as L
+    Xh, eh = O.hex_block(2)
+    Xt, et = O.tet_block(2)
+    Xt = Xt + torch.tensor([1.0, 0.0, 0.0], dtype=torch.float64)
+    # merge coincident nodes on x = 1
+    key = lambda x: tuple(np.round(x, 9))
+    ids = {key(x): i for i, x in enumerate(Xh.numpy())}
+    Xall = list(Xh.numpy())
+    remap = []
+    for x in Xt.numpy():
+        k = key(x)
+        if k not in ids:
+            ids[k] = len(Xall)
+            Xall.append(x)
+        remap.append(ids[k])
+    et = torch.tensor(np.array(remap)[et.numpy()])
+    X = torch.tensor(np.array(Xall))
+    m = O.Model(X, [O.Group("C3D8", eh, 1.0, 5.0), O.Group("C3D4", et, 1.0, 5.0)], [], [])
+    R, (ip, ix, vv) = m.assemble(torch.zeros(X.shape[0] * 3, dtype=torch.float64))
+    hp = _plan(X.shape[0], np.full(X.shape[0], 7, np.uint8), [("C3D8", eh.numpy()), ("C3D4", et.numpy())])
+    np.testing.assert_array_equal(hp.array(L.FEA_A_INDPTR), ip.numpy())
+    np.testing.assert_array_equal(hp.array(L.FEA_A_INDICES), ix.numpy())
+
+
+def test_host_plan_chunks_cover_all_nodes_and_incidences(golden):
+    from fea_b200 import _lib as L
+    g = golden("cfg1")
+    N = g["X"].shape[0]
+    mask = np.full(N, 7, np.uint8)
+    hp = _plan(N, mask, [("C3D4", g["elems"])])
+    cn = hp.array(L.G_BASE + L.A_CHUNKNODE)
+    ci = hp.array(L.G_BASE + L.A_CHUNKINC)
+    ni = hp.array(L.G_BASE + L.A_NODEINC)
+    assert cn[0] == 0 and cn[-1] == N and ci[0] == 0 and ci[-1] == ni[-1] == g["elems"].size
+    assert np.all(np.diff(ci) <= hp.scalar(L.G_BASE + L.S_THREADS))
+    assert np.all(ni[cn] == ci)
+    inc = hp.array(L.G_BASE + L.A_INC)
+    e, a = inc >> 4, inc & 15
+    node = g["elems"][e, a]
+    assert np.all(np.diff(node) >= 0)                 # incidences sorted by node
+    boff = hp.array(L.G_BASE + L.A_BOFF).reshape(-1, 4)
+    vbase = hp.array(L.FEA_A_VBASE)
+    ip = hp.array(L.FEA_A_INDPTR)
+    ix = hp.array(L.FEA_A_INDICES)
+    rd = hp.array(L.FEA_A_RDOF)
+    # every row offset addresses the column block of the element node in the CSR row
+    for q in range(0, inc.size, 97):
+        n = node[q]
+        for b in range(4):
+            c = g["elems"][e[q], b]
+            assert ix[vbase[n] + boff[q, b]] == rd[c]
+
+
+def test_plan_errors():
+    from fea_b200 import _lib as L
+    el = np.array([[0, 1, 2, 9]], np.int32)
+    with pytest.raises(L.FeaError) as ex:
+        _plan(4, np.full(4, 7, np.uint8), [("C3D4", el)])
+    assert ex.value.status == -2
+    # a node with more incidences than a chunk has threads
+    X, el = O.tet_block(1)
+    hub = np.array([[0, 1, 2, 3]] * 300, np.int32)
+    with pytest.raises(L.FeaError) as ex:
+        _plan(8, np.full(8, 7, np.uint8), [("C3D4", hub)])
+    assert ex.value.status == -3
+
+
+def test_empty_group_and_fully_fixed_mesh():
+    from fea_b200 import _lib as L
+    hp = _plan(5, np.zeros(5, np.uint8), [("C3D4", np.zeros((0, 4), np.int32))])
+    assert hp.scalar(L.FEA_S_NDOF) == 0 and hp.scalar(L.FEA_S_NNZ) == 0
+    X, el = O.tet_block(1)
+    hp = _plan(8, np.zeros(8, np.uint8), [("C3D4", el.numpy())])
+    assert hp.scalar(L.FEA_S_NDOF) == 0 and hp.scalar(L.FEA_S_NNZ) == 0

@@ -1,0 +1,248 @@
+"""CUDA path (through the C ABI) against the reference's golden fixtures and the oracle.
+
+Tolerances: element R / K / energy <= 1e-12 relative (2-norm over all
+entries); converged displacements <= 1e-8 relative; CSR pattern bit-exact.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import fea_oracle as O
+from tests.helpers import csr_from_api, fea_model, oracle_model, rel
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+CASES = [("cfg1", "C3D4"), ("tet3", "C3D4"), ("hex5", "C3D8")]
+
+
+@pytest.mark.parametrize("name,kind", CASES)
+def test_reduced_R_K_energy_vs_golden(golden, name, kind):
+    g = golden(name)
+    c, e, _ = fea_model(g, kind)
+    c.initialize()
+    asm = c.assembly
+    ip, ix = csr_from_api(asm)
+    np.testing.assert_array_equal(ip, g["indptr"])
+    np.testing.assert_array_equal(ix, g["indices"])
+    state = torch.from_numpy(g["state"]).cuda()
+    R, Kidx, Kv = asm.assemble_Stiffness_Matrix(GC=state)
+    assert rel(R, g["R"]) < TOL
+    assert rel(Kv, g["values"]) < TOL
+    assert Kidx.shape == (2, g["values"].shape[0])
+    E = asm._total_Potential_Energy(GC=state)
+    assert abs(float(E) - float(g["energy"])) <= TOL * abs(float(g["energy"]))
+    Rf = asm.assemble_force(GC=state)
+    assert rel(Rf, g["R"]) < TOL
+
+
+@pytest.mark.parametrize("name,kind", [("tet3", "C3D4"), ("hex5", "C3D8")])
+def test_element_level_structural_force(golden, name, kind):
+    g = golden(name)
+    c, e, _ = fea_model(g, kind)
+    c.initialize()
+    U = c.assembly._GC2RGC(torch.from_numpy(g["state"]).cuda())[0]
+    fi, Re, Kidx, Kval = e.structural_Force(U, None)
+    np.testing.assert_array_equal(fi.cpu().numpy(), g["elem_force_index"])
+    np.testing.assert_array_equal(Kidx.cpu().numpy(), g["elem_K_indices"])
+    assert rel(Re, g["elem_R"]) < TOL
+    assert rel(Kval, g["elem_K_values"]) < TOL
+    fi2, Re2 = e.structural_Force(U, torch.eye(3, dtype=torch.float64), if_onlyforce=True)
+    assert rel(Re2, g["elem_R"]) < TOL
+    Ee = float(e.potential_Energy(U))
+    assert abs(Ee - float(g["elem_energy"])) <= TOL * abs(float(g["elem_energy"]))
+
+
+def test_newton_hex_converges_to_reference(golden):
+    import fea_b200 as F
+    g = golden("hex5")
+    c, e, _ = fea_model(g, "C3D8", solver=F.solver.StaticImplicitSolver(rtol=1e-13, maximum_iteration=60))
+    c.initialize()
+    gc = c.solver.solve()
+    assert not isinstance(gc, bool)
+    assert rel(gc, g["gc_converged"]) < 1e-8
+
+
+def test_newton_tet_increments_match_reference(golden):
+    import fea_b200 as F
+    g = golden("cfg1")
+    c, e, load = fea_model(g, "C3D4", solver=F.solver.StaticImplicitSolver(rtol=1e-12, maximum_iteration=60))
+    c.initialize()
+    gc = c.assembly.GC.clone()
+    np.testing.assert_array_equal(gc.cpu().numpy(), g["gc0"])
+    for k in range(5):
+        load.pressure = float(g["p"]) * (k + 1) / 5
+        gc = c.solver.solve(GC0=gc)
+        assert not isinstance(gc, bool)
+        assert rel(gc, g["gc_increments"][k]) < 1e-8
+
+
+def test_default_newton_stop_test(golden):
+    """With the reference's absolute stop test the solve lands within its tolerance."""
+    g = golden("hex5")
+    c, e, _ = fea_model(g, "C3D8")
+    c.initialize()
+    gc = c.solver.solve()
+    R = c.assembly.assemble_force(GC=gc)
+    assert float(R.abs().max()) < 1e-6
+
+
+def test_lumped_mass_and_explicit_vs_golden(golden):
+    import fea_b200 as F
+    g = golden("explicit_tet4")
+    dt, steps = float(g["dt"]), int(g["steps"])
+    T = dt * steps
+    c, e, _ = fea_model(g, "C3D4", pressure=False, fixed=False,
+                        solver=F.solver.DynamicExplicitSolver(time_end=T * (1 - 1e-9), time_per_storage=0.5 * dt))
+    c.initialize()
+    assert rel(c.assembly.lumped_mass_inv(), g["minv"]) < 1e-14
+    c.solver._deltaT = dt
+    c.solver.solve(GC0=torch.zeros_like(c.assembly.GC), GV0=torch.from_numpy(g["gv0"]).cuda())
+    s = c.solver
+    assert len(s._GC_list) == int(g["n_stored"])
+    assert abs(s._time_list[-1] - float(g["time_final"])) < 1e-15
+    assert rel(s._GC_list[-1], g["u_final"]) < TOL
+    assert rel(s._GV_list[-1], g["v_final"]) < TOL
+    assert rel(s._GA_list[-1], g["a_final"]) < TOL
+
+
+def test_explicit_sparse_storage_matches_per_step_recurrence(golden):
+    """Storing rarely advances the same recurrence as storing every step."""
+    import fea_b200 as F
+    g = golden("explicit_tet4")
+    dt, steps = float(g["dt"]), int(g["steps"])
+    T = dt * steps
+    c, e, _ = fea_model(g, "C3D4", pressure=False, fixed=False,
+                        solver=F.solver.DynamicExplicitSolver(time_end=T * (1 - 1e-9), time_per_storage=7.3 * dt))
+    c.initialize()
+    c.solver._deltaT = dt
+    c.solver.solve(GC0=torch.zeros_like(c.assembly.GC), GV0=torch.from_numpy(g["gv0"]).cuda())
+    assert rel(c.solver._GC_list[-1], g["u_final"]) < TOL
+    assert rel(c.solver._GA_list[-1], g["a_final"]) < TOL
+
+
+def test_explicit_fp32_variant_close(golden):
+    import fea_b200 as F
+    g = golden("explicit_tet4")
+    dt, steps = float(g["dt"]), int(g["steps"])
+    T = dt * steps
+    c, e, _ = fea_model(g, "C3D4", pressure=False, fixed=False,
+                        solver=F.solver.DynamicExplicitSolver(time_end=T * (1 - 1e-9), time_per_storage=T, fp32=True))
+    c.initialize()
+    c.solver._deltaT = dt
+    c.solver.solve(GC0=torch.zeros_like(c.assembly.GC), GV0=torch.from_numpy(g["gv0"]).cuda())
+    assert rel(c.solver._GC_list[-1], g["u_final"]) < 1e-3
+
+
+def _oracle_csr_case(kind, n, jitter, seed, fixed_dofs=(0, 1, 2), pressure=True):
+    if kind == "C3D8":
+        X, el = O.hex_block(n, jitter=jitter, seed=seed)
+    else:
+        X, el = O.tet_block(n)
+    faces = torch.cat([f for _, _, f in O.boundary_faces(kind, el, X, 2, float(X[:, 2].max()))])
+    fixed = torch.nonzero(X[:, 2] < 1e-9).flatten().numpy()
+    return X, el, faces, fixed, fixed_dofs
+
+
+@pytest.mark.parametrize("kind,dofs", [("C3D8", (0, 1, 2)), ("C3D4", (2,)), ("C3D8", (0, 2))])
+def test_random_state_vs_oracle_partial_bcs(kind, dofs):
+    """Seeded states, partial Dirichlet sets (rows/cols of single DOFs removed)."""
+    import fea_b200 as F
+    X, el, faces, fixed, _ = _oracle_csr_case(kind, 3, 0.15, 7)
+    g = dict(X=X.numpy(), elems=el.numpy(), mu=1.3, kappa=20.0, p=0.07, fixed=fixed,
+             pressure_faces=faces.numpy())
+    m = O.Model(X, [O.Group(kind, el, 1.3, 20.0)], [O.PressureLoad(faces, 0.07)], [(fixed, dofs)])
+    part = F.Part(X)
+    cls = F.elements.C3D4 if kind == "C3D4" else F.elements.C3D8
+    e = cls(elems=el, elems_index=torch.arange(el.shape[0]), part=part)
+    e.set_materials(F.materials.NeoHookean(1.3, 20.0))
+    part.add_element(e)
+    top = [(idx.numpy(), fid) for idx, fid, _ in O.boundary_faces(kind, el, X, 2, float(X[:, 2].max()))]
+    part.add_surface_set("top", top)
+    part.set_nodes["bottom"] = fixed
+    asm = F.Assembly()
+    asm.add_part(part, "p")
+    asm.add_instance(F.Instance(part), "p")
+    asm.add_load(F.loads.Pressure("p", "top", 0.07))
+    asm.add_boundary(F.boundarys.Boundary_Condition("p", "bottom", indexDoF=list(dofs)))
+    asm.initialize()
+    gc = torch.randn(asm.GC.shape, generator=torch.Generator().manual_seed(11), dtype=torch.float64) * 0.02
+    R, (ip, ix, vv) = m.assemble(gc)
+    Rg, Kidx, Kg = asm.assemble_Stiffness_Matrix(GC=gc.cuda())
+    np.testing.assert_array_equal(asm.plan.indptr.cpu().numpy(), ip.numpy())
+    np.testing.assert_array_equal(asm.plan.indices.cpu().numpy(), ix.numpy())
+    assert rel(Rg, R) < TOL
+    assert rel(Kg, vv) < TOL
+    assert abs(float(asm._total_Potential_Energy(GC=gc.cuda())) - float(m.energy(gc))) < TOL * abs(float(m.energy(gc)))
+
+
+def test_assembly_deterministic_and_symmetric(golden):
+    g = golden("hex5")
+    c, e, _ = fea_model(g, "C3D8", pressure=False)
+    c.initialize()
+    state = torch.from_numpy(g["state"]).cuda()
+    R1, K1 = c.assembly.assemble_csr(state)
+    R2, K2 = c.assembly.assemble_csr(state)
+    assert torch.equal(R1, R2) and torch.equal(K1, K2)          # bitwise reproducible
+    P = c.assembly.plan
+    A = torch.sparse_csr_tensor(P.indptr, P.indices.long(), K1, (P.ndof, P.ndof)).to_dense()
+    assert float((A - A.T).abs().max()) <= 1e-12 * float(A.abs().max())
+
+
+def test_tangent_is_derivative_of_residual(golden):
+    """Central differences of R along a random direction reproduce K d."""
+    g = golden("tet3")
+    c, e, _ = fea_model(g, "C3D4")
+    c.initialize()
+    A = c.assembly
+    x = torch.from_numpy(g["state"]).cuda()
+    d = torch.randn(x.shape, generator=torch.Generator().manual_seed(5), dtype=torch.float64).cuda()
+    _, K = A.assemble_csr(x)
+    Kd = A.plan.spmv(K, d)
+    h = 1e-6
+    fd = (A.assemble_force(GC=x + h * d) - A.assemble_force(GC=x - h * d)) / (2 * h)
+    assert rel(fd, Kd) < 1e-7
+
+
+def test_rigid_translation_zero_residual(golden):
+    g = golden("hex5")
+    c, e, _ = fea_model(g, "C3D8", pressure=False, fixed=False)
+    c.initialize()
+    t = torch.tensor([0.3, -0.2, 0.1], dtype=torch.float64)
+    gc = t.repeat(c.assembly.plan.ndof // 3).cuda()
+    R = c.assembly.assemble_force(GC=gc)
+    assert float(R.abs().max()) < 1e-13
+
+
+def test_pcg_solves_reduced_system(golden):
+    g = golden("cfg1")
+    c, e, _ = fea_model(g, "C3D4")
+    c.initialize()
+    A = c.assembly
+    P = A.plan
+    R, K = A.assemble_csr(torch.from_numpy(g["state"]).cuda())
+    b = (-R).contiguous()
+    x = torch.zeros_like(b)
+    it, rr, st = P.pcg(K, b, x, 1e-24, 5000)
+    assert st == 0 and rr < 1e-24
+    xd = O.direct_solve(torch.from_numpy(g["indptr"]), torch.from_numpy(g["indices"]).long(),
+                        K.cpu(), b.cpu())
+    assert rel(x, xd) < 1e-9
+    # FP32 SpMV inner iterations with FP64 refinement reach the same tolerance
+    x2 = torch.zeros_like(b)
+    it2, outer, rr2, st2 = P.pcg_mixed(K, P.to_f32(K), b, x2, 1e-24, 1e-6, 20000)
+    assert st2 == 0 and rr2 < 1e-24 and outer >= 2
+    assert rel(x2, xd) < 1e-9
+
+
+def test_reference_conjugate_gradient_semantics(golden):
+    """_linear_solver.conjugate_gradient: plain CG on a COO input, squared-ratio stop test."""
+    import fea_b200 as F
+    g = golden("hex5")
+    ip = torch.from_numpy(g["indptr"]); ix = torch.from_numpy(g["indices"]).long(); vv = torch.from_numpy(g["values"])
+    rows = torch.repeat_interleave(torch.arange(ip.numel() - 1), ip[1:] - ip[:-1])
+    b = -torch.from_numpy(g["R"])
+    x = F.solver._linear_solver.conjugate_gradient(torch.stack([rows, ix]).cuda(), vv.cuda(), b.cuda(),
+                                                   torch.zeros(0), tol=1e-20, max_iter=20000)
+    xo, _ = O.conjugate_gradient(ip, ix, vv, b, tol=1e-20, max_iter=20000)
+    assert rel(x, xo) < 1e-8
