@@ -30,7 +30,8 @@ FEA_C3D4, FEA_C3D8, FEA_T3, FEA_Q4 = 4, 8, 3, 40
 (FEA_A_RDOF, FEA_A_MASK, FEA_A_DBASE, FEA_A_VBASE, FEA_A_ROWLEN, FEA_A_INDPTR, FEA_A_INDICES,
  FEA_A_ADJPTR, FEA_A_ADJCOL, FEA_A_ADJOFF) = range(10, 20)
 G_BASE, F_BASE = 30, 50
-(A_INC, A_BOFF, A_NODEINC, A_CHUNKNODE, A_CHUNKINC, S_NCHUNK, S_MAXVAL, S_THREADS, S_SMEM) = range(9)
+(A_INC, A_BOFF, A_NODEINC, A_CHUNKPTR, A_CHUNKINC, S_NCHUNK, S_MAXVAL, S_THREADS, S_SMEM, A_CHUNKLIST,
+ A_CHUNKDIM, A_SOFF, A_ROFF) = range(13)
 
 
 class FeaError(RuntimeError):
@@ -55,7 +56,9 @@ class Nodes(C.Structure):
 class Group(C.Structure):
     _fields_ = [("kind", C.c_int32), ("nn", C.c_int32), ("ne", C.c_int64),
                 ("conn_dev", C.c_void_p), ("inc_dev", C.c_void_p), ("boff_dev", C.c_void_p),
-                ("nodeinc_dev", C.c_void_p), ("chunknode_dev", C.c_void_p), ("chunkinc_dev", C.c_void_p),
+                ("nodeinc_dev", C.c_void_p), ("chunkptr_dev", C.c_void_p), ("chunkinc_dev", C.c_void_p),
+                ("chunklist_dev", C.c_void_p), ("chunkdim_dev", C.c_void_p), ("soff_dev", C.c_void_p),
+                ("roff_dev", C.c_void_p),
                 ("nchunk", C.c_int64), ("maxval", C.c_int32), ("threads", C.c_int32),
                 ("smem_doubles", C.c_int64)]
 

@@ -241,9 +241,17 @@ class Assembly:
         R = P.zeros(P.ndof) if R is None else R
         if want_K and K is None:
             K = torch.empty(P.nnz, dtype=torch.float64, device=P.device)
+        # the first group stores whole rows when it touches every active node;
+        # otherwise all groups accumulate into zeroed buffers
+        store_first = len(P.groups) > 0 and P.groups[0].covers_active
+        if not store_first:
+            R.zero_()
+            if want_K:
+                K.zero_()
         for gi, e in enumerate(self._mat_elems):
             mu, kappa = e.materials.parameters()
-            P.assemble_volume(gi, mu, kappa, gc, K=K if want_K else None, R=R, accumulate=gi > 0)
+            P.assemble_volume(gi, mu, kappa, gc, K=K if want_K else None, R=R,
+                              accumulate=(gi > 0 or not store_first))
         for fi, ld in enumerate(self._face_loads):
             P.assemble_pressure(fi, float(ld.pressure), self._Xinst, gc, K=K if want_K else None, R=R)
         return R, (K if want_K else None)

@@ -39,8 +39,12 @@ struct VolParams {
   const int32_t* __restrict__ inc;
   const uint16_t* __restrict__ boff;
   const int32_t* __restrict__ nodeinc;
-  const int32_t* __restrict__ chunknode;
+  const int32_t* __restrict__ chunkptr;
   const int32_t* __restrict__ chunkinc;
+  const int32_t* __restrict__ chunklist;
+  const int32_t* __restrict__ chunkdim;
+  const int32_t* __restrict__ soff;
+  const int32_t* __restrict__ roff;
   const double* __restrict__ gc;
   double* K;
   double* R;
@@ -167,6 +171,46 @@ __device__ __forceinline__ void element_strip(const VolParams& P, const int32_t*
   }
 }
 
+// Copy a chunk's shared-memory rows to the reduced K values and R: one flat
+// copy when the chunk's node rows are contiguous in HBM, else node by node.
+template <bool ACC>
+__device__ __forceinline__ void write_back(const int32_t* __restrict__ chunkptr, const int32_t* __restrict__ chunklist,
+                                           const int32_t* __restrict__ chunkdim, const int64_t* __restrict__ vbase,
+                                           const int32_t* __restrict__ dbase, const uint8_t* __restrict__ mask,
+                                           const int32_t* __restrict__ soff, const int32_t* __restrict__ roff, int ch,
+                                           const double* sm, double* K, int nv, double* R) {
+  const int l0 = chunkptr[ch], l1 = chunkptr[ch + 1];
+  const int nr = chunkdim[3 * ch + 1];
+  if (chunkdim[3 * ch + 2]) {
+    const int n0 = chunklist[l0];
+    if (K) {
+      double* out = K + vbase[n0];
+      for (int i = threadIdx.x; i < nv; i += blockDim.x) out[i] = ACC ? out[i] + sm[i] : sm[i];
+    }
+    if (R) {
+      double* out = R + dbase[n0];
+      for (int i = threadIdx.x; i < nr; i += blockDim.x) out[i] = ACC ? out[i] + sm[nv + i] : sm[nv + i];
+    }
+    return;
+  }
+  for (int l = l0; l < l1; ++l) {
+    const int n = chunklist[l];
+    if (K) {
+      const int len = (int)(vbase[n + 1] - vbase[n]);
+      double* out = K + vbase[n];
+      const double* src = sm + soff[n];
+      for (int i = threadIdx.x; i < len; i += blockDim.x) out[i] = ACC ? out[i] + src[i] : src[i];
+    }
+    if (R) {
+      const int f = popc3(mask[n]);
+      if ((int)threadIdx.x < f) {
+        double* out = R + dbase[n];
+        out[threadIdx.x] = ACC ? out[threadIdx.x] + sm[nv + roff[n] + threadIdx.x] : sm[nv + roff[n] + threadIdx.x];
+      }
+    }
+  }
+}
+
 template <int NN>
 struct VolTPB { static constexpr int v = NN == 8 ? 128 : 256; };
 
@@ -175,12 +219,9 @@ template <int NN, bool WR, bool ACC, bool ER>
 __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
   extern __shared__ double sm[];
   const int ch = blockIdx.x;
-  const int n0 = P.chunknode[ch], n1 = P.chunknode[ch + 1];
   const int i0 = P.chunkinc[ch], i1 = P.chunkinc[ch + 1];
-  const int64_t v0 = P.vbase[n0];
-  const int nv = (int)(P.vbase[n1] - v0);
-  const int d0 = P.dbase[n0];
-  const int nr = WR ? P.dbase[n1] - d0 : 0;
+  const int nv = P.chunkdim[3 * ch];
+  const int nr = WR ? P.chunkdim[3 * ch + 1] : 0;
   for (int i = threadIdx.x; i < nv + nr; i += blockDim.x) sm[i] = 0.0;
   __syncthreads();
 
@@ -209,9 +250,9 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
   int rowoff = 0, L = 0, dr = 0;
   if (act) {
     mn = P.mask[n];
-    rowoff = (int)(P.vbase[n] - v0);
+    rowoff = P.soff[n];
     L = P.rowlen[n];
-    dr = P.dbase[n] - d0;
+    dr = P.roff[n];
   }
   for (int k = 0; k < P.maxval; ++k) {
     if (rank == k) {
@@ -244,18 +285,8 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
     }
     __syncthreads();
   }
-  double* Kout = P.K + v0;
-  for (int i = threadIdx.x; i < nv; i += blockDim.x) {
-    if (ACC) Kout[i] += sm[i];
-    else Kout[i] = sm[i];
-  }
-  if (WR) {
-    double* Rout = P.R + d0;
-    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
-      if (ACC) Rout[i] += sm[nv + i];
-      else Rout[i] = sm[nv + i];
-    }
-  }
+  write_back<ACC>(P.chunkptr, P.chunklist, P.chunkdim, P.vbase, P.dbase, P.mask, P.soff, P.roff, ch, sm, P.K, nv,
+                  WR ? P.R : nullptr);
 }
 
 // R-only kernel: one thread per node, sequential over its incidences.
@@ -345,8 +376,12 @@ struct FaceParams {
   const int32_t* __restrict__ inc;
   const uint16_t* __restrict__ boff;
   const int32_t* __restrict__ nodeinc;
-  const int32_t* __restrict__ chunknode;
+  const int32_t* __restrict__ chunkptr;
   const int32_t* __restrict__ chunkinc;
+  const int32_t* __restrict__ chunklist;
+  const int32_t* __restrict__ chunkdim;
+  const int32_t* __restrict__ soff;
+  const int32_t* __restrict__ roff;
   const double* __restrict__ gc;
   double* K;
   double* R;
@@ -405,12 +440,9 @@ template <int NF>
 __global__ void __launch_bounds__(128) k_face_rk(FaceParams P) {
   extern __shared__ double sm[];
   const int ch = blockIdx.x;
-  const int n0 = P.chunknode[ch], n1 = P.chunknode[ch + 1];
   const int i0 = P.chunkinc[ch], i1 = P.chunkinc[ch + 1];
-  const int64_t v0 = P.vbase[n0];
-  const int nv = P.K ? (int)(P.vbase[n1] - v0) : 0;
-  const int d0 = P.dbase[n0];
-  const int nr = P.R ? P.dbase[n1] - d0 : 0;
+  const int nv = P.chunkdim[3 * ch];
+  const int nr = P.chunkdim[3 * ch + 1];
   for (int i = threadIdx.x; i < nv + nr; i += blockDim.x) sm[i] = 0.0;
   __syncthreads();
   const int q = i0 + threadIdx.x;
@@ -475,13 +507,13 @@ __global__ void __launch_bounds__(128) k_face_rk(FaceParams P) {
   int rowoff = 0, L = 0, dr = 0;
   if (act) {
     mn = P.mask[n];
-    rowoff = (int)(P.vbase[n] - v0);
+    rowoff = P.soff[n];
     L = P.rowlen[n];
-    dr = P.dbase[n] - d0;
+    dr = P.roff[n];
   }
   for (int k = 0; k < P.maxval; ++k) {
     if (rank == k) {
-      if (nv) {
+      if (P.K) {
 #pragma unroll
         for (int b = 0; b < NF; ++b) {
           const unsigned bo = P.boff[(int64_t)q * NF + b];
@@ -503,7 +535,7 @@ __global__ void __launch_bounds__(128) k_face_rk(FaceParams P) {
           }
         }
       }
-      if (nr) {
+      if (P.R) {
         int rj = 0;
 #pragma unroll
         for (int j = 0; j < 3; ++j)
@@ -512,8 +544,7 @@ __global__ void __launch_bounds__(128) k_face_rk(FaceParams P) {
     }
     __syncthreads();
   }
-  for (int i = threadIdx.x; i < nv; i += blockDim.x) P.K[v0 + i] += sm[i];
-  for (int i = threadIdx.x; i < nr; i += blockDim.x) P.R[d0 + i] += sm[nv + i];
+  write_back<true>(P.chunkptr, P.chunklist, P.chunkdim, P.vbase, P.dbase, P.mask, P.soff, P.roff, ch, sm, P.K, nv, P.R);
 }
 
 template <int NF>
@@ -612,8 +643,12 @@ static VolParams vol_params(const fea_nodes_t* N, const fea_group_t* G, double m
   P.inc = G->inc_dev;
   P.boff = G->boff_dev;
   P.nodeinc = G->nodeinc_dev;
-  P.chunknode = G->chunknode_dev;
+  P.chunkptr = G->chunkptr_dev;
   P.chunkinc = G->chunkinc_dev;
+  P.chunklist = G->chunklist_dev;
+  P.chunkdim = G->chunkdim_dev;
+  P.soff = G->soff_dev;
+  P.roff = G->roff_dev;
   P.gc = gc;
   P.K = P.R = P.elemR = nullptr;
   P.mu = mu;
@@ -711,8 +746,12 @@ static FaceParams face_params(const fea_nodes_t* N, const fea_group_t* G, double
   P.inc = G->inc_dev;
   P.boff = G->boff_dev;
   P.nodeinc = G->nodeinc_dev;
-  P.chunknode = G->chunknode_dev;
+  P.chunkptr = G->chunkptr_dev;
   P.chunkinc = G->chunkinc_dev;
+  P.chunklist = G->chunklist_dev;
+  P.chunkdim = G->chunkdim_dev;
+  P.soff = G->soff_dev;
+  P.roff = G->roff_dev;
   P.gc = gc;
   P.K = P.R = nullptr;
   P.p = p;

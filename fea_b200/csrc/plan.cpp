@@ -43,7 +43,12 @@ struct GatherList {            // one element group or one face group
   std::vector<int32_t> inc;      // e*16 + a
   std::vector<uint16_t> boff;    // [ninc, nn]
   std::vector<int32_t> nodeinc;  // [N+1]
-  std::vector<int32_t> chunknode, chunkinc;
+  std::vector<int32_t> chunklist;  // nodes with incidences, chunk by chunk
+  std::vector<int32_t> chunkptr;   // [nchunk+1] into chunklist
+  std::vector<int32_t> chunkinc;   // [nchunk+1] first incidence
+  std::vector<int32_t> chunkdim;   // [nchunk*3]: values, residual entries, contiguous flag
+  std::vector<int32_t> soff;       // [N] shared-memory offset of the node's values in its chunk
+  std::vector<int32_t> roff;       // [N] offset of its residual entries (after the chunk's values)
   int64_t maxval = 0, threads = 0, smem = 0;
 };
 
@@ -138,31 +143,53 @@ int build_gather(const fea_plan& P, int kind, int64_t ne, const int32_t* conn, c
     }
   });
   if (err) return err;
-  // chunks of consecutive nodes: incidences <= threads, shared doubles <= budget
+  // chunks of nodes that have incidences in this list (in node order):
+  // incidences <= threads, shared doubles <= budget
   G.threads = threads;
-  G.chunknode.push_back(0);
+  G.soff.assign(N, 0);
+  G.roff.assign(N, 0);
+  G.chunkptr.push_back(0);
   G.chunkinc.push_back(0);
-  int64_t cur_inc = 0, cur_sm = 0;
+  std::vector<int32_t> cur;
+  int64_t cur_inc = 0, cur_v = 0, cur_r = 0;
+  auto close = [&]() {
+    if (cur.empty()) return;
+    int32_t r = 0;
+    bool contig = true;
+    for (size_t i = 0; i < cur.size(); ++i) {
+      int32_t n = cur[i];
+      G.roff[n] = r;
+      r += popc3(P.mask[n]);
+      if (i + 1 < cur.size()) {
+        int32_t m = cur[i + 1];
+        if (P.vbase[n + 1] != P.vbase[m] || P.dbase[n + 1] != P.dbase[m]) contig = false;
+      }
+    }
+    for (int32_t n : cur) G.chunklist.push_back(n);
+    G.chunkptr.push_back((int32_t)G.chunklist.size());
+    G.chunkinc.push_back(G.nodeinc[cur.back() + 1]);
+    G.chunkdim.push_back((int32_t)cur_v);
+    G.chunkdim.push_back((int32_t)cur_r);
+    G.chunkdim.push_back(contig ? 1 : 0);
+    G.smem = std::max(G.smem, cur_v + cur_r);
+    cur.clear();
+    cur_inc = cur_v = cur_r = 0;
+  };
   for (int64_t n = 0; n < N; ++n) {
     int64_t ni = G.nodeinc[n + 1] - G.nodeinc[n];
+    if (ni == 0) continue;
     int64_t f = popc3(P.mask[n]);
-    int64_t sm = f * (int64_t)P.rowlen[n] + f;
-    if (ni > threads || sm > smem_budget) return FEA_ECHUNK;
-    if (cur_inc + ni > threads || cur_sm + sm > smem_budget) {
-      G.chunknode.push_back((int32_t)n);
-      G.chunkinc.push_back(G.nodeinc[n]);
-      G.smem = std::max(G.smem, cur_sm);
-      cur_inc = 0;
-      cur_sm = 0;
-    }
+    int64_t v = f * (int64_t)P.rowlen[n];
+    if (ni > threads || v + f > smem_budget) return FEA_ECHUNK;
+    if (cur_inc + ni > threads || cur_v + v + cur_r + f > smem_budget) close();
+    if (!cur.empty() && G.nodeinc[cur.back() + 1] != G.nodeinc[n]) close();
+    G.soff[n] = (int32_t)cur_v;
+    cur.push_back((int32_t)n);
     cur_inc += ni;
-    cur_sm += sm;
+    cur_v += v;
+    cur_r += f;
   }
-  G.smem = std::max(G.smem, cur_sm);
-  if (G.chunknode.back() != N) {
-    G.chunknode.push_back((int32_t)N);
-    G.chunkinc.push_back(G.nodeinc[N]);
-  }
+  close();
   return FEA_OK;
 }
 
@@ -327,12 +354,16 @@ extern "C" int fea_plan_get(const fea_plan* P, int32_t id, int32_t group, void* 
       case 0: return put(G->inc, dst, count);
       case 1: return put(G->boff, dst, count);
       case 2: return put(G->nodeinc, dst, count);
-      case 3: return put(G->chunknode, dst, count);
+      case 3: return put(G->chunkptr, dst, count);
       case 4: return put(G->chunkinc, dst, count);
-      case 5: return scalar((int64_t)G->chunknode.size() - 1, count);
+      case 5: return scalar((int64_t)G->chunkptr.size() - 1, count);
       case 6: return scalar(G->maxval, count);
       case 7: return scalar(G->threads, count);
       case 8: return scalar(G->smem, count);
+      case 9: return put(G->chunklist, dst, count);
+      case 10: return put(G->chunkdim, dst, count);
+      case 11: return put(G->soff, dst, count);
+      case 12: return put(G->roff, dst, count);
       default: return FEA_EINVAL;
     }
   }

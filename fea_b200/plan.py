@@ -33,8 +33,9 @@ class HostPlan:
     _DT = {L.FEA_A_RDOF: np.int32, L.FEA_A_MASK: np.uint8, L.FEA_A_DBASE: np.int32, L.FEA_A_VBASE: np.int64,
            L.FEA_A_ROWLEN: np.int32, L.FEA_A_INDPTR: np.int64, L.FEA_A_INDICES: np.int32,
            L.FEA_A_ADJPTR: np.int64, L.FEA_A_ADJCOL: np.int32, L.FEA_A_ADJOFF: np.int32}
-    _GDT = {L.A_INC: np.int32, L.A_BOFF: np.uint16, L.A_NODEINC: np.int32, L.A_CHUNKNODE: np.int32,
-            L.A_CHUNKINC: np.int32}
+    _GDT = {L.A_INC: np.int32, L.A_BOFF: np.uint16, L.A_NODEINC: np.int32, L.A_CHUNKPTR: np.int32,
+            L.A_CHUNKINC: np.int32, L.A_CHUNKLIST: np.int32, L.A_CHUNKDIM: np.int32, L.A_SOFF: np.int32,
+            L.A_ROFF: np.int32}
 
     def __init__(self, n_nodes, free_mask, groups, faces, vol_threads=0, smem_doubles=0):
         self._h = None
@@ -89,14 +90,23 @@ class GatherGroup:
         self.conn = dev(np.asarray(conn, dtype=np.int32))
         self.inc = dev(hp.array(base + L.A_INC, index))
         self.boff = dev(hp.array(base + L.A_BOFF, index).view(np.int16))
-        self.nodeinc = dev(hp.array(base + L.A_NODEINC, index))
-        self.chunknode = dev(hp.array(base + L.A_CHUNKNODE, index))
+        nodeinc = hp.array(base + L.A_NODEINC, index)
+        self.nodeinc = dev(nodeinc)
+        self.chunkptr = dev(hp.array(base + L.A_CHUNKPTR, index))
         self.chunkinc = dev(hp.array(base + L.A_CHUNKINC, index))
+        self.chunklist = dev(hp.array(base + L.A_CHUNKLIST, index))
+        self.chunkdim = dev(hp.array(base + L.A_CHUNKDIM, index))
+        self.soff = dev(hp.array(base + L.A_SOFF, index))
+        self.roff = dev(hp.array(base + L.A_ROFF, index))
         self.ne = int(self.conn.shape[0])
+        # True when every node with free DOFs has an incidence in this group
+        self.covers_active = bool(np.all((np.diff(nodeinc) > 0) | (hp.array(L.FEA_A_MASK) == 0)))
         self.desc = L.Group(kind, self.nn, self.ne, self.conn.data_ptr(), self.inc.data_ptr(), self.boff.data_ptr(),
-                            self.nodeinc.data_ptr(), self.chunknode.data_ptr(), self.chunkinc.data_ptr(),
-                            hp.scalar(base + L.S_NCHUNK, index), hp.scalar(base + L.S_MAXVAL, index),
-                            hp.scalar(base + L.S_THREADS, index), hp.scalar(base + L.S_SMEM, index))
+                            self.nodeinc.data_ptr(), self.chunkptr.data_ptr(), self.chunkinc.data_ptr(),
+                            self.chunklist.data_ptr(), self.chunkdim.data_ptr(), self.soff.data_ptr(),
+                            self.roff.data_ptr(), hp.scalar(base + L.S_NCHUNK, index),
+                            hp.scalar(base + L.S_MAXVAL, index), hp.scalar(base + L.S_THREADS, index),
+                            hp.scalar(base + L.S_SMEM, index))
         self.nchunk = int(self.desc.nchunk)
 
 

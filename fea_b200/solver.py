@@ -77,7 +77,13 @@ class StaticImplicitSolver(BaseSolver):
         return self.assembly.assemble_Stiffness_Matrix(GC=GC_now)
 
     def _line_search(self, GC0, dGC, R, energy0):
-        """Armijo backtracking, c1 = 0.3, halving, alpha < 1e-12 -> 0 (static_implicit.py:153-232)."""
+        """Armijo backtracking, c1 = 0.3, halving, alpha < 1e-12 -> 0 (static_implicit.py:153-232).
+
+        When the predicted energy decrease is below the round-off of the
+        energy itself (|dGC . R| <= 1e-10 |E|), the energy comparison carries
+        no information; there a trial step is accepted when it reduces the
+        residual norm instead.
+        """
         alpha, c1 = 1.0, 0.3
         deltaE = float((dGC * R).sum())
         if deltaE > 0:
@@ -86,16 +92,22 @@ class StaticImplicitSolver(BaseSolver):
             raise ValueError("dGC has nan or inf")
         e0 = float(energy0)
         step_max = float(dGC.abs().max())
+        roundoff = abs(deltaE) <= 1e-10 * abs(e0)
+        r0 = float(R.norm())
         while True:
             GCnew = GC0 + alpha * dGC
-            e_new = float(self.get_total_energy(GCnew))
-            if (not math.isfinite(e_new)) or e_new > e0 + c1 * deltaE * alpha or \
-                    alpha * step_max > self._maximum_step_length:
-                alpha *= 0.5
-                if alpha < 1e-12:
-                    return 0.0, GC0.clone(), energy0
+            if roundoff:
+                rn = float(self.assembly.assemble_force(GC=GCnew).norm())
+                ok = math.isfinite(rn) and rn < r0
             else:
+                e_new = float(self.get_total_energy(GCnew))
+                ok = math.isfinite(e_new) and e_new <= e0 + c1 * deltaE * alpha
+            if ok and alpha * step_max <= self._maximum_step_length:
+                e_new = float(self.get_total_energy(GCnew)) if roundoff else e_new
                 return alpha, GCnew, torch.tensor(e_new, dtype=torch.float64)
+            alpha *= 0.5
+            if alpha < 1e-12:
+                return 0.0, GC0.clone(), energy0
 
     def _solve_iteration(self, GC, tol_error):
         """Newton loop (static_implicit.py:234-350); returns GC or False."""

@@ -102,21 +102,29 @@ enum {
   FEA_A_G_INC = 30,      /* int32 [ninc] element*16 + local node           */
   FEA_A_G_BOFF = 31,     /* uint16 [ninc, nn] row offset per element node  */
   FEA_A_G_NODEINC = 32,  /* int32 [N+1] first incidence of each node       */
-  FEA_A_G_CHUNKNODE = 33,/* int32 [nchunk+1] first node of each chunk      */
+  FEA_A_G_CHUNKPTR = 33, /* int32 [nchunk+1] chunk -> range of CHUNKLIST   */
   FEA_A_G_CHUNKINC = 34, /* int32 [nchunk+1] first incidence of each chunk */
   FEA_S_G_NCHUNK = 35,   /* int64 scalar */
   FEA_S_G_MAXVAL = 36,   /* int64 scalar: max incidences of one node       */
   FEA_S_G_THREADS = 37,  /* int64 scalar: threads per chunk                */
   FEA_S_G_SMEM = 38,     /* int64 scalar: max shared doubles of a chunk    */
-  FEA_A_F_INC = 50,      /* same five arrays / four scalars for face groups */
+  FEA_A_G_CHUNKLIST = 39,/* int32 nodes with incidences, chunk by chunk   */
+  FEA_A_G_CHUNKDIM = 40, /* int32 [nchunk,3] values, residual entries, contiguous */
+  FEA_A_G_SOFF = 41,     /* int32 [N] shared offset of the node's values   */
+  FEA_A_G_ROFF = 42,     /* int32 [N] offset of its residual entries       */
+  FEA_A_F_INC = 50,      /* the same arrays / scalars for face groups      */
   FEA_A_F_BOFF = 51,
   FEA_A_F_NODEINC = 52,
-  FEA_A_F_CHUNKNODE = 53,
+  FEA_A_F_CHUNKPTR = 53,
   FEA_A_F_CHUNKINC = 54,
   FEA_S_F_NCHUNK = 55,
   FEA_S_F_MAXVAL = 56,
   FEA_S_F_THREADS = 57,
-  FEA_S_F_SMEM = 58
+  FEA_S_F_SMEM = 58,
+  FEA_A_F_CHUNKLIST = 59,
+  FEA_A_F_CHUNKDIM = 60,
+  FEA_A_F_SOFF = 61,
+  FEA_A_F_ROFF = 62
 };
 
 /* Copy array `id` (of element/face group `group`) into dst (host memory),
@@ -147,8 +155,12 @@ typedef struct {
   const int32_t* inc_dev;     /* FEA_A_*_INC                                  */
   const uint16_t* boff_dev;   /* FEA_A_*_BOFF                                 */
   const int32_t* nodeinc_dev; /* FEA_A_*_NODEINC                              */
-  const int32_t* chunknode_dev;
+  const int32_t* chunkptr_dev;
   const int32_t* chunkinc_dev;
+  const int32_t* chunklist_dev;
+  const int32_t* chunkdim_dev;
+  const int32_t* soff_dev;
+  const int32_t* roff_dev;
   int64_t nchunk;
   int32_t maxval;
   int32_t threads;

@@ -58,3 +58,14 @@ def rel(a, b):
 def csr_from_api(asm):
     P = asm.plan
     return P.indptr.cpu().numpy(), P.indices.cpu().numpy()
+
+
+def top_faces(kind, X, el, n):
+    """Surface set and face node lists of the z = max side, chosen by topology
+    (the nodes of a jittered block do not lie on a plane)."""
+    if kind == "C3D8":
+        pos = np.nonzero(np.arange(el.shape[0]) % n == n - 1)[0]
+        loc = [4, 5, 6, 7]                      # face 1 of C3D8
+        return [(pos, 1)], torch.as_tensor(np.asarray(el)[pos][:, loc])
+    sets = O.boundary_faces(kind, torch.as_tensor(el), torch.as_tensor(X), 2, float(np.asarray(X)[:, 2].max()))
+    return [(i.numpy(), f) for i, f, _ in sets], torch.cat([f for _, _, f in sets])

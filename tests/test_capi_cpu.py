@@ -97,12 +97,17 @@ def test_host_plan_chunks_cover_all_nodes_and_incidences(golden):
     N = g["X"].shape[0]
     mask = np.full(N, 7, np.uint8)
     hp = _plan(N, mask, [("C3D4", g["elems"])])
-    cn = hp.array(L.G_BASE + L.A_CHUNKNODE)
+    cp = hp.array(L.G_BASE + L.A_CHUNKPTR)
+    cl = hp.array(L.G_BASE + L.A_CHUNKLIST)
     ci = hp.array(L.G_BASE + L.A_CHUNKINC)
     ni = hp.array(L.G_BASE + L.A_NODEINC)
-    assert cn[0] == 0 and cn[-1] == N and ci[0] == 0 and ci[-1] == ni[-1] == g["elems"].size
+    dim = hp.array(L.G_BASE + L.A_CHUNKDIM).reshape(-1, 3)
+    assert np.array_equal(cl, np.arange(N))          # every node listed once, in order
+    assert cp[0] == 0 and cp[-1] == N and ci[0] == 0 and ci[-1] == ni[-1] == g["elems"].size
     assert np.all(np.diff(ci) <= hp.scalar(L.G_BASE + L.S_THREADS))
-    assert np.all(ni[cn] == ci)
+    assert np.all(ni[cl[cp[:-1]]] == ci[:-1])
+    assert np.all(dim[:, 2] == 1)                    # all-free rows are contiguous
+    assert dim[:, :2].sum(1).max() == hp.scalar(L.G_BASE + L.S_SMEM)
     inc = hp.array(L.G_BASE + L.A_INC)
     e, a = inc >> 4, inc & 15
     node = g["elems"][e, a]
@@ -118,6 +123,19 @@ def test_host_plan_chunks_cover_all_nodes_and_incidences(golden):
         for b in range(4):
             c = g["elems"][e[q], b]
             assert ix[vbase[n] + boff[q, b]] == rd[c]
+
+
+def test_face_chunks_list_only_surface_nodes(golden):
+    from fea_b200 import _lib as L
+    g = golden("hex5")
+    N = g["X"].shape[0]
+    mask = np.full(N, 7, np.uint8)
+    mask[g["fixed"]] = 0
+    faces = g["pressure_faces"]
+    hp = _plan(N, mask, [("C3D8", g["elems"])], [("Q4", faces)])
+    cl = hp.array(L.F_BASE + L.A_CHUNKLIST)
+    np.testing.assert_array_equal(cl, np.unique(faces))
+    assert hp.array(L.F_BASE + L.A_CHUNKINC)[-1] == faces.size
 
 
 def test_plan_errors():
@@ -141,3 +159,21 @@ def test_empty_group_and_fully_fixed_mesh():
     X, el = O.tet_block(1)
     hp = _plan(8, np.zeros(8, np.uint8), [("C3D4", el.numpy())])
     assert hp.scalar(L.FEA_S_NDOF) == 0 and hp.scalar(L.FEA_S_NNZ) == 0
+
+
+def test_product_meshes_match_oracle_meshes():
+    """The benchmark's mesh generators build the same meshes as the oracle's."""
+    from fea_b200 import meshes
+    for n in (1, 3):
+        X, el = meshes.hex_block(n, jitter=0.1, seed=4)
+        Xo, elo = O.hex_block(n, jitter=0.1, seed=4)
+        np.testing.assert_array_equal(X, Xo.numpy())
+        np.testing.assert_array_equal(el, elo.numpy())
+        X, el = meshes.tet_block(n)
+        Xo, elo = O.tet_block(n)
+        np.testing.assert_array_equal(X, Xo.numpy())
+        np.testing.assert_array_equal(el, elo.numpy())
+    X, el = meshes.tet_block(2)
+    sets, faces = meshes.plane_faces("C3D4", el, X, 2, 1.0)
+    ref = O.boundary_faces("C3D4", torch.from_numpy(el), torch.from_numpy(X), 2, 1.0)
+    np.testing.assert_array_equal(faces, torch.cat([f for _, _, f in ref]).numpy())
