@@ -289,6 +289,185 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
                   WR ? P.R : nullptr);
 }
 
+// ---- C3D8 R + K gather, 8 lanes per incidence ------------------------------
+// Lane g of an incidence evaluates Gauss point g (kinematics, material and
+// the 27 coefficients H_m[j][k] of the row node's strip) and writes them to
+// shared memory; after a warp barrier lane b contracts all Gauss points into
+// the 3x3 block K_ab = sum_g sum_m dN_b/dxi_m(g) H_m(g).  Per-thread state is
+// one 3x3 block instead of the whole strip, which keeps the kernel free of
+// register spills and its code small.
+constexpr int HEX_INC = 32;               // incidences per chunk
+constexpr int HEX_TPB = 8 * HEX_INC;      // threads per CTA
+constexpr int HEX_XS = 31;                // exchange stride (H[27], R[3], pad): odd -> conflict-free
+
+// corner signs of hex node / Gauss point c (brick.py:15-25, 151-160)
+__device__ __forceinline__ double csx(int c) { return (((c + 1) >> 1) & 1) ? 1.0 : -1.0; }
+__device__ __forceinline__ double csy(int c) { return ((c >> 1) & 1) ? 1.0 : -1.0; }
+__device__ __forceinline__ double csz(int c) { return (c >> 2) ? 1.0 : -1.0; }
+
+template <bool WR, bool ACC, bool ER>
+__global__ void __launch_bounds__(HEX_TPB) k_hex_rk(VolParams P, int ex0) {
+  extern __shared__ double sm[];
+  const double q3 = 0.57735026918962576451;   // 1/sqrt(3)
+  const int ch = blockIdx.x;
+  const int i0 = P.chunkinc[ch], i1 = P.chunkinc[ch + 1];
+  const int nv = P.chunkdim[3 * ch];
+  const int nr = WR ? P.chunkdim[3 * ch + 1] : 0;
+  for (int i = threadIdx.x; i < nv + nr; i += blockDim.x) sm[i] = 0.0;
+  const int li = threadIdx.x >> 3;            // incidence within the chunk
+  const int lane = threadIdx.x & 7;           // Gauss point (phase 1) / element node (phase 2)
+  const int q = i0 + li;
+  const bool act = q < i1;
+  double* xs = sm + ex0 + (li * 8) * HEX_XS;  // this incidence's exchange rows
+  int32_t cn[8];
+  int a = 0;
+  int64_t e = 0;
+  if (act) {
+    const int ea = P.inc[q];
+    e = ea >> 4;
+    a = ea & 15;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) cn[b] = P.conn[e * 8 + b];
+    // ---- phase 1: Gauss point g = lane ----------------------------------
+    const double px = csx(lane) * q3, py = csy(lane) * q3, pz = csz(lane) * q3;
+    const double fxp = 1.0 + px, fxm = 1.0 - px, fyp = 1.0 + py, fym = 1.0 - py, fzp = 1.0 + pz, fzm = 1.0 - pz;
+    double J0[9], Ju[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) J0[i] = Ju[i] = 0.0;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const double sx = (((b + 1) >> 1) & 1) ? 1.0 : -1.0, sy = ((b >> 1) & 1) ? 1.0 : -1.0, sz = (b >> 2) ? 1.0 : -1.0;
+      const double fx = sx > 0 ? fxp : fxm, fy = sy > 0 ? fyp : fym, fz = sz > 0 ? fzp : fzm;
+      const double d0 = 0.125 * sx * fy * fz, d1 = 0.125 * sy * fx * fz, d2 = 0.125 * sz * fx * fy;
+      const double* xb = P.X + 3 * (int64_t)cn[b];
+      const unsigned mb = P.mask[cn[b]];
+      const int32_t rb = P.rdof[cn[b]];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const double x = __ldg(xb + i), u = node_u(P.gc, rb, mb, i);
+        J0[3 * i] += x * d0; J0[3 * i + 1] += x * d1; J0[3 * i + 2] += x * d2;
+        Ju[3 * i] += u * d0; Ju[3 * i + 1] += u * d1; Ju[3 * i + 2] += u * d2;
+      }
+    }
+    double iJ[9], F[9], iF[9];
+    const double w = inv3(J0, iJ);           // Gauss weight 1
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        F[3 * I + i] = (I == i ? 1.0 : 0.0) + Ju[3 * I] * iJ[i] + Ju[3 * I + 1] * iJ[3 + i] + Ju[3 * I + 2] * iJ[6 + i];
+    const double J = inv3(F, iF);
+    const double mu = P.mu, kappa = P.kappa;
+    const double Jm = pow(J, -2.0 / 3.0);
+    double sF2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];
+    const double I1 = Jm * sF2, muJm = mu * Jm;
+    const double c2 = kappa * J * (J - 1.0) - mu * I1 / 3.0;
+    double Mq[9], Mf[9];
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        Mq[3 * m + k] = iJ[3 * m] * iF[k] + iJ[3 * m + 1] * iF[3 + k] + iJ[3 * m + 2] * iF[6 + k];
+        Mf[3 * m + k] = iJ[3 * m] * F[3 * k] + iJ[3 * m + 1] * F[3 * k + 1] + iJ[3 * m + 2] * F[3 * k + 2];
+      }
+    const double sax = csx(a), say = csy(a), saz = csz(a);
+    const double gx = 1.0 + sax * px, gy = 1.0 + say * py, gz = 1.0 + saz * pz;
+    const double da0 = 0.125 * sax * gy * gz, da1 = 0.125 * say * gx * gz, da2 = 0.125 * saz * gx * gy;
+    double qa[3], fa[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      qa[k] = da0 * Mq[k] + da1 * Mq[3 + k] + da2 * Mq[6 + k];
+      fa[k] = da0 * Mf[k] + da1 * Mf[3 + k] + da2 * Mf[6 + k];
+    }
+    double* xg = xs + lane * HEX_XS;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) xg[27 + j] = w * (muJm * fa[j] + c2 * qa[j]);
+    const double alpha = -2.0 / 3.0 * muJm;
+    const double beta = kappa * J * (2.0 * J - 1.0) + 2.0 / 9.0 * mu * I1;
+    const double gamma = mu * I1 / 3.0 - kappa * J * (J - 1.0);
+    double va[3], ua[3], ga[3], gav[3], gm[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      va[j] = w * (alpha * fa[j] + beta * qa[j]);
+      ua[j] = w * alpha * qa[j];
+      ga[j] = w * gamma * qa[j];
+      gav[j] = da0 * iJ[j] + da1 * iJ[3 + j] + da2 * iJ[6 + j];
+    }
+    const double wc = w * muJm;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) gm[m] = wc * (iJ[3 * m] * gav[0] + iJ[3 * m + 1] * gav[1] + iJ[3 * m + 2] * gav[2]);
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+          xg[(3 * j + k) * 3 + m] =
+              va[j] * Mq[3 * m + k] + ua[j] * Mf[3 * m + k] + ga[k] * Mq[3 * m + j] + (j == k ? gm[m] : 0.0);
+  }
+  __syncthreads();
+  // ---- phase 2: element node b = lane, sum over the 8 Gauss points --------
+  double acc[9];
+  double rj_sum = 0.0;
+  if (act) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) acc[i] = 0.0;
+    const double ux = csx(lane) * q3, uy = csy(lane) * q3, uz = csz(lane) * q3;
+    const double bx = csx(lane), by = csy(lane), bz = csz(lane);
+#pragma unroll
+    for (int g = 0; g < 8; ++g) {
+      const double gxs = (((g + 1) >> 1) & 1) ? 1.0 : -1.0, gys = ((g >> 1) & 1) ? 1.0 : -1.0, gzs = (g >> 2) ? 1.0 : -1.0;
+      const double fx = 1.0 + gxs * ux, fy = 1.0 + gys * uy, fz = 1.0 + gzs * uz;
+      const double d0 = 0.125 * bx * fy * fz, d1 = 0.125 * by * fx * fz, d2 = 0.125 * bz * fx * fy;
+      const double* xg = xs + g * HEX_XS;
+#pragma unroll
+      for (int jk = 0; jk < 9; ++jk) acc[jk] += d0 * xg[3 * jk] + d1 * xg[3 * jk + 1] + d2 * xg[3 * jk + 2];
+      if (lane < 3) rj_sum += xg[27 + lane];
+    }
+    if (ER && lane < 3) P.elemR[(int64_t)(3 * a + lane) * P.ne + e] = rj_sum;
+  }
+  // ---- per-node sums in incidence order ------------------------------------
+  int rank = -1, n = 0;
+  unsigned mn = 0;
+  int rowoff = 0, L = 0, dr = 0;
+  if (act) {
+    n = cn[a];
+    rank = q - P.nodeinc[n];
+    mn = P.mask[n];
+    rowoff = P.soff[n];
+    L = P.rowlen[n];
+    dr = P.roff[n];
+  }
+  for (int k = 0; k < P.maxval; ++k) {
+    if (rank == k) {
+      const unsigned bo = P.boff[(int64_t)q * 8 + lane];
+      if (bo != 0xFFFFu) {
+        const unsigned mc = P.mask[cn[lane]];
+        int rj = 0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          if (!(mn >> j & 1u)) continue;
+          double* row = sm + rowoff + rj * L + bo;
+          int rk = 0;
+#pragma unroll
+          for (int kk = 0; kk < 3; ++kk) {
+            if (!(mc >> kk & 1u)) continue;
+            row[rk] += acc[3 * j + kk];
+            ++rk;
+          }
+          ++rj;
+        }
+      }
+      if (WR && lane < 3 && (mn >> lane & 1u)) sm[nv + dr + rank3(mn, lane)] += rj_sum;
+    }
+    __syncthreads();
+  }
+  write_back<ACC>(P.chunkptr, P.chunklist, P.chunkdim, P.vbase, P.dbase, P.mask, P.soff, P.roff, ch, sm, P.K, nv,
+                  WR ? P.R : nullptr);
+}
+
 // R-only kernel: one thread per node, sequential over its incidences.
 template <int NN, bool ACC, bool ER>
 __global__ void __launch_bounds__(128) k_vol_r(VolParams P) {
@@ -679,6 +858,19 @@ static int launch_chunked(void (*kern)(Prm), int64_t nchunk, int threads, int64_
   return (int)cudaGetLastError();
 }
 
+template <class Prm>
+static int launch_chunked_ex(void (*kern)(Prm, int), int64_t nchunk, int threads, int64_t smem_doubles,
+                             cudaStream_t st, const Prm& p, int extra) {
+  size_t bytes = (size_t)smem_doubles * sizeof(double);
+  if (bytes > (size_t)smem_limit()) return FEA_ESMEM;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (err != cudaSuccess) return (int)err;
+  if (nchunk <= 0) return 0;
+  kern<<<(unsigned)nchunk, threads, bytes, st>>>(p, extra);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
 }  // namespace fea
 
 using namespace fea;
@@ -696,23 +888,29 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
   P.R = R;
   P.elemR = elemR;
   const bool hex = G->kind == FEA_C3D8;
-  const int tpb = hex ? VolTPB<8>::v : VolTPB<4>::v;
+  const int tpb = hex ? HEX_INC : VolTPB<4>::v;
   if (G->threads != tpb) return FEA_ECHUNK;
   if (K) {
     int64_t smem = G->smem_doubles;
     const bool acc = accumulate != 0, wr = R != nullptr, er = elemR != nullptr;
+    if (hex) {
+      const int64_t ex0 = smem;
+      const int64_t total = smem + (int64_t)HEX_INC * 8 * HEX_XS;
+#define FEA_HEX(WR_, ACC_, ER_)                                                                        \
+  if (wr == WR_ && acc == ACC_ && er == ER_)                                                           \
+    return launch_chunked_ex(k_hex_rk<WR_, ACC_, ER_>, G->nchunk, HEX_TPB, total, st, P, (int)ex0);
+      FEA_HEX(true, false, false) FEA_HEX(true, true, false) FEA_HEX(false, false, false)
+      FEA_HEX(false, true, false) FEA_HEX(true, false, true) FEA_HEX(true, true, true)
+      FEA_HEX(false, false, true) FEA_HEX(false, true, true)
+#undef FEA_HEX
+      return FEA_EINVAL;
+    }
 #define FEA_RK(NN_, WR_, ACC_, ER_)                                                                    \
   if (wr == WR_ && acc == ACC_ && er == ER_)                                                           \
     return launch_chunked(k_vol_rk<NN_, WR_, ACC_, ER_>, G->nchunk, tpb, smem, st, P);
-    if (hex) {
-      FEA_RK(8, true, false, false) FEA_RK(8, true, true, false) FEA_RK(8, false, false, false)
-      FEA_RK(8, false, true, false) FEA_RK(8, true, false, true) FEA_RK(8, true, true, true)
-      FEA_RK(8, false, false, true) FEA_RK(8, false, true, true)
-    } else {
-      FEA_RK(4, true, false, false) FEA_RK(4, true, true, false) FEA_RK(4, false, false, false)
-      FEA_RK(4, false, true, false) FEA_RK(4, true, false, true) FEA_RK(4, true, true, true)
-      FEA_RK(4, false, false, true) FEA_RK(4, false, true, true)
-    }
+    FEA_RK(4, true, false, false) FEA_RK(4, true, true, false) FEA_RK(4, false, false, false)
+    FEA_RK(4, false, true, false) FEA_RK(4, true, false, true) FEA_RK(4, true, true, true)
+    FEA_RK(4, false, false, true) FEA_RK(4, false, true, true)
 #undef FEA_RK
     return FEA_EINVAL;
   }

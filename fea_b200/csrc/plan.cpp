@@ -309,7 +309,7 @@ extern "C" int fea_plan_build(int64_t n_nodes, const uint8_t* free_mask, int32_t
   P->faces.resize(n_faces);
   const int64_t budget = smem_doubles > 0 ? smem_doubles : 12288;
   for (int g = 0; g < n_groups; ++g) {
-    int th = vol_threads > 0 ? vol_threads : (group_kind[g] == FEA_C3D8 ? 128 : 256);
+    int th = vol_threads > 0 ? vol_threads : (group_kind[g] == FEA_C3D8 ? 32 : 256);
     int r = build_gather(*P, group_kind[g], group_ne[g], group_conn[g], ginc[g], th, budget, P->groups[g]);
     if (r) return r;
   }

@@ -69,8 +69,8 @@ typedef struct fea_plan fea_plan;
  *                    element count, connectivity int32 [ne, nn] (host)
  *   faces            n_faces pressure face groups: kind (FEA_T3 / FEA_Q4),
  *                    face count, node lists int32 [nf, 3|4] (host)
- *   vol_threads      threads per gather chunk for the element kernels
- *                    (0 = default: 128 for C3D8, 256 for C3D4)
+ *   vol_threads      incidences per gather chunk for the element kernels
+ *                    (0 = default: 32 for C3D8 (8 lanes each), 256 for C3D4)
  *   smem_doubles     per-chunk shared-memory budget in doubles (0 = default)
  * The reduced DOF numbering is node-major over free DOFs, as GC in the
  * reference (assembly.py:170-183); the CSR pattern equals the reference's
