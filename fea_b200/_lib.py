@@ -78,7 +78,8 @@ def _sig(name, res, *args):
 fea_plan_build = _sig("fea_plan_build", I32, I64, P, I32, P, P, P, I32, P, P, P, I32, I64, C.POINTER(P))
 fea_plan_free = _sig("fea_plan_free", None, P)
 fea_plan_get = _sig("fea_plan_get", I32, P, I32, I32, P, C.POINTER(I64))
-fea_assemble_volume = _sig("fea_assemble_volume", I32, NP, GP, D, D, P, P, P, P, I32, P)
+fea_assemble_work_len = _sig("fea_assemble_work_len", I64, GP)
+fea_assemble_volume = _sig("fea_assemble_volume", I32, NP, GP, D, D, P, P, P, P, I32, P, I64, P)
 fea_assemble_pressure = _sig("fea_assemble_pressure", I32, NP, GP, D, P, P, P, P, P)
 fea_reduce_scratch_len = _sig("fea_reduce_scratch_len", I64, I64)
 fea_energy_volume = _sig("fea_energy_volume", I32, NP, GP, D, D, P, P, P, I64, P)
@@ -99,7 +100,7 @@ fea_version = _sig("fea_version", I32)
 fea_launch_count = _sig("fea_launch_count", I64)
 
 # every symbol the header declares (checked by the CPU test suite)
-EXPORTED = ["fea_plan_build", "fea_plan_free", "fea_plan_get", "fea_assemble_volume", "fea_assemble_pressure",
+EXPORTED = ["fea_plan_build", "fea_plan_free", "fea_plan_get", "fea_assemble_work_len", "fea_assemble_volume", "fea_assemble_pressure",
             "fea_reduce_scratch_len", "fea_energy_volume", "fea_energy_pressure", "fea_lumped_mass",
             "fea_invert_mass", "fea_pcg_work_len", "fea_pcg_solve", "fea_pcg_mixed_work_len",
             "fea_pcg_solve_mixed", "fea_spmv", "fea_convert_f32", "fea_explicit_work_len", "fea_explicit_run",

@@ -289,46 +289,46 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
                   WR ? P.R : nullptr);
 }
 
-// ---- C3D8 R + K gather, 8 lanes per incidence ------------------------------
-// Lane g of an incidence evaluates Gauss point g (kinematics, material and
-// the 27 coefficients H_m[j][k] of the row node's strip) and writes them to
-// shared memory; after a warp barrier lane b contracts all Gauss points into
-// the 3x3 block K_ab = sum_g sum_m dN_b/dxi_m(g) H_m(g).  Per-thread state is
-// one 3x3 block instead of the whole strip, which keeps the kernel free of
-// register spills and its code small.
-constexpr int HEX_INC = 32;               // incidences per chunk
-constexpr int HEX_TPB = 8 * HEX_INC;      // threads per CTA
-constexpr int HEX_XS = 31;                // exchange stride (H[27], R[3], pad): odd -> conflict-free
+// ---- C3D8 R + K: element kernel + staged-block gather -----------------------
+// k_hex_elem evaluates every element ONCE: 8 lanes per element, lane g
+// computes the kinematics of Gauss point g and the vectors q_b = F^-T g_b,
+// f_b = F g_b, g_b of all 8 nodes into shared memory; then lane a builds the
+// upper-triangular blocks K_ab it owns (circulant assignment: b = a + d mod 8,
+// d = 0..3, plus d = 4 for a < 4 — 36 blocks over 8 lanes) with its own row
+// vectors in registers,
+//   K_ab = sum_g (A_a q_b^T + B_a f_b^T + q_b C_a^T + wc (g_a . g_b) I),
+//   A_a = w(alpha f_a + beta q_a), B_a = w alpha q_a, C_a = w gamma q_a,
+// and the element residual R_a = sum_g w(mu J^-2/3 f_a + c2 q_a).  The 36
+// blocks and R_e are staged in HBM; k_hex_gather then sums them per node row
+// (transposing blocks stored under (b, a)) and writes each row range once.
+constexpr int HX_EPB = 8;                 // elements per CTA
+constexpr int HX_TPB = 8 * HX_EPB;        // threads per CTA
+constexpr int HX_VB = 10;                 // doubles per (gp, node) vector slot: q, f, g + pad
+constexpr int HX_VG = 81;                 // doubles per Gauss point (8 slots + 1 pad)
+constexpr int HX_SC = 8 * HX_VG;          // offset of the per-Gauss-point scalars (8 each)
+constexpr int HX_EL = 721;                // doubles per element (== 1 mod 16: conflict-free)
+constexpr int HX_STAGE = 36 * 9 + 24;     // staged doubles per element: 36 blocks + R_e
+constexpr int HX_GINC = 32;               // incidences per gather chunk (8 lanes each)
+constexpr int HX_GTPB = 8 * HX_GINC;
 
 // corner signs of hex node / Gauss point c (brick.py:15-25, 151-160)
 __device__ __forceinline__ double csx(int c) { return (((c + 1) >> 1) & 1) ? 1.0 : -1.0; }
 __device__ __forceinline__ double csy(int c) { return ((c >> 1) & 1) ? 1.0 : -1.0; }
 __device__ __forceinline__ double csz(int c) { return (c >> 2) ? 1.0 : -1.0; }
+// staged block slot of (row a, offset d = (b - a) mod 8), d <= 3 or (d == 4, a < 4)
+__device__ __forceinline__ int hx_slot(int a, int d) { return d < 4 ? a * 4 + d : 32 + a; }
 
-template <bool WR, bool ACC, bool ER>
-__global__ void __launch_bounds__(HEX_TPB) k_hex_rk(VolParams P, int ex0) {
-  extern __shared__ double sm[];
+template <bool ER>
+__global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __restrict__ stage) {
+  __shared__ double sv[HX_EPB * HX_EL];
   const double q3 = 0.57735026918962576451;   // 1/sqrt(3)
-  const int ch = blockIdx.x;
-  const int i0 = P.chunkinc[ch], i1 = P.chunkinc[ch + 1];
-  const int nv = P.chunkdim[3 * ch];
-  const int nr = WR ? P.chunkdim[3 * ch + 1] : 0;
-  for (int i = threadIdx.x; i < nv + nr; i += blockDim.x) sm[i] = 0.0;
-  const int li = threadIdx.x >> 3;            // incidence within the chunk
-  const int lane = threadIdx.x & 7;           // Gauss point (phase 1) / element node (phase 2)
-  const int q = i0 + li;
-  const bool act = q < i1;
-  double* xs = sm + ex0 + (li * 8) * HEX_XS;  // this incidence's exchange rows
-  int32_t cn[8];
-  int a = 0;
-  int64_t e = 0;
+  const int le = threadIdx.x >> 3;
+  const int lane = threadIdx.x & 7;
+  const int64_t e = (int64_t)blockIdx.x * HX_EPB + le;
+  const bool act = e < P.ne;
+  double* V = sv + le * HX_EL;
   if (act) {
-    const int ea = P.inc[q];
-    e = ea >> 4;
-    a = ea & 15;
-#pragma unroll
-    for (int b = 0; b < 8; ++b) cn[b] = P.conn[e * 8 + b];
-    // ---- phase 1: Gauss point g = lane ----------------------------------
+    // ---- phase 1: Gauss point g = lane --------------------------------------
     const double px = csx(lane) * q3, py = csy(lane) * q3, pz = csz(lane) * q3;
     const double fxp = 1.0 + px, fxm = 1.0 - px, fyp = 1.0 + py, fym = 1.0 - py, fzp = 1.0 + pz, fzm = 1.0 - pz;
     double J0[9], Ju[9];
@@ -339,9 +339,10 @@ __global__ void __launch_bounds__(HEX_TPB) k_hex_rk(VolParams P, int ex0) {
       const double sx = (((b + 1) >> 1) & 1) ? 1.0 : -1.0, sy = ((b >> 1) & 1) ? 1.0 : -1.0, sz = (b >> 2) ? 1.0 : -1.0;
       const double fx = sx > 0 ? fxp : fxm, fy = sy > 0 ? fyp : fym, fz = sz > 0 ? fzp : fzm;
       const double d0 = 0.125 * sx * fy * fz, d1 = 0.125 * sy * fx * fz, d2 = 0.125 * sz * fx * fy;
-      const double* xb = P.X + 3 * (int64_t)cn[b];
-      const unsigned mb = P.mask[cn[b]];
-      const int32_t rb = P.rdof[cn[b]];
+      const int32_t c = P.conn[e * 8 + b];
+      const double* xb = P.X + 3 * (int64_t)c;
+      const unsigned mb = P.mask[c];
+      const int32_t rb = P.rdof[c];
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
         const double x = __ldg(xb + i), u = node_u(P.gc, rb, mb, i);
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(HEX_TPB) k_hex_rk(VolParams P, int ex0) {
       }
     }
     double iJ[9], F[9], iF[9];
-    const double w = inv3(J0, iJ);           // Gauss weight 1
+    const double w = inv3(J0, iJ);             // Gauss weight 1
 #pragma unroll
     for (int I = 0; I < 3; ++I)
 #pragma unroll
@@ -363,7 +364,13 @@ __global__ void __launch_bounds__(HEX_TPB) k_hex_rk(VolParams P, int ex0) {
 #pragma unroll
     for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];
     const double I1 = Jm * sF2, muJm = mu * Jm;
-    const double c2 = kappa * J * (J - 1.0) - mu * I1 / 3.0;
+    double* S = V + HX_SC + lane * 8;
+    S[0] = w * (-2.0 / 3.0 * muJm);                                 // w alpha
+    S[1] = w * (kappa * J * (2.0 * J - 1.0) + 2.0 / 9.0 * mu * I1);  // w beta
+    S[2] = w * (mu * I1 / 3.0 - kappa * J * (J - 1.0));              // w gamma
+    S[3] = w * muJm;                                                 // w c (delta term, residual)
+    S[4] = w * (kappa * J * (J - 1.0) - mu * I1 / 3.0);              // w c2 (residual)
+    // Mq = J0^-1 F^-1, Mf = J0^-1 F^T: q_b = Mq^T dxi_b, f_b = Mf^T dxi_b, g_b = J0^-T dxi_b
     double Mq[9], Mf[9];
 #pragma unroll
     for (int m = 0; m < 3; ++m)
@@ -372,95 +379,156 @@ __global__ void __launch_bounds__(HEX_TPB) k_hex_rk(VolParams P, int ex0) {
         Mq[3 * m + k] = iJ[3 * m] * iF[k] + iJ[3 * m + 1] * iF[3 + k] + iJ[3 * m + 2] * iF[6 + k];
         Mf[3 * m + k] = iJ[3 * m] * F[3 * k] + iJ[3 * m + 1] * F[3 * k + 1] + iJ[3 * m + 2] * F[3 * k + 2];
       }
-    const double sax = csx(a), say = csy(a), saz = csz(a);
-    const double gx = 1.0 + sax * px, gy = 1.0 + say * py, gz = 1.0 + saz * pz;
-    const double da0 = 0.125 * sax * gy * gz, da1 = 0.125 * say * gx * gz, da2 = 0.125 * saz * gx * gy;
-    double qa[3], fa[3];
+    double* Vg = V + lane * HX_VG;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const double sx = (((b + 1) >> 1) & 1) ? 1.0 : -1.0, sy = ((b >> 1) & 1) ? 1.0 : -1.0, sz = (b >> 2) ? 1.0 : -1.0;
+      const double fx = sx > 0 ? fxp : fxm, fy = sy > 0 ? fyp : fym, fz = sz > 0 ? fzp : fzm;
+      const double d0 = 0.125 * sx * fy * fz, d1 = 0.125 * sy * fx * fz, d2 = 0.125 * sz * fx * fy;
+      double* o = Vg + b * HX_VB;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        o[k] = d0 * Mq[k] + d1 * Mq[3 + k] + d2 * Mq[6 + k];
+        o[3 + k] = d0 * Mf[k] + d1 * Mf[3 + k] + d2 * Mf[6 + k];
+        o[6 + k] = d0 * iJ[k] + d1 * iJ[3 + k] + d2 * iJ[6 + k];
+      }
+    }
+  }
+  __syncwarp();
+  if (!act) return;
+  // ---- phase 2: row node a = lane ------------------------------------------
+  const int a = lane;
+  const int nb = a < 4 ? 5 : 4;
+  double acc[5][9];
+  double racc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int d = 0; d < 5; ++d)
+#pragma unroll
+    for (int i = 0; i < 9; ++i) acc[d][i] = 0.0;
+#pragma unroll 1
+  for (int g = 0; g < 8; ++g) {
+    const double* S = V + HX_SC + g * 8;
+    const double wa = S[0], wb = S[1], wg = S[2], wc = S[3], wc2 = S[4];
+    const double* Va = V + g * HX_VG + a * HX_VB;
+    double qa[3], fa[3], ga[3], A[3], B[3], Cc[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      qa[k] = da0 * Mq[k] + da1 * Mq[3 + k] + da2 * Mq[6 + k];
-      fa[k] = da0 * Mf[k] + da1 * Mf[3 + k] + da2 * Mf[6 + k];
+      qa[k] = Va[k];
+      fa[k] = Va[3 + k];
+      ga[k] = Va[6 + k];
     }
-    double* xg = xs + lane * HEX_XS;
 #pragma unroll
-    for (int j = 0; j < 3; ++j) xg[27 + j] = w * (muJm * fa[j] + c2 * qa[j]);
-    const double alpha = -2.0 / 3.0 * muJm;
-    const double beta = kappa * J * (2.0 * J - 1.0) + 2.0 / 9.0 * mu * I1;
-    const double gamma = mu * I1 / 3.0 - kappa * J * (J - 1.0);
-    double va[3], ua[3], ga[3], gav[3], gm[3];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      va[j] = w * (alpha * fa[j] + beta * qa[j]);
-      ua[j] = w * alpha * qa[j];
-      ga[j] = w * gamma * qa[j];
-      gav[j] = da0 * iJ[j] + da1 * iJ[3 + j] + da2 * iJ[6 + j];
+    for (int k = 0; k < 3; ++k) {
+      A[k] = wa * fa[k] + wb * qa[k];
+      B[k] = wa * qa[k];
+      Cc[k] = wg * qa[k];
+      racc[k] += wc * fa[k] + wc2 * qa[k];
     }
-    const double wc = w * muJm;
 #pragma unroll
-    for (int m = 0; m < 3; ++m) gm[m] = wc * (iJ[3 * m] * gav[0] + iJ[3 * m + 1] * gav[1] + iJ[3 * m + 2] * gav[2]);
+    for (int d = 0; d < 5; ++d) {
+      if (d == 4 && nb == 4) break;
+      const double* Vb = V + g * HX_VG + ((a + d) & 7) * HX_VB;
+      double qb[3], fb[3], gb[3];
 #pragma unroll
-    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k) {
+        qb[k] = Vb[k];
+        fb[k] = Vb[3 + k];
+        gb[k] = Vb[6 + k];
+      }
+      const double dg = wc * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
 #pragma unroll
-      for (int k = 0; k < 3; ++k)
+      for (int j = 0; j < 3; ++j)
 #pragma unroll
-        for (int m = 0; m < 3; ++m)
-          xg[(3 * j + k) * 3 + m] =
-              va[j] * Mq[3 * m + k] + ua[j] * Mf[3 * m + k] + ga[k] * Mq[3 * m + j] + (j == k ? gm[m] : 0.0);
+        for (int k = 0; k < 3; ++k)
+          acc[d][3 * j + k] += A[j] * qb[k] + B[j] * fb[k] + qb[j] * Cc[k] + (j == k ? dg : 0.0);
+    }
   }
-  __syncthreads();
-  // ---- phase 2: element node b = lane, sum over the 8 Gauss points --------
-  double acc[9];
-  double rj_sum = 0.0;
+  double* out = stage + e * HX_STAGE;
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    if (d == 4 && nb == 4) break;
+    double* o = out + hx_slot(a, d) * 9;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) o[i] = acc[d][i];
+  }
+#pragma unroll
+  for (int j = 0; j < 3; ++j) out[324 + 3 * a + j] = racc[j];
+  if (ER) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) P.elemR[(int64_t)(3 * a + j) * P.ne + e] = racc[j];
+  }
+}
+
+// Per node row: 8 lanes per incidence, lane b fetches block (a, b) of the
+// incidence's element from the stage (transposed when stored as (b, a)).
+template <bool WR, bool ACC>
+__global__ void __launch_bounds__(HX_GTPB) k_hex_gather(VolParams P, const double* __restrict__ stage) {
+  extern __shared__ double sm[];
+  const int ch = blockIdx.x;
+  const int i0 = P.chunkinc[ch], i1 = P.chunkinc[ch + 1];
+  const int nv = P.chunkdim[3 * ch];
+  const int nr = WR ? P.chunkdim[3 * ch + 1] : 0;
+  for (int i = threadIdx.x; i < nv + nr; i += blockDim.x) sm[i] = 0.0;
+  const int li = threadIdx.x >> 3;
+  const int lane = threadIdx.x & 7;
+  const int q = i0 + li;
+  const bool act = q < i1;
+  double blk[9];
+  double rj = 0.0;
+  int rank = -1, a = 0;
+  int32_t n = 0, c = 0;
   if (act) {
+    const int ea = P.inc[q];
+    const int64_t e = ea >> 4;
+    a = ea & 15;
+    n = P.conn[e * 8 + a];
+    c = P.conn[e * 8 + lane];
+    rank = q - P.nodeinc[n];
+    const double* st = stage + e * HX_STAGE;
+    const int d = (lane - a) & 7;
+    if (d < 4 || (d == 4 && a < 4)) {
+      const double* s = st + hx_slot(a, d) * 9;
 #pragma unroll
-    for (int i = 0; i < 9; ++i) acc[i] = 0.0;
-    const double ux = csx(lane) * q3, uy = csy(lane) * q3, uz = csz(lane) * q3;
-    const double bx = csx(lane), by = csy(lane), bz = csz(lane);
+      for (int i = 0; i < 9; ++i) blk[i] = s[i];
+    } else {
+      const double* s = st + hx_slot(lane, (a - lane) & 7) * 9;
 #pragma unroll
-    for (int g = 0; g < 8; ++g) {
-      const double gxs = (((g + 1) >> 1) & 1) ? 1.0 : -1.0, gys = ((g >> 1) & 1) ? 1.0 : -1.0, gzs = (g >> 2) ? 1.0 : -1.0;
-      const double fx = 1.0 + gxs * ux, fy = 1.0 + gys * uy, fz = 1.0 + gzs * uz;
-      const double d0 = 0.125 * bx * fy * fz, d1 = 0.125 * by * fx * fz, d2 = 0.125 * bz * fx * fy;
-      const double* xg = xs + g * HEX_XS;
+      for (int j = 0; j < 3; ++j)
 #pragma unroll
-      for (int jk = 0; jk < 9; ++jk) acc[jk] += d0 * xg[3 * jk] + d1 * xg[3 * jk + 1] + d2 * xg[3 * jk + 2];
-      if (lane < 3) rj_sum += xg[27 + lane];
+        for (int k = 0; k < 3; ++k) blk[3 * j + k] = s[3 * k + j];
     }
-    if (ER && lane < 3) P.elemR[(int64_t)(3 * a + lane) * P.ne + e] = rj_sum;
+    if (WR && lane < 3) rj = st[324 + 3 * a + lane];
   }
-  // ---- per-node sums in incidence order ------------------------------------
-  int rank = -1, n = 0;
   unsigned mn = 0;
   int rowoff = 0, L = 0, dr = 0;
   if (act) {
-    n = cn[a];
-    rank = q - P.nodeinc[n];
     mn = P.mask[n];
     rowoff = P.soff[n];
     L = P.rowlen[n];
     dr = P.roff[n];
   }
+  __syncthreads();
   for (int k = 0; k < P.maxval; ++k) {
     if (rank == k) {
       const unsigned bo = P.boff[(int64_t)q * 8 + lane];
       if (bo != 0xFFFFu) {
-        const unsigned mc = P.mask[cn[lane]];
-        int rj = 0;
+        const unsigned mc = P.mask[c];
+        int rjj = 0;
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
           if (!(mn >> j & 1u)) continue;
-          double* row = sm + rowoff + rj * L + bo;
+          double* row = sm + rowoff + rjj * L + bo;
           int rk = 0;
 #pragma unroll
           for (int kk = 0; kk < 3; ++kk) {
             if (!(mc >> kk & 1u)) continue;
-            row[rk] += acc[3 * j + kk];
+            row[rk] += blk[3 * j + kk];
             ++rk;
           }
-          ++rj;
+          ++rjj;
         }
       }
-      if (WR && lane < 3 && (mn >> lane & 1u)) sm[nv + dr + rank3(mn, lane)] += rj_sum;
+      if (WR && lane < 3 && (mn >> lane & 1u)) sm[nv + dr + rank3(mn, lane)] += rj;
     }
     __syncthreads();
   }
@@ -858,9 +926,9 @@ static int launch_chunked(void (*kern)(Prm), int64_t nchunk, int threads, int64_
   return (int)cudaGetLastError();
 }
 
-template <class Prm>
-static int launch_chunked_ex(void (*kern)(Prm, int), int64_t nchunk, int threads, int64_t smem_doubles,
-                             cudaStream_t st, const Prm& p, int extra) {
+template <class Prm, class X>
+static int launch_chunked_ex(void (*kern)(Prm, X), int64_t nchunk, int threads, int64_t smem_doubles,
+                             cudaStream_t st, const Prm& p, X extra) {
   size_t bytes = (size_t)smem_doubles * sizeof(double);
   if (bytes > (size_t)smem_limit()) return FEA_ESMEM;
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -877,9 +945,14 @@ using namespace fea;
 
 extern "C" int64_t fea_reduce_scratch_len(int64_t n_items) { return (n_items + 255) / 256 + 1; }
 
+extern "C" int64_t fea_assemble_work_len(const fea_group_t* G) {
+  if (!G) return 0;
+  return G->kind == FEA_C3D8 ? G->ne * (int64_t)HX_STAGE : 0;
+}
+
 extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, double mu, double kappa,
                                    const double* gc, double* K, double* R, double* elemR, int32_t accumulate,
-                                   cudaStream_t st) {
+                                   double* work, int64_t work_len, cudaStream_t st) {
   if (!N || !G || !gc || (G->kind != FEA_C3D4 && G->kind != FEA_C3D8)) return FEA_EINVAL;
   if (G->nn != (G->kind == FEA_C3D8 ? 8 : 4)) return FEA_EINVAL;
   if (int r = ensure_tables()) return r;
@@ -888,20 +961,23 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
   P.R = R;
   P.elemR = elemR;
   const bool hex = G->kind == FEA_C3D8;
-  const int tpb = hex ? HEX_INC : VolTPB<4>::v;
+  const int tpb = hex ? HX_GINC : VolTPB<4>::v;
   if (G->threads != tpb) return FEA_ECHUNK;
   if (K) {
     int64_t smem = G->smem_doubles;
     const bool acc = accumulate != 0, wr = R != nullptr, er = elemR != nullptr;
     if (hex) {
-      const int64_t ex0 = smem;
-      const int64_t total = smem + (int64_t)HEX_INC * 8 * HEX_XS;
-#define FEA_HEX(WR_, ACC_, ER_)                                                                        \
-  if (wr == WR_ && acc == ACC_ && er == ER_)                                                           \
-    return launch_chunked_ex(k_hex_rk<WR_, ACC_, ER_>, G->nchunk, HEX_TPB, total, st, P, (int)ex0);
-      FEA_HEX(true, false, false) FEA_HEX(true, true, false) FEA_HEX(false, false, false)
-      FEA_HEX(false, true, false) FEA_HEX(true, false, true) FEA_HEX(true, true, true)
-      FEA_HEX(false, false, true) FEA_HEX(false, true, true)
+      if (!work || work_len < fea_assemble_work_len(G)) return FEA_EWORK;
+      const unsigned grid = (unsigned)((G->ne + HX_EPB - 1) / HX_EPB);
+      if (grid) {
+        if (er) k_hex_elem<true><<<grid, HX_TPB, 0, st>>>(P, work);
+        else k_hex_elem<false><<<grid, HX_TPB, 0, st>>>(P, work);
+        count_launch();
+        if (cudaError_t ce = cudaGetLastError()) return (int)ce;
+      }
+#define FEA_HEX(WR_, ACC_)                                                                             \
+  if (wr == WR_ && acc == ACC_) return launch_chunked_ex(k_hex_gather<WR_, ACC_>, G->nchunk, HX_GTPB, smem, st, P, (const double*)work);
+      FEA_HEX(true, false) FEA_HEX(true, true) FEA_HEX(false, false) FEA_HEX(false, true)
 #undef FEA_HEX
       return FEA_EINVAL;
     }

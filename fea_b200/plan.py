@@ -165,11 +165,22 @@ class DevicePlan:
         return self._coo
 
     # -- element / load kernels ---------------------------------------------
+    def stage(self, gi):
+        """Scratch of the element kernels of group gi (C3D8: staged element blocks)."""
+        g = self.groups[gi]
+        n = int(L.fea_assemble_work_len(C.byref(g.desc)))
+        if n == 0:
+            return None, 0
+        if getattr(g, "_stage", None) is None or g._stage.numel() < n:
+            g._stage = torch.empty(n, dtype=torch.float64, device=self.device)
+        return g._stage, n
+
     def assemble_volume(self, gi, mu, kappa, gc, K=None, R=None, elemR=None, accumulate=False):
         g = self.groups[gi]
+        w, wn = self.stage(gi) if K is not None else (None, 0)
         L.check(L.fea_assemble_volume(C.byref(self.nodes), C.byref(g.desc), float(mu), float(kappa), vptr(gc),
-                                      vptr(K), vptr(R), vptr(elemR), int(bool(accumulate)), stream()),
-                "fea_assemble_volume")
+                                      vptr(K), vptr(R), vptr(elemR), int(bool(accumulate)), vptr(w), int(wn),
+                                      stream()), "fea_assemble_volume")
 
     def assemble_pressure(self, fi, p, Xinst, gc, K=None, R=None):
         f = self.faces[fi]

@@ -172,10 +172,14 @@ typedef struct {
  * them (accumulate != 0).  gc_dev: reduced displacement [ndof].  Any of
  * K_dev / R_dev / elemR_dev may be NULL.  elemR_dev receives the unassembled
  * element residual in the reference's (a, j, e) order [nn*3*ne]; it is only
- * meaningful for a plan whose every element node is active. */
+ * meaningful for a plan whose every element node is active.
+ * work_dev: fea_assemble_work_len(group) doubles of scratch (C3D8 stages
+ * its 36 element blocks + residual there, 348 doubles per element; C3D4
+ * needs none). */
+int64_t fea_assemble_work_len(const fea_group_t* group);
 int fea_assemble_volume(const fea_nodes_t* nodes, const fea_group_t* group, double mu, double kappa,
                         const double* gc_dev, double* K_dev, double* R_dev, double* elemR_dev,
-                        int32_t accumulate, cudaStream_t stream);
+                        int32_t accumulate, double* work_dev, int64_t work_len, cudaStream_t stream);
 
 /* Follower pressure p on a face group: adds -p dV/dx to R and -p d2V/dx2 to
  * K (always accumulate).  Xinst_dev: instance node coordinates [N,3]. */

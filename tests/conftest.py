@@ -16,8 +16,11 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "slow: long-running CPU test")
     # the native library is built in-tree; (re)build it when missing or stale
     try:
-        from fea_b200 import _build
-        _build.build()
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("fea_b200_build", os.path.join(ROOT, "fea_b200", "_build.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build()
     except Exception as e:  # the tests that load the library report the failure
         sys.stderr.write("fea_b200 build failed: %s\n" % e)
 
