@@ -31,7 +31,7 @@ FEA_C3D4, FEA_C3D8, FEA_T3, FEA_Q4 = 4, 8, 3, 40
  FEA_A_ADJPTR, FEA_A_ADJCOL, FEA_A_ADJOFF) = range(10, 20)
 G_BASE, F_BASE = 30, 50
 (A_INC, A_BOFF, A_NODEINC, A_CHUNKPTR, A_CHUNKINC, S_NCHUNK, S_MAXVAL, S_THREADS, S_SMEM, A_CHUNKLIST,
- A_CHUNKDIM, A_SOFF, A_ROFF) = range(13)
+ A_CHUNKDIM, A_SOFF, A_ROFF, A_BLKPTR, A_BLKCON) = range(15)
 
 
 class FeaError(RuntimeError):
@@ -50,7 +50,8 @@ def check(status, what):
 class Nodes(C.Structure):
     _fields_ = [("n_nodes", C.c_int64), ("ndof", C.c_int64), ("nnz", C.c_int64),
                 ("X_dev", C.c_void_p), ("rdof_dev", C.c_void_p), ("mask_dev", C.c_void_p),
-                ("vbase_dev", C.c_void_p), ("rowlen_dev", C.c_void_p), ("dbase_dev", C.c_void_p)]
+                ("vbase_dev", C.c_void_p), ("rowlen_dev", C.c_void_p), ("dbase_dev", C.c_void_p),
+                ("adjptr_dev", C.c_void_p), ("adjcol_dev", C.c_void_p), ("adjoff_dev", C.c_void_p)]
 
 
 class Group(C.Structure):
@@ -58,7 +59,7 @@ class Group(C.Structure):
                 ("conn_dev", C.c_void_p), ("inc_dev", C.c_void_p), ("boff_dev", C.c_void_p),
                 ("nodeinc_dev", C.c_void_p), ("chunkptr_dev", C.c_void_p), ("chunkinc_dev", C.c_void_p),
                 ("chunklist_dev", C.c_void_p), ("chunkdim_dev", C.c_void_p), ("soff_dev", C.c_void_p),
-                ("roff_dev", C.c_void_p),
+                ("roff_dev", C.c_void_p), ("blkptr_dev", C.c_void_p), ("blkcon_dev", C.c_void_p),
                 ("nchunk", C.c_int64), ("maxval", C.c_int32), ("threads", C.c_int32),
                 ("smem_doubles", C.c_int64)]
 

@@ -45,6 +45,11 @@ struct VolParams {
   const int32_t* __restrict__ chunkdim;
   const int32_t* __restrict__ soff;
   const int32_t* __restrict__ roff;
+  const int64_t* __restrict__ adjptr;
+  const int32_t* __restrict__ adjcol;
+  const int32_t* __restrict__ adjoff;
+  const int64_t* __restrict__ blkptr;
+  const int32_t* __restrict__ blkcon;
   const double* __restrict__ gc;
   double* K;
   double* R;
@@ -304,9 +309,9 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
 constexpr int HX_EPB = 8;                 // elements per CTA
 constexpr int HX_TPB = 8 * HX_EPB;        // threads per CTA
 constexpr int HX_VB = 10;                 // doubles per (gp, node) vector slot: q, f, g + pad
-constexpr int HX_VG = 81;                 // doubles per Gauss point (8 slots + 1 pad)
+constexpr int HX_VG = 82;                 // doubles per Gauss point (8 slots + 2 pad, 16-byte rows)
 constexpr int HX_SC = 8 * HX_VG;          // offset of the per-Gauss-point scalars (8 each)
-constexpr int HX_EL = 721;                // doubles per element (== 1 mod 16: conflict-free)
+constexpr int HX_EL = HX_SC + 64;         // doubles per element (16-byte aligned)
 constexpr int HX_STAGE = 36 * 9 + 24;     // staged doubles per element: 36 blocks + R_e
 constexpr int HX_GINC = 32;               // incidences per gather chunk (8 lanes each)
 constexpr int HX_GTPB = 8 * HX_GINC;
@@ -320,7 +325,7 @@ __device__ __forceinline__ int hx_slot(int a, int d) { return d < 4 ? a * 4 + d 
 
 template <bool ER>
 __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __restrict__ stage) {
-  __shared__ double sv[HX_EPB * HX_EL];
+  __shared__ __align__(16) double sv[HX_EPB * HX_EL];
   const double q3 = 0.57735026918962576451;   // 1/sqrt(3)
   const int le = threadIdx.x >> 3;
   const int lane = threadIdx.x & 7;
@@ -385,13 +390,19 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
       const double sx = (((b + 1) >> 1) & 1) ? 1.0 : -1.0, sy = ((b >> 1) & 1) ? 1.0 : -1.0, sz = (b >> 2) ? 1.0 : -1.0;
       const double fx = sx > 0 ? fxp : fxm, fy = sy > 0 ? fyp : fym, fz = sz > 0 ? fzp : fzm;
       const double d0 = 0.125 * sx * fy * fz, d1 = 0.125 * sy * fx * fz, d2 = 0.125 * sz * fx * fy;
-      double* o = Vg + b * HX_VB;
+      double v[9];
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        o[k] = d0 * Mq[k] + d1 * Mq[3 + k] + d2 * Mq[6 + k];
-        o[3 + k] = d0 * Mf[k] + d1 * Mf[3 + k] + d2 * Mf[6 + k];
-        o[6 + k] = d0 * iJ[k] + d1 * iJ[3 + k] + d2 * iJ[6 + k];
+        v[k] = d0 * Mq[k] + d1 * Mq[3 + k] + d2 * Mq[6 + k];
+        v[3 + k] = d0 * Mf[k] + d1 * Mf[3 + k] + d2 * Mf[6 + k];
+        v[6 + k] = d0 * iJ[k] + d1 * iJ[3 + k] + d2 * iJ[6 + k];
       }
+      double2* o = reinterpret_cast<double2*>(Vg + b * HX_VB);   // 16-byte aligned slot
+      o[0] = make_double2(v[0], v[1]);
+      o[1] = make_double2(v[2], v[3]);
+      o[2] = make_double2(v[4], v[5]);
+      o[3] = make_double2(v[6], v[7]);
+      Vg[b * HX_VB + 8] = v[8];
     }
   }
   __syncwarp();
@@ -411,11 +422,11 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
     const double wa = S[0], wb = S[1], wg = S[2], wc = S[3], wc2 = S[4];
     const double* Va = V + g * HX_VG + a * HX_VB;
     double qa[3], fa[3], ga[3], A[3], B[3], Cc[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      qa[k] = Va[k];
-      fa[k] = Va[3 + k];
-      ga[k] = Va[6 + k];
+    {
+      const double2* v2 = reinterpret_cast<const double2*>(Va);
+      const double2 x0 = v2[0], x1 = v2[1], x2 = v2[2], x3 = v2[3];
+      qa[0] = x0.x; qa[1] = x0.y; qa[2] = x1.x; fa[0] = x1.y; fa[1] = x2.x; fa[2] = x2.y;
+      ga[0] = x3.x; ga[1] = x3.y; ga[2] = Va[8];
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -429,11 +440,11 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
       if (d == 4 && nb == 4) break;
       const double* Vb = V + g * HX_VG + ((a + d) & 7) * HX_VB;
       double qb[3], fb[3], gb[3];
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        qb[k] = Vb[k];
-        fb[k] = Vb[3 + k];
-        gb[k] = Vb[6 + k];
+      {
+        const double2* v2 = reinterpret_cast<const double2*>(Vb);
+        const double2 x0 = v2[0], x1 = v2[1], x2 = v2[2], x3 = v2[3];
+        qb[0] = x0.x; qb[1] = x0.y; qb[2] = x1.x; fb[0] = x1.y; fb[1] = x2.x; fb[2] = x2.y;
+        gb[0] = x3.x; gb[1] = x3.y; gb[2] = Vb[8];
       }
       const double dg = wc * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
 #pragma unroll
@@ -459,81 +470,76 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
   }
 }
 
-// Per node row: 8 lanes per incidence, lane b fetches block (a, b) of the
-// incidence's element from the stage (transposed when stored as (b, a)).
+// Per node row: one warp per row node n, one lane per node block (n, c) of
+// the row.  The lane sums the staged blocks of the block's contributors
+// (element order, fixed), transposing blocks stored as (b, a), and writes its
+// 3x3 (free DOFs only) straight into the node's contiguous CSR rows; the
+// diagonal lane also sums the node's residual.  No shared memory, no barriers.
 template <bool WR, bool ACC>
-__global__ void __launch_bounds__(HX_GTPB) k_hex_gather(VolParams P, const double* __restrict__ stage) {
-  extern __shared__ double sm[];
-  const int ch = blockIdx.x;
-  const int i0 = P.chunkinc[ch], i1 = P.chunkinc[ch + 1];
-  const int nv = P.chunkdim[3 * ch];
-  const int nr = WR ? P.chunkdim[3 * ch + 1] : 0;
-  for (int i = threadIdx.x; i < nv + nr; i += blockDim.x) sm[i] = 0.0;
-  const int li = threadIdx.x >> 3;
-  const int lane = threadIdx.x & 7;
-  const int q = i0 + li;
-  const bool act = q < i1;
-  double blk[9];
-  double rj = 0.0;
-  int rank = -1, a = 0;
-  int32_t n = 0, c = 0;
-  if (act) {
-    const int ea = P.inc[q];
-    const int64_t e = ea >> 4;
-    a = ea & 15;
-    n = P.conn[e * 8 + a];
-    c = P.conn[e * 8 + lane];
-    rank = q - P.nodeinc[n];
-    const double* st = stage + e * HX_STAGE;
-    const int d = (lane - a) & 7;
-    if (d < 4 || (d == 4 && a < 4)) {
-      const double* s = st + hx_slot(a, d) * 9;
+__global__ void __launch_bounds__(256) k_hex_blk(VolParams P, const double* __restrict__ stage) {
+  const int64_t n = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (n >= P.n_nodes) return;
+  const unsigned mn = P.mask[n];
+  if (!mn) return;
+  const int64_t p0 = P.adjptr[n], p1 = P.adjptr[n + 1];
+  const int L = P.rowlen[n];
+  const int64_t vb = P.vbase[n];
+  for (int64_t p = p0 + lane; p < p1; p += 32) {
+    const int32_t c = P.adjcol[p];
+    double blk[9], r[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-      for (int i = 0; i < 9; ++i) blk[i] = s[i];
-    } else {
-      const double* s = st + hx_slot(lane, (a - lane) & 7) * 9;
+    for (int i = 0; i < 9; ++i) blk[i] = 0.0;
+    const int64_t t1 = P.blkptr[p + 1];
+    for (int64_t t = P.blkptr[p]; t < t1; ++t) {
+      const int32_t code = P.blkcon[t];
+      const int64_t e = code >> 6;
+      const int a = (code >> 3) & 7, b = code & 7;
+      const double* st = stage + e * HX_STAGE;
+      const int d = (b - a) & 7;
+      if (d < 4 || (d == 4 && a < 4)) {
+        const double* sb = st + hx_slot(a, d) * 9;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) blk[i] += sb[i];
+      } else {
+        const double* sb = st + hx_slot(b, (a - b) & 7) * 9;
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+          for (int k = 0; k < 3; ++k) blk[3 * j + k] += sb[3 * k + j];
+      }
+      if (WR && c == n) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r[j] += st[324 + 3 * a + j];
+      }
+    }
+    const unsigned mc = P.mask[c];
+    const int off = P.adjoff[p];
+    int rj = 0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      if (!(mn >> j & 1u)) continue;
+      double* row = P.K + vb + (int64_t)rj * L + off;
+      int rk = 0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (!(mc >> k & 1u)) continue;
+        row[rk] = ACC ? row[rk] + blk[3 * j + k] : blk[3 * j + k];
+        ++rk;
+      }
+      ++rj;
+    }
+    if (WR && c == n) {
+      double* Rout = P.R + P.rdof[n];
+      int rr = 0;
 #pragma unroll
       for (int j = 0; j < 3; ++j)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) blk[3 * j + k] = s[3 * k + j];
-    }
-    if (WR && lane < 3) rj = st[324 + 3 * a + lane];
-  }
-  unsigned mn = 0;
-  int rowoff = 0, L = 0, dr = 0;
-  if (act) {
-    mn = P.mask[n];
-    rowoff = P.soff[n];
-    L = P.rowlen[n];
-    dr = P.roff[n];
-  }
-  __syncthreads();
-  for (int k = 0; k < P.maxval; ++k) {
-    if (rank == k) {
-      const unsigned bo = P.boff[(int64_t)q * 8 + lane];
-      if (bo != 0xFFFFu) {
-        const unsigned mc = P.mask[c];
-        int rjj = 0;
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          if (!(mn >> j & 1u)) continue;
-          double* row = sm + rowoff + rjj * L + bo;
-          int rk = 0;
-#pragma unroll
-          for (int kk = 0; kk < 3; ++kk) {
-            if (!(mc >> kk & 1u)) continue;
-            row[rk] += blk[3 * j + kk];
-            ++rk;
-          }
-          ++rjj;
+        if (mn >> j & 1u) {
+          Rout[rr] = ACC ? Rout[rr] + r[j] : r[j];
+          ++rr;
         }
-      }
-      if (WR && lane < 3 && (mn >> lane & 1u)) sm[nv + dr + rank3(mn, lane)] += rj;
     }
-    __syncthreads();
   }
-  write_back<ACC>(P.chunkptr, P.chunklist, P.chunkdim, P.vbase, P.dbase, P.mask, P.soff, P.roff, ch, sm, P.K, nv,
-                  WR ? P.R : nullptr);
 }
 
 // R-only kernel: one thread per node, sequential over its incidences.
@@ -896,6 +902,11 @@ static VolParams vol_params(const fea_nodes_t* N, const fea_group_t* G, double m
   P.chunkdim = G->chunkdim_dev;
   P.soff = G->soff_dev;
   P.roff = G->roff_dev;
+  P.adjptr = N->adjptr_dev;
+  P.adjcol = N->adjcol_dev;
+  P.adjoff = N->adjoff_dev;
+  P.blkptr = G->blkptr_dev;
+  P.blkcon = G->blkcon_dev;
   P.gc = gc;
   P.K = P.R = P.elemR = nullptr;
   P.mu = mu;
@@ -975,11 +986,15 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
         count_launch();
         if (cudaError_t ce = cudaGetLastError()) return (int)ce;
       }
-#define FEA_HEX(WR_, ACC_)                                                                             \
-  if (wr == WR_ && acc == ACC_) return launch_chunked_ex(k_hex_gather<WR_, ACC_>, G->nchunk, HX_GTPB, smem, st, P, (const double*)work);
-      FEA_HEX(true, false) FEA_HEX(true, true) FEA_HEX(false, false) FEA_HEX(false, true)
-#undef FEA_HEX
-      return FEA_EINVAL;
+      if (!G->blkptr_dev || !G->blkcon_dev || !N->adjptr_dev || !N->adjcol_dev || !N->adjoff_dev) return FEA_EINVAL;
+      const unsigned g2 = (unsigned)((N->n_nodes + 7) / 8);
+      if (g2) {
+        const double* cw = work;
+        if (wr) acc ? k_hex_blk<true, true><<<g2, 256, 0, st>>>(P, cw) : k_hex_blk<true, false><<<g2, 256, 0, st>>>(P, cw);
+        else acc ? k_hex_blk<false, true><<<g2, 256, 0, st>>>(P, cw) : k_hex_blk<false, false><<<g2, 256, 0, st>>>(P, cw);
+        count_launch();
+      }
+      return (int)cudaGetLastError();
     }
 #define FEA_RK(NN_, WR_, ACC_, ER_)                                                                    \
   if (wr == WR_ && acc == ACC_ && er == ER_)                                                           \

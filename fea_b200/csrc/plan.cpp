@@ -49,6 +49,8 @@ struct GatherList {            // one element group or one face group
   std::vector<int32_t> chunkdim;   // [nchunk*3]: values, residual entries, contiguous flag
   std::vector<int32_t> soff;       // [N] shared-memory offset of the node's values in its chunk
   std::vector<int32_t> roff;       // [N] offset of its residual entries (after the chunk's values)
+  std::vector<int64_t> blkptr;     // [nnzb+1] contributors of every (row node, column node) block
+  std::vector<int32_t> blkcon;     // e*64 + a*8 + b, element order ascending
   int64_t maxval = 0, threads = 0, smem = 0;
 };
 
@@ -193,6 +195,56 @@ int build_gather(const fea_plan& P, int kind, int64_t ne, const int32_t* conn, c
   return FEA_OK;
 }
 
+// Contributors of every node-level block (n, c): the (element, a, b) with
+// conn[e][a] = n and conn[e][b] = c, in ascending element order.
+int build_blocks(const fea_plan& P, int nn, const int32_t* conn, const Incidence& I, GatherList& G) {
+  const int64_t N = P.N;
+  std::vector<int32_t> cnt(P.nnzb, 0);
+  int err = FEA_OK;
+  parallel_for(N, [&](int64_t a0, int64_t a1) {
+    for (int64_t n = a0; n < a1; ++n) {
+      if (!P.mask[n]) continue;
+      const int32_t* col = P.adjcol.data() + P.adjptr[n];
+      int64_t ncol = P.adjptr[n + 1] - P.adjptr[n];
+      for (int64_t q = I.ptr[n]; q < I.ptr[n + 1]; ++q) {
+        int64_t e = I.ent[q] >> 4;
+        for (int b = 0; b < nn; ++b) {
+          int32_t c = conn[e * nn + b];
+          if (!P.mask[c]) continue;
+          const int32_t* it = std::lower_bound(col, col + ncol, c);
+          if (it == col + ncol || *it != c) { err = FEA_ERANGE; continue; }
+          cnt[P.adjptr[n] + (it - col)]++;
+        }
+      }
+    }
+  });
+  if (err) return err;
+  G.blkptr.assign(P.nnzb + 1, 0);
+  for (int64_t p = 0; p < P.nnzb; ++p) G.blkptr[p + 1] = G.blkptr[p] + cnt[p];
+  if (G.blkptr[P.nnzb] > 0 && (int64_t)I.ent.size() * nn >= INT64_MAX / 2) return FEA_ERANGE;
+  G.blkcon.resize(G.blkptr[P.nnzb]);
+  parallel_for(N, [&](int64_t a0, int64_t a1) {
+    std::vector<int64_t> fill;
+    for (int64_t n = a0; n < a1; ++n) {
+      if (!P.mask[n]) continue;
+      const int32_t* col = P.adjcol.data() + P.adjptr[n];
+      int64_t ncol = P.adjptr[n + 1] - P.adjptr[n];
+      fill.assign(G.blkptr.begin() + P.adjptr[n], G.blkptr.begin() + P.adjptr[n + 1]);
+      for (int64_t q = I.ptr[n]; q < I.ptr[n + 1]; ++q) {
+        int64_t e = I.ent[q] >> 4;
+        int a = (int)(I.ent[q] & 15);
+        for (int b = 0; b < nn; ++b) {
+          int32_t c = conn[e * nn + b];
+          if (!P.mask[c]) continue;
+          int64_t k = std::lower_bound(col, col + ncol, c) - col;
+          G.blkcon[fill[k]++] = (int32_t)(e * 64 + a * 8 + b);
+        }
+      }
+    }
+  });
+  return FEA_OK;
+}
+
 }  // namespace
 
 extern "C" int fea_plan_build(int64_t n_nodes, const uint8_t* free_mask, int32_t n_groups,
@@ -312,6 +364,8 @@ extern "C" int fea_plan_build(int64_t n_nodes, const uint8_t* free_mask, int32_t
     int th = vol_threads > 0 ? vol_threads : (group_kind[g] == FEA_C3D8 ? 32 : 256);
     int r = build_gather(*P, group_kind[g], group_ne[g], group_conn[g], ginc[g], th, budget, P->groups[g]);
     if (r) return r;
+    if (group_ne[g] >= (int64_t)1 << 25) return FEA_ERANGE;   // e*64 + a*8 + b must fit int32
+    if (group_kind[g] == FEA_C3D8 && (r = build_blocks(*P, 8, group_conn[g], ginc[g], P->groups[g]))) return r;
   }
   for (int g = 0; g < n_faces; ++g) {
     int r = build_gather(*P, face_kind[g], face_nf[g], face_conn[g], finc[g], 128, budget, P->faces[g]);
@@ -364,6 +418,8 @@ extern "C" int fea_plan_get(const fea_plan* P, int32_t id, int32_t group, void* 
       case 10: return put(G->chunkdim, dst, count);
       case 11: return put(G->soff, dst, count);
       case 12: return put(G->roff, dst, count);
+      case 13: return put(G->blkptr, dst, count);
+      case 14: return put(G->blkcon, dst, count);
       default: return FEA_EINVAL;
     }
   }

@@ -35,7 +35,7 @@ class HostPlan:
            L.FEA_A_ADJPTR: np.int64, L.FEA_A_ADJCOL: np.int32, L.FEA_A_ADJOFF: np.int32}
     _GDT = {L.A_INC: np.int32, L.A_BOFF: np.uint16, L.A_NODEINC: np.int32, L.A_CHUNKPTR: np.int32,
             L.A_CHUNKINC: np.int32, L.A_CHUNKLIST: np.int32, L.A_CHUNKDIM: np.int32, L.A_SOFF: np.int32,
-            L.A_ROFF: np.int32}
+            L.A_ROFF: np.int32, L.A_BLKPTR: np.int64, L.A_BLKCON: np.int32}
 
     def __init__(self, n_nodes, free_mask, groups, faces, vol_threads=0, smem_doubles=0):
         self._h = None
@@ -98,13 +98,18 @@ class GatherGroup:
         self.chunkdim = dev(hp.array(base + L.A_CHUNKDIM, index))
         self.soff = dev(hp.array(base + L.A_SOFF, index))
         self.roff = dev(hp.array(base + L.A_ROFF, index))
+        blkptr = hp.array(base + L.A_BLKPTR, index) if base == L.G_BASE else np.zeros(0, np.int64)
+        self.blkptr = dev(blkptr) if blkptr.size else None
+        self.blkcon = dev(hp.array(base + L.A_BLKCON, index)) if blkptr.size else None
         self.ne = int(self.conn.shape[0])
         # True when every node with free DOFs has an incidence in this group
         self.covers_active = bool(np.all((np.diff(nodeinc) > 0) | (hp.array(L.FEA_A_MASK) == 0)))
         self.desc = L.Group(kind, self.nn, self.ne, self.conn.data_ptr(), self.inc.data_ptr(), self.boff.data_ptr(),
                             self.nodeinc.data_ptr(), self.chunkptr.data_ptr(), self.chunkinc.data_ptr(),
                             self.chunklist.data_ptr(), self.chunkdim.data_ptr(), self.soff.data_ptr(),
-                            self.roff.data_ptr(), hp.scalar(base + L.S_NCHUNK, index),
+                            self.roff.data_ptr(), self.blkptr.data_ptr() if self.blkptr is not None else None,
+                            self.blkcon.data_ptr() if self.blkcon is not None else None,
+                            hp.scalar(base + L.S_NCHUNK, index),
                             hp.scalar(base + L.S_MAXVAL, index), hp.scalar(base + L.S_THREADS, index),
                             hp.scalar(base + L.S_SMEM, index))
         self.nchunk = int(self.desc.nchunk)
@@ -139,9 +144,13 @@ class DevicePlan:
             self.rowlen = dev(hp.array(L.FEA_A_ROWLEN))
             self.indptr = dev(hp.array(L.FEA_A_INDPTR))
             self.indices = dev(hp.array(L.FEA_A_INDICES))
+            self.adjptr = dev(hp.array(L.FEA_A_ADJPTR))
+            self.adjcol = dev(hp.array(L.FEA_A_ADJCOL))
+            self.adjoff = dev(hp.array(L.FEA_A_ADJOFF))
             self.nodes = L.Nodes(self.n_nodes, self.ndof, self.nnz, self.X.data_ptr(), self.rdof.data_ptr(),
                                  self.mask.data_ptr(), self.vbase.data_ptr(), self.rowlen.data_ptr(),
-                                 self.dbase.data_ptr())
+                                 self.dbase.data_ptr(), self.adjptr.data_ptr(), self.adjcol.data_ptr(),
+                                 self.adjoff.data_ptr())
             self.groups = [GatherGroup(hp, L.G_BASE, i, k, c, self.device) for i, (k, c) in enumerate(gl)]
             self.faces = [GatherGroup(hp, L.F_BASE, i, k, c, self.device) for i, (k, c) in enumerate(fl)]
         self._scratch = None

@@ -112,6 +112,8 @@ enum {
   FEA_A_G_CHUNKDIM = 40, /* int32 [nchunk,3] values, residual entries, contiguous */
   FEA_A_G_SOFF = 41,     /* int32 [N] shared offset of the node's values   */
   FEA_A_G_ROFF = 42,     /* int32 [N] offset of its residual entries       */
+  FEA_A_G_BLKPTR = 43,   /* int64 [nnzb+1] contributors of each node block (C3D8) */
+  FEA_A_G_BLKCON = 44,   /* int32 element*64 + a*8 + b, element order      */
   FEA_A_F_INC = 50,      /* the same arrays / scalars for face groups      */
   FEA_A_F_BOFF = 51,
   FEA_A_F_NODEINC = 52,
@@ -145,6 +147,9 @@ typedef struct {
   const int64_t* vbase_dev;   /* FEA_A_VBASE  */
   const int32_t* rowlen_dev;  /* FEA_A_ROWLEN */
   const int32_t* dbase_dev;   /* FEA_A_DBASE  */
+  const int64_t* adjptr_dev;  /* FEA_A_ADJPTR */
+  const int32_t* adjcol_dev;  /* FEA_A_ADJCOL */
+  const int32_t* adjoff_dev;  /* FEA_A_ADJOFF */
 } fea_nodes_t;
 
 typedef struct {
@@ -161,6 +166,8 @@ typedef struct {
   const int32_t* chunkdim_dev;
   const int32_t* soff_dev;
   const int32_t* roff_dev;
+  const int64_t* blkptr_dev;  /* C3D8 only */
+  const int32_t* blkcon_dev;
   int64_t nchunk;
   int32_t maxval;
   int32_t threads;

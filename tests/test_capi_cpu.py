@@ -177,3 +177,28 @@ def test_product_meshes_match_oracle_meshes():
     sets, faces = meshes.plane_faces("C3D4", el, X, 2, 1.0)
     ref = O.boundary_faces("C3D4", torch.from_numpy(el), torch.from_numpy(X), 2, 1.0)
     np.testing.assert_array_equal(faces, torch.cat([f for _, _, f in ref]).numpy())
+
+
+def test_block_contributor_lists(golden):
+    """Every (row node, column node) block lists exactly the (element, a, b) that
+    couple the two nodes, in ascending element order."""
+    from fea_b200 import _lib as L
+    g = golden("hex5")
+    N, el = g["X"].shape[0], g["elems"]
+    mask = np.full(N, 7, np.uint8)
+    mask[g["fixed"]] = 0
+    hp = _plan(N, mask, [("C3D8", el)])
+    adjptr, adjcol = hp.array(L.FEA_A_ADJPTR), hp.array(L.FEA_A_ADJCOL)
+    bp, bc = hp.array(L.G_BASE + L.A_BLKPTR), hp.array(L.G_BASE + L.A_BLKCON)
+    assert bp.size == adjcol.size + 1
+    expect = {}
+    for e in range(el.shape[0]):
+        for a in range(8):
+            for b in range(8):
+                n, c = el[e, a], el[e, b]
+                if mask[n] and mask[c]:
+                    expect.setdefault((n, c), []).append(e * 64 + a * 8 + b)
+    for n in range(N):
+        for p in range(adjptr[n], adjptr[n + 1]):
+            assert list(bc[bp[p]:bp[p + 1]]) == expect[(n, adjcol[p])]
+    assert bp[-1] == sum(len(v) for v in expect.values())
