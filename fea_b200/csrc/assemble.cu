@@ -490,47 +490,27 @@ __global__ void __launch_bounds__(256) k_hex_blk(VolParams P, const double* __re
     double blk[9], r[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int i = 0; i < 9; ++i) blk[i] = 0.0;
-    const int64_t t0 = P.blkptr[p];
-    const int cnt = (int)(P.blkptr[p + 1] - t0);    // <= 8 for C3D8
-    // contributors in batches of 4: every load of a batch is independent
-    for (int base = 0; base < cnt; base += 4) {
-      double v[4][9];
-      bool tr[4];
-      int av[4];
-      const double* stv[4];
+    const int64_t t1 = P.blkptr[p + 1];
+    for (int64_t t = P.blkptr[p]; t < t1; ++t) {
+      const int32_t code = P.blkcon[t];
+      const int64_t e = code >> 6;
+      const int a = (code >> 3) & 7, b = code & 7;
+      const double* st = stage + e * HX_STAGE;
+      const int d = (b - a) & 7;
+      if (d < 4 || (d == 4 && a < 4)) {
+        const double* sb = st + hx_slot(a, d) * 9;
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        tr[k] = false;
-        av[k] = 0;
-        stv[k] = nullptr;
-        if (base + k < cnt) {
-          const int32_t code = P.blkcon[t0 + base + k];
-          const int64_t e = code >> 6;
-          const int a = (code >> 3) & 7, b = code & 7;
-          const int d = (b - a) & 7;
-          const bool direct = d < 4 || (d == 4 && a < 4);
-          const double* st = stage + e * HX_STAGE;
-          const double* sb = st + (direct ? hx_slot(a, d) : hx_slot(b, (a - b) & 7)) * 9;
-#pragma unroll
-          for (int i = 0; i < 9; ++i) v[k][i] = sb[i];
-          tr[k] = !direct;
-          av[k] = a;
-          stv[k] = st;
-        } else {
-#pragma unroll
-          for (int i = 0; i < 9; ++i) v[k][i] = 0.0;
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
+        for (int i = 0; i < 9; ++i) blk[i] += sb[i];
+      } else {
+        const double* sb = st + hx_slot(b, (a - b) & 7) * 9;
 #pragma unroll
         for (int j = 0; j < 3; ++j)
 #pragma unroll
-          for (int kk = 0; kk < 3; ++kk) blk[3 * j + kk] += tr[k] ? v[k][3 * kk + j] : v[k][3 * j + kk];
-        if (WR && c == n && stv[k]) {
+          for (int k = 0; k < 3; ++k) blk[3 * j + k] += sb[3 * k + j];
+      }
+      if (WR && c == n) {
 #pragma unroll
-          for (int j = 0; j < 3; ++j) r[j] += stv[k][324 + 3 * av[k] + j];
-        }
+        for (int j = 0; j < 3; ++j) r[j] += st[324 + 3 * a + j];
       }
     }
     const unsigned mc = P.mask[c];
