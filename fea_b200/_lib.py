@@ -20,9 +20,12 @@ lib = C.CDLL(LIB_PATH)
 FEA_OK = 0
 ERRORS = {-1: "invalid argument", -2: "index out of range", -3: "a node does not fit one gather chunk",
           -4: "shared memory request exceeds the device limit", -5: "work buffer too small",
-          -6: "iteration cap reached", -7: "PCG breakdown (p.Ap <= 0 or non-finite)"}
+          -6: "iteration cap reached", -7: "PCG breakdown (p.Ap <= 0 or non-finite)",
+          -8: "size beyond the fixed limit of an allocation-free entry point"}
 FEA_ENOTCONV = -6
 FEA_EBREAKDOWN = -7
+FEA_ETOOBIG = -8
+FEA_NOALLOC_MAX_ELEMS = 4194304
 
 FEA_C3D4, FEA_C3D8, FEA_T3, FEA_Q4 = 4, 8, 3, 40
 
@@ -85,6 +88,7 @@ fea_assemble_pressure = _sig("fea_assemble_pressure", I32, NP, GP, D, P, P, P, P
 fea_reduce_scratch_len = _sig("fea_reduce_scratch_len", I64, I64)
 fea_energy_volume = _sig("fea_energy_volume", I32, NP, GP, D, D, P, P, P, I64, P)
 fea_energy_pressure = _sig("fea_energy_pressure", I32, NP, GP, P, P, P, P, I64, P)
+fea_energy_volume_noalloc = _sig("fea_energy_volume_noalloc", I32, NP, GP, D, D, P, P, P)
 fea_lumped_mass = _sig("fea_lumped_mass", I32, NP, GP, D, P, P)
 fea_invert_mass = _sig("fea_invert_mass", I32, I64, P, P)
 fea_pcg_work_len = _sig("fea_pcg_work_len", I64, I64)
@@ -102,7 +106,7 @@ fea_launch_count = _sig("fea_launch_count", I64)
 
 # every symbol the header declares (checked by the CPU test suite)
 EXPORTED = ["fea_plan_build", "fea_plan_free", "fea_plan_get", "fea_assemble_work_len", "fea_assemble_volume", "fea_assemble_pressure",
-            "fea_reduce_scratch_len", "fea_energy_volume", "fea_energy_pressure", "fea_lumped_mass",
+            "fea_reduce_scratch_len", "fea_energy_volume", "fea_energy_volume_noalloc", "fea_energy_pressure", "fea_lumped_mass",
             "fea_invert_mass", "fea_pcg_work_len", "fea_pcg_solve", "fea_pcg_mixed_work_len",
             "fea_pcg_solve_mixed", "fea_spmv", "fea_convert_f32", "fea_explicit_work_len", "fea_explicit_run",
             "fea_version", "fea_launch_count"]

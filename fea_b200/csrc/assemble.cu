@@ -21,6 +21,7 @@
 // contraction sum_il C_ijkl g_ai g_bl equals
 //   (alpha f_a + beta q_a)_j q_bk + alpha q_aj f_bk + gamma q_ak q_bj
 //   + mu J^-2/3 (g_a . g_b) delta_jk.
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 
@@ -1117,6 +1118,48 @@ extern "C" int fea_invert_mass(int64_t n, double* m, cudaStream_t st) {
   if (!m || n < 0) return FEA_EINVAL;
   if (n == 0) return FEA_OK;
   k_invert_mass<<<grid_for(n, 256), 256, 0, st>>>(n, m);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+// ---- allocation-free element energy ----------------------------------------
+// Same kernels and reduction order as fea_energy_volume, but the per-block
+// partial sums live in a fixed array that is part of this library's device
+// image instead of a caller-provided buffer.  It exists for callers that
+// cannot allocate device memory at the point of the call: hosts that hand all
+// device memory to their own pool allocator up front, or foreign-language
+// hosts that only pass pointers they already own.
+static constexpr int64_t kNoallocMaxElems = FEA_NOALLOC_MAX_ELEMS;
+static __device__ __align__(256) double g_noalloc_partials[(kNoallocMaxElems + 255) / 256];
+static std::atomic<double*> g_noalloc_ptr[64];   // device address of the array, per device ordinal
+
+extern "C" int fea_energy_volume_noalloc(const fea_nodes_t* N, const fea_group_t* G, double mu, double kappa,
+                                         const double* gc, double* out, cudaStream_t st) {
+  if (!N || !G || !gc || !out) return FEA_EINVAL;
+  if (G->kind != FEA_C3D4 && G->kind != FEA_C3D8) return FEA_EINVAL;
+  if (G->ne < 0) return FEA_EINVAL;
+  if (G->ne > kNoallocMaxElems) return FEA_ETOOBIG;
+  int dev = 0;
+  if (cudaError_t e = cudaGetDevice(&dev)) return (int)e;
+  if (dev < 0 || dev >= 64) return FEA_EINVAL;
+  double* part = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+  if (!part) {
+    // host code cannot use the array's name as a device address: resolve it
+    // once per device, with that device current
+    void* p = nullptr;
+    if (cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials)) return (int)e;
+    part = static_cast<double*>(p);
+    g_noalloc_ptr[dev].store(part, std::memory_order_release);
+  }
+  if (int r = ensure_tables()) return r;
+  VolParams P = vol_params(N, G, mu, kappa, gc);
+  const int64_t nb = (G->ne + 255) / 256;
+  if (nb > 0) {
+    if (G->kind == FEA_C3D8) k_vol_energy<8><<<(unsigned)nb, 256, 0, st>>>(P, part);
+    else k_vol_energy<4><<<(unsigned)nb, 256, 0, st>>>(P, part);
+    count_launch();
+  }
+  k_sum_partials<<<1, 256, 0, st>>>(part, nb, out, 0);
   count_launch();
   return (int)cudaGetLastError();
 }

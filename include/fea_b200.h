@@ -48,6 +48,7 @@ extern "C" {
 #define FEA_EWORK -5       /* caller-provided work buffer too small */
 #define FEA_ENOTCONV -6    /* iterative solver hit its iteration cap */
 #define FEA_EBREAKDOWN -7  /* PCG breakdown (p.Ap <= 0 or non-finite) */
+#define FEA_ETOOBIG -8     /* size beyond the fixed limit of an allocation-free entry point */
 
 /* element kinds (reference class names) */
 #define FEA_C3D4 4
@@ -201,6 +202,24 @@ int64_t fea_reduce_scratch_len(int64_t n_items);
 int fea_energy_volume(const fea_nodes_t* nodes, const fea_group_t* group, double mu, double kappa,
                       const double* gc_dev, double* out_dev, double* scratch_dev, int64_t scratch_len,
                       cudaStream_t stream);
+/* Allocation-free variant of fea_energy_volume (no counterpart in the
+ * reference).  For callers that cannot allocate device memory when they call
+ * the library — e.g. a host that reserves all device memory for its own pool
+ * allocator, or a foreign-language host that only passes pointers it already
+ * owns — and so cannot provide the scratch buffer fea_energy_volume needs.
+ * The scratch is a fixed array inside the library's device image, sized for
+ * at most FEA_NOALLOC_MAX_ELEMS elements per group; larger groups return
+ * FEA_ETOOBIG without launching.  Nothing is allocated (no cudaMalloc /
+ * cudaFree, no allocating library routine).  The first call on each device
+ * resolves the array's device address (cudaGetSymbolAddress) with that device
+ * current, so make that first call before any stream capture.  Every call
+ * shares the one array: calls that may overlap on the GPU (different streams
+ * or threads) race and must be serialised by the caller.  Same result as
+ * fea_energy_volume (same kernels and summation order). */
+#define FEA_NOALLOC_MAX_ELEMS 4194304
+int fea_energy_volume_noalloc(const fea_nodes_t* nodes, const fea_group_t* group, double mu, double kappa,
+                              const double* gc_dev, double* out_dev, cudaStream_t stream);
+
 /* Enclosed-volume functional V of a face group -> out_dev[0]. */
 int fea_energy_pressure(const fea_nodes_t* nodes, const fea_group_t* faces, const double* Xinst_dev,
                         const double* gc_dev, double* out_dev, double* scratch_dev, int64_t scratch_len,
