@@ -50,6 +50,10 @@ def args_():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--workload", default="assembly", choices=["assembly", "pcg", "explicit", "newton"],
+                    help="assembly (default, the headline line) or one of the other measured forms")
+    ap.add_argument("--explicit-n", type=int, default=70, help="cells per side of the Kuhn-tet cube")
+    ap.add_argument("--explicit-steps", type=int, default=10000)
     return ap.parse_args()
 
 
@@ -169,10 +173,168 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def build_block_model(n, p=-0.02):
+    import fea_b200 as F
+    X, el, clamp, end, faces = workload(n)
+    part = F.Part(X)
+    e = F.elements.C3D8(elems=el, elems_index=np.arange(el.shape[0]), part=part)
+    e.set_materials(F.materials.NeoHookean(1.0, 50.0))
+    part.add_element(e)
+    part.set_nodes["clamp"] = clamp
+    part.add_surface_set("end", [(end, 3)])
+    asm = F.Assembly()
+    asm.add_part(part, "block")
+    asm.add_instance(F.Instance(part), "block")
+    load = F.loads.Pressure("block", "end", p)
+    asm.add_load(load, "traction")
+    asm.add_boundary(F.boundarys.Boundary_Condition("block", "clamp"), "clamp")
+    asm.initialize()
+    return asm, el, X, load
+
+
+def run_pcg(a):
+    """FP64 Jacobi-PCG vs FP32-SpMV inner CG with FP64 refinement on the
+    reduced 64^3 system K(u0) x = -R(u0) at the initial state, to a relative
+    residual of 1e-8 (squared scaled ratio 1e-16); errors against an FP64
+    solve converged to 1e-12."""
+    import torch
+    asm, el, X, _ = build_block_model(a.n)
+    P = asm.plan
+    R, K = asm.assemble_csr(asm.GC)
+    b = (-R).contiguous()
+    xref = torch.zeros_like(b)
+    it_ref, rr_ref, _ = P.pcg(K, b, xref, 1e-24, 50000, check_every=50)
+    out = {}
+    for mode in ("fp64", "mixed"):
+        x = torch.zeros_like(b)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        if mode == "fp64":
+            it, rr, st = P.pcg(K, b, x, 1e-16, 50000, check_every=50)
+            outer = 1
+        else:
+            K32 = P.to_f32(K)
+            it, outer, rr, st = P.pcg_mixed(K, K32, b, x, 1e-16, 1e-6, 50000, check_every=50)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        r = b - P.spmv(K, x)
+        out[mode] = {"iterations": it, "outer": outer, "ms": ms, "ms_per_iter": ms / max(it, 1),
+                     "relres": float(r.norm() / b.norm()),
+                     "err_vs_fp64_1e-12": float((x - xref).norm() / xref.norm()), "status": st}
+    nnz, n = P.nnz, P.ndof
+    bytes64 = 12 * nnz + 8 * (n + 1) + 8 * n * 9
+    bytes32 = 8 * nnz + 8 * (n + 1) + 4 * n * 9
+    line = {"metric": "PCG time to relres 1e-8 (64^3 C3D8 reduced system)", "unit": "ms",
+            "value": out["mixed"]["ms"], "higher_is_better": False, "workload": "pcg", "dtype": "f64/f32",
+            "n": n, "nnz": nnz, "fp64": out["fp64"], "mixed": out["mixed"], "reference_iterations": it_ref,
+            "spmv_iteration_bytes": {"fp64": bytes64, "fp32": bytes32},
+            "achieved_GBs": {"fp64": bytes64 / (out["fp64"]["ms_per_iter"] * 1e-3) / 1e9,
+                             "mixed": bytes32 / (out["mixed"]["ms_per_iter"] * 1e-3) / 1e9}}
+    print(json.dumps(line), flush=True)
+
+
+def run_explicit(a):
+    """2.06M-tet cube (70^3 cells, 6 tets each), rho = 1, mu = 1, kappa = 10,
+    no boundary conditions, v0 ~ N(0, 0.01^2) per DOF (seed 0), dt = 0.5 x
+    min(altitude)/c, c = sqrt((kappa + 4 mu / 3) / rho); FP64 and FP32
+    element force (FP64 sums), energy drift and displacement difference."""
+    import torch
+    import fea_b200 as F
+    from fea_b200 import meshes
+    X, el = meshes.tet_block(a.explicit_n)
+    part = F.Part(X)
+    e = F.elements.C3D4(elems=el, elems_index=np.arange(el.shape[0]), part=part)
+    e.set_materials(F.materials.NeoHookean(1.0, 10.0))
+    e.set_density(1.0)
+    part.add_element(e)
+    asm = F.Assembly()
+    asm.add_part(part, "cube")
+    asm.add_instance(F.Instance(part), "cube")
+    asm.initialize()
+    P = asm.plan
+    minv = asm.lumped_mass_inv()
+    m = 1.0 / minv
+    sol = F.solver.DynamicExplicitSolver()
+    sol.assembly = asm
+    dt = sol.cfl_timestep(0.5)
+    v0 = (0.01 * torch.randn(P.ndof, generator=torch.Generator().manual_seed(0), dtype=torch.float64)).cuda()
+    eb = torch.zeros(1, dtype=torch.float64, device="cuda")
+
+    def energy(u, v):
+        P.energy_volume(0, 1.0, 10.0, u, eb)
+        return float(0.5 * (m * v * v).sum() + eb[0])
+
+    res = {}
+    for fp32 in (False, True):
+        u = torch.zeros(P.ndof, dtype=torch.float64, device="cuda")
+        v = v0.clone()
+        vh = torch.empty_like(u)
+        acc = torch.empty_like(u)
+        P.explicit_run(0, 1.0, 10.0, minv, dt, 0, u, vh, acc, v, fp32=fp32, init=True)
+        E0 = energy(u, v0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        P.explicit_run(0, 1.0, 10.0, minv, dt, a.explicit_steps, u, vh, acc, v, fp32=fp32, init=False)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        E1 = energy(u, v)
+        res["fp32" if fp32 else "fp64"] = {"ms_total": ms, "ms_per_step": ms / a.explicit_steps,
+                                           "energy_0": E0, "energy_end": E1, "energy_drift": (E1 - E0) / E0,
+                                           "u": u}
+    du = float((res["fp32"]["u"] - res["fp64"]["u"]).norm() / res["fp64"]["u"].norm())
+    for k in res:
+        res[k].pop("u")
+    E, N = el.shape[0], X.shape[0]
+    line = {"metric": "explicit central-difference steps/s (2.06M C3D4)", "unit": "steps/s",
+            "value": 1e3 / res["fp64"]["ms_per_step"], "higher_is_better": True, "workload": "explicit",
+            "elements": E, "nodes": N, "steps": a.explicit_steps, "dt": dt, "fp64": res["fp64"],
+            "fp32": res["fp32"], "fp32_vs_fp64_disp_rel": du,
+            "elements_per_s": E * 1e3 / res["fp64"]["ms_per_step"]}
+    print(json.dumps(line), flush=True)
+
+
+def run_newton(a):
+    """Full static Newton solve of the 64^3 block to 1e-8 relative residual."""
+    import torch
+    import fea_b200 as F
+    asm, el, X, _ = build_block_model(a.n)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        sol = F.solver.StaticImplicitSolver(rtol=1e-8, maximum_iteration=100, precision=prec)
+        sol.initialize(asm)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gc = sol.solve(GC0=asm.GC.clone())
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if isinstance(gc, bool):
+            raise RuntimeError("Newton solve (%s) failed" % prec)
+        R = asm.assemble_force(GC=gc)
+        out[prec] = {"seconds": dt, "newton_iters": len(sol.history), "history": sol.history, "gc": gc,
+                     "final_rel_residual": float(R.norm()) / sol.history[0]["rnorm"]}
+    d = float((out["mixed"]["gc"] - out["fp64"]["gc"]).norm() / out["fp64"]["gc"].norm())
+    for k in out:
+        out[k].pop("gc")
+    line = {"metric": "static Newton solve to 1e-8 (64^3 C3D8)", "unit": "s", "value": out["fp64"]["seconds"],
+            "higher_is_better": False, "workload": "newton", "fp64": out["fp64"], "mixed": out["mixed"],
+            "mixed_vs_fp64_disp_rel": d}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = args_()
     if a.impl == "reference":
         run_reference(a)
+        return
+    if a.workload != "assembly":
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        {"pcg": run_pcg, "explicit": run_explicit, "newton": run_newton}[a.workload](a)
         return
     import torch
     import torch.distributed as dist

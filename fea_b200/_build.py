@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfea_b200.so")
 
-CU_SOURCES = ["capi.cu", "assemble.cu", "pcg.cu", "explicit.cu"]
+CU_SOURCES = ["capi.cu", "assemble.cu", "pcg.cu", "explicit.cu", "adjoint.cu"]
 CPP_SOURCES = ["plan.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

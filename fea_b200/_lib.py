@@ -34,7 +34,7 @@ FEA_C3D4, FEA_C3D8, FEA_T3, FEA_Q4 = 4, 8, 3, 40
  FEA_A_ADJPTR, FEA_A_ADJCOL, FEA_A_ADJOFF) = range(10, 20)
 G_BASE, F_BASE = 30, 50
 (A_INC, A_BOFF, A_NODEINC, A_CHUNKPTR, A_CHUNKINC, S_NCHUNK, S_MAXVAL, S_THREADS, S_SMEM, A_CHUNKLIST,
- A_CHUNKDIM, A_SOFF, A_ROFF, A_BLKPTR, A_BLKCON) = range(15)
+ A_CHUNKDIM, A_SOFF, A_ROFF, A_BLKPTR, A_BLKCON, A_ALLPTR, A_ALLINC) = range(17)
 
 
 class FeaError(RuntimeError):
@@ -63,6 +63,7 @@ class Group(C.Structure):
                 ("nodeinc_dev", C.c_void_p), ("chunkptr_dev", C.c_void_p), ("chunkinc_dev", C.c_void_p),
                 ("chunklist_dev", C.c_void_p), ("chunkdim_dev", C.c_void_p), ("soff_dev", C.c_void_p),
                 ("roff_dev", C.c_void_p), ("blkptr_dev", C.c_void_p), ("blkcon_dev", C.c_void_p),
+                ("allptr_dev", C.c_void_p), ("allinc_dev", C.c_void_p),
                 ("nchunk", C.c_int64), ("maxval", C.c_int32), ("threads", C.c_int32),
                 ("smem_doubles", C.c_int64)]
 
@@ -101,6 +102,8 @@ fea_spmv = _sig("fea_spmv", I32, I64, P, P, P, P, P, P)
 fea_convert_f32 = _sig("fea_convert_f32", I32, I64, P, P, P)
 fea_explicit_work_len = _sig("fea_explicit_work_len", I64, I64)
 fea_explicit_run = _sig("fea_explicit_run", I32, NP, GP, D, D, P, D, I64, I32, I32, P, P, P, P, P, I64, P)
+fea_adjoint_vjp_volume = _sig("fea_adjoint_vjp_volume", I32, NP, GP, D, D, P, P, P, P, P, I64, P)
+fea_adjoint_hvp_pressure = _sig("fea_adjoint_hvp_pressure", I32, NP, GP, D, P, P, P, P, P)
 fea_version = _sig("fea_version", I32)
 fea_launch_count = _sig("fea_launch_count", I64)
 
@@ -109,4 +112,4 @@ EXPORTED = ["fea_plan_build", "fea_plan_free", "fea_plan_get", "fea_assemble_wor
             "fea_reduce_scratch_len", "fea_energy_volume", "fea_energy_volume_noalloc", "fea_energy_pressure", "fea_lumped_mass",
             "fea_invert_mass", "fea_pcg_work_len", "fea_pcg_solve", "fea_pcg_mixed_work_len",
             "fea_pcg_solve_mixed", "fea_spmv", "fea_convert_f32", "fea_explicit_work_len", "fea_explicit_run",
-            "fea_version", "fea_launch_count"]
+            "fea_adjoint_vjp_volume", "fea_adjoint_hvp_pressure", "fea_version", "fea_launch_count"]

@@ -51,6 +51,8 @@ struct GatherList {            // one element group or one face group
   std::vector<int32_t> roff;       // [N] offset of its residual entries (after the chunk's values)
   std::vector<int64_t> blkptr;     // [nnzb+1] contributors of every (row node, column node) block
   std::vector<int32_t> blkcon;     // e*64 + a*8 + b, element order ascending
+  std::vector<int32_t> allptr;     // [N+1] incidences of every node (constrained ones included)
+  std::vector<int32_t> allinc;     // e*16 + a, element order ascending
   int64_t maxval = 0, threads = 0, smem = 0;
 };
 
@@ -147,6 +149,10 @@ int build_gather(const fea_plan& P, int kind, int64_t ne, const int32_t* conn, c
   if (err) return err;
   // chunks of nodes that have incidences in this list (in node order):
   // incidences <= threads, shared doubles <= budget
+  G.allptr.assign(N + 1, 0);
+  for (int64_t n = 0; n < N; ++n) G.allptr[n + 1] = (int32_t)I.ptr[n + 1];
+  G.allinc.resize(I.ent.size());
+  for (size_t i = 0; i < I.ent.size(); ++i) G.allinc[i] = (int32_t)I.ent[i];
   G.threads = threads;
   G.soff.assign(N, 0);
   G.roff.assign(N, 0);
@@ -420,6 +426,8 @@ extern "C" int fea_plan_get(const fea_plan* P, int32_t id, int32_t group, void* 
       case 12: return put(G->roff, dst, count);
       case 13: return put(G->blkptr, dst, count);
       case 14: return put(G->blkcon, dst, count);
+      case 15: return put(G->allptr, dst, count);
+      case 16: return put(G->allinc, dst, count);
       default: return FEA_EINVAL;
     }
   }

@@ -35,7 +35,8 @@ class HostPlan:
            L.FEA_A_ADJPTR: np.int64, L.FEA_A_ADJCOL: np.int32, L.FEA_A_ADJOFF: np.int32}
     _GDT = {L.A_INC: np.int32, L.A_BOFF: np.uint16, L.A_NODEINC: np.int32, L.A_CHUNKPTR: np.int32,
             L.A_CHUNKINC: np.int32, L.A_CHUNKLIST: np.int32, L.A_CHUNKDIM: np.int32, L.A_SOFF: np.int32,
-            L.A_ROFF: np.int32, L.A_BLKPTR: np.int64, L.A_BLKCON: np.int32}
+            L.A_ROFF: np.int32, L.A_BLKPTR: np.int64, L.A_BLKCON: np.int32, L.A_ALLPTR: np.int32,
+            L.A_ALLINC: np.int32}
 
     def __init__(self, n_nodes, free_mask, groups, faces, vol_threads=0, smem_doubles=0):
         self._h = None
@@ -101,6 +102,8 @@ class GatherGroup:
         blkptr = hp.array(base + L.A_BLKPTR, index) if base == L.G_BASE else np.zeros(0, np.int64)
         self.blkptr = dev(blkptr) if blkptr.size else None
         self.blkcon = dev(hp.array(base + L.A_BLKCON, index)) if blkptr.size else None
+        self.allptr = dev(hp.array(base + L.A_ALLPTR, index))
+        self.allinc = dev(hp.array(base + L.A_ALLINC, index))
         self.ne = int(self.conn.shape[0])
         # True when every node with free DOFs has an incidence in this group
         self.covers_active = bool(np.all((np.diff(nodeinc) > 0) | (hp.array(L.FEA_A_MASK) == 0)))
@@ -109,6 +112,7 @@ class GatherGroup:
                             self.chunklist.data_ptr(), self.chunkdim.data_ptr(), self.soff.data_ptr(),
                             self.roff.data_ptr(), self.blkptr.data_ptr() if self.blkptr is not None else None,
                             self.blkcon.data_ptr() if self.blkcon is not None else None,
+                            self.allptr.data_ptr(), self.allinc.data_ptr(),
                             hp.scalar(base + L.S_NCHUNK, index),
                             hp.scalar(base + L.S_MAXVAL, index), hp.scalar(base + L.S_THREADS, index),
                             hp.scalar(base + L.S_SMEM, index))
@@ -209,6 +213,19 @@ class DevicePlan:
         s = self.scratch(n)
         L.check(L.fea_energy_pressure(C.byref(self.nodes), C.byref(f.desc), vptr(Xinst), vptr(gc), vptr(out),
                                       vptr(s), s.numel(), stream()), "fea_energy_pressure")
+
+    def adjoint_vjp_volume(self, gi, mu, kappa, gc, lam_full, dX, dmu):
+        """dX += d(lam . R_e)/dX (all nodes); dmu[0] = d(lam . R_e)/dmu."""
+        g = self.groups[gi]
+        s = self.scratch(L.fea_reduce_scratch_len(g.ne))
+        L.check(L.fea_adjoint_vjp_volume(C.byref(self.nodes), C.byref(g.desc), float(mu), float(kappa), vptr(gc),
+                                         vptr(lam_full), vptr(dX), vptr(dmu), vptr(s), s.numel(), stream()),
+                "fea_adjoint_vjp_volume")
+
+    def adjoint_hvp_pressure(self, fi, p, Xinst, gc, v_full, out):
+        """out += p d2V/dx2 v (all nodes) for face group fi."""
+        L.check(L.fea_adjoint_hvp_pressure(C.byref(self.nodes), C.byref(self.faces[fi].desc), float(p), vptr(Xinst),
+                                           vptr(gc), vptr(v_full), vptr(out), stream()), "fea_adjoint_hvp_pressure")
 
     def lumped_mass_inv(self, rhos):
         m = self.zeros(self.ndof)

@@ -115,6 +115,8 @@ enum {
   FEA_A_G_ROFF = 42,     /* int32 [N] offset of its residual entries       */
   FEA_A_G_BLKPTR = 43,   /* int64 [nnzb+1] contributors of each node block (C3D8) */
   FEA_A_G_BLKCON = 44,   /* int32 element*64 + a*8 + b, element order      */
+  FEA_A_G_ALLPTR = 45,   /* int32 [N+1] incidences of every node (all nodes) */
+  FEA_A_G_ALLINC = 46,   /* int32 element*16 + a                           */
   FEA_A_F_INC = 50,      /* the same arrays / scalars for face groups      */
   FEA_A_F_BOFF = 51,
   FEA_A_F_NODEINC = 52,
@@ -127,7 +129,9 @@ enum {
   FEA_A_F_CHUNKLIST = 59,
   FEA_A_F_CHUNKDIM = 60,
   FEA_A_F_SOFF = 61,
-  FEA_A_F_ROFF = 62
+  FEA_A_F_ROFF = 62,
+  FEA_A_F_ALLPTR = 65,
+  FEA_A_F_ALLINC = 66
 };
 
 /* Copy array `id` (of element/face group `group`) into dst (host memory),
@@ -169,6 +173,8 @@ typedef struct {
   const int32_t* roff_dev;
   const int64_t* blkptr_dev;  /* C3D8 only */
   const int32_t* blkcon_dev;
+  const int32_t* allptr_dev;  /* FEA_A_*_ALLPTR (adjoint kernels) */
+  const int32_t* allinc_dev;
   int64_t nchunk;
   int32_t maxval;
   int32_t threads;
@@ -279,6 +285,24 @@ int fea_explicit_run(const fea_nodes_t* nodes, const fea_group_t* group, double 
                      const double* minv_dev, double dt, int64_t steps, int32_t fp32, int32_t init,
                      double* u_dev, double* vh_dev, double* a_dev, double* v_dev,
                      double* work_dev, int64_t work_len, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Adjoint (sensitivities of the equilibrium; no kernel counterpart in the
+ * reference, which differentiates its torch graph: tests/gradient_test/
+ * test_grad.py:87-99).
+ *   fea_adjoint_vjp_volume: for the adjoint field lam [N,3] (all nodes,
+ *     zero on Dirichlet DOFs) adds d(lam . R_e)/dX [N,3] to dX_dev (every
+ *     node, constrained ones included) and writes d(lam . R_e)/dmu to
+ *     dmu_dev[0].  scratch: fea_reduce_scratch_len(ne) doubles.
+ *   fea_adjoint_hvp_pressure: adds p d2V/dx2 v (all nodes) to out_dev, the
+ *     X-derivative of v . (p dV/dx) of a pressure face group.
+ * ------------------------------------------------------------------------- */
+int fea_adjoint_vjp_volume(const fea_nodes_t* nodes, const fea_group_t* group, double mu, double kappa,
+                           const double* gc_dev, const double* lam_dev, double* dX_dev, double* dmu_dev,
+                           double* scratch_dev, int64_t scratch_len, cudaStream_t stream);
+int fea_adjoint_hvp_pressure(const fea_nodes_t* nodes, const fea_group_t* faces, double p,
+                             const double* Xinst_dev, const double* gc_dev, const double* v_dev,
+                             double* out_dev, cudaStream_t stream);
 
 /* Library version and the number of kernels this library has launched
  * (a host-side counter, for instrumentation). */
