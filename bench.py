@@ -3,7 +3,8 @@
 
 Workload (one GPU): a 64^3 C3D8 block on [0,1]^3, nodes jittered by
 U(-0.1h, 0.1h) (seed 0), compressible Neo-Hookean mu = 1, kappa = 50, the
-x = 0 face clamped, follower pressure p = -0.02 on the x = 1 face (Q4);
+x = 0 face clamped, follower pressure p = 0.02 on the x = 1 face (Q4, the
+reference's Pressure load convention);
 262,144 elements, 274,625 nodes, 811,200 free DOFs, 63,695,790 nonzeros.
 One step = one full assembly of the reduced residual R and tangent K at a
 seeded displacement state (all element groups and the pressure load), i.e.
@@ -37,6 +38,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "elem tangent+assembly GElem/s"
+PRESSURE = 0.02
 UNIT = "GElem/s"
 
 
@@ -173,7 +175,7 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
-def build_block_model(n, p=-0.02):
+def build_block_model(n, p=0.02):
     import fea_b200 as F
     X, el, clamp, end, faces = workload(n)
     part = F.Part(X)
@@ -193,10 +195,10 @@ def build_block_model(n, p=-0.02):
 
 
 def run_pcg(a):
-    """FP64 Jacobi-PCG vs FP32-SpMV inner CG with FP64 refinement on the
-    reduced 64^3 system K(u0) x = -R(u0) at the initial state, to a relative
-    residual of 1e-8 (squared scaled ratio 1e-16); errors against an FP64
-    solve converged to 1e-12."""
+    """FP64 Jacobi-PCG (node-row and plain-CSR SpMV) and FP32-SpMV inner CG
+    with FP64 refinement on the reduced 64^3 system K(u0) x = -R(u0) at the
+    initial state, to a relative residual of 1e-8 (squared scaled ratio
+    1e-16); errors against an FP64 solve converged to 1e-12."""
     import torch
     asm, el, X, _ = build_block_model(a.n)
     P = asm.plan
@@ -204,19 +206,18 @@ def run_pcg(a):
     b = (-R).contiguous()
     xref = torch.zeros_like(b)
     it_ref, rr_ref, _ = P.pcg(K, b, xref, 1e-24, 50000, check_every=50)
+    K32 = P.to_f32(K)
     out = {}
-    for mode in ("fp64", "mixed"):
+    for mode in ("fp64", "fp64_csr", "mixed"):
         x = torch.zeros_like(b)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        if mode == "fp64":
-            it, rr, st = P.pcg(K, b, x, 1e-16, 50000, check_every=50)
-            outer = 1
-        else:
-            K32 = P.to_f32(K)
+        if mode == "mixed":
             it, outer, rr, st = P.pcg_mixed(K, K32, b, x, 1e-16, 1e-6, 50000, check_every=50)
+        else:
+            it, rr, st = P.pcg(K, b, x, 1e-16, 50000, check_every=50, generic=(mode == "fp64_csr"))
+            outer = 1
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
@@ -225,13 +226,19 @@ def run_pcg(a):
                      "relres": float(r.norm() / b.norm()),
                      "err_vs_fp64_1e-12": float((x - xref).norm() / xref.norm()), "status": st}
     nnz, n = P.nnz, P.ndof
-    bytes64 = 12 * nnz + 8 * (n + 1) + 8 * n * 9
-    bytes32 = 8 * nnz + 8 * (n + 1) + 4 * n * 9
+    act = P.mask != 0
+    idx_bytes = 4 * int(P.rowlen[act].to(torch.int64).sum())
+    # per iteration: values + column lists once per node + 13 FP64 vector passes
+    bytes64 = 8 * nnz + idx_bytes + 8 * 13 * n
+    bytes64_csr = 12 * nnz + 8 * (n + 1) + 8 * 13 * n
+    bytes32 = 4 * nnz + idx_bytes + 56 * n
     line = {"metric": "PCG time to relres 1e-8 (64^3 C3D8 reduced system)", "unit": "ms",
             "value": out["mixed"]["ms"], "higher_is_better": False, "workload": "pcg", "dtype": "f64/f32",
-            "n": n, "nnz": nnz, "fp64": out["fp64"], "mixed": out["mixed"], "reference_iterations": it_ref,
-            "spmv_iteration_bytes": {"fp64": bytes64, "fp32": bytes32},
+            "n": n, "nnz": nnz, "fp64": out["fp64"], "fp64_csr": out["fp64_csr"], "mixed": out["mixed"],
+            "reference_iterations": it_ref,
+            "iteration_bytes": {"fp64": bytes64, "fp64_csr": bytes64_csr, "fp32_inner": bytes32},
             "achieved_GBs": {"fp64": bytes64 / (out["fp64"]["ms_per_iter"] * 1e-3) / 1e9,
+                             "fp64_csr": bytes64_csr / (out["fp64_csr"]["ms_per_iter"] * 1e-3) / 1e9,
                              "mixed": bytes32 / (out["mixed"]["ms_per_iter"] * 1e-3) / 1e9}}
     print(json.dumps(line), flush=True)
 
@@ -267,6 +274,13 @@ def run_explicit(a):
         P.energy_volume(0, 1.0, 10.0, u, eb)
         return float(0.5 * (m * v * v).sum() + eb[0])
 
+    def shadow_energy(u, vh, acc):
+        # 1/2 vh_{N+1/2} M vh_{N-1/2} + W(u_N): the quantity central
+        # differences conserve without the O((w dt)^2) oscillation of the
+        # synchronous kinetic energy of the high-frequency modes
+        P.energy_volume(0, 1.0, 10.0, u, eb)
+        return float(0.5 * (m * (vh + dt * acc) * vh).sum() + eb[0])
+
     res = {}
     for fp32 in (False, True):
         u = torch.zeros(P.ndof, dtype=torch.float64, device="cuda")
@@ -275,6 +289,7 @@ def run_explicit(a):
         acc = torch.empty_like(u)
         P.explicit_run(0, 1.0, 10.0, minv, dt, 0, u, vh, acc, v, fp32=fp32, init=True)
         E0 = energy(u, v0)
+        S0 = shadow_energy(u, vh, acc)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -282,10 +297,11 @@ def run_explicit(a):
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
-        E1 = energy(u, v)
+        E1 = energy(u, vh + 0.5 * dt * acc)          # v_N = vh_{N-1/2} + dt/2 a_N
+        S1 = shadow_energy(u, vh, acc)
         res["fp32" if fp32 else "fp64"] = {"ms_total": ms, "ms_per_step": ms / a.explicit_steps,
-                                           "energy_0": E0, "energy_end": E1, "energy_drift": (E1 - E0) / E0,
-                                           "u": u}
+                                           "energy_0": S0, "energy_end": S1, "energy_drift": (S1 - S0) / S0,
+                                           "sync_energy_change": (E1 - E0) / E0, "u": u}
     du = float((res["fp32"]["u"] - res["fp64"]["u"]).norm() / res["fp64"]["u"].norm())
     for k in res:
         res[k].pop("u")
@@ -303,19 +319,22 @@ def run_newton(a):
     import torch
     import fea_b200 as F
     asm, el, X, _ = build_block_model(a.n)
+    gc0 = asm.GC.clone()
     out = {}
     for prec in ("fp64", "mixed"):
         sol = F.solver.StaticImplicitSolver(rtol=1e-8, maximum_iteration=100, precision=prec)
         sol.initialize(asm)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        gc = sol.solve(GC0=asm.GC.clone())
+        gc = sol.solve(GC0=gc0.clone())
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         if isinstance(gc, bool):
+            print(json.dumps({"newton_failed": prec, "history": sol.history}), flush=True)
             raise RuntimeError("Newton solve (%s) failed" % prec)
         R = asm.assemble_force(GC=gc)
         out[prec] = {"seconds": dt, "newton_iters": len(sol.history), "history": sol.history, "gc": gc,
+                     "pcg_iters_total": sum(h.get("pcg_iters", 0) for h in sol.history),
                      "final_rel_residual": float(R.norm()) / sol.history[0]["rnorm"]}
     d = float((out["mixed"]["gc"] - out["fp64"]["gc"]).norm() / out["fp64"]["gc"].norm())
     for k in out:
@@ -360,7 +379,7 @@ def main():
     asm = F.Assembly()
     asm.add_part(part, "block")
     asm.add_instance(F.Instance(part), "block")
-    asm.add_load(F.loads.Pressure("block", "end", -0.02), "traction")
+    asm.add_load(F.loads.Pressure("block", "end", PRESSURE), "traction")
     asm.add_boundary(F.boundarys.Boundary_Condition("block", "clamp"), "clamp")
     asm.initialize()
     P = asm.plan
@@ -390,7 +409,7 @@ def main():
         P.assemble_volume(0, mu, kappa, gc, K=K, R=R)
         if ev is not None:
             ev[1].record(stream)
-        P.assemble_pressure(0, -0.02, asm._Xinst, gc, K=K, R=R)
+        P.assemble_pressure(0, PRESSURE, asm._Xinst, gc, K=K, R=R)
 
     for _ in range(a.warmup):
         step()

@@ -99,6 +99,11 @@ fea_pcg_mixed_work_len = _sig("fea_pcg_mixed_work_len", I64, I64)
 fea_pcg_solve_mixed = _sig("fea_pcg_solve_mixed", I32, I64, P, P, P, P, P, P, D, D, I32, I32, P, I64,
                            C.POINTER(I32), C.POINTER(I32), C.POINTER(D), P)
 fea_spmv = _sig("fea_spmv", I32, I64, P, P, P, P, P, P)
+fea_spmv_nodes = _sig("fea_spmv_nodes", I32, NP, P, P, P, P, P)
+fea_pcg_solve_nodes = _sig("fea_pcg_solve_nodes", I32, NP, P, P, P, P, D, I32, I32, P, I64, C.POINTER(I32),
+                           C.POINTER(D), P)
+fea_pcg_solve_mixed_nodes = _sig("fea_pcg_solve_mixed_nodes", I32, NP, P, P, P, P, P, D, D, I32, I32, P, I64,
+                                 C.POINTER(I32), C.POINTER(I32), C.POINTER(D), P)
 fea_convert_f32 = _sig("fea_convert_f32", I32, I64, P, P, P)
 fea_explicit_work_len = _sig("fea_explicit_work_len", I64, I64)
 fea_explicit_run = _sig("fea_explicit_run", I32, NP, GP, D, D, P, D, I64, I32, I32, P, P, P, P, P, I64, P)
@@ -111,5 +116,5 @@ fea_launch_count = _sig("fea_launch_count", I64)
 EXPORTED = ["fea_plan_build", "fea_plan_free", "fea_plan_get", "fea_assemble_work_len", "fea_assemble_volume", "fea_assemble_pressure",
             "fea_reduce_scratch_len", "fea_energy_volume", "fea_energy_volume_noalloc", "fea_energy_pressure", "fea_lumped_mass",
             "fea_invert_mass", "fea_pcg_work_len", "fea_pcg_solve", "fea_pcg_mixed_work_len",
-            "fea_pcg_solve_mixed", "fea_spmv", "fea_convert_f32", "fea_explicit_work_len", "fea_explicit_run",
+            "fea_pcg_solve_mixed", "fea_spmv", "fea_spmv_nodes", "fea_pcg_solve_nodes", "fea_pcg_solve_mixed_nodes", "fea_convert_f32", "fea_explicit_work_len", "fea_explicit_run",
             "fea_adjoint_vjp_volume", "fea_adjoint_hvp_pressure", "fea_version", "fea_launch_count"]

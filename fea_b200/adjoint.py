@@ -101,13 +101,14 @@ class ComplianceFunction(torch.autograd.Function):
         if isinstance(gc, bool):
             raise RuntimeError("equilibrium solve failed")
         C, dX, dmu, _ = compliance_gradient(asm, gc)
-        ctx.save_for_backward(dX, dmu[0].reshape(()))
-        return C.detach().reshape(())
+        # gradients are returned on the devices of the inputs they belong to
+        ctx.save_for_backward(dX.to(X.device), dmu[0].reshape(()).to(torch.as_tensor(mu).device))
+        return C.detach().reshape(()).to(X.device)
 
     @staticmethod
     def backward(ctx, g):
         dX, dmu = ctx.saved_tensors
-        return g * dX.to(g.device), g * dmu.to(g.device), None, None
+        return g.to(dX.device) * dX, g.to(dmu.device) * dmu, None, None
 
 
 def set_coordinates(asm, X):

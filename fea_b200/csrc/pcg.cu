@@ -12,38 +12,65 @@
 // One iteration = 3 kernels: (1) q = K p fused with p.q, (2) x, r, z update
 // fused with r.z, (3) p update.  Scalars (alpha, beta, r.z, status) stay on
 // the device; every dot product is a fixed-order two-level sum (per-block
-// partials, summed by the last block to finish), so results are bitwise
-// reproducible.  The host reads the status every `check_every` iterations.
+// partials over a fixed grid, summed by the last block to finish), so
+// results are bitwise reproducible.  The host reads the status every
+// `check_every` iterations.
+//
+// Two SpMV operators:
+//   CsrOp  — any CSR matrix; LANES threads per row.
+//   NodeOp — the plan's reduced matrix: the f free rows of node n are
+//            consecutive, share one column list of length L_n and sit at
+//            vbase[n] + j * L_n in the values.  One warp per node reads the
+//            column indices and gathers x once for all f rows, so index
+//            traffic is nnz / f * 4 bytes instead of nnz * 4.
 #include <cmath>
+#include <mutex>
+#include <unordered_map>
 
 #include "common.cuh"
 
 namespace fea {
 
 constexpr int PCG_TPB = 256;
+constexpr int PCG_WARPS = PCG_TPB / 32;
+constexpr int PCG_GRID = 148 * 8;   // fixed grid: bounds the partial count
 
 // device-side solver state (doubles, in the work buffer)
 enum { S_RZ = 0, S_RZ0, S_ALPHA, S_BETA, S_DONE, S_ITER, S_STATUS, S_PQ, S_COUNT, S_LEN = 16 };
 
 template <class V>
-struct CsrT {
+struct CsrOp {
   const int64_t* __restrict__ ptr;
   const int32_t* __restrict__ idx;
   const V* __restrict__ val;
+  int64_t n;      // rows
+  int64_t nnz;
 };
 
-// group of LANES threads per row: dot(row, x)
-template <int LANES, class V, class X>
-__device__ __forceinline__ double row_dot(const CsrT<V>& A, int64_t row, int64_t n, const X* __restrict__ x,
-                                          int lane) {
-  double s = 0.0;
-  if (row < n) {
-    const int64_t b = A.ptr[row], e = A.ptr[row + 1];
-    for (int64_t i = b + lane; i < e; i += LANES) s += (double)A.val[i] * (double)x[A.idx[i]];
-  }
+template <class V>
+struct NodeOp {
+  const int64_t* __restrict__ vbase;
+  const int32_t* __restrict__ rowlen;
+  const int32_t* __restrict__ dbase;
+  const uint8_t* __restrict__ mask;
+  const int32_t* __restrict__ idx;
+  const V* __restrict__ val;
+  int64_t n_nodes;
+  int64_t n;      // rows (free DOFs)
+};
+
+// block sum: warp shuffles, then the 8 warp sums in fixed order
+__device__ __forceinline__ double block_sum_w(double v, double* sh) {
 #pragma unroll
-  for (int o = LANES / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, LANES);
-  return s;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+#pragma unroll
+  for (int i = 0; i < PCG_WARPS; ++i) r += sh[i];
+  __syncthreads();
+  return r;
 }
 
 // last-block-done reduction of per-block partials in block order
@@ -59,34 +86,28 @@ __device__ __forceinline__ bool last_block(unsigned* counter) {
   return last;
 }
 
-__device__ __forceinline__ double sum_partials(const volatile double* part, int n, double* sh) {
-  double acc = 0.0;
-  for (int i = threadIdx.x; i < n; i += PCG_TPB) acc += part[i];
-  return block_sum<PCG_TPB>(acc, sh);
+// sum of n (<= a few thousand) partials written by other blocks of this
+// grid; L2 loads (.cg) issued back to back, fixed order per thread
+__device__ __forceinline__ double sum_partials(const double* part, int n, int stride, int off, double* sh) {
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int i = threadIdx.x;
+  for (; i + 3 * PCG_TPB < n; i += 4 * PCG_TPB) {
+    a0 += __ldcg(part + (int64_t)i * stride + off);
+    a1 += __ldcg(part + (int64_t)(i + PCG_TPB) * stride + off);
+    a2 += __ldcg(part + (int64_t)(i + 2 * PCG_TPB) * stride + off);
+    a3 += __ldcg(part + (int64_t)(i + 3 * PCG_TPB) * stride + off);
+  }
+  for (; i < n; i += PCG_TPB) a0 += __ldcg(part + (int64_t)i * stride + off);
+  return block_sum_w((a0 + a1) + (a2 + a3), sh);
 }
 
-// y = A x ; optionally partial dot(x, y) per block -> part
-template <int LANES, class V, class X>
-__global__ void __launch_bounds__(PCG_TPB) k_spmv_dot(CsrT<V> A, int64_t n, const X* __restrict__ x,
-                                                      X* __restrict__ y, double* st, double* part,
-                                                      unsigned* counter, int mode) {
-  // mode 0: plain y = Ax.  mode 1: PCG step 1 (alpha = rz / p.q).
-  __shared__ double sh[PCG_TPB];
-  if (mode == 1 && st[S_DONE] != 0.0) return;
-  const int groups = PCG_TPB / LANES;
-  const int lane = threadIdx.x % LANES;
-  const int64_t row = (int64_t)blockIdx.x * groups + threadIdx.x / LANES;
-  double contrib = 0.0;
-  const double s = row_dot<LANES>(A, row, n, x, lane);   // every lane takes part in the shuffles
-  if (row < n && lane == 0) {
-    y[row] = (X)s;
-    contrib = s * (double)x[row];
-  }
-  if (mode == 0) return;
-  double bs = block_sum<PCG_TPB>(contrib, sh);
+// PCG step 1 epilogue: alpha = rz / p.q (or breakdown)
+__device__ __forceinline__ void finish_pq(double contrib, double* st, double* part, unsigned* counter) {
+  __shared__ double sh[PCG_WARPS];
+  double bs = block_sum_w(contrib, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = bs;
   if (last_block(counter)) {
-    double pq = sum_partials(part, gridDim.x, sh);
+    double pq = sum_partials(part, gridDim.x, 1, 0, sh);
     if (threadIdx.x == 0) {
       st[S_PQ] = pq;
       if (!(pq > 0.0) || !isfinite(pq)) {
@@ -101,6 +122,134 @@ __global__ void __launch_bounds__(PCG_TPB) k_spmv_dot(CsrT<V> A, int64_t n, cons
   }
 }
 
+// ---- CSR operator: LANES threads per row, warp-uniform loop ----------------
+// y = A x ; mode 1: also p.q partials and the alpha epilogue
+template <int LANES, class V, class X>
+__global__ void __launch_bounds__(PCG_TPB) k_spmv_csr(CsrOp<V> A, const X* __restrict__ x, X* __restrict__ y,
+                                                      double* st, double* part, unsigned* counter, int mode) {
+  if (mode == 1 && st[S_DONE] != 0.0) return;
+  constexpr int RPW = 32 / LANES;                 // rows per warp
+  const int lane = threadIdx.x % LANES;
+  const int warp = threadIdx.x >> 5;
+  const int sub = (threadIdx.x & 31) / LANES;
+  double contrib = 0.0;
+  for (int64_t base = ((int64_t)blockIdx.x * PCG_WARPS + warp) * RPW; base < A.n;
+       base += (int64_t)gridDim.x * PCG_WARPS * RPW) {
+    const int64_t row = base + sub;
+    double s = 0.0;
+    if (row < A.n) {
+      const int64_t b = A.ptr[row], e = A.ptr[row + 1];
+      for (int64_t i = b + lane; i < e; i += LANES) s += (double)A.val[i] * (double)x[A.idx[i]];
+    }
+#pragma unroll
+    for (int o = LANES / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, LANES);
+    if (row < A.n && lane == 0) {
+      y[row] = (X)s;
+      contrib += s * (double)x[row];
+    }
+  }
+  if (mode == 1) finish_pq(contrib, st, part, counter);
+}
+
+// ---- node operator: one warp per node row block ------------------------------
+template <class V, class X>
+__global__ void __launch_bounds__(PCG_TPB) k_spmv_node(NodeOp<V> A, const X* __restrict__ x, X* __restrict__ y,
+                                                       double* st, double* part, unsigned* counter, int mode) {
+  if (mode == 1 && st[S_DONE] != 0.0) return;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  double contrib = 0.0;
+  for (int64_t nd = (int64_t)blockIdx.x * PCG_WARPS + warp; nd < A.n_nodes; nd += (int64_t)gridDim.x * PCG_WARPS) {
+    const unsigned m = A.mask[nd];
+    if (!m) continue;                              // warp-uniform
+    const int f = popc3(m);
+    const int L = A.rowlen[nd];
+    const int64_t vb = A.vbase[nd];
+    const int32_t* __restrict__ ci = A.idx + vb;   // shared column list of the f rows
+    const V* __restrict__ v0 = A.val + vb;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    // 96 columns per pass: indices, then gathers, then values, three deep
+    for (int q0 = 0; q0 < L; q0 += 96) {
+      const int qa = q0 + lane, qb = qa + 32, qc = qa + 64;
+      const bool ha = qa < L, hb = qb < L, hc = qc < L;
+      const int32_t ja = ha ? __ldg(ci + qa) : 0;
+      const int32_t jb = hb ? __ldg(ci + qb) : 0;
+      const int32_t jc = hc ? __ldg(ci + qc) : 0;
+      const double xa = ha ? (double)x[ja] : 0.0;
+      const double xb = hb ? (double)x[jb] : 0.0;
+      const double xc = hc ? (double)x[jc] : 0.0;
+      s0 += (ha ? (double)__ldcs(v0 + qa) : 0.0) * xa + (hb ? (double)__ldcs(v0 + qb) : 0.0) * xb +
+            (hc ? (double)__ldcs(v0 + qc) : 0.0) * xc;
+      if (f > 1) {
+        const V* v1 = v0 + L;
+        s1 += (ha ? (double)__ldcs(v1 + qa) : 0.0) * xa + (hb ? (double)__ldcs(v1 + qb) : 0.0) * xb +
+              (hc ? (double)__ldcs(v1 + qc) : 0.0) * xc;
+      }
+      if (f > 2) {
+        const V* v2 = v0 + 2 * (int64_t)L;
+        s2 += (ha ? (double)__ldcs(v2 + qa) : 0.0) * xa + (hb ? (double)__ldcs(v2 + qb) : 0.0) * xb +
+              (hc ? (double)__ldcs(v2 + qc) : 0.0) * xc;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if (lane == 0) {
+      const int64_t r = A.dbase[nd];
+      y[r] = (X)s0;
+      contrib += s0 * (double)x[r];
+      if (f > 1) { y[r + 1] = (X)s1; contrib += s1 * (double)x[r + 1]; }
+      if (f > 2) { y[r + 2] = (X)s2; contrib += s2 * (double)x[r + 2]; }
+    }
+  }
+  if (mode == 1) finish_pq(contrib, st, part, counter);
+}
+
+// 1/|K_jj| of the node rows (0 -> 1): the diagonal entry of row (n, j) is the
+// column dbase[n] + j of the shared column list (sorted), found by bisection
+template <class V>
+__global__ void k_dinv_node(NodeOp<V> A, double* __restrict__ dinv) {
+  const int64_t nd = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (nd >= A.n_nodes) return;
+  const unsigned m = A.mask[nd];
+  const int f = popc3(m);
+  const int L = A.rowlen[nd];
+  const int64_t vb = A.vbase[nd];
+  const int32_t r0 = A.dbase[nd];
+  for (int j = 0; j < f; ++j) {
+    int lo = 0, hi = L;
+    double dv = 0.0;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      const int32_t c = A.idx[vb + mid];
+      if (c == r0 + j) { dv = (double)A.val[vb + (int64_t)j * L + mid]; break; }
+      if (c < r0 + j) lo = mid + 1; else hi = mid;
+    }
+    dv = fabs(dv);
+    dinv[r0 + j] = dv == 0.0 ? 1.0 : 1.0 / dv;
+  }
+}
+
+template <class V>
+__global__ void k_dinv_csr(CsrOp<V> A, double* __restrict__ dinv, int identity) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (identity) { dinv[i] = 1.0; continue; }
+    int64_t lo = A.ptr[i], hi = A.ptr[i + 1];
+    double dv = 0.0;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      const int32_t c = A.idx[mid];
+      if (c == i) { dv = (double)A.val[mid]; break; }
+      if (c < i) lo = mid + 1; else hi = mid;
+    }
+    dv = fabs(dv);
+    dinv[i] = dv == 0.0 ? 1.0 : 1.0 / dv;
+  }
+}
+
 // x += alpha p; r -= alpha q; z = r / |d|; partial r.z; last block: beta, stop test
 template <class X>
 __global__ void __launch_bounds__(PCG_TPB) k_pcg_update(int64_t n, X* __restrict__ x, X* __restrict__ r,
@@ -108,7 +257,7 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_update(int64_t n, X* __restrict
                                                         const X* __restrict__ q, const double* __restrict__ dinv,
                                                         double* st, double* part, unsigned* counter, double tol,
                                                         int max_iter) {
-  __shared__ double sh[PCG_TPB];
+  __shared__ double sh[PCG_WARPS];
   if (st[S_DONE] != 0.0) return;
   const double alpha = st[S_ALPHA];
   double contrib = 0.0;
@@ -120,10 +269,10 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_update(int64_t n, X* __restrict
     z[i] = (X)zi;
     contrib += ri * zi;
   }
-  double bs = block_sum<PCG_TPB>(contrib, sh);
+  double bs = block_sum_w(contrib, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = bs;
   if (last_block(counter)) {
-    double rz = sum_partials(part, gridDim.x, sh);
+    double rz = sum_partials(part, gridDim.x, 1, 0, sh);
     if (threadIdx.x == 0) {
       double it = st[S_ITER] + 1.0;
       st[S_ITER] = it;
@@ -152,33 +301,17 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_p(int64_t n, X* __restrict__ p,
     p[i] = (X)((double)z[i] + beta * (double)p[i]);
 }
 
-// setup: dinv = 1/|diag| (0 -> 1), r = b - Ax (Ax in r on entry), z = dinv r,
-// p = z, partial r.z and b.dinv.b; last block initialises the state.
+// setup (dinv given): r = b - Ax (Ax in r on entry), z = dinv r, p = z,
+// partial r.z and b.dinv.b; last block initialises the state.
 template <class X>
-__global__ void __launch_bounds__(PCG_TPB) k_pcg_setup(CsrT<double> A, int64_t n, const double* __restrict__ b,
-                                                       X* __restrict__ r, X* __restrict__ z, X* __restrict__ p,
-                                                       double* __restrict__ dinv, double* st, double* part,
-                                                       unsigned* counter, int compute_dinv, double tol) {
-  __shared__ double sh[PCG_TPB];
+__global__ void __launch_bounds__(PCG_TPB) k_pcg_setup(int64_t n, const double* __restrict__ b, X* __restrict__ r,
+                                                       X* __restrict__ z, X* __restrict__ p,
+                                                       const double* __restrict__ dinv, double* st, double* part,
+                                                       unsigned* counter) {
+  __shared__ double sh[PCG_WARPS];
   double c_rz = 0.0, c_bb = 0.0;
   for (int64_t i = (int64_t)blockIdx.x * PCG_TPB + threadIdx.x; i < n; i += (int64_t)gridDim.x * PCG_TPB) {
-    double di;
-    if (compute_dinv) {
-      // diagonal entry: binary search for column i in row i
-      int64_t lo = A.ptr[i], hi = A.ptr[i + 1];
-      double dv = 0.0;
-      while (lo < hi) {
-        int64_t mid = (lo + hi) >> 1;
-        int32_t c = A.idx[mid];
-        if (c == i) { dv = A.val[mid]; break; }
-        if (c < i) lo = mid + 1; else hi = mid;
-      }
-      dv = fabs(dv);
-      di = (compute_dinv == 2 || dv == 0.0) ? 1.0 : 1.0 / dv;
-      dinv[i] = di;
-    } else {
-      di = dinv[i];
-    }
+    const double di = dinv[i];
     double ri = b[i] - (double)r[i];
     r[i] = (X)ri;
     double zi = ri * di;
@@ -187,20 +320,15 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_setup(CsrT<double> A, int64_t n
     c_rz += ri * zi;
     c_bb += b[i] * b[i] * di;
   }
-  double s1 = block_sum<PCG_TPB>(c_rz, sh);
-  double s2 = block_sum<PCG_TPB>(c_bb, sh);
+  double s1 = block_sum_w(c_rz, sh);
+  double s2 = block_sum_w(c_bb, sh);
   if (threadIdx.x == 0) {
     part[2 * blockIdx.x] = s1;
     part[2 * blockIdx.x + 1] = s2;
   }
   if (last_block(counter)) {
-    double a1 = 0.0, a2 = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += PCG_TPB) {
-      a1 += ((volatile double*)part)[2 * i];
-      a2 += ((volatile double*)part)[2 * i + 1];
-    }
-    double rz = block_sum<PCG_TPB>(a1, sh);
-    double bb = block_sum<PCG_TPB>(a2, sh);
+    double rz = sum_partials(part, gridDim.x, 2, 0, sh);
+    double bb = sum_partials(part, gridDim.x, 2, 1, sh);
     if (threadIdx.x == 0) {
       st[S_RZ] = rz;
       st[S_RZ0] = bb;
@@ -212,12 +340,6 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_setup(CsrT<double> A, int64_t n
       *counter = 0u;
     }
   }
-}
-
-template <class X>
-__global__ void k_copy_cast(int64_t n, const double* __restrict__ a, X* __restrict__ b) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) b[i] = (X)a[i];
 }
 
 __global__ void k_f64_to_f32(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
@@ -235,29 +357,84 @@ static int lanes_for(int64_t n, int64_t nnz) {
   return avg >= 40.0 ? 32 : (avg >= 12.0 ? 16 : 8);
 }
 
+// Grid of a PCG kernel: one wave of resident blocks (occupancy x SMs,
+// capped at PCG_GRID so the partials fit the work buffer), fewer if there
+// are fewer units.  A fixed function of kernel and device, so the partial
+// sums keep one order from call to call.
+static std::mutex g_occ_mu;
+static std::unordered_map<const void*, int> g_occ[64];
+
+template <class Kern>
+static unsigned occ_grid(Kern kern, int64_t units, int per_block, int threads = PCG_TPB) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int wave = PCG_GRID;
+  {
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    auto& m = g_occ[dev & 63];
+    auto it = m.find((const void*)kern);
+    if (it != m.end()) {
+      wave = it->second;
+    } else {
+      int sms = 148, nb = 1;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, 0);
+      wave = (int)std::min<int64_t>((int64_t)sms * std::max(nb, 1), PCG_GRID);
+      m[(const void*)kern] = wave;
+    }
+  }
+  const int64_t need = (units + per_block - 1) / per_block;
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, wave));
+}
+
+static unsigned fixed_grid(int64_t units, int per_block) {
+  int64_t g = (units + per_block - 1) / per_block;
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, PCG_GRID));
+}
+
 template <class V, class X>
-static void spmv_launch(const CsrT<V>& A, int64_t n, int64_t nnz, const X* x, X* y, double* st, double* part,
-                        unsigned* counter, int mode, cudaStream_t s) {
-  const int L = lanes_for(n, nnz);
-  const int rows_per_block = PCG_TPB / L;
-  const unsigned grid = (unsigned)((n + rows_per_block - 1) / rows_per_block);
-  if (L == 32) k_spmv_dot<32, V, X><<<grid, PCG_TPB, 0, s>>>(A, n, x, y, st, part, counter, mode);
-  else if (L == 16) k_spmv_dot<16, V, X><<<grid, PCG_TPB, 0, s>>>(A, n, x, y, st, part, counter, mode);
-  else k_spmv_dot<8, V, X><<<grid, PCG_TPB, 0, s>>>(A, n, x, y, st, part, counter, mode);
+static void spmv(const CsrOp<V>& A, const X* x, X* y, double* st, double* part, unsigned* counter, int mode,
+                 cudaStream_t s) {
+  const int L = lanes_for(A.n, A.nnz);
+  const int rpb = PCG_TPB / L;
+  if (L == 32) k_spmv_csr<32, V, X><<<occ_grid(k_spmv_csr<32, V, X>, A.n, rpb), PCG_TPB, 0, s>>>(A, x, y, st, part,
+                                                                                            counter, mode);
+  else if (L == 16) k_spmv_csr<16, V, X><<<occ_grid(k_spmv_csr<16, V, X>, A.n, rpb), PCG_TPB, 0, s>>>(A, x, y, st,
+                                                                                                 part, counter, mode);
+  else k_spmv_csr<8, V, X><<<occ_grid(k_spmv_csr<8, V, X>, A.n, rpb), PCG_TPB, 0, s>>>(A, x, y, st, part, counter,
+                                                                                  mode);
   count_launch();
 }
 
+template <class V, class X>
+static void spmv(const NodeOp<V>& A, const X* x, X* y, double* st, double* part, unsigned* counter, int mode,
+                 cudaStream_t s) {
+  k_spmv_node<V, X><<<occ_grid(k_spmv_node<V, X>, A.n_nodes, PCG_WARPS), PCG_TPB, 0, s>>>(A, x, y, st, part, counter,
+                                                                                        mode);
+  count_launch();
+}
+
+template <class V>
+static void diag_inv(const CsrOp<V>& A, double* dinv, int jacobi, cudaStream_t s) {
+  k_dinv_csr<V><<<fixed_grid(A.n, 256), 256, 0, s>>>(A, dinv, jacobi ? 0 : 1);
+  count_launch();
+}
+
+template <class V>
+static void diag_inv(const NodeOp<V>& A, double* dinv, int, cudaStream_t s) {
+  k_dinv_node<V><<<grid_for(A.n_nodes, 128), 128, 0, s>>>(A, dinv);
+  count_launch();
+}
+
+template <class X>
 static unsigned vec_grid(int64_t n) {
-  int64_t g = (n + PCG_TPB - 1) / PCG_TPB;
-  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 8));
+  // the update kernel's wave sizes all three vector kernels (same partials)
+  return occ_grid(k_pcg_update<X>, n, PCG_TPB);
 }
 
-static int64_t part_len(int64_t n) {
-  // partials of the SpMV grid (>= 1 row per 32 threads) and of the vector grid
-  return std::max<int64_t>((n + 7) / 8 + 1, 2 * 148 * 8 + 2);
-}
+static int64_t part_len(int64_t) { return 2 * PCG_GRID + 2; }
 
-// Work layout (doubles): st[S_LEN] | counter(1) | dinv[n] | r | z | p | q | part
+// Work layout (doubles): st[S_LEN] | counter(2) | dinv[n] | r | z | p | q | part
 struct PcgWork {
   double* st;
   unsigned* counter;
@@ -280,16 +457,15 @@ static PcgWork carve(double* w, int64_t n) {
 }
 
 // Run PCG iterations on (A, b) in precision X starting from x (in X), with
-// dinv given.  Returns status; *iters.
-template <class V, class X>
-static int pcg_core(const CsrT<V>& A, const CsrT<double>& A64, int64_t n, int64_t nnz, const double* b, X* x,
-                    X* r, X* z, X* p, X* q, double* dinv, double* st, unsigned* counter, double* part,
-                    int compute_dinv, double tol, int max_iter, int check_every, int* iters, double* relres,
-                    cudaStream_t s) {
-  // r = A x  (in the working precision), then setup
-  spmv_launch<V, X>(A, n, nnz, x, r, st, part, counter, 0, s);
-  const unsigned vg = vec_grid(n);
-  k_pcg_setup<X><<<vg, PCG_TPB, 0, s>>>(A64, n, b, r, z, p, dinv, st, part, counter, compute_dinv, tol);
+// dinv given.  Returns status; *iters.  A64 computes the FP64 residual of
+// the initial guess (same operator in FP64 values).
+template <class Op, class X>
+static int pcg_core(const Op& A, int64_t n, const double* b, X* x, X* r, X* z, X* p, X* q, const double* dinv,
+                    double* st, unsigned* counter, double* part, double tol, int max_iter, int check_every,
+                    int* iters, double* relres, cudaStream_t s) {
+  spmv(A, (const X*)x, r, st, part, counter, 0, s);       // r = A x
+  const unsigned vg = vec_grid<X>(n);
+  k_pcg_setup<X><<<vg, PCG_TPB, 0, s>>>(n, b, r, z, p, dinv, st, part, counter);
   count_launch();
   if (cudaError_t e = cudaGetLastError()) return (int)e;
   double host[S_LEN];
@@ -301,7 +477,7 @@ static int pcg_core(const CsrT<V>& A, const CsrT<double>& A64, int64_t n, int64_
     if (host[S_DONE] != 0.0 || it_done >= max_iter) break;
     const int batch = std::min(ce, max_iter - it_done);
     for (int k = 0; k < batch; ++k) {
-      spmv_launch<V, X>(A, n, nnz, p, q, st, part, counter, 1, s);
+      spmv(A, (const X*)p, q, st, part, counter, 1, s);
       k_pcg_update<X><<<vg, PCG_TPB, 0, s>>>(n, x, r, z, p, q, dinv, st, part, counter, tol, max_iter);
       k_pcg_p<X><<<vg, PCG_TPB, 0, s>>>(n, p, z, st);
       count_launch(2);
@@ -314,20 +490,112 @@ static int pcg_core(const CsrT<V>& A, const CsrT<double>& A64, int64_t n, int64_
   return (int)host[S_STATUS];
 }
 
+template <class Op>
+static int pcg_fp64(const Op& A, int64_t n, const double* b, double* x, double tol, int max_iter, int check_every,
+                    int jacobi, double* work, int32_t* iters, double* relres, cudaStream_t s) {
+  PcgWork W = carve(work, n);
+  cudaMemsetAsync(W.counter, 0, 2 * sizeof(unsigned), s);
+  diag_inv(A, W.dinv, jacobi, s);
+  int it = 0;
+  int r = pcg_core<Op, double>(A, n, b, x, W.r, W.z, W.p, W.q, W.dinv, W.st, W.counter, W.part, tol, max_iter,
+                               check_every, &it, relres, s);
+  if (iters) *iters = it;
+  return r;
+}
+
+// Mixed precision: outer FP64 residual r = b - A x (stop test as above);
+// inner FP32 PCG on A32 d = r to `inner_tol`; x += d.
+template <class Op64, class Op32>
+static int pcg_mixed(const Op64& A, const Op32& A32, int64_t n, const double* b, double* x, double tol,
+                     double inner_tol, int max_iter, int check_every, double* work, int32_t* iters, int32_t* outer,
+                     double* relres, cudaStream_t s) {
+  PcgWork W = carve(work, n);                 // r = FP64 residual, q = FP64 A x
+  double* st2 = work + S_LEN + 2 + 5 * n + part_len(n);
+  unsigned* counter2 = (unsigned*)(st2 + S_LEN);
+  float* f = (float*)(st2 + S_LEN + 2);
+  float *xf = f, *rf = f + n, *zf = f + 2 * n, *pf = f + 3 * n, *qf = f + 4 * n;
+  cudaMemsetAsync(W.counter, 0, 2 * sizeof(unsigned), s);
+  cudaMemsetAsync(counter2, 0, 2 * sizeof(unsigned), s);
+  diag_inv(A, W.dinv, 1, s);
+  const unsigned vg = vec_grid<double>(n);
+  int total = 0, nouter = 0;
+  double rel = 0.0;
+  int status = FEA_ENOTCONV;
+  while (total < max_iter) {
+    // FP64 residual, stop test, and the inner right-hand side = r
+    spmv(A, (const double*)x, W.r, nullptr, nullptr, nullptr, 0, s);
+    k_pcg_setup<double><<<vg, PCG_TPB, 0, s>>>(n, b, W.r, W.z, W.p, W.dinv, W.st, W.part, W.counter);
+    count_launch();
+    double host[S_LEN];
+    cudaMemcpyAsync(host, W.st, sizeof(host), cudaMemcpyDeviceToHost, s);
+    if (cudaError_t e = cudaStreamSynchronize(s)) return (int)e;
+    rel = host[S_RZ] / host[S_RZ0];
+    if (host[S_DONE] != 0.0 || rel < tol) {
+      status = FEA_OK;
+      break;
+    }
+    // inner solve: b_inner = r (FP64 in W.r), x_inner = 0
+    cudaMemsetAsync(xf, 0, sizeof(float) * n, s);
+    int it = 0;
+    double rr = 0.0;
+    int ri = pcg_core<Op32, float>(A32, n, W.r, xf, rf, zf, pf, qf, W.dinv, st2, counter2, W.part, inner_tol,
+                                   max_iter - total, check_every, &it, &rr, s);
+    total += it;
+    ++nouter;
+    k_axpy_f32<<<grid_for(n, 256), 256, 0, s>>>(n, x, xf);
+    count_launch();
+    if (ri == FEA_EBREAKDOWN) { status = ri; break; }
+    if (ri > 0) return ri;
+    if (it == 0) { status = FEA_EBREAKDOWN; break; }
+  }
+  if (iters) *iters = total;
+  if (outer) *outer = nouter;
+  if (relres) *relres = rel;
+  return status;
+}
+
+template <class V>
+static NodeOp<V> node_op(const fea_nodes_t* N, const int32_t* idx, const V* val) {
+  return NodeOp<V>{N->vbase_dev, N->rowlen_dev, N->dbase_dev, N->mask_dev, idx, val, N->n_nodes, N->ndof};
+}
+
+static bool nodes_ok(const fea_nodes_t* N) {
+  return N && N->n_nodes >= 0 && N->ndof >= 0 && (N->ndof == 0 || (N->vbase_dev && N->rowlen_dev && N->dbase_dev &&
+                                                                   N->mask_dev));
+}
+
+static int read_nnz(const int64_t* ip, int64_t n, int64_t* nnz, cudaStream_t s) {
+  *nnz = 0;
+  if (cudaError_t e = cudaMemcpyAsync(nnz, ip + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s)) return (int)e;
+  return (int)cudaStreamSynchronize(s);
+}
+
 }  // namespace fea
 
 using namespace fea;
 
 extern "C" int64_t fea_pcg_work_len(int64_t n) { return S_LEN + 2 + 5 * n + part_len(n); }
 
+extern "C" int64_t fea_pcg_mixed_work_len(int64_t n) {
+  // FP64: st | counter | dinv | r | z | p | q | part ; FP32 inner: st2 | counter2 | x,r,z,p,q (floats)
+  return fea_pcg_work_len(n) + S_LEN + 2 + (5 * n + 1) / 2;
+}
+
 extern "C" int fea_spmv(int64_t n, const int64_t* ip, const int32_t* ix, const double* v, const double* x,
                         double* y, cudaStream_t s) {
   if (n < 0 || !ip || !ix || !v || !x || !y) return FEA_EINVAL;
   if (n == 0) return FEA_OK;
   int64_t nnz = 0;
-  cudaMemcpy(&nnz, ip + n, sizeof(int64_t), cudaMemcpyDeviceToHost);
-  CsrT<double> A{ip, ix, v};
-  spmv_launch<double, double>(A, n, nnz, x, y, nullptr, nullptr, nullptr, 0, s);
+  if (int r = read_nnz(ip, n, &nnz, s)) return r;
+  spmv(CsrOp<double>{ip, ix, v, n, nnz}, x, y, nullptr, nullptr, nullptr, 0, s);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int fea_spmv_nodes(const fea_nodes_t* N, const int32_t* ix, const double* v, const double* x, double* y,
+                              cudaStream_t s) {
+  if (!nodes_ok(N) || !ix || !v || !x || !y) return FEA_EINVAL;
+  if (N->ndof == 0) return FEA_OK;
+  spmv(node_op<double>(N, ix, v), x, y, nullptr, nullptr, nullptr, 0, s);
   return (int)cudaGetLastError();
 }
 
@@ -348,23 +616,21 @@ extern "C" int fea_pcg_solve(int64_t n, const int64_t* ip, const int32_t* ix, co
   if (relres) *relres = 0.0;
   if (n == 0) return FEA_OK;
   int64_t nnz = 0;
-  if (cudaError_t e = cudaMemcpyAsync(&nnz, ip + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s)) return (int)e;
-  if (cudaError_t e = cudaStreamSynchronize(s)) return (int)e;
-  PcgWork W = carve(work, n);
-  cudaMemsetAsync(W.counter, 0, sizeof(unsigned), s);
-  CsrT<double> A{ip, ix, v};
-  int it = 0;
-  int r = pcg_core<double, double>(A, A, n, nnz, b, x, W.r, W.z, W.p, W.q, W.dinv, W.st, W.counter, W.part,
-                                   jacobi ? 1 : 2, tol, max_iter, check_every, &it, relres, s);
-  if (iters) *iters = it;
-  return r;
+  if (int r = read_nnz(ip, n, &nnz, s)) return r;
+  return pcg_fp64(CsrOp<double>{ip, ix, v, n, nnz}, n, b, x, tol, max_iter, check_every, jacobi, work, iters,
+                  relres, s);
 }
 
-// Mixed precision: outer FP64 residual r = b - A x (stop test as above);
-// inner FP32 PCG on A32 d = r to `inner_tol`; x += d.
-extern "C" int64_t fea_pcg_mixed_work_len(int64_t n) {
-  // FP64 outer: st | counter | dinv | r64 | part ; FP32 inner: x,r,z,p,q (floats) + st2
-  return fea_pcg_work_len(n) + (5 * n + 1) / 2 + S_LEN + 2;
+extern "C" int fea_pcg_solve_nodes(const fea_nodes_t* N, const int32_t* ix, const double* v, const double* b,
+                                   double* x, double tol, int32_t max_iter, int32_t check_every, double* work,
+                                   int64_t work_len, int32_t* iters, double* relres, cudaStream_t s) {
+  if (!nodes_ok(N) || !ix || !v || !b || !x || !work || max_iter < 0) return FEA_EINVAL;
+  const int64_t n = N->ndof;
+  if (work_len < fea_pcg_work_len(n)) return FEA_EWORK;
+  if (iters) *iters = 0;
+  if (relres) *relres = 0.0;
+  if (n == 0) return FEA_OK;
+  return pcg_fp64(node_op<double>(N, ix, v), n, b, x, tol, max_iter, check_every, 1, work, iters, relres, s);
 }
 
 extern "C" int fea_pcg_solve_mixed(int64_t n, const int64_t* ip, const int32_t* ix, const double* v,
@@ -378,52 +644,22 @@ extern "C" int fea_pcg_solve_mixed(int64_t n, const int64_t* ip, const int32_t* 
   if (relres) *relres = 0.0;
   if (n == 0) return FEA_OK;
   int64_t nnz = 0;
-  if (cudaError_t e = cudaMemcpyAsync(&nnz, ip + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s)) return (int)e;
-  if (cudaError_t e = cudaStreamSynchronize(s)) return (int)e;
-  PcgWork W = carve(work, n);                 // r = FP64 residual, q = FP64 A x
-  double* st2 = work + fea_pcg_work_len(n);
-  unsigned* counter2 = (unsigned*)(st2 + S_LEN);
-  float* f = (float*)(st2 + S_LEN + 2);
-  float *xf = f, *rf = f + n, *zf = f + 2 * n, *pf = f + 3 * n, *qf = f + 4 * n;
-  cudaMemsetAsync(W.counter, 0, sizeof(unsigned), s);
-  cudaMemsetAsync(counter2, 0, sizeof(unsigned), s);
-  CsrT<double> A{ip, ix, v};
-  CsrT<float> A32{ip, ix, v32};
-  const unsigned vg = vec_grid(n);
-  int total = 0, nouter = 0;
-  double rel = 0.0;
-  int status = FEA_ENOTCONV;
-  bool first = true;
-  while (total < max_iter) {
-    // FP64 residual, stop test, and the inner right-hand side rf = r
-    spmv_launch<double, double>(A, n, nnz, x, W.r, nullptr, nullptr, nullptr, 0, s);
-    k_pcg_setup<double><<<vg, PCG_TPB, 0, s>>>(A, n, b, W.r, W.z, W.p, W.dinv, W.st, W.part, W.counter,
-                                               first ? 1 : 0, tol);
-    count_launch();
-    first = false;
-    double host[S_LEN];
-    cudaMemcpyAsync(host, W.st, sizeof(host), cudaMemcpyDeviceToHost, s);
-    if (cudaError_t e = cudaStreamSynchronize(s)) return (int)e;
-    rel = host[S_RZ] / host[S_RZ0];
-    if (host[S_DONE] != 0.0 || rel < tol) {
-      status = FEA_OK;
-      break;
-    }
-    // inner solve: b_inner = r (FP64 in W.r), x_inner = 0
-    cudaMemsetAsync(xf, 0, sizeof(float) * n, s);
-    int it = 0;
-    double rr = 0.0;
-    int ri = pcg_core<float, float>(A32, A, n, nnz, W.r, xf, rf, zf, pf, qf, W.dinv, st2, counter2, W.part, 0,
-                                    inner_tol, max_iter - total, check_every, &it, &rr, s);
-    total += it;
-    ++nouter;
-    k_axpy_f32<<<grid_for(n, 256), 256, 0, s>>>(n, x, xf);
-    count_launch();
-    if (ri == FEA_EBREAKDOWN) { status = ri; break; }
-    if (it == 0) { status = FEA_EBREAKDOWN; break; }
-  }
-  if (iters) *iters = total;
-  if (outer) *outer = nouter;
-  if (relres) *relres = rel;
-  return status;
+  if (int r = read_nnz(ip, n, &nnz, s)) return r;
+  return pcg_mixed(CsrOp<double>{ip, ix, v, n, nnz}, CsrOp<float>{ip, ix, v32, n, nnz}, n, b, x, tol, inner_tol,
+                   max_iter, check_every, work, iters, outer, relres, s);
+}
+
+extern "C" int fea_pcg_solve_mixed_nodes(const fea_nodes_t* N, const int32_t* ix, const double* v, const float* v32,
+                                         const double* b, double* x, double tol, double inner_tol, int32_t max_iter,
+                                         int32_t check_every, double* work, int64_t work_len, int32_t* iters,
+                                         int32_t* outer, double* relres, cudaStream_t s) {
+  if (!nodes_ok(N) || !ix || !v || !v32 || !b || !x || !work || max_iter < 0) return FEA_EINVAL;
+  const int64_t n = N->ndof;
+  if (work_len < fea_pcg_mixed_work_len(n)) return FEA_EWORK;
+  if (iters) *iters = 0;
+  if (outer) *outer = 0;
+  if (relres) *relres = 0.0;
+  if (n == 0) return FEA_OK;
+  return pcg_mixed(node_op<double>(N, ix, v), node_op<float>(N, ix, v32), n, b, x, tol, inner_tol, max_iter,
+                   check_every, work, iters, outer, relres, s);
 }

@@ -236,34 +236,57 @@ class DevicePlan:
         return m
 
     # -- linear algebra --------------------------------------------------------
-    def spmv(self, values, x, y=None):
+    def spmv(self, values, x, y=None, generic=False):
+        """y = K x on the plan's reduced matrix (node-row kernel; generic=True
+        runs the plain CSR kernel on the same arrays)."""
         y = self.zeros(self.ndof) if y is None else y
-        L.check(L.fea_spmv(self.ndof, vptr(self.indptr), vptr(self.indices), vptr(values), vptr(x), vptr(y),
-                           stream()), "fea_spmv")
+        if generic:
+            L.check(L.fea_spmv(self.ndof, vptr(self.indptr), vptr(self.indices), vptr(values), vptr(x), vptr(y),
+                               stream()), "fea_spmv")
+        else:
+            L.check(L.fea_spmv_nodes(C.byref(self.nodes), vptr(self.indices), vptr(values), vptr(x), vptr(y),
+                                     stream()), "fea_spmv_nodes")
         return y
 
-    def pcg(self, values, b, x, tol, max_iter, check_every=20, jacobi=True, raise_on_cap=False):
-        """Jacobi-PCG, in place on x. Returns (iterations, relres, status)."""
+    def pcg(self, values, b, x, tol, max_iter, check_every=20, jacobi=True, raise_on_cap=False,
+            raise_on_breakdown=True, generic=False):
+        """Jacobi-PCG, in place on x. Returns (iterations, relres, status).
+        The node-row solver runs unless jacobi is False or generic is True."""
         n = self.ndof
         wl = L.fea_pcg_work_len(n)
         w = self.scratch(wl)
         it, rr = C.c_int32(0), C.c_double(0.0)
-        st = L.fea_pcg_solve(n, vptr(self.indptr), vptr(self.indices), vptr(values), vptr(b), vptr(x), float(tol),
-                             int(max_iter), int(check_every), int(bool(jacobi)), vptr(w), w.numel(), C.byref(it),
-                             C.byref(rr), stream())
-        if st not in (L.FEA_OK, L.FEA_ENOTCONV) or (raise_on_cap and st == L.FEA_ENOTCONV):
+        if generic or not jacobi:
+            st = L.fea_pcg_solve(n, vptr(self.indptr), vptr(self.indices), vptr(values), vptr(b), vptr(x),
+                                 float(tol), int(max_iter), int(check_every), int(bool(jacobi)), vptr(w), w.numel(),
+                                 C.byref(it), C.byref(rr), stream())
+        else:
+            st = L.fea_pcg_solve_nodes(C.byref(self.nodes), vptr(self.indices), vptr(values), vptr(b), vptr(x),
+                                       float(tol), int(max_iter), int(check_every), vptr(w), w.numel(), C.byref(it),
+                                       C.byref(rr), stream())
+        ok = [L.FEA_OK, L.FEA_ENOTCONV] + ([] if raise_on_breakdown else [L.FEA_EBREAKDOWN])
+        if st not in ok or (raise_on_cap and st == L.FEA_ENOTCONV):
             L.check(st, "fea_pcg_solve")
         return int(it.value), float(rr.value), st
 
-    def pcg_mixed(self, values, values32, b, x, tol, inner_tol, max_iter, check_every=20):
+    def pcg_mixed(self, values, values32, b, x, tol, inner_tol, max_iter, check_every=20, raise_on_breakdown=True,
+                  generic=False):
         n = self.ndof
         wl = L.fea_pcg_mixed_work_len(n)
         w = self.scratch(wl)
         it, outer, rr = C.c_int32(0), C.c_int32(0), C.c_double(0.0)
-        st = L.fea_pcg_solve_mixed(n, vptr(self.indptr), vptr(self.indices), vptr(values), vptr(values32), vptr(b),
-                                   vptr(x), float(tol), float(inner_tol), int(max_iter), int(check_every), vptr(w),
-                                   w.numel(), C.byref(it), C.byref(outer), C.byref(rr), stream())
-        if st not in (L.FEA_OK, L.FEA_ENOTCONV):
+        if generic:
+            st = L.fea_pcg_solve_mixed(n, vptr(self.indptr), vptr(self.indices), vptr(values), vptr(values32),
+                                       vptr(b), vptr(x), float(tol), float(inner_tol), int(max_iter),
+                                       int(check_every), vptr(w), w.numel(), C.byref(it), C.byref(outer),
+                                       C.byref(rr), stream())
+        else:
+            st = L.fea_pcg_solve_mixed_nodes(C.byref(self.nodes), vptr(self.indices), vptr(values), vptr(values32),
+                                             vptr(b), vptr(x), float(tol), float(inner_tol), int(max_iter),
+                                             int(check_every), vptr(w), w.numel(), C.byref(it), C.byref(outer),
+                                             C.byref(rr), stream())
+        ok = [L.FEA_OK, L.FEA_ENOTCONV] + ([] if raise_on_breakdown else [L.FEA_EBREAKDOWN])
+        if st not in ok:
             L.check(st, "fea_pcg_solve_mixed")
         return int(it.value), int(outer.value), float(rr.value), st
 

@@ -7,7 +7,9 @@ the device Jacobi-PCG (static_implicit.py:352-405: symmetric Jacobi scaling
 + CG is Jacobi-PCG).  Where the reference switches to its CPU direct solver
 (scaled residual below 1e-3, or repeated small steps, static_implicit.py:
 384-388) this solver runs the PCG to a tight tolerance instead.  ``rtol``
-adds a relative stop test ||R|| / ||R_first|| <= rtol.
+adds a relative stop test ||R|| / ||R_first|| <= rtol; in that mode a
+residual that has stopped falling below ``floor_rtol`` (1e-9) of the first
+one is the round-off floor and also ends the iteration.
 
 DynamicExplicitSolver keeps the reference's time and storage bookkeeping
 (dynamic_explicit.py:66-145) and advances the state with the fused
@@ -51,6 +53,7 @@ class StaticImplicitSolver(BaseSolver):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         self.precision = precision
         self.verbose = verbose
+        self.floor_rtol = 1e-9
         self._iter_now = 0
         self._maximum_step_length = 1e10
         self._low_alpha_count = 0
@@ -129,6 +132,8 @@ class StaticImplicitSolver(BaseSolver):
             self.history.append(dict(iter=self._iter_now, rmax=rmax, rnorm=rnorm))
             if self.rtol is not None and rnorm <= self.rtol * max(r_first, 1e-300):
                 break
+            if self._at_floor(r_first):
+                break
             dGC = self._solve_linear_equation(Kv, -R, self._iter_now, alpha, dGC)
             alpha, GCnew, energynew = self._line_search(GC, dGC, R, energy)
             self.history[-1].update(alpha=alpha)
@@ -141,6 +146,8 @@ class StaticImplicitSolver(BaseSolver):
             else:
                 low_alpha = max(0, low_alpha - 5)
             if low_alpha > 10:
+                if self.rtol is not None and rnorm <= self.floor_rtol * r_first:
+                    break
                 return False
             GC = GCnew
             energy = self.get_total_energy(GC)
@@ -149,6 +156,17 @@ class StaticImplicitSolver(BaseSolver):
             if self.rtol is None and ((float(dGC.abs().max()) < tol_error and rmax < tol_error) or rmax < 1e-6):
                 break
         return GC
+
+    def _at_floor(self, r_first):
+        """Relative-residual mode only: the residual has stopped falling
+        (no halving over the last three iterations) below ``floor_rtol`` of
+        the first residual, i.e. Newton has reached the round-off floor of
+        the residual evaluation and further iterations cannot reach ``rtol``."""
+        h = self.history
+        if self.rtol is None or len(h) < 4 or r_first == 0.0:
+            return False
+        last = h[-1]["rnorm"]
+        return last <= self.floor_rtol * r_first and last > 0.5 * min(x["rnorm"] for x in h[-4:-1])
 
     def _solve_linear_equation(self, K_values, R, iter_now=0, alpha0=None, dGC0=None, tol_error=None):
         """K dGC = R by device PCG, warm-started from the previous step (static_implicit.py:352-405)."""
@@ -164,12 +182,20 @@ class StaticImplicitSolver(BaseSolver):
         else:
             tol = self.pcg_tol
             cap = 6000 if (iter_now % 20 == 0 or self._low_alpha_count > 0) else self.pcg_max_iter
+        x0 = x.clone()
         if self.precision == "mixed":
             v32 = P.to_f32(K_values)
-            it, outer, rr, st = P.pcg_mixed(K_values, v32, R.contiguous(), x, tol, 1e-4, cap)
+            it, outer, rr, st = P.pcg_mixed(K_values, v32, R.contiguous(), x, tol, 1e-4, cap,
+                                            raise_on_breakdown=False)
         else:
-            it, rr, st = P.pcg(K_values, R.contiguous(), x, tol, cap)
-        self.history[-1].update(pcg_iters=it, pcg_relres=rr, pcg_tight=tight)
+            it, rr, st = P.pcg(K_values, R.contiguous(), x, tol, cap, raise_on_breakdown=False)
+        self.history[-1].update(pcg_iters=it, pcg_relres=rr, pcg_tight=tight, pcg_status=st)
+        if st == L.FEA_EBREAKDOWN:
+            # K is not positive definite along the search space: keep the
+            # iterate reached before the negative curvature (truncated CG);
+            # with no progress, take the Jacobi-scaled residual direction
+            if not bool(torch.isfinite(x).all()) or bool(torch.equal(x, x0)):
+                x = R / self._diag(K_values).abs()
         return x
 
     def _scaled_rmax(self, K_values, R):

@@ -266,6 +266,26 @@ int fea_pcg_solve_mixed(int64_t n, const int64_t* indptr_dev, const int32_t* ind
 /* y = K x (FP64) */
 int fea_spmv(int64_t n, const int64_t* indptr_dev, const int32_t* indices_dev, const double* values_dev,
              const double* x_dev, double* y_dev, cudaStream_t stream);
+
+/* The same solvers and SpMV on a matrix in the plan's reduced layout (the
+ * values written by fea_assemble_volume / fea_assemble_pressure; indices_dev
+ * = FEA_A_INDICES).  The f free rows of node n share one column list of
+ * length rowlen[n] and start at vbase[n] + j * rowlen[n], so one warp per
+ * node reads the column indices and gathers x once for all f rows.  Always
+ * Jacobi-preconditioned (the path of StaticImplicitSolver._solve_linear_equation,
+ * static_implicit.py:352-405); work lengths as fea_pcg_work_len(ndof) /
+ * fea_pcg_mixed_work_len(ndof); results equal those of fea_pcg_solve /
+ * fea_pcg_solve_mixed on the same CSR up to the order of the row sums. */
+int fea_spmv_nodes(const fea_nodes_t* nodes, const int32_t* indices_dev, const double* values_dev,
+                   const double* x_dev, double* y_dev, cudaStream_t stream);
+int fea_pcg_solve_nodes(const fea_nodes_t* nodes, const int32_t* indices_dev, const double* values_dev,
+                        const double* b_dev, double* x_dev, double tol, int32_t max_iter, int32_t check_every,
+                        double* work_dev, int64_t work_len, int32_t* iters, double* relres, cudaStream_t stream);
+int fea_pcg_solve_mixed_nodes(const fea_nodes_t* nodes, const int32_t* indices_dev, const double* values_dev,
+                              const float* values32_dev, const double* b_dev, double* x_dev, double tol,
+                              double inner_tol, int32_t max_iter, int32_t check_every, double* work_dev,
+                              int64_t work_len, int32_t* iters, int32_t* outer, double* relres,
+                              cudaStream_t stream);
 /* values32 = (float) values */
 int fea_convert_f32(int64_t nnz, const double* values_dev, float* values32_dev, cudaStream_t stream);
 

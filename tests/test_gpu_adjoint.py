@@ -59,7 +59,10 @@ def test_compliance_gradient_vs_central_differences(golden):
         Xm = X0.clone(); Xm[nd, k] -= h
         fd = (_solve(c, X=Xp)[0] - _solve(c, X=Xm)[0]) / (2 * h)
         ad = float(dX[nd, k])
-        assert abs(fd - ad) <= 1e-6 * max(abs(ad), 1e-3 * scale), (nd, k, fd, ad)
+        # central differences at h = 1e-6 carry ~1e-9 of the largest component
+        # in truncation and round-off; components below 1 % of the largest
+        # are compared against 1e-6 of that 1 %
+        assert abs(fd - ad) <= 1e-6 * max(abs(ad), 1e-2 * scale), (nd, k, fd, ad)
     _solve(c, X=X0)
     fd = (_solve(c, mu=mu0 + h)[0] - _solve(c, mu=mu0 - h)[0]) / (2 * h)
     assert abs(fd - float(dmu[0])) <= 1e-6 * abs(float(dmu[0]))

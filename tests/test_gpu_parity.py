@@ -227,6 +227,50 @@ def test_pcg_solves_reduced_system(golden):
     assert rel(x2, xd) < 1e-9
 
 
+@pytest.mark.parametrize("kind,dofs", [("C3D8", (0, 2)), ("C3D4", (1,)), ("C3D8", (0, 1, 2))])
+def test_node_row_spmv_and_pcg_match_csr(kind, dofs):
+    """The node-row SpMV / PCG (shared column list per node) against the plain
+    CSR kernels and the oracle's CSR product, with partially fixed nodes
+    (rows of 1 and 2 free DOFs) in the pattern."""
+    import fea_b200 as F
+    n = 4
+    X, el = O.hex_block(n, jitter=0.1, seed=2) if kind == "C3D8" else O.tet_block(n)
+    fixed = torch.nonzero(X[:, 0] < 1e-9).flatten().numpy()
+    part = F.Part(X)
+    cls = F.elements.C3D4 if kind == "C3D4" else F.elements.C3D8
+    e = cls(elems=el, elems_index=torch.arange(el.shape[0]), part=part)
+    e.set_materials(F.materials.NeoHookean(1.0, 10.0))
+    part.add_element(e)
+    part.set_nodes["x0"] = fixed
+    part.set_nodes["x1"] = torch.nonzero(X[:, 0] > 1 - 1e-9).flatten().numpy()   # keeps K nonsingular
+    asm = F.Assembly()
+    asm.add_part(part, "p")
+    asm.add_instance(F.Instance(part), "p")
+    asm.add_boundary(F.boundarys.Boundary_Condition("p", "x0", indexDoF=list(dofs)), "bc0")
+    asm.add_boundary(F.boundarys.Boundary_Condition("p", "x1"), "bc1")
+    asm.initialize()
+    P = asm.plan
+    gc = torch.randn(asm.GC.shape, generator=torch.Generator().manual_seed(3), dtype=torch.float64) * 1e-3
+    R, K = asm.assemble_csr(gc.cuda())
+    v = torch.randn(P.ndof, generator=torch.Generator().manual_seed(4), dtype=torch.float64).cuda()
+    y_node = P.spmv(K, v)
+    y_csr = P.spmv(K, v, generic=True)
+    y_o = O.csr_matvec(P.indptr.cpu(), P.indices.cpu().long(), K.cpu(), v.cpu())
+    assert rel(y_node, y_o) < 1e-14 and rel(y_csr, y_o) < 1e-14
+    b = (-R).contiguous()
+    xs = {}
+    for mode in ("node", "csr"):
+        x = torch.zeros_like(b)
+        it, rr, st = P.pcg(K, b, x, 1e-26, 20000, generic=(mode == "csr"))
+        assert st == 0 and rr < 1e-26
+        xs[mode] = x
+    xd = O.direct_solve(P.indptr.cpu(), P.indices.cpu().long(), K.cpu(), b.cpu())
+    assert rel(xs["node"], xd) < 1e-9 and rel(xs["csr"], xd) < 1e-9
+    x2 = torch.zeros_like(b)
+    it2, outer, rr2, st2 = P.pcg_mixed(K, P.to_f32(K), b, x2, 1e-24, 1e-6, 20000)
+    assert st2 == 0 and rel(x2, xd) < 1e-9
+
+
 def test_reference_conjugate_gradient_semantics(golden):
     """_linear_solver.conjugate_gradient: plain CG on a COO input, squared-ratio stop test."""
     import fea_b200 as F
