@@ -158,52 +158,87 @@ __global__ void __launch_bounds__(PCG_TPB) k_spmv_node(NodeOp<V> A, const X* __r
   if (mode == 1 && st[S_DONE] != 0.0) return;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
+  const int64_t step = (int64_t)gridDim.x * PCG_WARPS;
   double contrib = 0.0;
-  for (int64_t nd = (int64_t)blockIdx.x * PCG_WARPS + warp; nd < A.n_nodes; nd += (int64_t)gridDim.x * PCG_WARPS) {
-    const unsigned m = A.mask[nd];
-    if (!m) continue;                              // warp-uniform
-    const int f = popc3(m);
-    const int L = A.rowlen[nd];
-    const int64_t vb = A.vbase[nd];
-    const int32_t* __restrict__ ci = A.idx + vb;   // shared column list of the f rows
-    const V* __restrict__ v0 = A.val + vb;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-    // 96 columns per pass: indices, then gathers, then values, three deep
-    for (int q0 = 0; q0 < L; q0 += 96) {
-      const int qa = q0 + lane, qb = qa + 32, qc = qa + 64;
-      const bool ha = qa < L, hb = qb < L, hc = qc < L;
-      const int32_t ja = ha ? __ldg(ci + qa) : 0;
-      const int32_t jb = hb ? __ldg(ci + qb) : 0;
-      const int32_t jc = hc ? __ldg(ci + qc) : 0;
-      const double xa = ha ? (double)x[ja] : 0.0;
-      const double xb = hb ? (double)x[jb] : 0.0;
-      const double xc = hc ? (double)x[jc] : 0.0;
-      s0 += (ha ? (double)__ldcs(v0 + qa) : 0.0) * xa + (hb ? (double)__ldcs(v0 + qb) : 0.0) * xb +
-            (hc ? (double)__ldcs(v0 + qc) : 0.0) * xc;
-      if (f > 1) {
-        const V* v1 = v0 + L;
-        s1 += (ha ? (double)__ldcs(v1 + qa) : 0.0) * xa + (hb ? (double)__ldcs(v1 + qb) : 0.0) * xb +
-              (hc ? (double)__ldcs(v1 + qc) : 0.0) * xc;
-      }
-      if (f > 2) {
-        const V* v2 = v0 + 2 * (int64_t)L;
-        s2 += (ha ? (double)__ldcs(v2 + qa) : 0.0) * xa + (hb ? (double)__ldcs(v2 + qb) : 0.0) * xb +
-              (hc ? (double)__ldcs(v2 + qc) : 0.0) * xc;
-      }
-    }
+  // One warp walks nodes nd, nd + step, ...  The metadata and the first 96
+  // column indices of the next node are loaded while the current node is
+  // processed, so its gathers of x need not wait for a DRAM round trip.
+  int64_t nd = (int64_t)blockIdx.x * PCG_WARPS + warp;
+  unsigned m = 0;
+  int L = 0;
+  int64_t vb = 0;
+  int32_t jn[3] = {0, 0, 0};
+  if (nd < A.n_nodes) {
+    m = A.mask[nd];
+    L = m ? A.rowlen[nd] : 0;
+    vb = A.vbase[nd];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    for (int k = 0; k < 3; ++k) jn[k] = lane + 32 * k < L ? __ldg(A.idx + vb + lane + 32 * k) : 0;
+  }
+  while (nd < A.n_nodes) {
+    const int64_t nx = nd + step;
+    unsigned m2 = 0;
+    int L2 = 0;
+    int64_t vb2 = 0;
+    if (nx < A.n_nodes) {
+      m2 = A.mask[nx];
+      L2 = A.rowlen[nx];
+      vb2 = A.vbase[nx];
     }
-    if (lane == 0) {
-      const int64_t r = A.dbase[nd];
-      y[r] = (X)s0;
-      contrib += s0 * (double)x[r];
-      if (f > 1) { y[r + 1] = (X)s1; contrib += s1 * (double)x[r + 1]; }
-      if (f > 2) { y[r + 2] = (X)s2; contrib += s2 * (double)x[r + 2]; }
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    const int f = popc3(m);
+    if (m) {                                        // warp-uniform
+      const V* __restrict__ v0 = A.val + vb;
+      // 96 columns per pass: values issued first, then the gathers of x
+      // (L2-resident), then the FMAs
+      for (int q0 = 0; q0 < L; q0 += 96) {
+        int32_t j[3];
+        bool h[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const int q = q0 + lane + 32 * k;
+          h[k] = q < L;
+          j[k] = q0 == 0 ? jn[k] : (h[k] ? __ldg(A.idx + vb + q) : 0);
+        }
+        double va[3][3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const int q = q0 + lane + 32 * k;
+            va[r][k] = (r < f && h[k]) ? (double)__ldcs(v0 + (int64_t)r * L + q) : 0.0;
+          }
+        double xv[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) xv[k] = h[k] ? (double)x[j[k]] : 0.0;
+        s0 += va[0][0] * xv[0] + va[0][1] * xv[1] + va[0][2] * xv[2];
+        s1 += va[1][0] * xv[0] + va[1][1] * xv[1] + va[1][2] * xv[2];
+        s2 += va[2][0] * xv[0] + va[2][1] * xv[1] + va[2][2] * xv[2];
+      }
     }
+    // column indices of the next node's first pass
+    const int Ln = m2 ? L2 : 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) jn[k] = lane + 32 * k < Ln ? __ldg(A.idx + vb2 + lane + 32 * k) : 0;
+    if (m) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      }
+      if (lane == 0) {
+        const int64_t r = A.dbase[nd];
+        y[r] = (X)s0;
+        contrib += s0 * (double)x[r];
+        if (f > 1) { y[r + 1] = (X)s1; contrib += s1 * (double)x[r + 1]; }
+        if (f > 2) { y[r + 2] = (X)s2; contrib += s2 * (double)x[r + 2]; }
+      }
+    }
+    nd = nx;
+    m = m2;
+    L = Ln;
+    vb = vb2;
   }
   if (mode == 1) finish_pq(contrib, st, part, counter);
 }
