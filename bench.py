@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -52,11 +53,20 @@ def args_():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
-    ap.add_argument("--workload", default="assembly", choices=["assembly", "pcg", "explicit", "newton"],
+    ap.add_argument("--workload", default="assembly", choices=["assembly", "pcg", "explicit", "newton", "adjoint", "serving"],
                     help="assembly (default, the headline line) or one of the other measured forms")
     ap.add_argument("--explicit-n", type=int, default=70, help="cells per side of the Kuhn-tet cube")
     ap.add_argument("--explicit-steps", type=int, default=10000)
     ap.add_argument("--pcg-max-iter", type=int, default=50000, help="iteration cap of each PCG solve")
+    ap.add_argument("--adjoint-n", type=int, default=40, help="elements per side of the compliance block")
+    ap.add_argument("--fd-samples", type=int, default=200, help="coordinates checked by central differences")
+    ap.add_argument("--serve-requests", type=int, default=512)
+    ap.add_argument("--serve-rates", default="inf", help="comma-separated Poisson arrival rates (requests/s)")
+    ap.add_argument("--serve-min-elems", type=int, default=2000)
+    ap.add_argument("--serve-max-elems", type=int, default=200000)
+    ap.add_argument("--serve-slots", type=int, default=32)
+    ap.add_argument("--serve-round", type=int, default=32, help="PCG iterations per captured round")
+    ap.add_argument("--serve-plain", type=int, default=1, help="also time the one-at-a-time path")
     return ap.parse_args()
 
 
@@ -346,6 +356,149 @@ def run_newton(a):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(a):
+    """Compliance f.u of an n^3 C3D8 block (mu = 1, kappa = 50, bottom face
+    z = 0 clamped, pressure 0.03 on the top face): gradients w.r.t. all
+    nodal coordinates and mu from the hand-written adjoint behind
+    ComplianceFunction; checked against central differences (h = 1e-6) on
+    seeded random coordinates and against torch autograd of the oracle's
+    residual (lam . dR/dX)."""
+    import torch
+    import fea_b200 as F
+    from fea_b200 import adjoint, meshes
+    from oracle import fea_oracle as O
+    n = a.adjoint_n
+    X, el = meshes.hex_block(n)
+    E, N = el.shape[0], X.shape[0]
+    top = np.nonzero(np.arange(E) % n == n - 1)[0]
+    clamp = np.nonzero(np.arange(N) % (n + 1) == 0)[0]
+    part = F.Part(X)
+    e = F.elements.C3D8(elems=el, elems_index=np.arange(E), part=part)
+    e.set_materials(F.materials.NeoHookean(1.0, 50.0))
+    part.add_element(e)
+    part.set_nodes["bottom"] = clamp
+    part.add_surface_set("top", [(top, 1)])
+    asm = F.Assembly()
+    asm.add_part(part, "block")
+    asm.add_instance(F.Instance(part), "block")
+    asm.add_load(F.loads.Pressure("block", "top", 0.03), "pressure")
+    asm.add_boundary(F.boundarys.Boundary_Condition("block", "bottom"), "clamp")
+    asm.initialize()
+    solver = F.solver.StaticImplicitSolver(rtol=1e-12, maximum_iteration=80)
+    solver.initialize(asm)
+    # forward solve + adjoint through the autograd Function
+    Xt = torch.from_numpy(X).clone().requires_grad_(True)
+    mu = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    C = adjoint.ComplianceFunction.apply(Xt, mu, asm, solver)
+    C.backward()
+    torch.cuda.synchronize()
+    t_full = time.perf_counter() - t0
+    newton_iters = len(solver.history)
+    gstar = asm.GC.clone()
+    # adjoint gradient alone at the equilibrium (adjoint PCG + VJP kernels)
+    reps = 5
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        Cg, dX, dmu, it_adj, lam = adjoint.compliance_gradient(asm, gstar, return_lambda=True)
+    torch.cuda.synchronize()
+    t_grad = (time.perf_counter() - t0) / reps
+    gX = dX.cpu()
+    scale = float(gX.abs().max())
+    # central differences, warm-started from the equilibrium
+    def comp(Xn, mu_v=1.0):
+        adjoint.set_coordinates(asm, Xn)
+        asm._mat_elems[0].materials.mu = torch.tensor(mu_v, dtype=torch.float64)
+        gc = solver.solve(GC0=gstar.clone())
+        if isinstance(gc, bool):
+            raise RuntimeError("equilibrium solve failed")
+        return float(torch.dot(adjoint.external_force(asm, gc), gc))
+    h = 1e-6
+    rng = np.random.default_rng(0)
+    free_nodes = np.setdiff1d(np.arange(N), clamp)
+    nodes = rng.choice(free_nodes, size=a.fd_samples, replace=False)
+    comps = rng.integers(0, 3, size=a.fd_samples)
+    X0 = torch.from_numpy(X).clone()
+    errs, raw = [], []
+    t0 = time.perf_counter()
+    for nd, k in zip(nodes, comps):
+        Xp = X0.clone(); Xp[nd, k] += h
+        Xm = X0.clone(); Xm[nd, k] -= h
+        fd = (comp(Xp) - comp(Xm)) / (2 * h)
+        ad = float(gX[nd, k])
+        errs.append(abs(fd - ad) / max(abs(ad), 1e-2 * scale))
+        if abs(ad) >= 1e-2 * scale:
+            raw.append(abs(fd - ad) / abs(ad))
+    fd_mu = (comp(X0, 1.0 + h) - comp(X0, 1.0 - h)) / (2 * h)
+    t_fd = time.perf_counter() - t0
+    comp(X0, 1.0)
+    # lam . dR/dX of the kernels against torch autograd of the oracle residual
+    dXk, _ = adjoint.residual_vjp(asm, gstar, lam)
+    Xo = torch.from_numpy(X).clone().requires_grad_(True)
+    faces = torch.from_numpy(el[top][:, [4, 5, 6, 7]])
+    m = O.Model(Xo, [O.Group("C3D8", torch.from_numpy(el), 1.0, 50.0)], [O.PressureLoad(faces, 0.03)],
+                [(clamp, (0, 1, 2))])
+    Ro, _ = m.assemble(gstar.cpu(), want_K=False)
+    (Ro * lam.cpu()).sum().backward()
+    auto_rel = float((dXk.cpu() - Xo.grad).norm() / Xo.grad.norm())
+    line = {"metric": "compliance gradient evals/s (%d^3 C3D8, dC/dX all nodes + dC/dmu)" % n,
+            "value": 1.0 / t_grad, "unit": "evals/s", "higher_is_better": True, "workload": "adjoint",
+            "elements": E, "ndof": asm.plan.ndof, "compliance": float(Cg),
+            "gradient_s": t_grad, "adjoint_pcg_iters": it_adj,
+            "forward_plus_backward_s": t_full, "forward_newton_iters": newton_iters,
+            "fd_samples": int(a.fd_samples), "fd_step": h, "fd_seconds": t_fd,
+            "fd_max_rel_err": max(errs), "fd_max_rel_err_components_above_1pct": max(raw) if raw else None,
+            "fd_components_above_1pct": len(raw),
+            "dmu_adjoint": float(dmu[0]), "dmu_fd": fd_mu, "dmu_rel_err": abs(fd_mu - float(dmu[0])) / abs(float(dmu[0])),
+            "vjp_vs_oracle_autograd_rel": auto_rel}
+    print(json.dumps(line), flush=True)
+
+
+def run_serving(a):
+    """Stream of seeded cantilever static solves (C3D4, Newton to 1e-8):
+    solves/s and p50/p99 latency of the continuous-batching server against
+    solving the same requests one at a time through StaticImplicitSolver."""
+    import torch
+    from fea_b200 import serving
+    out = []
+    for rate in [float(x) for x in a.serve_rates.split(",")]:
+        reqs = serving.make_requests(a.serve_requests, rate, seed=0, min_elems=a.serve_min_elems,
+                                     max_elems=a.serve_max_elems)
+        if not math.isfinite(rate):
+            for r in reqs:
+                r.arrival = 0.0
+
+        def summary(res, wall):
+            lat = np.array([r.latency for r in res])
+            span = max(r.done for r in res) - min(r.arrival for r in res)
+            return {"solves_per_s": len(res) / span, "p50_s": float(np.percentile(lat, 50)),
+                    "p99_s": float(np.percentile(lat, 99)), "makespan_s": span, "wall_s": wall,
+                    "newton_iters": int(sum(r.newton_iters for r in res)), "pcg_iters": int(sum(r.pcg_iters for r in res))}
+        # warm-up: one small request through both paths
+        w = serving.make_requests(1, float("inf"), seed=99, min_elems=2000, max_elems=2000)
+        w[0].arrival = 0.0
+        serving.serve(w, max_slots=a.serve_slots, round_iters=a.serve_round, keep=False)
+        serving.solve_plain(w, keep=False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        served, stats = serving.serve(reqs, max_slots=a.serve_slots, round_iters=a.serve_round)
+        rec = {"rate_per_s": rate, "served": summary(served, time.perf_counter() - t0), "server": stats}
+        if a.serve_plain:
+            t0 = time.perf_counter()
+            plain = serving.solve_plain(reqs)
+            rec["plain"] = summary(plain, time.perf_counter() - t0)
+            rec["speedup_solves_per_s"] = rec["served"]["solves_per_s"] / rec["plain"]["solves_per_s"]
+            rec["max_rel_diff_served_vs_plain"] = max(float((x.gc - y.gc).norm() / y.gc.norm())
+                                                      for x, y in zip(served, plain))
+        out.append(rec)
+    line = {"metric": "served static solves/s (C3D4 cantilevers, Newton to 1e-8)", "unit": "solves/s",
+            "value": out[0]["served"]["solves_per_s"], "higher_is_better": True, "workload": "serving",
+            "requests": a.serve_requests, "elems": [a.serve_min_elems, a.serve_max_elems], "runs": out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = args_()
     if a.impl == "reference":
@@ -354,7 +507,8 @@ def main():
     if a.workload != "assembly":
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        {"pcg": run_pcg, "explicit": run_explicit, "newton": run_newton}[a.workload](a)
+        {"pcg": run_pcg, "explicit": run_explicit, "newton": run_newton, "adjoint": run_adjoint,
+         "serving": run_serving}[a.workload](a)
         return
     import torch
     import torch.distributed as dist

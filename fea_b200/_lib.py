@@ -68,6 +68,12 @@ class Group(C.Structure):
                 ("smem_doubles", C.c_int64)]
 
 
+class PcgbSlot(C.Structure):
+    _fields_ = [("n", C.c_int64), ("nnz", C.c_int64), ("indptr_dev", C.c_void_p), ("indices_dev", C.c_void_p),
+                ("values_dev", C.c_void_p), ("b_dev", C.c_void_p), ("x_dev", C.c_void_p), ("work_dev", C.c_void_p),
+                ("work_len", C.c_int64), ("tol", C.c_double), ("max_iter", C.c_int32), ("active", C.c_int32)]
+
+
 P = C.c_void_p
 I32, I64, D = C.c_int32, C.c_int64, C.c_double
 NP, GP = C.POINTER(Nodes), C.POINTER(Group)
@@ -105,6 +111,12 @@ fea_pcg_solve_nodes = _sig("fea_pcg_solve_nodes", I32, NP, P, P, P, P, D, I32, I
 fea_pcg_solve_mixed_nodes = _sig("fea_pcg_solve_mixed_nodes", I32, NP, P, P, P, P, P, D, D, I32, I32, P, I64,
                                  C.POINTER(I32), C.POINTER(I32), C.POINTER(D), P)
 fea_convert_f32 = _sig("fea_convert_f32", I32, I64, P, P, P)
+fea_pcgb_work_len = _sig("fea_pcgb_work_len", I64, I64)
+fea_pcgb_table_bytes = _sig("fea_pcgb_table_bytes", I64, I32, I64)
+fea_pcgb_set = _sig("fea_pcgb_set", I32, P, I32, I64, I32, C.POINTER(PcgbSlot), P)
+fea_pcgb_start = _sig("fea_pcgb_start", I32, P, I32, I64, I32, I64, I64, P)
+fea_pcgb_iterate = _sig("fea_pcgb_iterate", I32, P, I32, I64, I32, P)
+fea_pcgb_state = _sig("fea_pcgb_state", I32, P, I32, I32, P, P)
 fea_explicit_work_len = _sig("fea_explicit_work_len", I64, I64)
 fea_explicit_run = _sig("fea_explicit_run", I32, NP, GP, D, D, P, D, I64, I32, I32, P, P, P, P, P, I64, P)
 fea_adjoint_vjp_volume = _sig("fea_adjoint_vjp_volume", I32, NP, GP, D, D, P, P, P, P, P, I64, P)
@@ -116,5 +128,6 @@ fea_launch_count = _sig("fea_launch_count", I64)
 EXPORTED = ["fea_plan_build", "fea_plan_free", "fea_plan_get", "fea_assemble_work_len", "fea_assemble_volume", "fea_assemble_pressure",
             "fea_reduce_scratch_len", "fea_energy_volume", "fea_energy_volume_noalloc", "fea_energy_pressure", "fea_lumped_mass",
             "fea_invert_mass", "fea_pcg_work_len", "fea_pcg_solve", "fea_pcg_mixed_work_len",
-            "fea_pcg_solve_mixed", "fea_spmv", "fea_spmv_nodes", "fea_pcg_solve_nodes", "fea_pcg_solve_mixed_nodes", "fea_convert_f32", "fea_explicit_work_len", "fea_explicit_run",
+            "fea_pcg_solve_mixed", "fea_spmv", "fea_spmv_nodes", "fea_pcg_solve_nodes", "fea_pcg_solve_mixed_nodes", "fea_convert_f32", "fea_pcgb_work_len", "fea_pcgb_table_bytes", "fea_pcgb_set", "fea_pcgb_start",
+            "fea_pcgb_iterate", "fea_pcgb_state", "fea_explicit_work_len", "fea_explicit_run",
             "fea_adjoint_vjp_volume", "fea_adjoint_hvp_pressure", "fea_version", "fea_launch_count"]

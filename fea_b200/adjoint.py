@@ -66,9 +66,9 @@ def external_force(asm, GC):
     return -Rp
 
 
-def compliance_gradient(asm, GC, pcg_tol=1e-26, pcg_max_iter=200000):
+def compliance_gradient(asm, GC, pcg_tol=1e-26, pcg_max_iter=200000, return_lambda=False):
     """(C, dC/dX [N_total, 3], [dC/dmu per group], adjoint iterations) at an
-    equilibrium GC."""
+    equilibrium GC; with return_lambda, the adjoint field is appended."""
     P = asm.plan
     gc = asm._gc(GC=GC)
     R, K = asm.assemble_csr(gc)
@@ -81,6 +81,8 @@ def compliance_gradient(asm, GC, pcg_tol=1e-26, pcg_max_iter=200000):
     it, rr, st = P.pcg(K, rhs, lam, pcg_tol, pcg_max_iter, check_every=50)
     dX, dmu = residual_vjp(asm, gc, lam)
     dCdX = -(dX + Hu)
+    if return_lambda:
+        return C, dCdX, [-d for d in dmu], it, lam
     return C, dCdX, [-d for d in dmu], it
 
 

@@ -24,7 +24,9 @@
 //            column indices and gathers x once for all f rows, so index
 //            traffic is nnz / f * 4 bytes instead of nnz * 4.
 #include <cmath>
+#include <cstring>
 #include <mutex>
+#include <vector>
 #include <unordered_map>
 
 #include "common.cuh"
@@ -605,6 +607,250 @@ static int read_nnz(const int64_t* ip, int64_t n, int64_t* nnz, cudaStream_t s) 
   return (int)cudaStreamSynchronize(s);
 }
 
+// ---- batched PCG over independent systems ("slots") ---------------------
+// Every slot's rows are cut into chunks of PCGB_ROWS consecutive rows; one CTA
+// processes one chunk at a time (grid-stride over the chunk list of all
+// active slots), and each slot keeps its own scalars, partial sums (one per
+// chunk) and completion counter.  A slot's arithmetic depends only on its
+// own chunking, so its iterates are the same bits whether it runs alone or
+// beside other slots.
+constexpr int PCGB_ROWS = 256;
+
+struct PcgbSlotDev {
+  const int64_t* ptr;
+  const int32_t* idx;
+  const double* val;
+  const double* b;
+  double* x;
+  double* st;
+  unsigned* counter;
+  double *dinv, *r, *z, *p, *q, *part;
+  int64_t n;
+  int32_t nchunk, lanes;
+  double tol;
+  int32_t max_iter, pad;
+};
+
+struct PcgbHeader {
+  int64_t nchunks;
+  int64_t nslots;
+};
+
+struct PcgbView {
+  PcgbHeader* hdr;
+  PcgbSlotDev* slots;
+  int32_t* chunk_slot;
+  int32_t* chunk_local;
+};
+
+static PcgbView pcgb_view(void* table, int32_t max_slots) {
+  PcgbView v;
+  char* c = (char*)table;
+  v.hdr = (PcgbHeader*)c;
+  v.slots = (PcgbSlotDev*)(c + 64);
+  v.chunk_slot = (int32_t*)(c + 64 + sizeof(PcgbSlotDev) * (size_t)max_slots);
+  return v;
+}
+
+static int64_t pcgb_slot_chunks(int64_t n) { return (n + PCGB_ROWS - 1) / PCGB_ROWS; }
+
+// rows of one chunk, LANES threads per row: q = A p, returns this thread's p.q share
+template <int LANES>
+__device__ __forceinline__ double pcgb_rows_spmv(const PcgbSlotDev& S, int64_t row0) {
+  constexpr int RPP = PCG_TPB / LANES;           // rows per pass
+  const int lane = threadIdx.x % LANES;
+  const int sub = threadIdx.x / LANES;
+  double contrib = 0.0;
+  for (int k = 0; k < PCGB_ROWS; k += RPP) {
+    const int64_t row = row0 + k + sub;
+    double s = 0.0;
+    if (row < S.n) {
+      const int64_t b = S.ptr[row], e = S.ptr[row + 1];
+      for (int64_t i = b + lane; i < e; i += LANES) s += S.val[i] * S.p[S.idx[i]];
+    }
+#pragma unroll
+    for (int o = LANES / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, LANES);
+    if (row < S.n && lane == 0) {
+      S.q[row] = s;
+      contrib += s * S.p[row];
+    }
+  }
+  return contrib;
+}
+
+__device__ __forceinline__ bool pcgb_last(unsigned* counter, int nchunk) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == (unsigned)(nchunk - 1);
+  __syncthreads();
+  return last;
+}
+
+__global__ void __launch_bounds__(PCG_TPB) k_pcgb_spmv(PcgbView V) {
+  __shared__ double sh[PCG_WARPS];
+  const int64_t nch = V.hdr->nchunks;
+  for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
+    const PcgbSlotDev& S = V.slots[V.chunk_slot[c]];
+    if (S.st[S_DONE] != 0.0) continue;            // block-uniform
+    const int local = V.chunk_local[c];
+    const int64_t row0 = (int64_t)local * PCGB_ROWS;
+    double contrib;
+    if (S.lanes == 32) contrib = pcgb_rows_spmv<32>(S, row0);
+    else if (S.lanes == 16) contrib = pcgb_rows_spmv<16>(S, row0);
+    else contrib = pcgb_rows_spmv<8>(S, row0);
+    const double bs = block_sum_w(contrib, sh);
+    if (threadIdx.x == 0) S.part[local] = bs;
+    if (pcgb_last(S.counter, S.nchunk)) {
+      const double pq = sum_partials(S.part, S.nchunk, 1, 0, sh);
+      if (threadIdx.x == 0) {
+        S.st[S_PQ] = pq;
+        if (!(pq > 0.0) || !isfinite(pq)) {
+          S.st[S_STATUS] = (double)FEA_EBREAKDOWN;
+          S.st[S_DONE] = 1.0;
+          S.st[S_ALPHA] = 0.0;
+        } else {
+          S.st[S_ALPHA] = S.st[S_RZ] / pq;
+        }
+        *S.counter = 0u;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(PCG_TPB) k_pcgb_update(PcgbView V) {
+  __shared__ double sh[PCG_WARPS];
+  const int64_t nch = V.hdr->nchunks;
+  for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
+    const PcgbSlotDev& S = V.slots[V.chunk_slot[c]];
+    if (S.st[S_DONE] != 0.0) continue;
+    const int local = V.chunk_local[c];
+    const int64_t i = (int64_t)local * PCGB_ROWS + threadIdx.x;
+    const double alpha = S.st[S_ALPHA];
+    double contrib = 0.0;
+    if (i < S.n) {
+      S.x[i] += alpha * S.p[i];
+      const double ri = S.r[i] - alpha * S.q[i];
+      S.r[i] = ri;
+      const double zi = ri * S.dinv[i];
+      S.z[i] = zi;
+      contrib = ri * zi;
+    }
+    const double bs = block_sum_w(contrib, sh);
+    if (threadIdx.x == 0) S.part[local] = bs;
+    if (pcgb_last(S.counter, S.nchunk)) {
+      const double rz = sum_partials(S.part, S.nchunk, 1, 0, sh);
+      if (threadIdx.x == 0) {
+        const double it = S.st[S_ITER] + 1.0;
+        S.st[S_ITER] = it;
+        S.st[S_BETA] = rz / S.st[S_RZ];
+        S.st[S_RZ] = rz;
+        if (!isfinite(rz)) {
+          S.st[S_STATUS] = (double)FEA_EBREAKDOWN;
+          S.st[S_DONE] = 1.0;
+        } else if (rz / S.st[S_RZ0] < S.tol) {
+          S.st[S_DONE] = 1.0;
+        } else if (it >= (double)S.max_iter) {
+          S.st[S_STATUS] = (double)FEA_ENOTCONV;
+          S.st[S_DONE] = 1.0;
+        }
+        *S.counter = 0u;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(PCG_TPB) k_pcgb_p(PcgbView V) {
+  const int64_t nch = V.hdr->nchunks;
+  for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
+    const PcgbSlotDev& S = V.slots[V.chunk_slot[c]];
+    if (S.st[S_DONE] != 0.0) continue;
+    const int64_t i = (int64_t)V.chunk_local[c] * PCGB_ROWS + threadIdx.x;
+    if (i < S.n) S.p[i] = S.z[i] + S.st[S_BETA] * S.p[i];
+  }
+}
+
+// start of one slot: dinv, r = b - A x, z, p, r.z and b.dinv.b; one CTA per chunk
+template <int LANES>
+__device__ __forceinline__ double pcgb_row_ax(const PcgbSlotDev& S, int64_t row, int lane) {
+  double s = 0.0;
+  if (row < S.n) {
+    const int64_t b = S.ptr[row], e = S.ptr[row + 1];
+    for (int64_t i = b + lane; i < e; i += LANES) s += S.val[i] * S.x[S.idx[i]];
+  }
+#pragma unroll
+  for (int o = LANES / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, LANES);
+  return s;
+}
+
+template <int LANES>
+__global__ void __launch_bounds__(PCG_TPB) k_pcgb_start(PcgbView V, int32_t slot) {
+  __shared__ double sh[PCG_WARPS];
+  const PcgbSlotDev& S = V.slots[slot];
+  constexpr int RPP = PCG_TPB / LANES;
+  const int lane = threadIdx.x % LANES, sub = threadIdx.x / LANES;
+  const int64_t row0 = (int64_t)blockIdx.x * PCGB_ROWS;
+  // r = A x (into r)
+  for (int k = 0; k < PCGB_ROWS; k += RPP) {
+    const int64_t row = row0 + k + sub;
+    const double s = pcgb_row_ax<LANES>(S, row, lane);
+    if (row < S.n && lane == 0) S.r[row] = s;
+  }
+  __syncthreads();
+  double c_rz = 0.0, c_bb = 0.0;
+  const int64_t i = row0 + threadIdx.x;
+  if (i < S.n) {
+    int64_t lo = S.ptr[i], hi = S.ptr[i + 1];
+    double dv = 0.0;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      const int32_t c = S.idx[mid];
+      if (c == i) { dv = S.val[mid]; break; }
+      if (c < i) lo = mid + 1; else hi = mid;
+    }
+    dv = fabs(dv);
+    const double di = dv == 0.0 ? 1.0 : 1.0 / dv;
+    S.dinv[i] = di;
+    const double ri = S.b[i] - S.r[i];
+    S.r[i] = ri;
+    const double zi = ri * di;
+    S.z[i] = zi;
+    S.p[i] = zi;
+    c_rz = ri * zi;
+    c_bb = S.b[i] * S.b[i] * di;
+  }
+  const double s1 = block_sum_w(c_rz, sh);
+  const double s2 = block_sum_w(c_bb, sh);
+  if (threadIdx.x == 0) {
+    S.part[2 * blockIdx.x] = s1;
+    S.part[2 * blockIdx.x + 1] = s2;
+  }
+  if (pcgb_last(S.counter, S.nchunk)) {
+    const double rz = sum_partials(S.part, S.nchunk, 2, 0, sh);
+    const double bb = sum_partials(S.part, S.nchunk, 2, 1, sh);
+    if (threadIdx.x == 0) {
+      S.st[S_RZ] = rz;
+      S.st[S_RZ0] = bb == 0.0 ? 1.0 : bb;
+      S.st[S_ITER] = 0.0;
+      S.st[S_STATUS] = 0.0;
+      S.st[S_DONE] = (bb == 0.0 || rz == 0.0 || rz / (bb == 0.0 ? 1.0 : bb) < S.tol || S.max_iter <= 0) ? 1.0 : 0.0;
+      *S.counter = 0u;
+    }
+  }
+}
+
+// compact per-slot state for the host: done, iterations, status, r.z / b.b
+__global__ void k_pcgb_state(PcgbView V, int32_t nslots, double* out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots) return;
+  const double* st = V.slots[s].st;
+  if (!st) return;
+  out[4 * s + 0] = st[S_DONE];
+  out[4 * s + 1] = st[S_ITER];
+  out[4 * s + 2] = st[S_STATUS];
+  out[4 * s + 3] = st[S_RZ] / st[S_RZ0];
+}
+
 }  // namespace fea
 
 using namespace fea;
@@ -697,4 +943,105 @@ extern "C" int fea_pcg_solve_mixed_nodes(const fea_nodes_t* N, const int32_t* ix
   if (n == 0) return FEA_OK;
   return pcg_mixed(node_op<double>(N, ix, v), node_op<float>(N, ix, v32), n, b, x, tol, inner_tol, max_iter,
                    check_every, work, iters, outer, relres, s);
+}
+
+// ---- batched PCG C ABI ------------------------------------------------------
+extern "C" int64_t fea_pcgb_work_len(int64_t n) {
+  return S_LEN + 2 + 5 * n + 2 * pcgb_slot_chunks(n) + 2;
+}
+
+extern "C" int64_t fea_pcgb_table_bytes(int32_t max_slots, int64_t max_chunks) {
+  if (max_slots <= 0 || max_chunks <= 0) return 0;
+  return 64 + (int64_t)sizeof(PcgbSlotDev) * max_slots + 8 * max_chunks;
+}
+
+extern "C" int fea_pcgb_set(void* table, int32_t max_slots, int64_t max_chunks, int32_t nslots,
+                            const fea_pcgb_slot_t* slots, cudaStream_t s) {
+  if (!table || max_slots <= 0 || max_chunks <= 0 || nslots < 0 || nslots > max_slots || (nslots && !slots))
+    return FEA_EINVAL;
+  std::vector<PcgbSlotDev> dev(nslots);
+  std::vector<int32_t> cs, cl;
+  for (int32_t k = 0; k < nslots; ++k) {
+    const fea_pcgb_slot_t& h = slots[k];
+    PcgbSlotDev& d = dev[k];
+    std::memset(&d, 0, sizeof(d));
+    if (h.n < 0) return FEA_EINVAL;
+    if (!h.work_dev) continue;                       // empty slot
+    if (h.n > 0 && (!h.indptr_dev || !h.indices_dev || !h.values_dev || !h.b_dev || !h.x_dev)) return FEA_EINVAL;
+    if (h.work_len < fea_pcgb_work_len(h.n)) return FEA_EWORK;
+    if (pcgb_slot_chunks(h.n) >= INT32_MAX) return FEA_ERANGE;
+    double* w = h.work_dev;
+    d.ptr = h.indptr_dev; d.idx = h.indices_dev; d.val = h.values_dev; d.b = h.b_dev; d.x = h.x_dev;
+    d.st = w;
+    d.counter = (unsigned*)(w + S_LEN);
+    d.dinv = w + S_LEN + 2;
+    d.r = d.dinv + h.n; d.z = d.r + h.n; d.p = d.z + h.n; d.q = d.p + h.n; d.part = d.q + h.n;
+    d.n = h.n;
+    d.nchunk = (int32_t)pcgb_slot_chunks(h.n);
+    d.lanes = 8;
+    if (h.n > 0 && h.nnz > 0) d.lanes = lanes_for(h.n, h.nnz);
+    d.tol = h.tol;
+    d.max_iter = h.max_iter;
+    if (h.active)
+      for (int32_t c = 0; c < d.nchunk; ++c) { cs.push_back(k); cl.push_back(c); }
+    // completion counters are zero between kernels; a new work buffer starts so
+    if (cudaError_t e = cudaMemsetAsync(d.counter, 0, 2 * sizeof(unsigned), s)) return (int)e;
+  }
+  if ((int64_t)cs.size() > max_chunks) return FEA_ERANGE;
+  PcgbView V = pcgb_view(table, max_slots);
+  V.chunk_local = V.chunk_slot + max_chunks;
+  PcgbHeader hdr{(int64_t)cs.size(), (int64_t)nslots};
+  if (cudaError_t e = cudaMemcpyAsync(V.hdr, &hdr, sizeof(hdr), cudaMemcpyHostToDevice, s)) return (int)e;
+  if (nslots)
+    if (cudaError_t e = cudaMemcpyAsync(V.slots, dev.data(), sizeof(PcgbSlotDev) * nslots, cudaMemcpyHostToDevice, s))
+      return (int)e;
+  if (!cs.empty()) {
+    if (cudaError_t e = cudaMemcpyAsync(V.chunk_slot, cs.data(), 4 * cs.size(), cudaMemcpyHostToDevice, s))
+      return (int)e;
+    if (cudaError_t e = cudaMemcpyAsync(V.chunk_local, cl.data(), 4 * cl.size(), cudaMemcpyHostToDevice, s))
+      return (int)e;
+  }
+  // the host vectors above are released on return: finish the copies first
+  return (int)cudaStreamSynchronize(s);
+}
+
+extern "C" int fea_pcgb_start(void* table, int32_t max_slots, int64_t max_chunks, int32_t slot, int64_t n,
+                              int64_t nnz, cudaStream_t s) {
+  if (!table || slot < 0 || slot >= max_slots || n < 0 || max_chunks <= 0) return FEA_EINVAL;
+  if (n == 0) return FEA_OK;
+  PcgbView V = pcgb_view(table, max_slots);
+  V.chunk_local = V.chunk_slot + max_chunks;
+  const int L = lanes_for(n, nnz);
+  const unsigned grid = (unsigned)pcgb_slot_chunks(n);
+  // the slot's completion counter starts at zero
+  if (L == 32) k_pcgb_start<32><<<grid, PCG_TPB, 0, s>>>(V, slot);
+  else if (L == 16) k_pcgb_start<16><<<grid, PCG_TPB, 0, s>>>(V, slot);
+  else k_pcgb_start<8><<<grid, PCG_TPB, 0, s>>>(V, slot);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+extern "C" int fea_pcgb_iterate(void* table, int32_t max_slots, int64_t max_chunks, int32_t iters, cudaStream_t s) {
+  if (!table || max_slots <= 0 || max_chunks <= 0 || iters < 0) return FEA_EINVAL;
+  PcgbView V = pcgb_view(table, max_slots);
+  V.chunk_local = V.chunk_slot + max_chunks;
+  const unsigned grid = occ_grid(k_pcgb_spmv, max_chunks, 1);
+  const unsigned g2 = occ_grid(k_pcgb_update, max_chunks, 1);
+  const unsigned g3 = occ_grid(k_pcgb_p, max_chunks, 1);
+  for (int32_t k = 0; k < iters; ++k) {
+    k_pcgb_spmv<<<grid, PCG_TPB, 0, s>>>(V);
+    k_pcgb_update<<<g2, PCG_TPB, 0, s>>>(V);
+    k_pcgb_p<<<g3, PCG_TPB, 0, s>>>(V);
+    count_launch(3);
+  }
+  return (int)cudaGetLastError();
+}
+
+extern "C" int fea_pcgb_state(void* table, int32_t max_slots, int32_t nslots, double* out_dev, cudaStream_t s) {
+  if (!table || nslots < 0 || nslots > max_slots || (nslots && !out_dev)) return FEA_EINVAL;
+  if (!nslots) return FEA_OK;
+  PcgbView V = pcgb_view(table, max_slots);
+  k_pcgb_state<<<(nslots + 127) / 128, 128, 0, s>>>(V, nslots, out_dev);
+  count_launch();
+  return (int)cudaGetLastError();
 }

@@ -6,6 +6,8 @@
   unit-cube and explicit-dynamics workloads).
 - plane_faces: element faces lying on a coordinate plane, as surface-set
   entries (element labels, face id) plus the face node lists.
+- tet_beam: a Kuhn-split box of about a given number of C3D4 elements with
+  near-cubic cells (the serving workload's cantilevers).
 Node numbering is (i, j, k) lexicographic with k fastest.
 """
 from __future__ import annotations
@@ -70,3 +72,22 @@ def plane_faces(kind, elems, X, axis, value, tol=1e-9):
             sets.append((np.nonzero(m)[0], fid))
             faces.append(fn[m])
     return sets, (np.concatenate(faces) if faces else np.zeros((0, len(FACES[kind][0])), np.int64))
+
+
+def beam_dims(length, width, height, n_elems):
+    """Cells per side of tet_beam: about n_elems / 6 cells, as cubic as possible."""
+    cells = max(1.0, n_elems / 6.0)
+    s = (cells / (length * width * height)) ** (1.0 / 3.0)
+    return tuple(max(1, int(round(v * s))) for v in (length, width, height))
+
+
+def tet_beam(length, width, height, n_elems):
+    """C3D4 mesh of [1 - length, 1] x [-width/2, width/2] x [-height/2, height/2]
+    with about n_elems elements (6 per cell, cells as close to cubes as the
+    counts allow).  The free end x = 1 lies close to the origin but not
+    through it: the enclosed-volume pressure load inverts [x, x_xi, x_eta]
+    per face, which is singular for a face whose plane holds the origin."""
+    dims = beam_dims(length, width, height, n_elems)
+    X, el = tet_block(0, dims=dims, lengths=(length, width, height))
+    X = X - np.array([length - 1.0, width / 2.0, height / 2.0])
+    return X, el

@@ -25,6 +25,20 @@ import torch
 from . import _lib as L
 
 
+class LinearSolve:
+    """One tangent solve K x = b asked for by the Newton iteration: K in the
+    plan's CSR order, b, the warm start x (updated in place), the squared
+    scaled-residual tolerance and the iteration cap; the solver of the
+    request fills in iterations, relres and the status code."""
+
+    __slots__ = ("K", "b", "x", "x0", "tol", "cap", "tight", "it", "rr", "status")
+
+    def __init__(self, K, b, x, tol, cap, tight):
+        self.K, self.b, self.x, self.x0 = K, b, x, x.clone()
+        self.tol, self.cap, self.tight = tol, cap, tight
+        self.it, self.rr, self.status = 0, 0.0, L.FEA_OK
+
+
 class BaseSolver:
     def __init__(self) -> None:
         self.assembly = None
@@ -113,7 +127,22 @@ class StaticImplicitSolver(BaseSolver):
                 return 0.0, GC0.clone(), energy0
 
     def _solve_iteration(self, GC, tol_error):
-        """Newton loop (static_implicit.py:234-350); returns GC or False."""
+        """Newton loop (static_implicit.py:234-350); returns GC or False.
+        The linear solves asked for by the loop run on this device's PCG."""
+        gen = self._newton(GC, tol_error)
+        try:
+            req = next(gen)
+            while True:
+                self._run_linear(req)
+                req = gen.send(None)
+        except StopIteration as stop:
+            return stop.value
+
+    def _newton(self, GC, tol_error):
+        """The Newton loop as a generator: it yields a ``LinearSolve`` for each
+        tangent solve and resumes once the caller has filled in its result
+        (``_run_linear`` here; the batched engine of ``fea_b200.serving``
+        when many solves share the device).  Returns GC or False."""
         self._iter_now = 0
         energy = self.get_total_energy(GC)
         dGC = torch.zeros_like(GC)
@@ -134,7 +163,9 @@ class StaticImplicitSolver(BaseSolver):
                 break
             if self._at_floor(r_first):
                 break
-            dGC = self._solve_linear_equation(Kv, -R, self._iter_now, alpha, dGC)
+            req = self._linear_request(Kv, -R, self._iter_now, alpha, dGC)
+            yield req
+            dGC = self._linear_finish(req, Kv, -R)
             alpha, GCnew, energynew = self._line_search(GC, dGC, R, energy)
             self.history[-1].update(alpha=alpha)
             if alpha == 0 and rmax > tol_error and self.rtol is None:
@@ -170,11 +201,18 @@ class StaticImplicitSolver(BaseSolver):
 
     def _solve_linear_equation(self, K_values, R, iter_now=0, alpha0=None, dGC0=None, tol_error=None):
         """K dGC = R by device PCG, warm-started from the previous step (static_implicit.py:352-405)."""
-        P = self.assembly.plan
+        req = self._linear_request(K_values, R, iter_now, alpha0, dGC0)
+        self._run_linear(req)
+        return self._linear_finish(req, K_values, R)
+
+    def _linear_request(self, K_values, R, iter_now=0, alpha0=None, dGC0=None):
+        """The PCG tolerance and cap for this Newton iteration: loose solves
+        far from equilibrium, a tight solve where the reference switches to
+        its exact solver (scaled residual below 1e-3, or repeated small
+        steps, static_implicit.py:384-388)."""
         x = (torch.zeros_like(R) if dGC0 is None else dGC0.clone()).contiguous()
         alpha0 = 1e-10 if alpha0 is None else alpha0
         self._low_alpha_count = self._low_alpha_count + 1 if alpha0 < 1e-1 else 0
-        # scaled residual max|R/sqrt|diag K||, the reference's switch to an exact solve
         tight = self._low_alpha_count > 3 or self._scaled_rmax(K_values, R) < 1e-3
         if tight:
             tol, cap = self.tight_pcg_tol, self.tight_pcg_max_iter
@@ -182,19 +220,25 @@ class StaticImplicitSolver(BaseSolver):
         else:
             tol = self.pcg_tol
             cap = 6000 if (iter_now % 20 == 0 or self._low_alpha_count > 0) else self.pcg_max_iter
-        x0 = x.clone()
+        return LinearSolve(K_values, R.contiguous(), x, tol, cap, tight)
+
+    def _run_linear(self, req):
+        P = self.assembly.plan
         if self.precision == "mixed":
-            v32 = P.to_f32(K_values)
-            it, outer, rr, st = P.pcg_mixed(K_values, v32, R.contiguous(), x, tol, 1e-4, cap,
-                                            raise_on_breakdown=False)
+            v32 = P.to_f32(req.K)
+            req.it, outer, req.rr, req.status = P.pcg_mixed(req.K, v32, req.b, req.x, req.tol, 1e-4, req.cap,
+                                                            raise_on_breakdown=False)
         else:
-            it, rr, st = P.pcg(K_values, R.contiguous(), x, tol, cap, raise_on_breakdown=False)
-        self.history[-1].update(pcg_iters=it, pcg_relres=rr, pcg_tight=tight, pcg_status=st)
-        if st == L.FEA_EBREAKDOWN:
+            req.it, req.rr, req.status = P.pcg(req.K, req.b, req.x, req.tol, req.cap, raise_on_breakdown=False)
+
+    def _linear_finish(self, req, K_values, R):
+        self.history[-1].update(pcg_iters=req.it, pcg_relres=req.rr, pcg_tight=req.tight, pcg_status=req.status)
+        x = req.x
+        if req.status == L.FEA_EBREAKDOWN:
             # K is not positive definite along the search space: keep the
             # iterate reached before the negative curvature (truncated CG);
             # with no progress, take the Jacobi-scaled residual direction
-            if not bool(torch.isfinite(x).all()) or bool(torch.equal(x, x0)):
+            if not bool(torch.isfinite(x).all()) or bool(torch.equal(x, req.x0)):
                 x = R / self._diag(K_values).abs()
         return x
 

@@ -202,3 +202,21 @@ def test_block_contributor_lists(golden):
         for p in range(adjptr[n], adjptr[n + 1]):
             assert list(bc[bp[p]:bp[p + 1]]) == expect[(n, adjcol[p])]
     assert bp[-1] == sum(len(v) for v in expect.values())
+
+
+def test_serving_requests_are_seeded_and_bounded():
+    from fea_b200 import meshes, serving
+    a = serving.make_requests(20, 5.0, seed=3)
+    b = serving.make_requests(20, 5.0, seed=3)
+    assert [vars(x) for x in a] == [vars(x) for x in b]
+    assert all(4 <= r.length <= 16 and 1 <= r.width <= 2 and 1 <= r.height <= 2 for r in a)
+    assert all(2000 <= r.n_elems <= 200000 and abs(r.kappa - 20 * r.mu) < 1e-12 for r in a)
+    assert all(0.005 <= r.pressure <= 0.05 for r in a)
+    assert all(serving.load_parameter(r.length, r.width, r.height, r.mu, r.kappa, r.pressure)
+               <= serving.STABLE_LOAD for r in a)
+    assert all(x.arrival < y.arrival for x, y in zip(a, a[1:]))
+    for r in a[:4]:
+        X, el = meshes.tet_beam(r.length, r.width, r.height, r.n_elems)
+        assert serving.request_rows(r) == 3 * X.shape[0]
+        assert 0.5 * r.n_elems <= el.shape[0] <= 2.0 * r.n_elems
+        assert abs(X[:, 0].max() - 1.0) < 1e-12 and abs(X[:, 0].min() - (1.0 - r.length)) < 1e-9
