@@ -246,6 +246,20 @@ class BatchedPCG:
                 "fea_pcgb_state")
         return self.state.view(-1, 4).cpu().numpy()
 
+    def poll_async(self):
+        """Queue the state copy behind the current round; wait() returns it."""
+        if not hasattr(self, "_host_state"):
+            self._host_state = torch.empty(4 * self.max_slots, dtype=torch.float64, pin_memory=True)
+            self._ev = torch.cuda.Event()
+        L.check(L.fea_pcgb_state(vptr(self.table), self.max_slots, self.max_slots, vptr(self.state), stream()),
+                "fea_pcgb_state")
+        self._host_state.copy_(self.state, non_blocking=True)
+        self._ev.record()
+
+    def wait(self):
+        self._ev.synchronize()
+        return self._host_state.view(-1, 4).numpy()
+
 
 class _Job:
     __slots__ = ("req", "asm", "solver", "gen", "lin", "work", "slot", "admitted", "bytes")
@@ -282,30 +296,38 @@ def serve(requests, max_slots=32, round_iters=32, mem_budget=32 << 30, use_graph
     t0 = time.perf_counter()
     busy_rounds = 0
 
+    work_stream = torch.cuda.Stream()
+    main = torch.cuda.current_stream()
+
     def finish(job, value):
         nonlocal mem_used
         if isinstance(value, bool):
             raise RuntimeError("request %d did not converge" % job.req.rid)
-        torch.cuda.synchronize()
+        work_stream.synchronize()
         results[job.req.rid] = Result(job.req.rid, value.cpu() if keep else None, len(job.solver.history),
                                       sum(h.get("pcg_iters", 0) for h in job.solver.history), job.req.arrival,
                                       job.admitted, time.perf_counter() - t0)
         mem_used -= job.bytes
 
     def advance(job, first=False):
-        """Run the job's Newton iteration up to its next tangent solve."""
-        try:
-            job.lin = next(job.gen) if first else job.gen.send(None)
-        except StopIteration as stop:
-            finish(job, stop.value)
-            return False
-        if job.work is None:
-            job.work = torch.empty(int(L.fea_pcgb_work_len(job.asm.plan.ndof)), dtype=torch.float64, device=dev)
+        """Run the job's Newton iteration up to its next tangent solve (on the
+        work stream, while the GPU iterates the other slots)."""
+        with torch.cuda.stream(work_stream):
+            try:
+                job.lin = next(job.gen) if first else job.gen.send(None)
+            except StopIteration as stop:
+                finish(job, stop.value)
+                return False
+            if job.work is None:
+                job.work = torch.empty(int(L.fea_pcgb_work_len(job.asm.plan.ndof)), dtype=torch.float64,
+                                       device=dev)
         queue_slot.append(job)
         return True
 
     slots = [None] * max_slots
-    while waiting or preparing or ready or queue_slot or any(j is not None for j in slots):
+    finished = []                      # jobs whose solve ended in the last polled round
+    in_flight = False
+    while waiting or preparing or ready or queue_slot or finished or in_flight or any(j is not None for j in slots):
         now = time.perf_counter() - t0
         # admit arrived requests into preparation while memory allows
         while waiting and waiting[0].arrival <= now and free_streams:
@@ -320,10 +342,27 @@ def serve(requests, max_slots=32, round_iters=32, mem_budget=32 << 30, use_graph
             req, st_, nb, adm = preparing.pop(fut)
             free_streams.append(st_)
             asm, sol = fut.result()
-            ready.append(_Job(req, asm, sol, adm, nb))
+            with torch.cuda.stream(work_stream):
+                ready.append(_Job(req, asm, sol, adm, nb))
+        # host work of the jobs that left the batch, overlapping the round in flight
         for job in ready:
             advance(job, first=True)
         ready.clear()
+        for job in finished:
+            advance(job)
+        finished.clear()
+        if in_flight:
+            state = eng.wait()
+            in_flight = False
+            busy_rounds += 1
+            for k, job in enumerate(slots):
+                if job is None or state[k, 0] == 0.0:
+                    continue
+                lin = job.lin
+                lin.it, lin.status, lin.rr = int(state[k, 1]), int(state[k, 2]), float(state[k, 3])
+                slots[k] = None
+                eng.release(k)
+                finished.append(job)
         # free slots to waiting solves
         fresh = []
         for k in range(max_slots):
@@ -334,25 +373,20 @@ def serve(requests, max_slots=32, round_iters=32, mem_budget=32 << 30, use_graph
                 eng.assign(k, job.asm.plan, job.lin, job.work)
                 fresh.append(k)
         if not any(j is not None for j in slots):
-            if waiting and not preparing:
-                time.sleep(max(0.0, min(0.002, waiting[0].arrival - (time.perf_counter() - t0))))
-            else:
-                time.sleep(0.0005)
+            if not finished:
+                if waiting and not preparing:
+                    time.sleep(max(0.0, min(0.002, waiting[0].arrival - (time.perf_counter() - t0))))
+                else:
+                    time.sleep(0.0005)
             continue
         eng.sync()
-        for k in fresh:
-            eng.start(k)
+        if fresh:
+            main.wait_stream(work_stream)
+            for k in fresh:
+                eng.start(k)
         eng.run_round()
-        busy_rounds += 1
-        state = eng.poll()
-        for k, job in enumerate(slots):
-            if job is None or state[k, 0] == 0.0:
-                continue
-            lin = job.lin
-            lin.it, lin.status, lin.rr = int(state[k, 1]), int(state[k, 2]), float(state[k, 3])
-            slots[k] = None
-            eng.release(k)
-            advance(job)
+        eng.poll_async()
+        in_flight = True
     pool.shutdown()
     stats = {"rounds": busy_rounds, "graph": eng.graph is not None, "max_slots": max_slots,
              "round_iters": round_iters, "wall_s": time.perf_counter() - t0}
