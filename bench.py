@@ -357,8 +357,9 @@ def run_newton(a):
 
 
 def run_adjoint(a):
-    """Compliance f.u of an n^3 C3D8 block (mu = 1, kappa = 50, bottom face
-    z = 0 clamped, pressure 0.03 on the top face): gradients w.r.t. all
+    """Compliance f.u of an n^3 C3D8 block (nodes jittered as in the assembly
+    workload, mu = 1, kappa = 50, bottom node plane clamped, pressure 0.03 on
+    the top faces): gradients w.r.t. all
     nodal coordinates and mu from the hand-written adjoint behind
     ComplianceFunction; checked against central differences (h = 1e-6) on
     seeded random coordinates and against torch autograd of the oracle's
@@ -368,7 +369,7 @@ def run_adjoint(a):
     from fea_b200 import adjoint, meshes
     from oracle import fea_oracle as O
     n = a.adjoint_n
-    X, el = meshes.hex_block(n)
+    X, el = meshes.hex_block(n, jitter=0.1, seed=0)
     E, N = el.shape[0], X.shape[0]
     top = np.nonzero(np.arange(E) % n == n - 1)[0]
     clamp = np.nonzero(np.arange(N) % (n + 1) == 0)[0]
