@@ -455,13 +455,27 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
           acc[d][3 * j + k] += A[j] * qb[k] + B[j] * fb[k] + qb[j] * Cc[k] + (j == k ? dg : 0.0);
     }
   }
-  double* out = stage + e * HX_STAGE;
+  double* out = stage + e * HX_STAGE;   // 2784 B per element: 16-byte aligned
 #pragma unroll
   for (int d = 0; d < 5; ++d) {
     if (d == 4 && nb == 4) break;
-    double* o = out + hx_slot(a, d) * 9;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) o[i] = acc[d][i];
+    const int slot = hx_slot(a, d);
+    double* o = out + slot * 9;            // even slots start 16-byte aligned, odd ones 8 bytes past
+    if (slot & 1) {
+      o[0] = acc[d][0];
+      double2* o2 = reinterpret_cast<double2*>(o + 1);
+      o2[0] = make_double2(acc[d][1], acc[d][2]);
+      o2[1] = make_double2(acc[d][3], acc[d][4]);
+      o2[2] = make_double2(acc[d][5], acc[d][6]);
+      o2[3] = make_double2(acc[d][7], acc[d][8]);
+    } else {
+      double2* o2 = reinterpret_cast<double2*>(o);
+      o2[0] = make_double2(acc[d][0], acc[d][1]);
+      o2[1] = make_double2(acc[d][2], acc[d][3]);
+      o2[2] = make_double2(acc[d][4], acc[d][5]);
+      o2[3] = make_double2(acc[d][6], acc[d][7]);
+      o[8] = acc[d][8];
+    }
   }
 #pragma unroll
   for (int j = 0; j < 3; ++j) out[324 + 3 * a + j] = racc[j];
