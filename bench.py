@@ -88,6 +88,30 @@ def algorithmic_bytes(E, nn, nnz, N, n):
     return E * 4 * nn + E * 4 * (3 * nn) ** 2 + 8 * nnz + 48 * N + 8 * n
 
 
+def dist_barrier(world):
+    """Barrier across the ranks (no-op on one rank)."""
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def dist_max(x, world, device):
+    """Max of a per-rank time over all ranks (the job finishes with its slowest rank)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t)
+
+
+def job_rate(world, units_per_rank, ms):
+    """Whole-job throughput in G units/s: every rank processes its own units
+    (weak scaling) in the max-over-ranks time ms."""
+    return world * units_per_rank / (ms * 1e-3) / 1e9
+
+
 def sample_clocks(stop, out, dev):
     cmd = ["nvidia-smi", "-i", str(dev), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
            "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -546,15 +570,10 @@ def main():
     stream = torch.cuda.current_stream()
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        dist_barrier(world)
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t)
+        return dist_max(x, world, "cuda")
 
     # element kernel timed live: events around the volume kernel of every step
     mu, kappa = 1.0, 50.0
@@ -593,7 +612,7 @@ def main():
         th.join(timeout=10)
     ms = max_over_ranks(t_start.elapsed_time(t_end) / a.steps)
     kern_ms = statistics.mean(s.elapsed_time(t) for s, t in evs)
-    value = world * E / (ms * 1e-3) / 1e9
+    value = job_rate(world, E, ms)
 
     # end to end through the public API, host buffers
     gc_h = gc.cpu().pin_memory()
@@ -647,7 +666,7 @@ def main():
                      "traffic": traffic, "algorithmic_bytes": B, "kernel_ms": kern_ms,
                      "kernel": "k_hex_elem + k_hex_blk (C3D8 element blocks, then node-row gather into CSR)",
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650"},
-        "e2e": {"value": world * E / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": e2e_ms,
+        "e2e": {"value": job_rate(world, E, e2e_ms), "unit": UNIT, "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": 8 * ndof, "d2h_bytes_per_step": 8 * ndof,
                 "api": "Assembly.assemble_Stiffness_Matrix"},
         "gpu_launches": int(launches),
