@@ -71,7 +71,9 @@ class Group(C.Structure):
 class PcgbSlot(C.Structure):
     _fields_ = [("n", C.c_int64), ("nnz", C.c_int64), ("indptr_dev", C.c_void_p), ("indices_dev", C.c_void_p),
                 ("values_dev", C.c_void_p), ("b_dev", C.c_void_p), ("x_dev", C.c_void_p), ("work_dev", C.c_void_p),
-                ("work_len", C.c_int64), ("tol", C.c_double), ("max_iter", C.c_int32), ("active", C.c_int32)]
+                ("work_len", C.c_int64), ("tol", C.c_double), ("max_iter", C.c_int32), ("active", C.c_int32),
+                ("n_nodes", C.c_int64), ("vbase_dev", C.c_void_p), ("rowlen_dev", C.c_void_p),
+                ("dbase_dev", C.c_void_p), ("mask_dev", C.c_void_p)]
 
 
 P = C.c_void_p
@@ -111,12 +113,12 @@ fea_pcg_solve_nodes = _sig("fea_pcg_solve_nodes", I32, NP, P, P, P, P, D, I32, I
 fea_pcg_solve_mixed_nodes = _sig("fea_pcg_solve_mixed_nodes", I32, NP, P, P, P, P, P, D, D, I32, I32, P, I64,
                                  C.POINTER(I32), C.POINTER(I32), C.POINTER(D), P)
 fea_convert_f32 = _sig("fea_convert_f32", I32, I64, P, P, P)
-fea_pcgb_work_len = _sig("fea_pcgb_work_len", I64, I64)
+fea_pcgb_work_len = _sig("fea_pcgb_work_len", I64, I64, I64)
 fea_pcgb_table_bytes = _sig("fea_pcgb_table_bytes", I64, I32, I64)
 fea_pcgb_set = _sig("fea_pcgb_set", I32, P, I32, I64, I32, C.POINTER(PcgbSlot), P)
 fea_pcgb_start = _sig("fea_pcgb_start", I32, P, I32, I64, I32, I64, I64, P)
 fea_pcgb_iterate = _sig("fea_pcgb_iterate", I32, P, I32, I64, I32, P)
-fea_pcgb_state = _sig("fea_pcgb_state", I32, P, I32, I32, P, P)
+fea_pcgb_state = _sig("fea_pcgb_state", I32, P, I32, I64, I32, P, P)
 fea_explicit_work_len = _sig("fea_explicit_work_len", I64, I64)
 fea_explicit_run = _sig("fea_explicit_run", I32, NP, GP, D, D, P, D, I64, I32, I32, P, P, P, P, P, I64, P)
 fea_adjoint_vjp_volume = _sig("fea_adjoint_vjp_volume", I32, NP, GP, D, D, P, P, P, P, P, I64, P)

@@ -245,6 +245,73 @@ __global__ void __launch_bounds__(PCG_TPB) k_spmv_node(NodeOp<V> A, const X* __r
   if (mode == 1) finish_pq(contrib, st, part, counter);
 }
 
+// Node rows with LPN < 32 lanes per node (32 / LPN nodes per warp): more
+// nodes, and more loads, in flight per warp; used for the FP32 values of the
+// mixed solver, whose 4-byte loads leave the one-node-per-warp kernel
+// latency-bound.  Column passes of 3 LPN; loops and shuffles warp-uniform.
+template <int LPN, class V, class X>
+__global__ void __launch_bounds__(PCG_TPB) k_spmv_node_sub(NodeOp<V> A, const X* __restrict__ x, X* __restrict__ y,
+                                                           double* st, double* part, unsigned* counter, int mode) {
+  if (mode == 1 && st[S_DONE] != 0.0) return;
+  constexpr int NPW = 32 / LPN;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int sub = lane / LPN, hl = lane % LPN;
+  const int64_t step = (int64_t)gridDim.x * PCG_WARPS * NPW;
+  double contrib = 0.0;
+  for (int64_t base = ((int64_t)blockIdx.x * PCG_WARPS + warp) * NPW; base < A.n_nodes; base += step) {
+    const int64_t nd = base + sub;
+    const bool valid = nd < A.n_nodes;
+    const unsigned m = valid ? A.mask[nd] : 0u;
+    const int L = m ? A.rowlen[nd] : 0;
+    const int64_t vb = valid ? A.vbase[nd] : 0;
+    const int f = popc3(m);
+    int Lmax = L;
+#pragma unroll
+    for (int o = 16; o >= LPN; o >>= 1) Lmax = max(Lmax, __shfl_xor_sync(0xffffffffu, Lmax, o));
+    const V* __restrict__ v0 = A.val + vb;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int q0 = 0; q0 < Lmax; q0 += 3 * LPN) {
+      int32_t j[3];
+      bool h[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int q = q0 + hl + LPN * k;
+        h[k] = q < L;
+        j[k] = h[k] ? __ldg(A.idx + vb + q) : 0;
+      }
+      double va[3][3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const int q = q0 + hl + LPN * k;
+          va[r][k] = (r < f && h[k]) ? (double)__ldcs(v0 + (int64_t)r * L + q) : 0.0;
+        }
+      double xv[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) xv[k] = h[k] ? (double)x[j[k]] : 0.0;
+      s0 += va[0][0] * xv[0] + va[0][1] * xv[1] + va[0][2] * xv[2];
+      s1 += va[1][0] * xv[0] + va[1][1] * xv[1] + va[1][2] * xv[2];
+      s2 += va[2][0] * xv[0] + va[2][1] * xv[1] + va[2][2] * xv[2];
+    }
+#pragma unroll
+    for (int o = LPN / 2; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o, LPN);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o, LPN);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o, LPN);
+    }
+    if (hl == 0 && m) {
+      const int64_t r = A.dbase[nd];
+      y[r] = (X)s0;
+      contrib += s0 * (double)x[r];
+      if (f > 1) { y[r + 1] = (X)s1; contrib += s1 * (double)x[r + 1]; }
+      if (f > 2) { y[r + 2] = (X)s2; contrib += s2 * (double)x[r + 2]; }
+    }
+  }
+  if (mode == 1) finish_pq(contrib, st, part, counter);
+}
+
 // 1/|K_jj| of the node rows (0 -> 1): the diagonal entry of row (n, j) is the
 // column dbase[n] + j of the shared column list (sorted), found by bisection
 template <class V>
@@ -446,8 +513,13 @@ static void spmv(const CsrOp<V>& A, const X* x, X* y, double* st, double* part, 
 template <class V, class X>
 static void spmv(const NodeOp<V>& A, const X* x, X* y, double* st, double* part, unsigned* counter, int mode,
                  cudaStream_t s) {
-  k_spmv_node<V, X><<<occ_grid(k_spmv_node<V, X>, A.n_nodes, PCG_WARPS), PCG_TPB, 0, s>>>(A, x, y, st, part, counter,
-                                                                                        mode);
+  if (sizeof(V) == 4) {
+    k_spmv_node_sub<16, V, X><<<occ_grid(k_spmv_node_sub<16, V, X>, A.n_nodes, 2 * PCG_WARPS), PCG_TPB, 0, s>>>(
+        A, x, y, st, part, counter, mode);
+  } else {
+    k_spmv_node<V, X><<<occ_grid(k_spmv_node<V, X>, A.n_nodes, PCG_WARPS), PCG_TPB, 0, s>>>(A, x, y, st, part,
+                                                                                          counter, mode);
+  }
   count_launch();
 }
 
@@ -608,13 +680,17 @@ static int read_nnz(const int64_t* ip, int64_t n, int64_t* nnz, cudaStream_t s) 
 }
 
 // ---- batched PCG over independent systems ("slots") ---------------------
-// Every slot's rows are cut into chunks of PCGB_ROWS consecutive rows; one CTA
-// processes one chunk at a time (grid-stride over the chunk list of all
-// active slots), and each slot keeps its own scalars, partial sums (one per
-// chunk) and completion counter.  A slot's arithmetic depends only on its
-// own chunking, so its iterates are the same bits whether it runs alone or
-// beside other slots.
-constexpr int PCGB_ROWS = 256;
+// Work items are warp-sized and a fixed function of the slot alone: SpMV
+// items of 16 nodes (plan layout: two nodes at a time per warp, 16 lanes
+// each, with the next pair's column indices prefetched) or 16 rows (plain
+// CSR), update items of 256 rows.  Each item's warp writes one partial sum
+// and counts itself on the slot's counter; the warp that completes the
+// slot's count sums the partials in item order and updates the slot's
+// scalars.  Warps walk the item lists of all active slots in grid-stride
+// order with no block-level barrier.  A slot's arithmetic depends only on
+// its own items, so its iterates are the same bits alone or batched.
+constexpr int PCGB_ROWS = 256;      // rows per update item and per start chunk
+constexpr int PCGB_GROUP = 16;      // nodes (plan layout) or rows (CSR) per SpMV item
 
 struct PcgbSlotDev {
   const int64_t* ptr;
@@ -623,87 +699,206 @@ struct PcgbSlotDev {
   const double* b;
   double* x;
   double* st;
-  unsigned* counter;
-  double *dinv, *r, *z, *p, *q, *part;
-  int64_t n;
-  int32_t nchunk, lanes;
+  unsigned* counter;       // [0] SpMV items, [1] update items, [2] start chunks
+  double *dinv, *r, *z, *p, *q;
+  double *part_s, *part_u, *part_0;
+  const int64_t* vbase;    // plan layout (node rows), or NULL: plain CSR rows
+  const int32_t* rowlen;
+  const int32_t* dbase;
+  const uint8_t* mask;
+  int64_t n, n_nodes;
+  int32_t nitem_s, nitem_u, nchunk0, lanes;
   double tol;
   int32_t max_iter, pad;
 };
 
 struct PcgbHeader {
-  int64_t nchunks;
+  int64_t nitem_s;
+  int64_t nitem_u;
   int64_t nslots;
 };
 
 struct PcgbView {
   PcgbHeader* hdr;
   PcgbSlotDev* slots;
-  int32_t* chunk_slot;
-  int32_t* chunk_local;
+  int32_t *s_slot, *s_local, *u_slot, *u_local;
 };
 
-static PcgbView pcgb_view(void* table, int32_t max_slots) {
+static PcgbView pcgb_view(void* table, int32_t max_slots, int64_t max_items) {
   PcgbView v;
   char* c = (char*)table;
   v.hdr = (PcgbHeader*)c;
   v.slots = (PcgbSlotDev*)(c + 64);
-  v.chunk_slot = (int32_t*)(c + 64 + sizeof(PcgbSlotDev) * (size_t)max_slots);
+  v.s_slot = (int32_t*)(c + 64 + sizeof(PcgbSlotDev) * (size_t)max_slots);
+  v.s_local = v.s_slot + max_items;
+  v.u_slot = v.s_local + max_items;
+  v.u_local = v.u_slot + max_items;
   return v;
 }
 
-static int64_t pcgb_slot_chunks(int64_t n) { return (n + PCGB_ROWS - 1) / PCGB_ROWS; }
+static int64_t pcgb_items_s(int64_t n, int64_t n_nodes) {
+  return n_nodes > 0 ? (n_nodes + PCGB_GROUP - 1) / PCGB_GROUP : (n + PCGB_GROUP - 1) / PCGB_GROUP;
+}
+static int64_t pcgb_items_u(int64_t n) { return (n + PCGB_ROWS - 1) / PCGB_ROWS; }
 
-// rows of one chunk, LANES threads per row: q = A p, returns this thread's p.q share
-template <int LANES>
-__device__ __forceinline__ double pcgb_rows_spmv(const PcgbSlotDev& S, int64_t row0) {
-  constexpr int RPP = PCG_TPB / LANES;           // rows per pass
-  const int lane = threadIdx.x % LANES;
-  const int sub = threadIdx.x / LANES;
+__device__ __forceinline__ bool pcgb_warp_last(unsigned* counter, int total, int lane) {
+  unsigned old = 0u;
+  if (lane == 0) {
+    __threadfence();
+    old = atomicAdd(counter, 1u);
+  }
+  old = __shfl_sync(0xffffffffu, old, 0);
+  return old == (unsigned)(total - 1);
+}
+
+__device__ __forceinline__ double pcgb_warp_sum(const double* part, int n, int stride, int off, int lane) {
+  // 8 independent L2 loads per lane in flight per batch, fixed order
+  double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int i0 = 0; i0 < n; i0 += 256) {
+    double v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int i = i0 + 32 * k + lane;
+      v[k] = i < n ? __ldcg(part + (int64_t)i * stride + off) : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] += v[k];
+  }
+  double v = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// q = A p over nodes [n0, n1) of a plan-layout slot: half-warp h takes nodes
+// n0 + 2i + h (16 lanes, 48 columns per pass); the next pair's metadata and
+// first column indices are prefetched.  Returns p.q over those rows (lane 0).
+__device__ __forceinline__ double pcgb_nodes_spmv(const PcgbSlotDev& S, int64_t n0, int64_t n1, int lane) {
+  const int h = lane >> 4, hl = lane & 15;
   double contrib = 0.0;
-  for (int k = 0; k < PCGB_ROWS; k += RPP) {
-    const int64_t row = row0 + k + sub;
+  int64_t nd = n0 + h;
+  unsigned m = 0;
+  int L = 0;
+  int64_t vb = 0;
+  int32_t jn[3] = {0, 0, 0};
+  if (nd < n1) {
+    m = S.mask[nd];
+    L = m ? S.rowlen[nd] : 0;
+    vb = S.vbase[nd];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) jn[k] = hl + 16 * k < L ? __ldg(S.idx + vb + hl + 16 * k) : 0;
+  }
+  for (int64_t base = n0; base < n1; base += 2) {          // warp-uniform
+    const int64_t nx = nd + 2;
+    unsigned m2 = 0;
+    int L2 = 0;
+    int64_t vb2 = 0;
+    if (nx < n1) {
+      m2 = S.mask[nx];
+      L2 = S.rowlen[nx];
+      vb2 = S.vbase[nx];
+    }
+    const int f = popc3(m);
+    int Lmax = L;
+    Lmax = max(Lmax, __shfl_xor_sync(0xffffffffu, Lmax, 16));
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    const double* __restrict__ v0 = S.val + vb;
+    for (int q0 = 0; q0 < Lmax; q0 += 48) {
+      int32_t j[3];
+      bool hv[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int q = q0 + hl + 16 * k;
+        hv[k] = q < L;
+        j[k] = q0 == 0 ? jn[k] : (hv[k] ? __ldg(S.idx + vb + q) : 0);
+      }
+      double va[3][3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const int q = q0 + hl + 16 * k;
+          va[r][k] = (r < f && hv[k]) ? __ldcs(v0 + (int64_t)r * L + q) : 0.0;
+        }
+      double xv[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) xv[k] = hv[k] ? S.p[j[k]] : 0.0;
+      s0 += va[0][0] * xv[0] + va[0][1] * xv[1] + va[0][2] * xv[2];
+      s1 += va[1][0] * xv[0] + va[1][1] * xv[1] + va[1][2] * xv[2];
+      s2 += va[2][0] * xv[0] + va[2][1] * xv[1] + va[2][2] * xv[2];
+    }
+    const int Ln = m2 ? L2 : 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) jn[k] = hl + 16 * k < Ln ? __ldg(S.idx + vb2 + hl + 16 * k) : 0;
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o, 16);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o, 16);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o, 16);
+    }
+    if (m && hl < f) {
+      const int64_t r = S.dbase[nd] + hl;
+      const double sr = hl == 0 ? s0 : (hl == 1 ? s1 : s2);
+      S.q[r] = sr;
+      contrib += sr * S.p[r];
+    }
+    nd = nx;
+    m = m2;
+    L = Ln;
+    vb = vb2;
+  }
+  // lanes 0-2 and 16-18 hold the sums: fixed tree over the warp
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, o);
+  return lane == 0 ? contrib : 0.0;
+}
+
+// q = A p over CSR rows [r0, r1), LANES lanes per row; returns p.q (lane 0)
+template <int LANES>
+__device__ __forceinline__ double pcgb_rows_spmv(const PcgbSlotDev& S, int64_t r0, int64_t r1, int lane) {
+  constexpr int RPP = 32 / LANES;
+  const int sl = lane % LANES, sub = lane / LANES;
+  double contrib = 0.0;
+  for (int64_t base = r0; base < r1; base += RPP) {
+    const int64_t row = base + sub;
     double s = 0.0;
-    if (row < S.n) {
+    if (row < r1) {
       const int64_t b = S.ptr[row], e = S.ptr[row + 1];
-      for (int64_t i = b + lane; i < e; i += LANES) s += S.val[i] * S.p[S.idx[i]];
+      for (int64_t i = b + sl; i < e; i += LANES) s += S.val[i] * S.p[S.idx[i]];
     }
 #pragma unroll
     for (int o = LANES / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, LANES);
-    if (row < S.n && lane == 0) {
+    if (row < r1 && sl == 0) {
       S.q[row] = s;
       contrib += s * S.p[row];
     }
   }
-  return contrib;
-}
-
-__device__ __forceinline__ bool pcgb_last(unsigned* counter, int nchunk) {
-  __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == (unsigned)(nchunk - 1);
-  __syncthreads();
-  return last;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, o);
+  return lane == 0 ? contrib : 0.0;
 }
 
 __global__ void __launch_bounds__(PCG_TPB) k_pcgb_spmv(PcgbView V) {
-  __shared__ double sh[PCG_WARPS];
-  const int64_t nch = V.hdr->nchunks;
-  for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
-    const PcgbSlotDev& S = V.slots[V.chunk_slot[c]];
-    if (S.st[S_DONE] != 0.0) continue;            // block-uniform
-    const int local = V.chunk_local[c];
-    const int64_t row0 = (int64_t)local * PCGB_ROWS;
-    double contrib;
-    if (S.lanes == 32) contrib = pcgb_rows_spmv<32>(S, row0);
-    else if (S.lanes == 16) contrib = pcgb_rows_spmv<16>(S, row0);
-    else contrib = pcgb_rows_spmv<8>(S, row0);
-    const double bs = block_sum_w(contrib, sh);
-    if (threadIdx.x == 0) S.part[local] = bs;
-    if (pcgb_last(S.counter, S.nchunk)) {
-      const double pq = sum_partials(S.part, S.nchunk, 1, 0, sh);
-      if (threadIdx.x == 0) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * PCG_WARPS;
+  const int64_t nit = V.hdr->nitem_s;
+  for (int64_t it = (int64_t)blockIdx.x * PCG_WARPS + (threadIdx.x >> 5); it < nit; it += nw) {
+    const PcgbSlotDev& S = V.slots[V.s_slot[it]];
+    if (S.st[S_DONE] != 0.0) continue;            // warp-uniform
+    const int g = V.s_local[it];
+    double c;
+    if (S.vbase) {
+      const int64_t n0 = (int64_t)g * PCGB_GROUP;
+      c = pcgb_nodes_spmv(S, n0, min(n0 + PCGB_GROUP, S.n_nodes), lane);
+    } else {
+      const int64_t r0 = (int64_t)g * PCGB_GROUP, r1 = min(r0 + PCGB_GROUP, S.n);
+      c = S.lanes == 32 ? pcgb_rows_spmv<32>(S, r0, r1, lane)
+                        : (S.lanes == 16 ? pcgb_rows_spmv<16>(S, r0, r1, lane) : pcgb_rows_spmv<8>(S, r0, r1, lane));
+    }
+    if (lane == 0) S.part_s[g] = c;
+    if (pcgb_warp_last(S.counter + 0, S.nitem_s, lane)) {
+      const double pq = pcgb_warp_sum(S.part_s, S.nitem_s, 1, 0, lane);
+      if (lane == 0) {
         S.st[S_PQ] = pq;
         if (!(pq > 0.0) || !isfinite(pq)) {
           S.st[S_STATUS] = (double)FEA_EBREAKDOWN;
@@ -712,37 +907,61 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcgb_spmv(PcgbView V) {
         } else {
           S.st[S_ALPHA] = S.st[S_RZ] / pq;
         }
-        *S.counter = 0u;
+        S.counter[0] = 0u;
       }
     }
   }
 }
 
 __global__ void __launch_bounds__(PCG_TPB) k_pcgb_update(PcgbView V) {
-  __shared__ double sh[PCG_WARPS];
-  const int64_t nch = V.hdr->nchunks;
-  for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
-    const PcgbSlotDev& S = V.slots[V.chunk_slot[c]];
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * PCG_WARPS;
+  const int64_t nit = V.hdr->nitem_u;
+  for (int64_t it = (int64_t)blockIdx.x * PCG_WARPS + (threadIdx.x >> 5); it < nit; it += nw) {
+    const PcgbSlotDev& S = V.slots[V.u_slot[it]];
     if (S.st[S_DONE] != 0.0) continue;
-    const int local = V.chunk_local[c];
-    const int64_t i = (int64_t)local * PCGB_ROWS + threadIdx.x;
+    const int l = V.u_local[it];
     const double alpha = S.st[S_ALPHA];
-    double contrib = 0.0;
-    if (i < S.n) {
-      S.x[i] += alpha * S.p[i];
-      const double ri = S.r[i] - alpha * S.q[i];
-      S.r[i] = ri;
-      const double zi = ri * S.dinv[i];
-      S.z[i] = zi;
-      contrib = ri * zi;
+    double* __restrict__ x = S.x;
+    double* __restrict__ r = S.r;
+    double* __restrict__ z = S.z;
+    const double* __restrict__ p = S.p;
+    const double* __restrict__ q = S.q;
+    const double* __restrict__ dinv = S.dinv;
+    constexpr int K = PCGB_ROWS / 32;
+    double xv[K], pv[K], rv[K], qv[K], dv[K];
+    const int64_t i0 = (int64_t)l * PCGB_ROWS + lane;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {              // all loads of the item first
+      const int64_t i = i0 + 32 * k;
+      const bool in = i < S.n;
+      xv[k] = in ? x[i] : 0.0;
+      pv[k] = in ? p[i] : 0.0;
+      rv[k] = in ? r[i] : 0.0;
+      qv[k] = in ? q[i] : 0.0;
+      dv[k] = in ? dinv[i] : 0.0;
     }
-    const double bs = block_sum_w(contrib, sh);
-    if (threadIdx.x == 0) S.part[local] = bs;
-    if (pcgb_last(S.counter, S.nchunk)) {
-      const double rz = sum_partials(S.part, S.nchunk, 1, 0, sh);
-      if (threadIdx.x == 0) {
-        const double it = S.st[S_ITER] + 1.0;
-        S.st[S_ITER] = it;
+    double c = 0.0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int64_t i = i0 + 32 * k;
+      if (i < S.n) {
+        x[i] = xv[k] + alpha * pv[k];
+        const double ri = rv[k] - alpha * qv[k];
+        r[i] = ri;
+        const double zi = ri * dv[k];
+        z[i] = zi;
+        c += ri * zi;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) S.part_u[l] = c;
+    if (pcgb_warp_last(S.counter + 1, S.nitem_u, lane)) {
+      const double rz = pcgb_warp_sum(S.part_u, S.nitem_u, 1, 0, lane);
+      if (lane == 0) {
+        const double iter = S.st[S_ITER] + 1.0;
+        S.st[S_ITER] = iter;
         S.st[S_BETA] = rz / S.st[S_RZ];
         S.st[S_RZ] = rz;
         if (!isfinite(rz)) {
@@ -750,27 +969,46 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcgb_update(PcgbView V) {
           S.st[S_DONE] = 1.0;
         } else if (rz / S.st[S_RZ0] < S.tol) {
           S.st[S_DONE] = 1.0;
-        } else if (it >= (double)S.max_iter) {
+        } else if (iter >= (double)S.max_iter) {
           S.st[S_STATUS] = (double)FEA_ENOTCONV;
           S.st[S_DONE] = 1.0;
         }
-        *S.counter = 0u;
+        S.counter[1] = 0u;
       }
     }
   }
 }
 
 __global__ void __launch_bounds__(PCG_TPB) k_pcgb_p(PcgbView V) {
-  const int64_t nch = V.hdr->nchunks;
-  for (int64_t c = blockIdx.x; c < nch; c += gridDim.x) {
-    const PcgbSlotDev& S = V.slots[V.chunk_slot[c]];
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * PCG_WARPS;
+  const int64_t nit = V.hdr->nitem_u;
+  for (int64_t it = (int64_t)blockIdx.x * PCG_WARPS + (threadIdx.x >> 5); it < nit; it += nw) {
+    const PcgbSlotDev& S = V.slots[V.u_slot[it]];
     if (S.st[S_DONE] != 0.0) continue;
-    const int64_t i = (int64_t)V.chunk_local[c] * PCGB_ROWS + threadIdx.x;
-    if (i < S.n) S.p[i] = S.z[i] + S.st[S_BETA] * S.p[i];
+    const double beta = S.st[S_BETA];
+    const int l = V.u_local[it];
+    double* __restrict__ p = S.p;
+    const double* __restrict__ z = S.z;
+    constexpr int K = PCGB_ROWS / 32;
+    double zv[K], pv[K];
+    const int64_t i0 = (int64_t)l * PCGB_ROWS + lane;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int64_t i = i0 + 32 * k;
+      zv[k] = i < S.n ? z[i] : 0.0;
+      pv[k] = i < S.n ? p[i] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int64_t i = i0 + 32 * k;
+      if (i < S.n) p[i] = zv[k] + beta * pv[k];
+    }
   }
 }
 
-// start of one slot: dinv, r = b - A x, z, p, r.z and b.dinv.b; one CTA per chunk
+// start of one slot: dinv, r = b - A x, z, p, r.z and b.dinv.b; one CTA per
+// 256-row chunk (CSR rows: the initial residual is computed once per solve)
 template <int LANES>
 __device__ __forceinline__ double pcgb_row_ax(const PcgbSlotDev& S, int64_t row, int lane) {
   double s = 0.0;
@@ -790,7 +1028,6 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcgb_start(PcgbView V, int32_t slot
   constexpr int RPP = PCG_TPB / LANES;
   const int lane = threadIdx.x % LANES, sub = threadIdx.x / LANES;
   const int64_t row0 = (int64_t)blockIdx.x * PCGB_ROWS;
-  // r = A x (into r)
   for (int k = 0; k < PCGB_ROWS; k += RPP) {
     const int64_t row = row0 + k + sub;
     const double s = pcgb_row_ax<LANES>(S, row, lane);
@@ -822,19 +1059,24 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcgb_start(PcgbView V, int32_t slot
   const double s1 = block_sum_w(c_rz, sh);
   const double s2 = block_sum_w(c_bb, sh);
   if (threadIdx.x == 0) {
-    S.part[2 * blockIdx.x] = s1;
-    S.part[2 * blockIdx.x + 1] = s2;
+    S.part_0[2 * blockIdx.x] = s1;
+    S.part_0[2 * blockIdx.x + 1] = s2;
   }
-  if (pcgb_last(S.counter, S.nchunk)) {
-    const double rz = sum_partials(S.part, S.nchunk, 2, 0, sh);
-    const double bb = sum_partials(S.part, S.nchunk, 2, 1, sh);
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(S.counter + 2, 1u) == (unsigned)(S.nchunk0 - 1);
+  __syncthreads();
+  if (last) {
+    const double rz = sum_partials(S.part_0, S.nchunk0, 2, 0, sh);
+    const double bb = sum_partials(S.part_0, S.nchunk0, 2, 1, sh);
     if (threadIdx.x == 0) {
       S.st[S_RZ] = rz;
       S.st[S_RZ0] = bb == 0.0 ? 1.0 : bb;
       S.st[S_ITER] = 0.0;
       S.st[S_STATUS] = 0.0;
       S.st[S_DONE] = (bb == 0.0 || rz == 0.0 || rz / (bb == 0.0 ? 1.0 : bb) < S.tol || S.max_iter <= 0) ? 1.0 : 0.0;
-      *S.counter = 0u;
+      S.counter[2] = 0u;
     }
   }
 }
@@ -946,74 +1188,82 @@ extern "C" int fea_pcg_solve_mixed_nodes(const fea_nodes_t* N, const int32_t* ix
 }
 
 // ---- batched PCG C ABI ------------------------------------------------------
-extern "C" int64_t fea_pcgb_work_len(int64_t n) {
-  return S_LEN + 2 + 5 * n + 2 * pcgb_slot_chunks(n) + 2;
+extern "C" int64_t fea_pcgb_work_len(int64_t n, int64_t n_nodes) {
+  return S_LEN + 2 + 5 * n + pcgb_items_s(n, n_nodes) + pcgb_items_u(n) + 2 * pcgb_items_u(n) + 2;
 }
 
-extern "C" int64_t fea_pcgb_table_bytes(int32_t max_slots, int64_t max_chunks) {
-  if (max_slots <= 0 || max_chunks <= 0) return 0;
-  return 64 + (int64_t)sizeof(PcgbSlotDev) * max_slots + 8 * max_chunks;
+extern "C" int64_t fea_pcgb_table_bytes(int32_t max_slots, int64_t max_items) {
+  if (max_slots <= 0 || max_items <= 0) return 0;
+  return 64 + (int64_t)sizeof(PcgbSlotDev) * max_slots + 16 * max_items;
 }
 
-extern "C" int fea_pcgb_set(void* table, int32_t max_slots, int64_t max_chunks, int32_t nslots,
+extern "C" int fea_pcgb_set(void* table, int32_t max_slots, int64_t max_items, int32_t nslots,
                             const fea_pcgb_slot_t* slots, cudaStream_t s) {
-  if (!table || max_slots <= 0 || max_chunks <= 0 || nslots < 0 || nslots > max_slots || (nslots && !slots))
+  if (!table || max_slots <= 0 || max_items <= 0 || nslots < 0 || nslots > max_slots || (nslots && !slots))
     return FEA_EINVAL;
   std::vector<PcgbSlotDev> dev(nslots);
-  std::vector<int32_t> cs, cl;
+  std::vector<int32_t> ss, sl, us, ul;
   for (int32_t k = 0; k < nslots; ++k) {
     const fea_pcgb_slot_t& h = slots[k];
     PcgbSlotDev& d = dev[k];
     std::memset(&d, 0, sizeof(d));
-    if (h.n < 0) return FEA_EINVAL;
+    if (h.n < 0 || h.n_nodes < 0) return FEA_EINVAL;
     if (!h.work_dev) continue;                       // empty slot
     if (h.n > 0 && (!h.indptr_dev || !h.indices_dev || !h.values_dev || !h.b_dev || !h.x_dev)) return FEA_EINVAL;
-    if (h.work_len < fea_pcgb_work_len(h.n)) return FEA_EWORK;
-    if (pcgb_slot_chunks(h.n) >= INT32_MAX) return FEA_ERANGE;
+    const int64_t nn = h.vbase_dev ? h.n_nodes : 0;
+    if (h.vbase_dev && (!h.rowlen_dev || !h.dbase_dev || !h.mask_dev)) return FEA_EINVAL;
+    if (h.work_len < fea_pcgb_work_len(h.n, nn)) return FEA_EWORK;
+    const int64_t is = pcgb_items_s(h.n, nn), iu = pcgb_items_u(h.n);
+    if (is >= INT32_MAX || iu >= INT32_MAX) return FEA_ERANGE;
     double* w = h.work_dev;
     d.ptr = h.indptr_dev; d.idx = h.indices_dev; d.val = h.values_dev; d.b = h.b_dev; d.x = h.x_dev;
     d.st = w;
     d.counter = (unsigned*)(w + S_LEN);
     d.dinv = w + S_LEN + 2;
-    d.r = d.dinv + h.n; d.z = d.r + h.n; d.p = d.z + h.n; d.q = d.p + h.n; d.part = d.q + h.n;
+    d.r = d.dinv + h.n; d.z = d.r + h.n; d.p = d.z + h.n; d.q = d.p + h.n;
+    d.part_s = d.q + h.n; d.part_u = d.part_s + is; d.part_0 = d.part_u + iu;
+    if (h.vbase_dev) { d.vbase = h.vbase_dev; d.rowlen = h.rowlen_dev; d.dbase = h.dbase_dev; d.mask = h.mask_dev; }
     d.n = h.n;
-    d.nchunk = (int32_t)pcgb_slot_chunks(h.n);
-    d.lanes = 8;
-    if (h.n > 0 && h.nnz > 0) d.lanes = lanes_for(h.n, h.nnz);
+    d.n_nodes = nn;
+    d.nitem_s = (int32_t)is;
+    d.nitem_u = (int32_t)iu;
+    d.nchunk0 = (int32_t)iu;
+    d.lanes = (h.n > 0 && h.nnz > 0) ? lanes_for(h.n, h.nnz) : 8;
     d.tol = h.tol;
     d.max_iter = h.max_iter;
-    if (h.active)
-      for (int32_t c = 0; c < d.nchunk; ++c) { cs.push_back(k); cl.push_back(c); }
+    if (h.active) {
+      for (int32_t c = 0; c < d.nitem_s; ++c) { ss.push_back(k); sl.push_back(c); }
+      for (int32_t c = 0; c < d.nitem_u; ++c) { us.push_back(k); ul.push_back(c); }
+    }
     // completion counters are zero between kernels; a new work buffer starts so
-    if (cudaError_t e = cudaMemsetAsync(d.counter, 0, 2 * sizeof(unsigned), s)) return (int)e;
+    if (cudaError_t e = cudaMemsetAsync(d.counter, 0, 4 * sizeof(unsigned), s)) return (int)e;
   }
-  if ((int64_t)cs.size() > max_chunks) return FEA_ERANGE;
-  PcgbView V = pcgb_view(table, max_slots);
-  V.chunk_local = V.chunk_slot + max_chunks;
-  PcgbHeader hdr{(int64_t)cs.size(), (int64_t)nslots};
+  if ((int64_t)ss.size() > max_items || (int64_t)us.size() > max_items) return FEA_ERANGE;
+  PcgbView V = pcgb_view(table, max_slots, max_items);
+  PcgbHeader hdr{(int64_t)ss.size(), (int64_t)us.size(), (int64_t)nslots};
   if (cudaError_t e = cudaMemcpyAsync(V.hdr, &hdr, sizeof(hdr), cudaMemcpyHostToDevice, s)) return (int)e;
   if (nslots)
     if (cudaError_t e = cudaMemcpyAsync(V.slots, dev.data(), sizeof(PcgbSlotDev) * nslots, cudaMemcpyHostToDevice, s))
       return (int)e;
-  if (!cs.empty()) {
-    if (cudaError_t e = cudaMemcpyAsync(V.chunk_slot, cs.data(), 4 * cs.size(), cudaMemcpyHostToDevice, s))
-      return (int)e;
-    if (cudaError_t e = cudaMemcpyAsync(V.chunk_local, cl.data(), 4 * cl.size(), cudaMemcpyHostToDevice, s))
-      return (int)e;
-  }
+  auto put = [&](int32_t* dst, const std::vector<int32_t>& v) -> int {
+    if (v.empty()) return 0;
+    return (int)cudaMemcpyAsync(dst, v.data(), 4 * v.size(), cudaMemcpyHostToDevice, s);
+  };
+  if (int r = put(V.s_slot, ss)) return r;
+  if (int r = put(V.s_local, sl)) return r;
+  if (int r = put(V.u_slot, us)) return r;
+  if (int r = put(V.u_local, ul)) return r;
   // the host vectors above are released on return: finish the copies first
   return (int)cudaStreamSynchronize(s);
 }
 
-extern "C" int fea_pcgb_start(void* table, int32_t max_slots, int64_t max_chunks, int32_t slot, int64_t n,
+extern "C" int fea_pcgb_start(void* table, int32_t max_slots, int64_t max_items, int32_t slot, int64_t n,
                               int64_t nnz, cudaStream_t s) {
-  if (!table || slot < 0 || slot >= max_slots || n < 0 || max_chunks <= 0) return FEA_EINVAL;
+  if (!table || slot < 0 || slot >= max_slots || n < 0 || max_items <= 0) return FEA_EINVAL;
   if (n == 0) return FEA_OK;
-  PcgbView V = pcgb_view(table, max_slots);
-  V.chunk_local = V.chunk_slot + max_chunks;
+  PcgbView V = pcgb_view(table, max_slots, max_items);
   const int L = lanes_for(n, nnz);
-  const unsigned grid = (unsigned)pcgb_slot_chunks(n);
-  // the slot's completion counter starts at zero
+  const unsigned grid = (unsigned)pcgb_items_u(n);
   if (L == 32) k_pcgb_start<32><<<grid, PCG_TPB, 0, s>>>(V, slot);
   else if (L == 16) k_pcgb_start<16><<<grid, PCG_TPB, 0, s>>>(V, slot);
   else k_pcgb_start<8><<<grid, PCG_TPB, 0, s>>>(V, slot);
@@ -1021,15 +1271,15 @@ extern "C" int fea_pcgb_start(void* table, int32_t max_slots, int64_t max_chunks
   return (int)cudaGetLastError();
 }
 
-extern "C" int fea_pcgb_iterate(void* table, int32_t max_slots, int64_t max_chunks, int32_t iters, cudaStream_t s) {
-  if (!table || max_slots <= 0 || max_chunks <= 0 || iters < 0) return FEA_EINVAL;
-  PcgbView V = pcgb_view(table, max_slots);
-  V.chunk_local = V.chunk_slot + max_chunks;
-  const unsigned grid = occ_grid(k_pcgb_spmv, max_chunks, 1);
-  const unsigned g2 = occ_grid(k_pcgb_update, max_chunks, 1);
-  const unsigned g3 = occ_grid(k_pcgb_p, max_chunks, 1);
+extern "C" int fea_pcgb_iterate(void* table, int32_t max_slots, int64_t max_items, int32_t iters, cudaStream_t s) {
+  if (!table || max_slots <= 0 || max_items <= 0 || iters < 0) return FEA_EINVAL;
+  PcgbView V = pcgb_view(table, max_slots, max_items);
+  const int64_t warps_needed = max_items;
+  const unsigned g1 = occ_grid(k_pcgb_spmv, warps_needed, PCG_WARPS);
+  const unsigned g2 = occ_grid(k_pcgb_update, warps_needed, PCG_WARPS);
+  const unsigned g3 = occ_grid(k_pcgb_p, warps_needed, PCG_WARPS);
   for (int32_t k = 0; k < iters; ++k) {
-    k_pcgb_spmv<<<grid, PCG_TPB, 0, s>>>(V);
+    k_pcgb_spmv<<<g1, PCG_TPB, 0, s>>>(V);
     k_pcgb_update<<<g2, PCG_TPB, 0, s>>>(V);
     k_pcgb_p<<<g3, PCG_TPB, 0, s>>>(V);
     count_launch(3);
@@ -1037,10 +1287,11 @@ extern "C" int fea_pcgb_iterate(void* table, int32_t max_slots, int64_t max_chun
   return (int)cudaGetLastError();
 }
 
-extern "C" int fea_pcgb_state(void* table, int32_t max_slots, int32_t nslots, double* out_dev, cudaStream_t s) {
-  if (!table || nslots < 0 || nslots > max_slots || (nslots && !out_dev)) return FEA_EINVAL;
+extern "C" int fea_pcgb_state(void* table, int32_t max_slots, int64_t max_items, int32_t nslots, double* out_dev,
+                              cudaStream_t s) {
+  if (!table || nslots < 0 || nslots > max_slots || max_items <= 0 || (nslots && !out_dev)) return FEA_EINVAL;
   if (!nslots) return FEA_OK;
-  PcgbView V = pcgb_view(table, max_slots);
+  PcgbView V = pcgb_view(table, max_slots, max_items);
   k_pcgb_state<<<(nslots + 127) / 128, 128, 0, s>>>(V, nslots, out_dev);
   count_launch();
   return (int)cudaGetLastError();

@@ -175,9 +175,9 @@ def solve_plain(requests, clock=None, keep=True):
 class BatchedPCG:
     """Device table and slots of the batched PCG (fea_pcgb_*)."""
 
-    def __init__(self, max_slots, max_chunks, round_iters=32, use_graph=True, device=None):
+    def __init__(self, max_slots, max_items, round_iters=32, use_graph=True, device=None):
         self.device = torch.device(device if device is not None else "cuda")
-        self.max_slots, self.max_chunks = int(max_slots), int(max_chunks)
+        self.max_slots, self.max_chunks = int(max_slots), int(max_items)
         nbytes = int(L.fea_pcgb_table_bytes(self.max_slots, self.max_chunks))
         self.table = torch.zeros((nbytes + 7) // 8, dtype=torch.float64, device=self.device)
         self.desc = (L.PcgbSlot * self.max_slots)()
@@ -202,14 +202,28 @@ class BatchedPCG:
     def free_slots(self):
         return [k for k in range(self.max_slots) if self.keep[k] is None]
 
-    def assign(self, k, plan, lin, work):
-        """Slot k solves lin (a solver.LinearSolve) on plan's CSR; work: pcgb work buffer."""
+    @staticmethod
+    def work_len(plan):
+        """Work doubles of a slot on plan's matrix, node-row or CSR SpMV."""
+        return int(max(L.fea_pcgb_work_len(plan.ndof, plan.n_nodes), L.fea_pcgb_work_len(plan.ndof, 0)))
+
+    def assign(self, k, plan, lin, work, node_rows=True):
+        """Slot k solves lin (a solver.LinearSolve) on plan's matrix; work: pcgb
+        work buffer of work_len(plan) doubles.  node_rows: SpMV over the plan's
+        node rows (else CSR rows)."""
         d = self.desc[k]
         d.n, d.nnz = plan.ndof, plan.nnz
         d.indptr_dev, d.indices_dev = plan.indptr.data_ptr(), plan.indices.data_ptr()
         d.values_dev, d.b_dev, d.x_dev = lin.K.data_ptr(), lin.b.data_ptr(), lin.x.data_ptr()
         d.work_dev, d.work_len = work.data_ptr(), work.numel()
         d.tol, d.max_iter, d.active = float(lin.tol), int(lin.cap), 1
+        if node_rows:
+            d.n_nodes = plan.n_nodes
+            d.vbase_dev, d.rowlen_dev, d.dbase_dev = plan.vbase.data_ptr(), plan.rowlen.data_ptr(), plan.dbase.data_ptr()
+            d.mask_dev = plan.mask.data_ptr()
+        else:
+            d.n_nodes = 0
+            d.vbase_dev = d.rowlen_dev = d.dbase_dev = d.mask_dev = None
         self.keep[k] = (plan, lin, work)
         self._dirty = True
 
@@ -242,8 +256,8 @@ class BatchedPCG:
         self.rounds += 1
 
     def poll(self):
-        L.check(L.fea_pcgb_state(vptr(self.table), self.max_slots, self.max_slots, vptr(self.state), stream()),
-                "fea_pcgb_state")
+        L.check(L.fea_pcgb_state(vptr(self.table), self.max_slots, self.max_chunks, self.max_slots, vptr(self.state),
+                                 stream()), "fea_pcgb_state")
         return self.state.view(-1, 4).cpu().numpy()
 
     def poll_async(self):
@@ -251,8 +265,8 @@ class BatchedPCG:
         if not hasattr(self, "_host_state"):
             self._host_state = torch.empty(4 * self.max_slots, dtype=torch.float64, pin_memory=True)
             self._ev = torch.cuda.Event()
-        L.check(L.fea_pcgb_state(vptr(self.table), self.max_slots, self.max_slots, vptr(self.state), stream()),
-                "fea_pcgb_state")
+        L.check(L.fea_pcgb_state(vptr(self.table), self.max_slots, self.max_chunks, self.max_slots, vptr(self.state),
+                                 stream()), "fea_pcgb_state")
         self._host_state.copy_(self.state, non_blocking=True)
         self._ev.record()
 
@@ -284,7 +298,9 @@ def serve(requests, max_slots=32, round_iters=32, mem_budget=32 << 30, use_graph
     """Serve `requests` (arrival times honoured) with continuous batching.
     Returns (results in request order, server statistics)."""
     dev = torch.device("cuda")
-    max_chunks = max_slots * (max((request_rows(r) + 255) // 256 for r in requests) if requests else 1)
+    # items of the largest admissible batch: SpMV items of 16 nodes (3 rows
+    # per node at most) outnumber update items of 256 rows
+    max_chunks = max_slots * (max((request_rows(r) // 3 + 15) // 16 + 1 for r in requests) if requests else 1)
     eng = BatchedPCG(max_slots, max_chunks, round_iters, use_graph, dev)
     waiting = sorted(requests, key=lambda r: r.arrival)
     prep_streams = [torch.cuda.Stream() for _ in range(prep_threads)]
@@ -309,9 +325,18 @@ def serve(requests, max_slots=32, round_iters=32, mem_budget=32 << 30, use_graph
                                       job.admitted, time.perf_counter() - t0)
         mem_used -= job.bytes
 
+    timing = {"newton_host_s": 0.0, "wait_s": 0.0, "prep_s": 0.0}
+
     def advance(job, first=False):
         """Run the job's Newton iteration up to its next tangent solve (on the
         work stream, while the GPU iterates the other slots)."""
+        t_a = time.perf_counter()
+        try:
+            return _advance(job, first)
+        finally:
+            timing["newton_host_s"] += time.perf_counter() - t_a
+
+    def _advance(job, first):
         with torch.cuda.stream(work_stream):
             try:
                 job.lin = next(job.gen) if first else job.gen.send(None)
@@ -319,8 +344,7 @@ def serve(requests, max_slots=32, round_iters=32, mem_budget=32 << 30, use_graph
                 finish(job, stop.value)
                 return False
             if job.work is None:
-                job.work = torch.empty(int(L.fea_pcgb_work_len(job.asm.plan.ndof)), dtype=torch.float64,
-                                       device=dev)
+                job.work = torch.empty(BatchedPCG.work_len(job.asm.plan), dtype=torch.float64, device=dev)
         queue_slot.append(job)
         return True
 
@@ -352,7 +376,9 @@ def serve(requests, max_slots=32, round_iters=32, mem_budget=32 << 30, use_graph
             advance(job)
         finished.clear()
         if in_flight:
+            t_w = time.perf_counter()
             state = eng.wait()
+            timing["wait_s"] += time.perf_counter() - t_w
             in_flight = False
             busy_rounds += 1
             for k, job in enumerate(slots):
@@ -389,6 +415,6 @@ def serve(requests, max_slots=32, round_iters=32, mem_budget=32 << 30, use_graph
         in_flight = True
     pool.shutdown()
     stats = {"rounds": busy_rounds, "graph": eng.graph is not None, "max_slots": max_slots,
-             "round_iters": round_iters, "wall_s": time.perf_counter() - t0}
+             "round_iters": round_iters, "wall_s": time.perf_counter() - t0, **timing}
     return [results[r.rid] for r in sorted(requests, key=lambda r: r.rid)], stats
 

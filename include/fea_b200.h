@@ -287,17 +287,19 @@ int fea_pcg_solve_mixed_nodes(const fea_nodes_t* nodes, const int32_t* indices_d
                               int64_t work_len, int32_t* iters, int32_t* outer, double* relres,
                               cudaStream_t stream);
 /* ---------------------------------------------------------------------------
- * Batched Jacobi-PCG over independent CSR systems ("slots"), for serving
- * many static solves at once (no counterpart in the reference, which solves
- * one system at a time with _linear_solver.conjugate_gradient,
- * _linear_solver.py:6-42).  Each slot's rows are cut into fixed chunks of 256
- * rows; every kernel walks the chunk list of all active slots, and each slot
- * keeps its own scalars, partial sums and stop test (same test and status
- * codes as fea_pcg_solve with jacobi = 1).  A slot's iterates do not depend
- * on the other slots: alone or in a batch, it computes the same bits.
- *   table: fea_pcgb_table_bytes(max_slots, max_chunks) bytes of device memory.
+ * Batched Jacobi-PCG over independent systems ("slots"), for serving many
+ * static solves at once (no counterpart in the reference, which solves one
+ * system at a time with _linear_solver.conjugate_gradient,
+ * _linear_solver.py:6-42).  Work items are warp-sized and fixed per slot:
+ * SpMV items of 16 nodes (plan layout) or 16 rows (CSR), update items of 256
+ * rows; every kernel walks the item lists of all active slots, and each slot
+ * keeps its own scalars, per-item partial sums and stop test (same test and
+ * status codes as fea_pcg_solve with jacobi = 1).  A slot's iterates do not
+ * depend on the other slots: alone or in a batch, it computes the same bits.
+ *   table: fea_pcgb_table_bytes(max_slots, max_items) bytes of device memory;
+ *     max_items bounds the items of all active slots in each list.
  *   fea_pcgb_set: loads the slot table (host array of nslots descriptors;
- *     work == NULL marks an empty slot) and the chunk list of the active
+ *     work == NULL marks an empty slot) and the item lists of the active
  *     slots; synchronises `stream`.
  *   fea_pcgb_start: initial residual, Jacobi scaling and state of one slot
  *     (x holds the initial guess).
@@ -315,20 +317,28 @@ typedef struct {
   const double* values_dev;
   const double* b_dev;
   double* x_dev;               /* initial guess in, iterate out               */
-  double* work_dev;            /* fea_pcgb_work_len(n) doubles; NULL: empty   */
+  double* work_dev;            /* fea_pcgb_work_len(n, n_nodes) doubles; NULL: empty */
   int64_t work_len;
   double tol;
   int32_t max_iter;
   int32_t active;              /* 0: kept in the table, not iterated          */
+  /* Optional plan layout of the matrix (vbase_dev NULL: plain CSR rows): the
+   * fea_nodes_t arrays, so that the SpMV runs node rows. */
+  int64_t n_nodes;
+  const int64_t* vbase_dev;
+  const int32_t* rowlen_dev;
+  const int32_t* dbase_dev;
+  const uint8_t* mask_dev;
 } fea_pcgb_slot_t;
-int64_t fea_pcgb_work_len(int64_t n);
-int64_t fea_pcgb_table_bytes(int32_t max_slots, int64_t max_chunks);
-int fea_pcgb_set(void* table_dev, int32_t max_slots, int64_t max_chunks, int32_t nslots,
+int64_t fea_pcgb_work_len(int64_t n, int64_t n_nodes);
+int64_t fea_pcgb_table_bytes(int32_t max_slots, int64_t max_items);
+int fea_pcgb_set(void* table_dev, int32_t max_slots, int64_t max_items, int32_t nslots,
                  const fea_pcgb_slot_t* slots, cudaStream_t stream);
-int fea_pcgb_start(void* table_dev, int32_t max_slots, int64_t max_chunks, int32_t slot, int64_t n, int64_t nnz,
+int fea_pcgb_start(void* table_dev, int32_t max_slots, int64_t max_items, int32_t slot, int64_t n, int64_t nnz,
                    cudaStream_t stream);
-int fea_pcgb_iterate(void* table_dev, int32_t max_slots, int64_t max_chunks, int32_t iters, cudaStream_t stream);
-int fea_pcgb_state(void* table_dev, int32_t max_slots, int32_t nslots, double* out_dev, cudaStream_t stream);
+int fea_pcgb_iterate(void* table_dev, int32_t max_slots, int64_t max_items, int32_t iters, cudaStream_t stream);
+int fea_pcgb_state(void* table_dev, int32_t max_slots, int64_t max_items, int32_t nslots, double* out_dev,
+                   cudaStream_t stream);
 
 /* values32 = (float) values */
 int fea_convert_f32(int64_t nnz, const double* values_dev, float* values32_dev, cudaStream_t stream);

@@ -29,14 +29,14 @@ def test_batched_pcg_slots_match_single_solves():
         asm = serving.build_assembly(r)
         R, K = asm.assemble_csr(asm.GC)
         systems.append((asm, (-R).contiguous(), K.clone()))
-    eng = serving.BatchedPCG(4, 4 * 64, round_iters=16)
+    eng = serving.BatchedPCG(4, 4 * 1024, round_iters=16)
     xs, works = [], []
     import fea_b200._lib as L
     from fea_b200.solver import LinearSolve
     for k, (asm, b, K) in enumerate(systems):
         x = torch.zeros_like(b)
-        w = torch.empty(int(L.fea_pcgb_work_len(asm.plan.ndof)), dtype=torch.float64, device="cuda")
-        eng.assign(k, asm.plan, LinearSolve(K, b, x, 1e-24, 20000, True), w)
+        w = torch.empty(serving.BatchedPCG.work_len(asm.plan), dtype=torch.float64, device="cuda")
+        eng.assign(k, asm.plan, LinearSolve(K, b, x, 1e-24, 20000, True), w, node_rows=(k != 1))
         xs.append(x)
         works.append(w)
     eng.sync()
@@ -57,9 +57,9 @@ def test_batched_pcg_slots_match_single_solves():
         assert float(r.norm() / b.norm()) < 1e-10
     # the first system alone in the engine gives the same bits
     asm, b, K = systems[0]
-    eng1 = serving.BatchedPCG(1, 64, round_iters=16)
+    eng1 = serving.BatchedPCG(1, 1024, round_iters=16)
     x = torch.zeros_like(b)
-    w = torch.empty(int(L.fea_pcgb_work_len(asm.plan.ndof)), dtype=torch.float64, device="cuda")
+    w = torch.empty(serving.BatchedPCG.work_len(asm.plan), dtype=torch.float64, device="cuda")
     eng1.assign(0, asm.plan, LinearSolve(K, b, x, 1e-24, 20000, True), w)
     eng1.sync()
     eng1.start(0)
