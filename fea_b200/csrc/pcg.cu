@@ -456,6 +456,53 @@ __global__ void k_axpy_f32(int64_t n, double* __restrict__ x, const float* __res
   if (i < n) x[i] += (double)d[i];
 }
 
+// Residual replacement of the mixed solver (after x64 += x32, x32 = 0):
+// r64 = b - A x64 (A x64 in r64 on entry), r32 = float(r64), z32 =
+// float(r32 dinv), and in the last block: the true stop test
+// (r64.D^-1 r64)/(b.D^-1 b) into st64, rho' = r32.z32 and beta' = rho' beta /
+// rho (the FP32 recurrence continues with the true residual and the same
+// search direction), and the FP32 done flag cleared unless the true residual
+// has converged.
+__global__ void __launch_bounds__(PCG_TPB) k_mixed_replace(int64_t n, const double* __restrict__ b,
+                                                           double* __restrict__ r64, const double* __restrict__ dinv,
+                                                           float* __restrict__ r32, float* __restrict__ z32,
+                                                           double* st64, double* st32, double* part,
+                                                           unsigned* counter, double tol) {
+  __shared__ double sh[PCG_WARPS];
+  double c_rr = 0.0, c_rz = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * PCG_TPB + threadIdx.x; i < n; i += (int64_t)gridDim.x * PCG_TPB) {
+    const double ri = b[i] - r64[i];
+    r64[i] = ri;
+    const float rf = (float)ri;
+    r32[i] = rf;
+    const double zi = (double)rf * dinv[i];
+    const float zf = (float)zi;
+    z32[i] = zf;
+    c_rr += ri * ri * dinv[i];
+    c_rz += (double)rf * zi;
+  }
+  const double s1 = block_sum_w(c_rr, sh);
+  const double s2 = block_sum_w(c_rz, sh);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = s1;
+    part[2 * blockIdx.x + 1] = s2;
+  }
+  if (last_block(counter)) {
+    const double rr = sum_partials(part, gridDim.x, 2, 0, sh);
+    const double rho = sum_partials(part, gridDim.x, 2, 1, sh);
+    if (threadIdx.x == 0) {
+      st64[S_RZ] = rr;
+      const bool conv = rr / st64[S_RZ0] < tol;
+      st64[S_DONE] = conv ? 1.0 : 0.0;
+      const double rho_old = st32[S_RZ], beta = st32[S_BETA];
+      st32[S_BETA] = rho_old != 0.0 ? rho * beta / rho_old : 0.0;
+      st32[S_RZ] = rho;
+      if (st32[S_STATUS] == 0.0) st32[S_DONE] = conv ? 1.0 : 0.0;
+      *counter = 0u;
+    }
+  }
+}
+
 static int lanes_for(int64_t n, int64_t nnz) {
   double avg = n ? (double)nnz / (double)n : 0.0;
   return avg >= 40.0 ? 32 : (avg >= 12.0 ? 16 : 8);
@@ -618,7 +665,13 @@ template <class Op64, class Op32>
 static int pcg_mixed(const Op64& A, const Op32& A32, int64_t n, const double* b, double* x, double tol,
                      double inner_tol, int max_iter, int check_every, double* work, int32_t* iters, int32_t* outer,
                      double* relres, cudaStream_t s) {
-  PcgWork W = carve(work, n);                 // r = FP64 residual, q = FP64 A x
+  // FP32 CG with FP64 residual replacement: the FP32 iterate x32 holds the
+  // correction since the last replacement; every `check_every` iterations
+  // x64 += x32, the true residual b - A x64 is formed in FP64 and replaces
+  // the FP32 one, and the recurrence continues with the same search
+  // direction.  The stop test is the FP64 one, on the true residual.
+  (void)inner_tol;
+  PcgWork W = carve(work, n);                 // st64 and r64 (FP64 residual), dinv
   double* st2 = work + S_LEN + 2 + 5 * n + part_len(n);
   unsigned* counter2 = (unsigned*)(st2 + S_LEN);
   float* f = (float*)(st2 + S_LEN + 2);
@@ -627,38 +680,59 @@ static int pcg_mixed(const Op64& A, const Op32& A32, int64_t n, const double* b,
   cudaMemsetAsync(counter2, 0, 2 * sizeof(unsigned), s);
   diag_inv(A, W.dinv, 1, s);
   const unsigned vg = vec_grid<double>(n);
-  int total = 0, nouter = 0;
-  double rel = 0.0;
+  const unsigned vgf = vec_grid<float>(n);
+  // FP64 residual of the initial guess and the reference norm b.D^-1 b
+  spmv(A, (const double*)x, W.r, nullptr, nullptr, nullptr, 0, s);
+  k_pcg_setup<double><<<vg, PCG_TPB, 0, s>>>(n, b, W.r, W.z, W.p, W.dinv, W.st, W.part, W.counter);
+  count_launch();
+  double h64[S_LEN];
+  cudaMemcpyAsync(h64, W.st, sizeof(h64), cudaMemcpyDeviceToHost, s);
+  if (cudaError_t e = cudaStreamSynchronize(s)) return (int)e;
+  double rel = h64[S_RZ] / h64[S_RZ0];
+  int total = 0, nrep = 0;
   int status = FEA_ENOTCONV;
-  while (total < max_iter) {
-    // FP64 residual, stop test, and the inner right-hand side = r
-    spmv(A, (const double*)x, W.r, nullptr, nullptr, nullptr, 0, s);
-    k_pcg_setup<double><<<vg, PCG_TPB, 0, s>>>(n, b, W.r, W.z, W.p, W.dinv, W.st, W.part, W.counter);
-    count_launch();
-    double host[S_LEN];
-    cudaMemcpyAsync(host, W.st, sizeof(host), cudaMemcpyDeviceToHost, s);
-    if (cudaError_t e = cudaStreamSynchronize(s)) return (int)e;
-    rel = host[S_RZ] / host[S_RZ0];
-    if (host[S_DONE] != 0.0 || rel < tol) {
-      status = FEA_OK;
-      break;
-    }
-    // inner solve: b_inner = r (FP64 in W.r), x_inner = 0
+  if (h64[S_DONE] != 0.0 || rel < tol) {
+    status = FEA_OK;
+  } else {
+    // FP32 start from r64: x32 = 0, r32 = r64, z32, p32, rho; stop test scale from b
     cudaMemsetAsync(xf, 0, sizeof(float) * n, s);
-    int it = 0;
-    double rr = 0.0;
-    int ri = pcg_core<Op32, float>(A32, n, W.r, xf, rf, zf, pf, qf, W.dinv, st2, counter2, W.part, inner_tol,
-                                   max_iter - total, check_every, &it, &rr, s);
-    total += it;
-    ++nouter;
-    k_axpy_f32<<<grid_for(n, 256), 256, 0, s>>>(n, x, xf);
+    cudaMemsetAsync(rf, 0, sizeof(float) * n, s);
+    k_pcg_setup<float><<<vgf, PCG_TPB, 0, s>>>(n, W.r, rf, zf, pf, W.dinv, st2, W.part, counter2);
     count_launch();
-    if (ri == FEA_EBREAKDOWN) { status = ri; break; }
-    if (ri > 0) return ri;
-    if (it == 0) { status = FEA_EBREAKDOWN; break; }
+    cudaMemcpyAsync(st2 + S_RZ0, W.st + S_RZ0, sizeof(double), cudaMemcpyDeviceToDevice, s);
+    const int ce = std::max(1, check_every);
+    while (total < max_iter) {
+      const int batch = std::min(ce, max_iter - total);
+      for (int k = 0; k < batch; ++k) {
+        spmv(A32, (const float*)pf, qf, st2, W.part, counter2, 1, s);
+        k_pcg_update<float><<<vgf, PCG_TPB, 0, s>>>(n, xf, rf, zf, pf, qf, W.dinv, st2, W.part, counter2, 0.0,
+                                                   max_iter);
+        count_launch();
+        if (k + 1 < batch) {
+          k_pcg_p<float><<<vgf, PCG_TPB, 0, s>>>(n, pf, zf, st2);
+          count_launch();
+        }
+      }
+      total += batch;
+      // replacement: x64 += x32, r64 = b - A x64, r32 / z32 / rho / beta from it
+      k_axpy_f32<<<grid_for(n, 256), 256, 0, s>>>(n, x, xf);
+      cudaMemsetAsync(xf, 0, sizeof(float) * n, s);
+      spmv(A, (const double*)x, W.r, nullptr, nullptr, nullptr, 0, s);
+      k_mixed_replace<<<vg, PCG_TPB, 0, s>>>(n, b, W.r, W.dinv, rf, zf, W.st, st2, W.part, W.counter, tol);
+      k_pcg_p<float><<<vgf, PCG_TPB, 0, s>>>(n, pf, zf, st2);
+      count_launch(3);
+      ++nrep;
+      double h32[S_LEN];
+      cudaMemcpyAsync(h64, W.st, sizeof(h64), cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(h32, st2, sizeof(h32), cudaMemcpyDeviceToHost, s);
+      if (cudaError_t e = cudaStreamSynchronize(s)) return (int)e;
+      rel = h64[S_RZ] / h64[S_RZ0];
+      if (rel < tol) { status = FEA_OK; break; }
+      if (h32[S_STATUS] == (double)FEA_EBREAKDOWN) { status = FEA_EBREAKDOWN; break; }
+    }
   }
   if (iters) *iters = total;
-  if (outer) *outer = nouter;
+  if (outer) *outer = nrep;
   if (relres) *relres = rel;
   return status;
 }

@@ -253,9 +253,15 @@ int fea_pcg_solve(int64_t n, const int64_t* indptr_dev, const int32_t* indices_d
                   const double* b_dev, double* x_dev, double tol, int32_t max_iter, int32_t check_every,
                   int32_t jacobi, double* work_dev, int64_t work_len, int32_t* iters, double* relres,
                   cudaStream_t stream);
-/* FP32 SpMV inner CG with FP64 iterative refinement of the residual.
- * values32_dev: float copy of values.  inner_tol: squared-ratio reduction
- * asked of each inner solve.  work: fea_pcg_mixed_work_len(n) doubles. */
+/* FP32-SpMV CG with FP64 refinement of the residual: the iterations run in
+ * FP32 (float values, vectors and SpMV; FP64 accumulation of the dot
+ * products) on the correction since the last refinement; every check_every
+ * iterations the correction is added to the FP64 solution, the true residual
+ * b - A x is formed in FP64 and replaces the FP32 one, and the recurrence
+ * continues with the same search direction (residual replacement, no
+ * restart).  The stop test is fea_pcg_solve's, on the FP64 residual.
+ * values32_dev: float copy of values.  inner_tol: unused.  outer: number of
+ * refinements.  work: fea_pcg_mixed_work_len(n) doubles. */
 int64_t fea_pcg_mixed_work_len(int64_t n);
 int fea_pcg_solve_mixed(int64_t n, const int64_t* indptr_dev, const int32_t* indices_dev,
                         const double* values_dev, const float* values32_dev,
