@@ -282,3 +282,81 @@ def test_reference_conjugate_gradient_semantics(golden):
                                                    torch.zeros(0), tol=1e-20, max_iter=20000)
     xo, _ = O.conjugate_gradient(ip, ix, vv, b, tol=1e-20, max_iter=20000)
     assert rel(x, xo) < 1e-8
+
+
+def _free_block(kind, n, jitter=0.0, rho=1.0):
+    """Unit block through the public API, without loads or boundary conditions."""
+    import fea_b200 as F
+    from tests.test_oracle_known_answers import KAPPA, MU
+    X, el = O.hex_block(n, jitter=jitter, seed=9) if kind == "C3D8" else O.tet_block(n)
+    part = F.Part(X)
+    cls = F.elements.C3D4 if kind == "C3D4" else F.elements.C3D8
+    e = cls(elems=el, elems_index=torch.arange(el.shape[0]), part=part)
+    e.set_materials(F.materials.NeoHookean(MU, KAPPA))
+    e.set_density(rho)
+    part.add_element(e)
+    asm = F.Assembly()
+    asm.add_part(part, "p")
+    asm.add_instance(F.Instance(part), "p")
+    asm.initialize()
+    return asm, X, el
+
+
+@pytest.mark.parametrize("kind", ["C3D8", "C3D4"])
+def test_rigid_rotation_zero_residual(kind):
+    """u = (Q - I) X with Q a rotation: F = Q, no stress, R = 0 and energy 0."""
+    from tests.test_oracle_known_answers import rotation
+    asm, X, _ = _free_block(kind, 3, jitter=0.1 if kind == "C3D8" else 0.0)
+    u = (X @ rotation().T - X).reshape(-1).cuda()
+    assert float(asm.assemble_force(GC=u).abs().max()) < 1e-13
+    R, _, Kv = asm.assemble_Stiffness_Matrix(GC=u)
+    assert float(R.abs().max()) < 1e-13 and bool(torch.isfinite(Kv).all())
+    assert abs(float(asm._total_Potential_Energy(GC=u))) < 1e-13
+
+
+@pytest.mark.parametrize("kind", ["C3D8", "C3D4"])
+def test_uniaxial_stretch_closed_form(kind):
+    """F = diag(lam, 1, 1): the x-force on the face x = 1 is the closed-form P11
+    times the face area 1; the block as a whole is in equilibrium."""
+    from tests.test_oracle_known_answers import uniaxial_P11, uniaxial_W
+    lam = 1.05
+    asm, X, _ = _free_block(kind, 3)
+    u = torch.zeros_like(X)
+    u[:, 0] = (lam - 1.0) * X[:, 0]
+    R = asm.assemble_force(GC=u.reshape(-1).cuda()).cpu().reshape(-1, 3)
+    P11 = uniaxial_P11(lam)
+    face = (X[:, 0] - 1.0).abs() < 1e-12
+    assert abs(float(R[face, 0].sum()) - P11) < 1e-12 * P11
+    assert abs(float(R[:, 0].sum())) < 1e-12 * P11
+    W = uniaxial_W(lam)
+    assert abs(float(asm._total_Potential_Energy(GC=u.reshape(-1).cuda())) - W) < 1e-12 * W
+
+
+def test_patch_test_jittered_c3d8():
+    """u = (F - I) X is reproduced exactly by trilinear hexes on a jittered
+    block: every interior node is in equilibrium, with and without K."""
+    from tests.test_oracle_known_answers import PATCH_F, interior_nodes
+    n = 4
+    asm, X, _ = _free_block("C3D8", n, jitter=0.15)
+    u = (X @ torch.tensor(PATCH_F, dtype=torch.float64).T - X).reshape(-1).cuda()
+    R = asm.assemble_force(GC=u).cpu().reshape(-1, 3)
+    scale = float(R.abs().max())
+    assert scale > 1e-3
+    assert float(R[interior_nodes(n)].abs().max()) < 1e-12 * scale
+    R2, _, _ = asm.assemble_Stiffness_Matrix(GC=u)
+    assert rel(R2, R.reshape(-1)) < TOL
+
+
+@pytest.mark.parametrize("kind", ["C3D8", "C3D4"])
+def test_lumped_mass_totals_rho_volume(kind):
+    """Row-sum lumped mass summed per direction = rho * mesh volume, and equal
+    to the oracle's lumped mass entry by entry."""
+    rho = 2.5
+    asm, X, el = _free_block(kind, 3, jitter=0.1 if kind == "C3D8" else 0.0, rho=rho)
+    m = (1.0 / asm.lumped_mass_inv()).cpu().reshape(-1, 3)
+    _, w, _ = O.preload_gaussian(kind, X, el)
+    vol = float(w.sum())
+    for d in range(3):
+        assert abs(float(m[:, d].sum()) - rho * vol) < 1e-12 * rho * vol
+    ref = O.Model(X, [O.Group(kind, el, 1.0, 1.0, rho)], [], []).lumped_mass_inv()
+    assert rel(asm.lumped_mass_inv(), ref) < 1e-14

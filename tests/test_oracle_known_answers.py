@@ -1,0 +1,90 @@
+"""Known-answer checks of the oracle itself (CPU): rigid rotation, the
+closed-form uniaxial Neo-Hookean stress, the patch test on a jittered C3D8
+block, and the lumped mass total rho * volume.  The same checks run through
+the CUDA path in test_gpu_parity.py."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import fea_oracle as O
+
+MU, KAPPA = 1.3, 20.0
+
+
+def _block(kind, n, jitter=0.0, rho=1.0):
+    X, el = O.hex_block(n, jitter=jitter, seed=9) if kind == "C3D8" else O.tet_block(n)
+    return O.Model(X, [O.Group(kind, el, MU, KAPPA, rho)], [], [])
+
+
+def rotation(a=0.7, b=0.3):
+    c, s = np.cos(a), np.sin(a)
+    Qz = torch.tensor([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]], dtype=torch.float64)
+    c, s = np.cos(b), np.sin(b)
+    Qx = torch.tensor([[1.0, 0.0, 0.0], [0.0, c, -s], [0.0, s, c]], dtype=torch.float64)
+    return Qz @ Qx
+
+
+def uniaxial_P11(lam, mu=MU, kappa=KAPPA):
+    """P11 of W = mu/2 (J^-2/3 I1 - 3) + kappa/2 (J-1)^2 at F = diag(lam, 1, 1):
+    dW/dF11 = mu J^-2/3 (lam - I1 / (3 J)) + kappa (J - 1) with J = lam, I1 = lam^2 + 2."""
+    return mu * lam ** (-2.0 / 3.0) * (lam - (lam ** 2 + 2.0) / (3.0 * lam)) + kappa * (lam - 1.0)
+
+
+def uniaxial_W(lam, mu=MU, kappa=KAPPA):
+    return mu / 2 * (lam ** (-2.0 / 3.0) * (lam ** 2 + 2.0) - 3.0) + kappa / 2 * (lam - 1.0) ** 2
+
+
+def interior_nodes(n):
+    i = np.arange((n + 1) ** 3)
+    ijk = np.stack([i // (n + 1) ** 2, i // (n + 1) % (n + 1), i % (n + 1)], 1)
+    return torch.from_numpy(np.all((ijk > 0) & (ijk < n), axis=1))
+
+
+PATCH_F = [[1.04, 0.02, -0.01], [0.015, 0.97, 0.03], [-0.02, 0.01, 1.02]]
+
+
+@pytest.mark.parametrize("kind", ["C3D8", "C3D4"])
+def test_rigid_rotation_zero_residual(kind):
+    m = _block(kind, 3, jitter=0.1 if kind == "C3D8" else 0.0)
+    u = m.X @ rotation().T - m.X
+    R, _ = m.assemble(u.reshape(-1), want_K=False)
+    assert float(R.abs().max()) < 1e-13
+    assert abs(float(m.energy(u.reshape(-1)))) < 1e-13
+
+
+@pytest.mark.parametrize("kind", ["C3D8", "C3D4"])
+def test_uniaxial_stretch_closed_form(kind):
+    lam = 1.05
+    m = _block(kind, 3)
+    u = torch.zeros_like(m.X)
+    u[:, 0] = (lam - 1.0) * m.X[:, 0]
+    R, _ = m.assemble(u.reshape(-1), want_K=False)
+    R = R.reshape(-1, 3)
+    P11 = uniaxial_P11(lam)
+    face = (m.X[:, 0] - 1.0).abs() < 1e-12
+    assert abs(float(R[face, 0].sum()) - P11) < 1e-12 * P11
+    assert abs(float(R[:, 0].sum())) < 1e-12 * P11
+    assert abs(float(m.energy(u.reshape(-1))) - uniaxial_W(lam)) < 1e-12 * uniaxial_W(lam)
+
+
+def test_patch_test_jittered_c3d8():
+    n = 4
+    m = _block("C3D8", n, jitter=0.15)
+    u = m.X @ torch.tensor(PATCH_F, dtype=torch.float64).T - m.X
+    R, _ = m.assemble(u.reshape(-1), want_K=False)
+    R = R.reshape(-1, 3)
+    scale = float(R.abs().max())
+    assert scale > 1e-3
+    assert float(R[interior_nodes(n)].abs().max()) < 1e-12 * scale
+
+
+@pytest.mark.parametrize("kind", ["C3D8", "C3D4"])
+def test_lumped_mass_totals_rho_volume(kind):
+    rho = 2.5
+    m = _block(kind, 3, jitter=0.1 if kind == "C3D8" else 0.0, rho=rho)
+    mass = (1.0 / m.lumped_mass_inv()).reshape(-1, 3)
+    _, w, _ = O.preload_gaussian(kind, m.X, m.groups[0].elems)
+    vol = float(w.sum())
+    assert abs(vol - 1.0) < 0.05
+    for d in range(3):
+        assert abs(float(mass[:, d].sum()) - rho * vol) < 1e-12 * rho * vol
