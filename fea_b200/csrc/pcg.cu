@@ -245,11 +245,16 @@ __global__ void __launch_bounds__(PCG_TPB) k_spmv_node(NodeOp<V> A, const X* __r
   if (mode == 1) finish_pq(contrib, st, part, counter);
 }
 
-// Node rows with LPN < 32 lanes per node (32 / LPN nodes per warp): more
-// nodes, and more loads, in flight per warp; used for the FP32 values of the
-// mixed solver, whose 4-byte loads leave the one-node-per-warp kernel
-// latency-bound.  Column passes of 3 LPN; loops and shuffles warp-uniform.
-template <int LPN, class V, class X>
+// Node rows with LPN < 32 lanes per node (32 / LPN nodes per warp), CPL
+// columns per lane per pass: more nodes, and more loads, in flight per warp;
+// used for the FP32 values of the mixed solver, whose 4-byte loads leave the
+// one-node-per-warp kernel latency-bound.  The next nodes' metadata and
+// first-pass column indices are loaded while the current nodes are
+// processed.  Used with LPN = 16, CPL = 3 (48-column passes): 96-column
+// passes (CPL = 6) need 77 registers, 3 CTAs per SM, and ran the FP32
+// iteration 0.237 ms against 0.134 ms at 64^3.  Loops and shuffles
+// warp-uniform.
+template <int LPN, int CPL, class V, class X>
 __global__ void __launch_bounds__(PCG_TPB) k_spmv_node_sub(NodeOp<V> A, const X* __restrict__ x, X* __restrict__ y,
                                                            double* st, double* part, unsigned* counter, int mode) {
   if (mode == 1 && st[S_DONE] != 0.0) return;
@@ -259,55 +264,88 @@ __global__ void __launch_bounds__(PCG_TPB) k_spmv_node_sub(NodeOp<V> A, const X*
   const int sub = lane / LPN, hl = lane % LPN;
   const int64_t step = (int64_t)gridDim.x * PCG_WARPS * NPW;
   double contrib = 0.0;
-  for (int64_t base = ((int64_t)blockIdx.x * PCG_WARPS + warp) * NPW; base < A.n_nodes; base += step) {
-    const int64_t nd = base + sub;
-    const bool valid = nd < A.n_nodes;
-    const unsigned m = valid ? A.mask[nd] : 0u;
-    const int L = m ? A.rowlen[nd] : 0;
-    const int64_t vb = valid ? A.vbase[nd] : 0;
+  int64_t base = ((int64_t)blockIdx.x * PCG_WARPS + warp) * NPW;
+  int64_t nd = base + sub;
+  unsigned m = 0;
+  int L = 0;
+  int64_t vb = 0;
+  int32_t db = 0;
+  int32_t jn[CPL];
+#pragma unroll
+  for (int k = 0; k < CPL; ++k) jn[k] = 0;
+  if (nd < A.n_nodes) {
+    m = A.mask[nd];
+    L = m ? A.rowlen[nd] : 0;
+    vb = A.vbase[nd];
+    db = A.dbase[nd];
+#pragma unroll
+    for (int k = 0; k < CPL; ++k) jn[k] = hl + LPN * k < L ? __ldg(A.idx + vb + hl + LPN * k) : 0;
+  }
+  for (; base < A.n_nodes; base += step) {                  // warp-uniform
+    const int64_t nx = nd + step;
+    unsigned m2 = 0;
+    int L2 = 0;
+    int64_t vb2 = 0;
+    int32_t db2 = 0;
+    if (nx < A.n_nodes) {
+      m2 = A.mask[nx];
+      L2 = A.rowlen[nx];
+      vb2 = A.vbase[nx];
+      db2 = A.dbase[nx];
+    }
     const int f = popc3(m);
     int Lmax = L;
 #pragma unroll
     for (int o = 16; o >= LPN; o >>= 1) Lmax = max(Lmax, __shfl_xor_sync(0xffffffffu, Lmax, o));
     const V* __restrict__ v0 = A.val + vb;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-    for (int q0 = 0; q0 < Lmax; q0 += 3 * LPN) {
-      int32_t j[3];
-      bool h[3];
+    for (int q0 = 0; q0 < Lmax; q0 += CPL * LPN) {
+      int32_t j[CPL];
+      bool h[CPL];
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
+      for (int k = 0; k < CPL; ++k) {
         const int q = q0 + hl + LPN * k;
         h[k] = q < L;
-        j[k] = h[k] ? __ldg(A.idx + vb + q) : 0;
+        j[k] = q0 == 0 ? jn[k] : (h[k] ? __ldg(A.idx + vb + q) : 0);
       }
-      double va[3][3];
+      V va[3][CPL];
 #pragma unroll
       for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
+        for (int k = 0; k < CPL; ++k) {
           const int q = q0 + hl + LPN * k;
-          va[r][k] = (r < f && h[k]) ? (double)__ldcs(v0 + (int64_t)r * L + q) : 0.0;
+          va[r][k] = (r < f && h[k]) ? __ldcs(v0 + (int64_t)r * L + q) : (V)0;
         }
-      double xv[3];
+      X xv[CPL];
 #pragma unroll
-      for (int k = 0; k < 3; ++k) xv[k] = h[k] ? (double)x[j[k]] : 0.0;
-      s0 += va[0][0] * xv[0] + va[0][1] * xv[1] + va[0][2] * xv[2];
-      s1 += va[1][0] * xv[0] + va[1][1] * xv[1] + va[1][2] * xv[2];
-      s2 += va[2][0] * xv[0] + va[2][1] * xv[1] + va[2][2] * xv[2];
+      for (int k = 0; k < CPL; ++k) xv[k] = h[k] ? x[j[k]] : (X)0;
+#pragma unroll
+      for (int k = 0; k < CPL; ++k) {
+        s0 += (double)va[0][k] * (double)xv[k];
+        s1 += (double)va[1][k] * (double)xv[k];
+        s2 += (double)va[2][k] * (double)xv[k];
+      }
     }
+    const int Ln = m2 ? L2 : 0;
+#pragma unroll
+    for (int k = 0; k < CPL; ++k) jn[k] = hl + LPN * k < Ln ? __ldg(A.idx + vb2 + hl + LPN * k) : 0;
 #pragma unroll
     for (int o = LPN / 2; o > 0; o >>= 1) {
       s0 += __shfl_xor_sync(0xffffffffu, s0, o, LPN);
       s1 += __shfl_xor_sync(0xffffffffu, s1, o, LPN);
       s2 += __shfl_xor_sync(0xffffffffu, s2, o, LPN);
     }
-    if (hl == 0 && m) {
-      const int64_t r = A.dbase[nd];
-      y[r] = (X)s0;
-      contrib += s0 * (double)x[r];
-      if (f > 1) { y[r + 1] = (X)s1; contrib += s1 * (double)x[r + 1]; }
-      if (f > 2) { y[r + 2] = (X)s2; contrib += s2 * (double)x[r + 2]; }
+    if (m && hl < f) {
+      const int64_t r = db + hl;
+      const double sr = hl == 0 ? s0 : (hl == 1 ? s1 : s2);
+      y[r] = (X)sr;
+      contrib += sr * (double)x[r];
     }
+    nd = nx;
+    m = m2;
+    L = Ln;
+    vb = vb2;
+    db = db2;
   }
   if (mode == 1) finish_pq(contrib, st, part, counter);
 }
@@ -354,7 +392,13 @@ __global__ void k_dinv_csr(CsrOp<V> A, double* __restrict__ dinv, int identity) 
   }
 }
 
-// x += alpha p; r -= alpha q; z = r / |d|; partial r.z; last block: beta, stop test
+// x += alpha p; r -= alpha q; z = r / |d|; partial r.z; last block: beta, stop test.
+// Each thread takes PCG_VU rows a grid stride apart and issues all their
+// loads before any arithmetic (one resident wave covers the vector in one
+// pass up to PCG_VU x 303k rows), so the loads of a thread overlap instead
+// of paying one round trip per row.
+constexpr int PCG_VU = 4;
+
 template <class X>
 __global__ void __launch_bounds__(PCG_TPB) k_pcg_update(int64_t n, X* __restrict__ x, X* __restrict__ r,
                                                         X* __restrict__ z, const X* __restrict__ p,
@@ -365,13 +409,33 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_update(int64_t n, X* __restrict
   if (st[S_DONE] != 0.0) return;
   const double alpha = st[S_ALPHA];
   double contrib = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * PCG_TPB + threadIdx.x; i < n; i += (int64_t)gridDim.x * PCG_TPB) {
-    x[i] = (X)((double)x[i] + alpha * (double)p[i]);
-    double ri = (double)r[i] - alpha * (double)q[i];
-    r[i] = (X)ri;
-    double zi = ri * dinv[i];
-    z[i] = (X)zi;
-    contrib += ri * zi;
+  const int64_t stride = (int64_t)gridDim.x * PCG_TPB;
+  for (int64_t i0 = (int64_t)blockIdx.x * PCG_TPB + threadIdx.x; i0 < n; i0 += PCG_VU * stride) {
+    X xv[PCG_VU], rv[PCG_VU], pv[PCG_VU], qv[PCG_VU];
+    double dv[PCG_VU];
+#pragma unroll
+    for (int u = 0; u < PCG_VU; ++u) {
+      const int64_t i = i0 + u * stride;
+      if (i < n) {
+        xv[u] = x[i];
+        rv[u] = r[i];
+        pv[u] = p[i];
+        qv[u] = q[i];
+        dv[u] = dinv[i];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PCG_VU; ++u) {
+      const int64_t i = i0 + u * stride;
+      if (i < n) {
+        x[i] = (X)((double)xv[u] + alpha * (double)pv[u]);
+        const double ri = (double)rv[u] - alpha * (double)qv[u];
+        r[i] = (X)ri;
+        const double zi = ri * dv[u];
+        z[i] = (X)zi;
+        contrib += ri * zi;
+      }
+    }
   }
   double bs = block_sum_w(contrib, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = bs;
@@ -401,8 +465,23 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcg_p(int64_t n, X* __restrict__ p,
                                                    const double* st) {
   if (st[S_DONE] != 0.0) return;
   const double beta = st[S_BETA];
-  for (int64_t i = (int64_t)blockIdx.x * PCG_TPB + threadIdx.x; i < n; i += (int64_t)gridDim.x * PCG_TPB)
-    p[i] = (X)((double)z[i] + beta * (double)p[i]);
+  const int64_t stride = (int64_t)gridDim.x * PCG_TPB;
+  for (int64_t i0 = (int64_t)blockIdx.x * PCG_TPB + threadIdx.x; i0 < n; i0 += PCG_VU * stride) {
+    X zv[PCG_VU], pv[PCG_VU];
+#pragma unroll
+    for (int u = 0; u < PCG_VU; ++u) {
+      const int64_t i = i0 + u * stride;
+      if (i < n) {
+        zv[u] = z[i];
+        pv[u] = p[i];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PCG_VU; ++u) {
+      const int64_t i = i0 + u * stride;
+      if (i < n) p[i] = (X)((double)zv[u] + beta * (double)pv[u]);
+    }
+  }
 }
 
 // setup (dinv given): r = b - Ax (Ax in r on entry), z = dinv r, p = z,
@@ -561,7 +640,7 @@ template <class V, class X>
 static void spmv(const NodeOp<V>& A, const X* x, X* y, double* st, double* part, unsigned* counter, int mode,
                  cudaStream_t s) {
   if (sizeof(V) == 4) {
-    k_spmv_node_sub<16, V, X><<<occ_grid(k_spmv_node_sub<16, V, X>, A.n_nodes, 2 * PCG_WARPS), PCG_TPB, 0, s>>>(
+    k_spmv_node_sub<16, 3, V, X><<<occ_grid(k_spmv_node_sub<16, 3, V, X>, A.n_nodes, 2 * PCG_WARPS), PCG_TPB, 0, s>>>(
         A, x, y, st, part, counter, mode);
   } else {
     k_spmv_node<V, X><<<occ_grid(k_spmv_node<V, X>, A.n_nodes, PCG_WARPS), PCG_TPB, 0, s>>>(A, x, y, st, part,
