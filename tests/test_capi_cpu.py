@@ -220,3 +220,53 @@ def test_serving_requests_are_seeded_and_bounded():
         assert serving.request_rows(r) == 3 * X.shape[0]
         assert 0.5 * r.n_elems <= el.shape[0] <= 2.0 * r.n_elems
         assert abs(X[:, 0].max() - 1.0) < 1e-12 and abs(X[:, 0].min() - (1.0 - r.length)) < 1e-9
+
+
+def _hand_csr(n, free):
+    """CSR of an n^3 C3D8 block built from the neighbour rule alone: nodes
+    (i,j,k) and (i',j',k') share an element iff every index differs by at
+    most 1; DOFs numbered in node order over the free ones."""
+    N = (n + 1) ** 3
+    ijk = [(i // (n + 1) ** 2, i // (n + 1) % (n + 1), i % (n + 1)) for i in range(N)]
+    dof = {}
+    for a in range(N):
+        for d in range(3):
+            if free[a][d]:
+                dof[(a, d)] = len(dof)
+    indptr, indices = [0], []
+    for a in range(N):
+        for d in range(3):
+            if not free[a][d]:
+                continue
+            cols = sorted(dof[(c, e)] for c in range(N) for e in range(3)
+                          if free[c][e] and all(abs(p - q) <= 1 for p, q in zip(ijk[a], ijk[c])))
+            indices += cols
+            indptr.append(len(indices))
+    return np.array(indptr), np.array(indices)
+
+
+@pytest.mark.parametrize("clamp", [False, True])
+def test_csr_of_eight_hex_mesh_by_hand(clamp):
+    """2x2x2 C3D8 block (8 elements, 27 nodes): all free, 8 corner nodes
+    couple to 8 nodes, 12 edge nodes to 12, 6 face nodes to 18 and the centre
+    to 27, so nnz = 9 (64 + 144 + 108 + 27) = 3087; with x = 0 clamped the
+    9 nodes there drop out of rows and columns."""
+    from fea_b200 import _lib as L
+    X, el = O.hex_block(2)
+    N = X.shape[0]
+    fixed = np.nonzero(X[:, 0].numpy() < 1e-9)[0] if clamp else np.zeros(0, np.int64)
+    free = [[i not in set(fixed.tolist())] * 3 for i in range(N)]
+    ip, ix = _hand_csr(2, free)
+    if not clamp:
+        assert ip[-1] == 3087 and len(ip) == 82
+    else:
+        assert len(ip) == 3 * 18 + 1
+    mask = np.full(N, 7, np.uint8)
+    mask[fixed] = 0
+    hp = _plan(N, mask, [("C3D8", el.numpy())])
+    np.testing.assert_array_equal(hp.array(L.FEA_A_INDPTR), ip)
+    np.testing.assert_array_equal(hp.array(L.FEA_A_INDICES), ix)
+    m = O.Model(X, [O.Group("C3D8", el, 1.0, 10.0)], [], [(fixed, (0, 1, 2))] if clamp else [])
+    _, (oip, oix, _) = m.assemble(torch.zeros(int(m.free_mask().sum()), dtype=torch.float64))
+    np.testing.assert_array_equal(oip.numpy(), ip)
+    np.testing.assert_array_equal(oix.numpy(), ix)
