@@ -34,7 +34,7 @@ FEA_C3D4, FEA_C3D8, FEA_T3, FEA_Q4 = 4, 8, 3, 40
  FEA_A_ADJPTR, FEA_A_ADJCOL, FEA_A_ADJOFF) = range(10, 20)
 G_BASE, F_BASE = 30, 50
 (A_INC, A_BOFF, A_NODEINC, A_CHUNKPTR, A_CHUNKINC, S_NCHUNK, S_MAXVAL, S_THREADS, S_SMEM, A_CHUNKLIST,
- A_CHUNKDIM, A_SOFF, A_ROFF, A_BLKPTR, A_BLKCON, A_ALLPTR, A_ALLINC) = range(17)
+ A_CHUNKDIM, A_SOFF, A_ROFF, A_BLKPTR, A_BLKCON, A_ALLPTR, A_ALLINC, A_INCPOS) = range(18)
 
 
 class FeaError(RuntimeError):
@@ -65,7 +65,7 @@ class Group(C.Structure):
                 ("roff_dev", C.c_void_p), ("blkptr_dev", C.c_void_p), ("blkcon_dev", C.c_void_p),
                 ("allptr_dev", C.c_void_p), ("allinc_dev", C.c_void_p),
                 ("nchunk", C.c_int64), ("maxval", C.c_int32), ("threads", C.c_int32),
-                ("smem_doubles", C.c_int64)]
+                ("smem_doubles", C.c_int64), ("incpos_dev", C.c_void_p)]
 
 
 class PcgbSlot(C.Structure):

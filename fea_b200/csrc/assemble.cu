@@ -51,6 +51,7 @@ struct VolParams {
   const int32_t* __restrict__ adjoff;
   const int64_t* __restrict__ blkptr;
   const int32_t* __restrict__ blkcon;
+  const int32_t* __restrict__ incpos;
   const double* __restrict__ gc;
   double* K;
   double* R;
@@ -304,29 +305,53 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
 // vectors in registers,
 //   K_ab = sum_g (A_a q_b^T + B_a f_b^T + q_b C_a^T + wc (g_a . g_b) I),
 //   A_a = w(alpha f_a + beta q_a), B_a = w alpha q_a, C_a = w gamma q_a,
-// and the element residual R_a = sum_g w(mu J^-2/3 f_a + c2 q_a).  The 36
-// blocks and R_e are staged in HBM; k_hex_gather then sums them per node row
-// (transposing blocks stored under (b, a)) and writes each row range once.
+// and the element residual R_a = sum_g w(mu J^-2/3 f_a + c2 q_a).  The
+// lanes then exchange their blocks through shared memory and lane a writes
+// the element's full block row (a, 0..7), transposing the blocks another lane
+// computed, and R_a as one 76-double record at the position of incidence
+// (e, a) in the node-major incidence list: every node's records are
+// contiguous in HBM, in element order.  k_hex_gat copies a node's records to
+// shared memory with coalesced 128-bit loads, sums them per column block and
+// writes each row range once.
 constexpr int HX_EPB = 8;                 // elements per CTA
 constexpr int HX_TPB = 8 * HX_EPB;        // threads per CTA
 constexpr int HX_VB = 10;                 // doubles per (gp, node) vector slot: q, f, g + pad
 constexpr int HX_VG = 82;                 // doubles per Gauss point (8 slots + 2 pad, 16-byte rows)
 constexpr int HX_SC = 8 * HX_VG;          // offset of the per-Gauss-point scalars (8 each)
 constexpr int HX_EL = HX_SC + 64;         // doubles per element (16-byte aligned)
-constexpr int HX_STAGE = 36 * 9 + 24;     // staged doubles per element: 36 blocks + R_e
+constexpr int HX_REC = 8 * 9 + 4;         // staged doubles per incidence: block row, R_a, pad (608 B)
+constexpr int HX_GW = 4;                  // warps (row nodes) per gather CTA
 constexpr int HX_GINC = 32;               // incidences per gather chunk (8 lanes each)
-constexpr int HX_GTPB = 8 * HX_GINC;
 
 // corner signs of hex node / Gauss point c (brick.py:15-25, 151-160)
 __device__ __forceinline__ double csx(int c) { return (((c + 1) >> 1) & 1) ? 1.0 : -1.0; }
 __device__ __forceinline__ double csy(int c) { return ((c >> 1) & 1) ? 1.0 : -1.0; }
 __device__ __forceinline__ double csz(int c) { return (c >> 2) ? 1.0 : -1.0; }
-// staged block slot of (row a, offset d = (b - a) mod 8), d <= 3 or (d == 4, a < 4)
-__device__ __forceinline__ int hx_slot(int a, int d) { return d < 4 ? a * 4 + d : 32 + a; }
+// Offset in an element's exchange area of double k of the record of row a:
+// k < 72 is entry w = k mod 9 of block (a, b = k / 9), held by lane a at slot
+// 8d + a, d = (b - a) mod 8, when d <= 3 or (d == 4, a < 4), else as the
+// transpose of block (b, a) at slot 8((a - b) mod 8) + b; k = 72..75 is R_a
+// and a zero pad.
+__device__ __forceinline__ int hx_rec_off(int a, int k) {
+  if (k >= 72) return 360 + 4 * a + (k - 72);
+  const int b = k / 9, w = k - 9 * b;
+  const int d = (b - a) & 7;
+  if (d < 4 || (d == 4 && a < 4)) return (8 * d + a) * 10 + w;
+  const int j = w / 3, kk = w - 3 * j;
+  return (8 * ((a - b) & 7) + b) * 10 + 3 * kk + j;
+}
 
 template <bool ER>
 __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __restrict__ stage) {
   __shared__ __align__(16) double sv[HX_EPB * HX_EL];
+  // hx_tbl[a * 38 + k2]: exchange-area offsets of doubles 2k2 and 2k2 + 1 of
+  // the record of row a
+  __shared__ uint32_t hx_tbl[8 * (HX_REC / 2)];
+  for (int i = threadIdx.x; i < 8 * (HX_REC / 2); i += HX_TPB) {
+    const int ra = i / (HX_REC / 2), k = 2 * (i - ra * (HX_REC / 2));
+    hx_tbl[i] = (uint32_t)hx_rec_off(ra, k) | ((uint32_t)hx_rec_off(ra, k + 1) << 16);
+  }
+  __syncthreads();                             // every thread reaches it: no early exit in this kernel
   const double q3 = 0.57735026918962576451;   // 1/sqrt(3)
   const int le = threadIdx.x >> 3;
   const int lane = threadIdx.x & 7;
@@ -407,8 +432,7 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
     }
   }
   __syncwarp();
-  if (!act) return;
-  // ---- phase 2: row node a = lane ------------------------------------------
+  // ---- phase 2: row node a = lane (lanes of an inactive element idle) --------
   const int a = lane;
   const int nb = a < 4 ? 5 : 4;
   double acc[5][9];
@@ -418,7 +442,7 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
 #pragma unroll
     for (int i = 0; i < 9; ++i) acc[d][i] = 0.0;
 #pragma unroll 1
-  for (int g = 0; g < 8; ++g) {
+  for (int g = 0; g < (act ? 8 : 0); ++g) {
     const double* S = V + HX_SC + g * 8;
     const double wa = S[0], wb = S[1], wg = S[2], wc = S[3], wc2 = S[4];
     const double* Va = V + g * HX_VG + a * HX_VB;
@@ -455,48 +479,78 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
           acc[d][3 * j + k] += A[j] * qb[k] + B[j] * fb[k] + qb[j] * Cc[k] + (j == k ? dg : 0.0);
     }
   }
-  double* out = stage + e * HX_STAGE;   // 2784 B per element: 16-byte aligned
+  // ---- phase 3: block rows to the incidence records ----------------------------
+  // The blocks go to an exchange area in V (slot 8d + a, 10 doubles each:
+  // 128-bit stores, conflict-free within an element's 8 lanes; R_a at
+  // 360 + 4a), then the warp writes its 32 records (4 elements x 8 rows) as
+  // one flat range of 32 x 38 double2, so that each store instruction covers
+  // one or two whole records; hx_tbl maps record position -> exchange offset.
+  __syncwarp();                                          // V is no longer read
+  if (act) {
 #pragma unroll
-  for (int d = 0; d < 5; ++d) {
-    if (d == 4 && nb == 4) break;
-    const int slot = hx_slot(a, d);
-    double* o = out + slot * 9;            // even slots start 16-byte aligned, odd ones 8 bytes past
-    if (slot & 1) {
-      o[0] = acc[d][0];
-      double2* o2 = reinterpret_cast<double2*>(o + 1);
-      o2[0] = make_double2(acc[d][1], acc[d][2]);
-      o2[1] = make_double2(acc[d][3], acc[d][4]);
-      o2[2] = make_double2(acc[d][5], acc[d][6]);
-      o2[3] = make_double2(acc[d][7], acc[d][8]);
-    } else {
-      double2* o2 = reinterpret_cast<double2*>(o);
-      o2[0] = make_double2(acc[d][0], acc[d][1]);
-      o2[1] = make_double2(acc[d][2], acc[d][3]);
-      o2[2] = make_double2(acc[d][4], acc[d][5]);
-      o2[3] = make_double2(acc[d][6], acc[d][7]);
-      o[8] = acc[d][8];
+    for (int d = 0; d < 5; ++d) {
+      if (d == 4 && nb == 4) break;
+      double2* o = reinterpret_cast<double2*>(V + (8 * d + a) * 10);
+      o[0] = make_double2(acc[d][0], acc[d][1]);
+      o[1] = make_double2(acc[d][2], acc[d][3]);
+      o[2] = make_double2(acc[d][4], acc[d][5]);
+      o[3] = make_double2(acc[d][6], acc[d][7]);
+      o[4] = make_double2(acc[d][8], 0.0);
+    }
+    double2* o = reinterpret_cast<double2*>(V + 360 + 4 * a);
+    o[0] = make_double2(racc[0], racc[1]);
+    o[1] = make_double2(racc[2], 0.0);
+  }
+  const int32_t myrec = act ? P.incpos[e * 8 + a] : -1;
+  __syncwarp();
+  {
+    const int wl = threadIdx.x & 31;
+    const double* Vw = sv + (threadIdx.x >> 5) * 4 * HX_EL;   // the warp's 4 elements
+#pragma unroll 8
+    for (int it = 0; it < HX_REC / 2; ++it) {
+      const int q = it * 32 + wl;                             // double2 index over the 32 records
+      const int r = q / (HX_REC / 2), k2 = q - r * (HX_REC / 2);
+      const int32_t rec = __shfl_sync(0xffffffffu, myrec, r);
+      const uint32_t t2 = hx_tbl[(r & 7) * (HX_REC / 2) + k2];
+      const double* Ve = Vw + (r >> 3) * HX_EL;
+      if (rec >= 0)
+        reinterpret_cast<double2*>(stage + (int64_t)rec * HX_REC)[k2] = make_double2(Ve[t2 & 0xFFFFu], Ve[t2 >> 16]);
     }
   }
-#pragma unroll
-  for (int j = 0; j < 3; ++j) out[324 + 3 * a + j] = racc[j];
   if (ER) {
 #pragma unroll
     for (int j = 0; j < 3; ++j) P.elemR[(int64_t)(3 * a + j) * P.ne + e] = racc[j];
   }
 }
 
-// Per node row: one warp per row node n, one lane per node block (n, c) of
-// the row.  The lane sums the staged blocks of the block's contributors
-// (element order, fixed), transposing blocks stored as (b, a), and writes its
-// 3x3 (free DOFs only) straight into the node's contiguous CSR rows; the
-// diagonal lane also sums the node's residual.  No shared memory, no barriers.
+// Per node row: one warp per row node n.  The warp copies the node's
+// incidence records (contiguous, element order) to shared memory with
+// coalesced 128-bit loads; then one lane per node block (n, c) of the row
+// sums the blocks of the block's contributors (element order, fixed) and
+// writes its 3x3 (free DOFs only) straight into the node's contiguous CSR
+// rows; the diagonal lane also sums the node's residual.  cap = the most
+// incidences of one node (shared memory per warp: cap records).  Staging the
+// contributor codes and the lanes' block metadata in shared memory alongside
+// the records measured slower (203 us vs 196 us at 48^3).
 template <bool WR, bool ACC>
-__global__ void __launch_bounds__(256) k_hex_blk(VolParams P, const double* __restrict__ stage) {
-  const int64_t n = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__global__ void __launch_bounds__(HX_GW * 32) k_hex_gat(VolParams P, const double* __restrict__ stage, int cap) {
+  extern __shared__ __align__(16) double gsm[];
+  const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
+  const int64_t n = (int64_t)blockIdx.x * HX_GW + warp;
   if (n >= P.n_nodes) return;
   const unsigned mn = P.mask[n];
   if (!mn) return;
+  const int o0 = P.nodeinc[n];
+  const int cnt = min(P.nodeinc[n + 1] - o0, cap);
+  double* S = gsm + (int64_t)warp * cap * HX_REC;
+  {
+    const double2* src = reinterpret_cast<const double2*>(stage + (int64_t)o0 * HX_REC);
+    double2* dst = reinterpret_cast<double2*>(S);
+    const int n2 = cnt * (HX_REC / 2);
+    for (int i = lane; i < n2; i += 32) dst[i] = __ldcs(src + i);
+  }
+  __syncwarp();
   const int64_t p0 = P.adjptr[n], p1 = P.adjptr[n + 1];
   const int L = P.rowlen[n];
   const int64_t vb = P.vbase[n];
@@ -508,24 +562,14 @@ __global__ void __launch_bounds__(256) k_hex_blk(VolParams P, const double* __re
     const int64_t t1 = P.blkptr[p + 1];
     for (int64_t t = P.blkptr[p]; t < t1; ++t) {
       const int32_t code = P.blkcon[t];
-      const int64_t e = code >> 6;
-      const int a = (code >> 3) & 7, b = code & 7;
-      const double* st = stage + e * HX_STAGE;
-      const int d = (b - a) & 7;
-      if (d < 4 || (d == 4 && a < 4)) {
-        const double* sb = st + hx_slot(a, d) * 9;
+      if ((code >> 3) >= cnt) continue;          // never taken: codes index the node's incidences
+      const double* sb = S + (code >> 3) * HX_REC + (code & 7) * 9;
 #pragma unroll
-        for (int i = 0; i < 9; ++i) blk[i] += sb[i];
-      } else {
-        const double* sb = st + hx_slot(b, (a - b) & 7) * 9;
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-#pragma unroll
-          for (int k = 0; k < 3; ++k) blk[3 * j + k] += sb[3 * k + j];
-      }
+      for (int i = 0; i < 9; ++i) blk[i] += sb[i];
       if (WR && c == n) {
+        const double* sr = S + (code >> 3) * HX_REC + 72;
 #pragma unroll
-        for (int j = 0; j < 3; ++j) r[j] += st[324 + 3 * a + j];
+        for (int j = 0; j < 3; ++j) r[j] += sr[j];
       }
     }
     const unsigned mc = P.mask[c];
@@ -922,6 +966,7 @@ static VolParams vol_params(const fea_nodes_t* N, const fea_group_t* G, double m
   P.adjoff = N->adjoff_dev;
   P.blkptr = G->blkptr_dev;
   P.blkcon = G->blkcon_dev;
+  P.incpos = G->incpos_dev;
   P.gc = gc;
   P.K = P.R = P.elemR = nullptr;
   P.mu = mu;
@@ -973,7 +1018,7 @@ extern "C" int64_t fea_reduce_scratch_len(int64_t n_items) { return (n_items + 2
 
 extern "C" int64_t fea_assemble_work_len(const fea_group_t* G) {
   if (!G) return 0;
-  return G->kind == FEA_C3D8 ? G->ne * (int64_t)HX_STAGE : 0;
+  return G->kind == FEA_C3D8 ? G->ne * 8 * (int64_t)HX_REC : 0;
 }
 
 extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, double mu, double kappa,
@@ -994,6 +1039,13 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
     const bool acc = accumulate != 0, wr = R != nullptr, er = elemR != nullptr;
     if (hex) {
       if (!work || work_len < fea_assemble_work_len(G)) return FEA_EWORK;
+      if (((uintptr_t)work & 15) != 0) return FEA_EINVAL;
+      if (!G->incpos_dev || !G->blkptr_dev || !G->blkcon_dev || !N->adjptr_dev || !N->adjcol_dev ||
+          !N->adjoff_dev)
+        return FEA_EINVAL;
+      const int cap = std::max<int>(G->maxval, 1);
+      const size_t gbytes = (size_t)HX_GW * cap * HX_REC * sizeof(double);
+      if (gbytes > (size_t)smem_limit()) return FEA_ESMEM;
       const unsigned grid = (unsigned)((G->ne + HX_EPB - 1) / HX_EPB);
       if (grid) {
         if (er) k_hex_elem<true><<<grid, HX_TPB, 0, st>>>(P, work);
@@ -1001,12 +1053,15 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
         count_launch();
         if (cudaError_t ce = cudaGetLastError()) return (int)ce;
       }
-      if (!G->blkptr_dev || !G->blkcon_dev || !N->adjptr_dev || !N->adjcol_dev || !N->adjoff_dev) return FEA_EINVAL;
-      const unsigned g2 = (unsigned)((N->n_nodes + 7) / 8);
+      const unsigned g2 = (unsigned)((N->n_nodes + HX_GW - 1) / HX_GW);
       if (g2) {
         const double* cw = work;
-        if (wr) acc ? k_hex_blk<true, true><<<g2, 256, 0, st>>>(P, cw) : k_hex_blk<true, false><<<g2, 256, 0, st>>>(P, cw);
-        else acc ? k_hex_blk<false, true><<<g2, 256, 0, st>>>(P, cw) : k_hex_blk<false, false><<<g2, 256, 0, st>>>(P, cw);
+        void (*gk)(VolParams, const double*, int) =
+            wr ? (acc ? k_hex_gat<true, true> : k_hex_gat<true, false>)
+               : (acc ? k_hex_gat<false, true> : k_hex_gat<false, false>);
+        if (cudaError_t ce = cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gbytes))
+          return (int)ce;
+        gk<<<g2, HX_GW * 32, gbytes, st>>>(P, cw, cap);
         count_launch();
       }
       return (int)cudaGetLastError();

@@ -50,7 +50,8 @@ struct GatherList {            // one element group or one face group
   std::vector<int32_t> soff;       // [N] shared-memory offset of the node's values in its chunk
   std::vector<int32_t> roff;       // [N] offset of its residual entries (after the chunk's values)
   std::vector<int64_t> blkptr;     // [nnzb+1] contributors of every (row node, column node) block
-  std::vector<int32_t> blkcon;     // e*64 + a*8 + b, element order ascending
+  std::vector<int32_t> blkcon;     // i*8 + b: the row node's i-th incidence, column node b of its element
+  std::vector<int32_t> incpos;     // [ne*nn] incidence index of (e, a), -1 for a node without rows
   std::vector<int32_t> allptr;     // [N+1] incidences of every node (constrained ones included)
   std::vector<int32_t> allinc;     // e*16 + a, element order ascending
   int64_t maxval = 0, threads = 0, smem = 0;
@@ -147,6 +148,8 @@ int build_gather(const fea_plan& P, int kind, int64_t ne, const int32_t* conn, c
     }
   });
   if (err) return err;
+  G.incpos.assign((size_t)ne * nn, -1);
+  for (int64_t o = 0; o < ninc; ++o) G.incpos[(size_t)(G.inc[o] >> 4) * nn + (G.inc[o] & 15)] = (int32_t)o;
   // chunks of nodes that have incidences in this list (in node order):
   // incidences <= threads, shared doubles <= budget
   G.allptr.assign(N + 1, 0);
@@ -202,7 +205,9 @@ int build_gather(const fea_plan& P, int kind, int64_t ne, const int32_t* conn, c
 }
 
 // Contributors of every node-level block (n, c): the (element, a, b) with
-// conn[e][a] = n and conn[e][b] = c, in ascending element order.
+// conn[e][a] = n and conn[e][b] = c, in ascending element order, each coded
+// as i*8 + b with i the position of (e, a) among n's incidences (the record
+// of the staged block row in the C3D8 assembly).
 int build_blocks(const fea_plan& P, int nn, const int32_t* conn, const Incidence& I, GatherList& G) {
   const int64_t N = P.N;
   std::vector<int32_t> cnt(P.nnzb, 0);
@@ -238,12 +243,12 @@ int build_blocks(const fea_plan& P, int nn, const int32_t* conn, const Incidence
       fill.assign(G.blkptr.begin() + P.adjptr[n], G.blkptr.begin() + P.adjptr[n + 1]);
       for (int64_t q = I.ptr[n]; q < I.ptr[n + 1]; ++q) {
         int64_t e = I.ent[q] >> 4;
-        int a = (int)(I.ent[q] & 15);
+        const int64_t i = q - I.ptr[n];
         for (int b = 0; b < nn; ++b) {
           int32_t c = conn[e * nn + b];
           if (!P.mask[c]) continue;
           int64_t k = std::lower_bound(col, col + ncol, c) - col;
-          G.blkcon[fill[k]++] = (int32_t)(e * 64 + a * 8 + b);
+          G.blkcon[fill[k]++] = (int32_t)(i * 8 + b);
         }
       }
     }
@@ -428,6 +433,7 @@ extern "C" int fea_plan_get(const fea_plan* P, int32_t id, int32_t group, void* 
       case 14: return put(G->blkcon, dst, count);
       case 15: return put(G->allptr, dst, count);
       case 16: return put(G->allinc, dst, count);
+      case 17: return put(G->incpos, dst, count);
       default: return FEA_EINVAL;
     }
   }

@@ -36,7 +36,7 @@ class HostPlan:
     _GDT = {L.A_INC: np.int32, L.A_BOFF: np.uint16, L.A_NODEINC: np.int32, L.A_CHUNKPTR: np.int32,
             L.A_CHUNKINC: np.int32, L.A_CHUNKLIST: np.int32, L.A_CHUNKDIM: np.int32, L.A_SOFF: np.int32,
             L.A_ROFF: np.int32, L.A_BLKPTR: np.int64, L.A_BLKCON: np.int32, L.A_ALLPTR: np.int32,
-            L.A_ALLINC: np.int32}
+            L.A_ALLINC: np.int32, L.A_INCPOS: np.int32}
 
     def __init__(self, n_nodes, free_mask, groups, faces, vol_threads=0, smem_doubles=0):
         self._h = None
@@ -102,6 +102,7 @@ class GatherGroup:
         blkptr = hp.array(base + L.A_BLKPTR, index) if base == L.G_BASE else np.zeros(0, np.int64)
         self.blkptr = dev(blkptr) if blkptr.size else None
         self.blkcon = dev(hp.array(base + L.A_BLKCON, index)) if blkptr.size else None
+        self.incpos = dev(hp.array(base + L.A_INCPOS, index)) if blkptr.size else None
         self.allptr = dev(hp.array(base + L.A_ALLPTR, index))
         self.allinc = dev(hp.array(base + L.A_ALLINC, index))
         self.ne = int(self.conn.shape[0])
@@ -115,7 +116,8 @@ class GatherGroup:
                             self.allptr.data_ptr(), self.allinc.data_ptr(),
                             hp.scalar(base + L.S_NCHUNK, index),
                             hp.scalar(base + L.S_MAXVAL, index), hp.scalar(base + L.S_THREADS, index),
-                            hp.scalar(base + L.S_SMEM, index))
+                            hp.scalar(base + L.S_SMEM, index),
+                            self.incpos.data_ptr() if self.incpos is not None else None)
         self.nchunk = int(self.desc.nchunk)
 
 
@@ -179,7 +181,7 @@ class DevicePlan:
 
     # -- element / load kernels ---------------------------------------------
     def stage(self, gi):
-        """Scratch of the element kernels of group gi (C3D8: staged element blocks)."""
+        """Scratch of the element kernels of group gi (C3D8: staged block rows, one record per incidence)."""
         g = self.groups[gi]
         n = int(L.fea_assemble_work_len(C.byref(g.desc)))
         if n == 0:

@@ -114,9 +114,10 @@ enum {
   FEA_A_G_SOFF = 41,     /* int32 [N] shared offset of the node's values   */
   FEA_A_G_ROFF = 42,     /* int32 [N] offset of its residual entries       */
   FEA_A_G_BLKPTR = 43,   /* int64 [nnzb+1] contributors of each node block (C3D8) */
-  FEA_A_G_BLKCON = 44,   /* int32 element*64 + a*8 + b, element order      */
+  FEA_A_G_BLKCON = 44,   /* int32 i*8 + b: i-th incidence of the row node, element order */
   FEA_A_G_ALLPTR = 45,   /* int32 [N+1] incidences of every node (all nodes) */
   FEA_A_G_ALLINC = 46,   /* int32 element*16 + a                           */
+  FEA_A_G_INCPOS = 47,   /* int32 [ne, nn] incidence index of (e, a), -1: node without rows */
   FEA_A_F_INC = 50,      /* the same arrays / scalars for face groups      */
   FEA_A_F_BOFF = 51,
   FEA_A_F_NODEINC = 52,
@@ -179,6 +180,7 @@ typedef struct {
   int32_t maxval;
   int32_t threads;
   int64_t smem_doubles;
+  const int32_t* incpos_dev;  /* FEA_A_G_INCPOS (C3D8 only) */
 } fea_group_t;
 
 /* Element residual and tangent of one Neo-Hookean group, gathered per node
@@ -187,8 +189,9 @@ typedef struct {
  * K_dev / R_dev / elemR_dev may be NULL.  elemR_dev receives the unassembled
  * element residual in the reference's (a, j, e) order [nn*3*ne]; it is only
  * meaningful for a plan whose every element node is active.
- * work_dev: fea_assemble_work_len(group) doubles of scratch (C3D8 stages
- * its 36 element blocks + residual there, 348 doubles per element; C3D4
+ * work_dev: fea_assemble_work_len(group) doubles of scratch, 16-byte
+ * aligned (C3D8 stages there, for every incidence (element, node a), the
+ * element's block row (a, 0..7) and R_a: 76 doubles, ne*8*76 in all; C3D4
  * needs none). */
 int64_t fea_assemble_work_len(const fea_group_t* group);
 int fea_assemble_volume(const fea_nodes_t* nodes, const fea_group_t* group, double mu, double kappa,

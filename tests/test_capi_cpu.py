@@ -181,7 +181,9 @@ def test_product_meshes_match_oracle_meshes():
 
 def test_block_contributor_lists(golden):
     """Every (row node, column node) block lists exactly the (element, a, b) that
-    couple the two nodes, in ascending element order."""
+    couple the two nodes, in ascending element order, coded as i*8 + b with i
+    the position of (e, a) among the row node's incidences; INCPOS maps every
+    (e, a) of a node with rows to that incidence's record."""
     from fea_b200 import _lib as L
     g = golden("hex5")
     N, el = g["X"].shape[0], g["elems"]
@@ -190,14 +192,26 @@ def test_block_contributor_lists(golden):
     hp = _plan(N, mask, [("C3D8", el)])
     adjptr, adjcol = hp.array(L.FEA_A_ADJPTR), hp.array(L.FEA_A_ADJCOL)
     bp, bc = hp.array(L.G_BASE + L.A_BLKPTR), hp.array(L.G_BASE + L.A_BLKCON)
+    nodeinc, inc = hp.array(L.G_BASE + L.A_NODEINC), hp.array(L.G_BASE + L.A_INC)
+    incpos = hp.array(L.G_BASE + L.A_INCPOS).reshape(-1, 8)
     assert bp.size == adjcol.size + 1
+    rank = {}
+    for e in range(el.shape[0]):                       # incidences in element order
+        for a in range(8):
+            n = el[e, a]
+            if mask[n]:
+                rank[(e, a)] = sum(1 for (e2, _a2) in rank if el[e2, _a2] == n)
+                assert incpos[e, a] == nodeinc[n] + rank[(e, a)]
+                assert inc[incpos[e, a]] == e * 16 + a
+            else:
+                assert incpos[e, a] == -1
     expect = {}
     for e in range(el.shape[0]):
         for a in range(8):
             for b in range(8):
                 n, c = el[e, a], el[e, b]
                 if mask[n] and mask[c]:
-                    expect.setdefault((n, c), []).append(e * 64 + a * 8 + b)
+                    expect.setdefault((n, c), []).append(rank[(e, a)] * 8 + b)
     for n in range(N):
         for p in range(adjptr[n], adjptr[n + 1]):
             assert list(bc[bp[p]:bp[p + 1]]) == expect[(n, adjcol[p])]
