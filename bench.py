@@ -664,7 +664,7 @@ def main():
                    "l2": "K values %.0f MB > 126 MB L2, no flush" % (8 * nnz / 1e6)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "algorithmic_bytes": B, "kernel_ms": kern_ms,
-                     "kernel": "k_hex_elem + k_hex_gat (C3D8 block rows staged per incidence, then node-row gather into CSR)",
+                     "kernel": "k_hex_elem + k_hex_gat (C3D8 upper block rows staged node by node, then node-row gather with transposed writes into CSR)",
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650"},
         "e2e": {"value": job_rate(world, E, e2e_ms), "unit": UNIT, "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": 8 * ndof, "d2h_bytes_per_step": 8 * ndof,

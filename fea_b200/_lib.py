@@ -31,10 +31,10 @@ FEA_C3D4, FEA_C3D8, FEA_T3, FEA_Q4 = 4, 8, 3, 40
 
 (FEA_S_NDOF, FEA_S_NNZ, FEA_S_NNZB) = (0, 1, 2)
 (FEA_A_RDOF, FEA_A_MASK, FEA_A_DBASE, FEA_A_VBASE, FEA_A_ROWLEN, FEA_A_INDPTR, FEA_A_INDICES,
- FEA_A_ADJPTR, FEA_A_ADJCOL, FEA_A_ADJOFF) = range(10, 20)
+ FEA_A_ADJPTR, FEA_A_ADJCOL, FEA_A_ADJOFF, FEA_A_MOFF) = range(10, 21)
 G_BASE, F_BASE = 30, 50
 (A_INC, A_BOFF, A_NODEINC, A_CHUNKPTR, A_CHUNKINC, S_NCHUNK, S_MAXVAL, S_THREADS, S_SMEM, A_CHUNKLIST,
- A_CHUNKDIM, A_SOFF, A_ROFF, A_BLKPTR, A_BLKCON, A_ALLPTR, A_ALLINC, A_INCPOS) = range(18)
+ A_CHUNKDIM, A_SOFF, A_ROFF, A_BLKPTR, A_BLKCON, A_ALLPTR, A_ALLINC, A_INCPOS, A_RECBASE, A_NODEBLK) = range(20)
 
 
 class FeaError(RuntimeError):
@@ -54,7 +54,8 @@ class Nodes(C.Structure):
     _fields_ = [("n_nodes", C.c_int64), ("ndof", C.c_int64), ("nnz", C.c_int64),
                 ("X_dev", C.c_void_p), ("rdof_dev", C.c_void_p), ("mask_dev", C.c_void_p),
                 ("vbase_dev", C.c_void_p), ("rowlen_dev", C.c_void_p), ("dbase_dev", C.c_void_p),
-                ("adjptr_dev", C.c_void_p), ("adjcol_dev", C.c_void_p), ("adjoff_dev", C.c_void_p)]
+                ("adjptr_dev", C.c_void_p), ("adjcol_dev", C.c_void_p), ("adjoff_dev", C.c_void_p),
+                ("moff_dev", C.c_void_p)]
 
 
 class Group(C.Structure):
@@ -65,7 +66,8 @@ class Group(C.Structure):
                 ("roff_dev", C.c_void_p), ("blkptr_dev", C.c_void_p), ("blkcon_dev", C.c_void_p),
                 ("allptr_dev", C.c_void_p), ("allinc_dev", C.c_void_p),
                 ("nchunk", C.c_int64), ("maxval", C.c_int32), ("threads", C.c_int32),
-                ("smem_doubles", C.c_int64), ("incpos_dev", C.c_void_p)]
+                ("smem_doubles", C.c_int64), ("incpos_dev", C.c_void_p), ("recbase_dev", C.c_void_p),
+                ("nodeblk_dev", C.c_void_p), ("nblk", C.c_int64), ("maxblk", C.c_int32), ("reserved", C.c_int32)]
 
 
 class PcgbSlot(C.Structure):

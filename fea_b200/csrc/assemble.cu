@@ -52,6 +52,9 @@ struct VolParams {
   const int64_t* __restrict__ blkptr;
   const int32_t* __restrict__ blkcon;
   const int32_t* __restrict__ incpos;
+  const int32_t* __restrict__ recbase;
+  const int64_t* __restrict__ nodeblk;
+  const int32_t* __restrict__ moff;
   const double* __restrict__ gc;
   double* K;
   double* R;
@@ -307,51 +310,35 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
 //   A_a = w(alpha f_a + beta q_a), B_a = w alpha q_a, C_a = w gamma q_a,
 // and the element residual R_a = sum_g w(mu J^-2/3 f_a + c2 q_a).  The
 // lanes then exchange their blocks through shared memory and lane a writes
-// the element's full block row (a, 0..7), transposing the blocks another lane
-// computed, and R_a as one 76-double record at the position of incidence
-// (e, a) in the node-major incidence list: every node's records are
-// contiguous in HBM, in element order.  k_hex_gat copies a node's records to
-// shared memory with coalesced 128-bit loads, sums them per column block and
-// writes each row range once.
+// the upper part of the element's block row a — the blocks (a, b) whose
+// column node is active and numbered >= row node, transposing the blocks
+// another lane computed — as the record of incidence (e, a): the records of
+// a node are contiguous in HBM, in element order (its record region); R_a
+// goes to the incidence's slot of a separate array.  k_hex_gat copies a
+// node's region to shared memory with coalesced loads, sums it per upper
+// column block and writes each block into the node's rows and its transpose
+// into the column node's rows: every CSR value written once.
 constexpr int HX_EPB = 8;                 // elements per CTA
 constexpr int HX_TPB = 8 * HX_EPB;        // threads per CTA
 constexpr int HX_VB = 10;                 // doubles per (gp, node) vector slot: q, f, g + pad
 constexpr int HX_VG = 82;                 // doubles per Gauss point (8 slots + 2 pad, 16-byte rows)
 constexpr int HX_SC = 8 * HX_VG;          // offset of the per-Gauss-point scalars (8 each)
 constexpr int HX_EL = HX_SC + 64;         // doubles per element (16-byte aligned)
-constexpr int HX_REC = 8 * 9 + 4;         // staged doubles per incidence: block row, R_a, pad (608 B)
 constexpr int HX_GW = 4;                  // warps (row nodes) per gather CTA
+
+// Offset of the residual slots in the C3D8 scratch: after the staged blocks,
+// rounded to 16 bytes.
+__host__ __device__ inline int64_t hx_rslot_base(int64_t nblk) { return (nblk * 9 + 1) & ~(int64_t)1; }
 constexpr int HX_GINC = 32;               // incidences per gather chunk (8 lanes each)
 
 // corner signs of hex node / Gauss point c (brick.py:15-25, 151-160)
 __device__ __forceinline__ double csx(int c) { return (((c + 1) >> 1) & 1) ? 1.0 : -1.0; }
 __device__ __forceinline__ double csy(int c) { return ((c >> 1) & 1) ? 1.0 : -1.0; }
 __device__ __forceinline__ double csz(int c) { return (c >> 2) ? 1.0 : -1.0; }
-// Offset in an element's exchange area of double k of the record of row a:
-// k < 72 is entry w = k mod 9 of block (a, b = k / 9), held by lane a at slot
-// 8d + a, d = (b - a) mod 8, when d <= 3 or (d == 4, a < 4), else as the
-// transpose of block (b, a) at slot 8((a - b) mod 8) + b; k = 72..75 is R_a
-// and a zero pad.
-__device__ __forceinline__ int hx_rec_off(int a, int k) {
-  if (k >= 72) return 360 + 4 * a + (k - 72);
-  const int b = k / 9, w = k - 9 * b;
-  const int d = (b - a) & 7;
-  if (d < 4 || (d == 4 && a < 4)) return (8 * d + a) * 10 + w;
-  const int j = w / 3, kk = w - 3 * j;
-  return (8 * ((a - b) & 7) + b) * 10 + 3 * kk + j;
-}
-
 template <bool ER>
-__global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __restrict__ stage) {
+__global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __restrict__ stage,
+                                                     double* __restrict__ rslot) {
   __shared__ __align__(16) double sv[HX_EPB * HX_EL];
-  // hx_tbl[a * 38 + k2]: exchange-area offsets of doubles 2k2 and 2k2 + 1 of
-  // the record of row a
-  __shared__ uint32_t hx_tbl[8 * (HX_REC / 2)];
-  for (int i = threadIdx.x; i < 8 * (HX_REC / 2); i += HX_TPB) {
-    const int ra = i / (HX_REC / 2), k = 2 * (i - ra * (HX_REC / 2));
-    hx_tbl[i] = (uint32_t)hx_rec_off(ra, k) | ((uint32_t)hx_rec_off(ra, k + 1) << 16);
-  }
-  __syncthreads();                             // every thread reaches it: no early exit in this kernel
   const double q3 = 0.57735026918962576451;   // 1/sqrt(3)
   const int le = threadIdx.x >> 3;
   const int lane = threadIdx.x & 7;
@@ -401,6 +388,11 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
     S[2] = w * (mu * I1 / 3.0 - kappa * J * (J - 1.0));              // w gamma
     S[3] = w * muJm;                                                 // w c (delta term, residual)
     S[4] = w * (kappa * J * (J - 1.0) - mu * I1 / 3.0);              // w c2 (residual)
+    {
+      const int32_t cg = P.conn[e * 8 + lane];                       // node `lane` of the element, for phase 3
+      S[5] = (double)cg;
+      S[6] = (double)P.mask[cg];
+    }
     // Mq = J0^-1 F^-1, Mf = J0^-1 F^T: q_b = Mq^T dxi_b, f_b = Mf^T dxi_b, g_b = J0^-T dxi_b
     double Mq[9], Mf[9];
 #pragma unroll
@@ -479,12 +471,11 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
           acc[d][3 * j + k] += A[j] * qb[k] + B[j] * fb[k] + qb[j] * Cc[k] + (j == k ? dg : 0.0);
     }
   }
-  // ---- phase 3: block rows to the incidence records ----------------------------
+  // ---- phase 3: upper block row a to the incidence record --------------------
   // The blocks go to an exchange area in V (slot 8d + a, 10 doubles each:
-  // 128-bit stores, conflict-free within an element's 8 lanes; R_a at
-  // 360 + 4a), then the warp writes its 32 records (4 elements x 8 rows) as
-  // one flat range of 32 x 38 double2, so that each store instruction covers
-  // one or two whole records; hx_tbl maps record position -> exchange offset.
+  // 128-bit stores, conflict-free within an element's 8 lanes); lane a then
+  // writes the blocks (a, b) of active column nodes numbered >= its own node,
+  // in ascending b, taking the transpose of a block another lane owns.
   __syncwarp();                                          // V is no longer read
   if (act) {
 #pragma unroll
@@ -497,24 +488,34 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
       o[3] = make_double2(acc[d][6], acc[d][7]);
       o[4] = make_double2(acc[d][8], 0.0);
     }
-    double2* o = reinterpret_cast<double2*>(V + 360 + 4 * a);
-    o[0] = make_double2(racc[0], racc[1]);
-    o[1] = make_double2(racc[2], 0.0);
   }
-  const int32_t myrec = act ? P.incpos[e * 8 + a] : -1;
   __syncwarp();
-  {
-    const int wl = threadIdx.x & 31;
-    const double* Vw = sv + (threadIdx.x >> 5) * 4 * HX_EL;   // the warp's 4 elements
-#pragma unroll 8
-    for (int it = 0; it < HX_REC / 2; ++it) {
-      const int q = it * 32 + wl;                             // double2 index over the 32 records
-      const int r = q / (HX_REC / 2), k2 = q - r * (HX_REC / 2);
-      const int32_t rec = __shfl_sync(0xffffffffu, myrec, r);
-      const uint32_t t2 = hx_tbl[(r & 7) * (HX_REC / 2) + k2];
-      const double* Ve = Vw + (r >> 3) * HX_EL;
-      if (rec >= 0)
-        reinterpret_cast<double2*>(stage + (int64_t)rec * HX_REC)[k2] = make_double2(Ve[t2 & 0xFFFFu], Ve[t2 >> 16]);
+  if (act) {
+    const int32_t rb = P.recbase[e * 8 + a];
+    if (rb >= 0) {
+      const double na = V[HX_SC + a * 8 + 5];
+      double* out = stage + (int64_t)rb * 9;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const double* Sb = V + HX_SC + b * 8;
+        if (Sb[6] == 0.0 || Sb[5] < na) continue;
+        const int d = (b - a) & 7;
+        if (d < 4 || (d == 4 && a < 4)) {
+          const double* sb = V + (8 * d + a) * 10;
+#pragma unroll
+          for (int i = 0; i < 9; ++i) out[i] = sb[i];
+        } else {
+          const double* sb = V + (8 * ((a - b) & 7) + b) * 10;
+#pragma unroll
+          for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) out[3 * j + k] = sb[3 * k + j];
+        }
+        out += 9;
+      }
+      double2* ro = reinterpret_cast<double2*>(rslot + (int64_t)P.incpos[e * 8 + a] * 4);
+      ro[0] = make_double2(racc[0], racc[1]);
+      ro[1] = make_double2(racc[2], 0.0);
     }
   }
   if (ER) {
@@ -523,17 +524,20 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
   }
 }
 
-// Per node row: one warp per row node n.  The warp copies the node's
-// incidence records (contiguous, element order) to shared memory with
-// coalesced 128-bit loads; then one lane per node block (n, c) of the row
-// sums the blocks of the block's contributors (element order, fixed) and
-// writes its 3x3 (free DOFs only) straight into the node's contiguous CSR
-// rows; the diagonal lane also sums the node's residual.  cap = the most
-// incidences of one node (shared memory per warp: cap records).  Staging the
-// contributor codes and the lanes' block metadata in shared memory alongside
-// the records measured slower (203 us vs 196 us at 48^3).
+// Per node row: one warp per row node n.  The warp copies the node's record
+// region (its staged upper blocks, element order) to shared memory with
+// coalesced loads; then one lane per upper node block (n, c >= n) sums the
+// blocks of the block's contributors (element order, fixed), writes its 3x3
+// (free DOFs only) into the node's contiguous CSR rows and, for c != n, the
+// transpose into c's rows at n's column offset there; the diagonal lane
+// writes the node's residual, the sum over its incidences in element order
+// (lane i loads incidence i's slot; the sum runs through shuffles).  The
+// lanes' block metadata and residual slots are loaded before the region
+// copy.  capb = the most staged blocks of one node (shared memory per warp:
+// capb blocks).
 template <bool WR, bool ACC>
-__global__ void __launch_bounds__(HX_GW * 32) k_hex_gat(VolParams P, const double* __restrict__ stage, int cap) {
+__global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const double* __restrict__ stage,
+                                                        const double* __restrict__ rslot, int capb) {
   extern __shared__ __align__(16) double gsm[];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -541,62 +545,125 @@ __global__ void __launch_bounds__(HX_GW * 32) k_hex_gat(VolParams P, const doubl
   if (n >= P.n_nodes) return;
   const unsigned mn = P.mask[n];
   if (!mn) return;
-  const int o0 = P.nodeinc[n];
-  const int cnt = min(P.nodeinc[n + 1] - o0, cap);
-  double* S = gsm + (int64_t)warp * cap * HX_REC;
+  const int64_t b0 = P.nodeblk[n];
+  const int64_t nbk_all = P.nodeblk[n + 1] - b0;
+  const int nbk = nbk_all < capb ? (int)nbk_all : capb;
+  const int64_t p0 = P.adjptr[n], p1 = P.adjptr[n + 1];
+  const int q0 = P.nodeinc[n], nq = P.nodeinc[n + 1] - q0;
+  // the lane's first block and its metadata
+  int64_t p = p0 + lane;
+  int32_t c = -1;
+  if (p < p1) c = P.adjcol[p];
+  int64_t t0 = 0, t1 = 0, vbc = 0;
+  int off = 0, om = 0, Lc = 0;
+  unsigned mc = 0;
+  if (c >= n) {
+    t0 = P.blkptr[p];
+    t1 = P.blkptr[p + 1];
+    off = P.adjoff[p];
+    om = P.moff[p];
+    mc = P.mask[c];
+    vbc = P.vbase[c];
+    Lc = P.rowlen[c];
+  }
+  double rq[3] = {0.0, 0.0, 0.0};
+  if (WR && lane < nq) {
+    const double* sr = rslot + (int64_t)(q0 + lane) * 4;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) rq[j] = sr[j];
+  }
+  double* S = gsm + (int64_t)warp * capb * 9;
   {
-    const double2* src = reinterpret_cast<const double2*>(stage + (int64_t)o0 * HX_REC);
-    double2* dst = reinterpret_cast<double2*>(S);
-    const int n2 = cnt * (HX_REC / 2);
-    for (int i = lane; i < n2; i += 32) dst[i] = __ldcs(src + i);
+    const double* src = stage + b0 * 9;
+    const int nd = nbk * 9;
+    for (int i = lane; i < nd; i += 32) S[i] = __ldcs(src + i);
+  }
+  double r[3] = {0.0, 0.0, 0.0};
+  if (WR) {                                      // warp-uniform: incidences in order
+    for (int qb = 0; qb < nq; qb += 32) {
+      if (qb > 0) {
+        rq[0] = rq[1] = rq[2] = 0.0;
+        if (qb + lane < nq) {
+          const double* sr = rslot + (int64_t)(q0 + qb + lane) * 4;
+#pragma unroll
+          for (int j = 0; j < 3; ++j) rq[j] = sr[j];
+        }
+      }
+      const int m = min(32, nq - qb);
+      for (int i = 0; i < m; ++i) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r[j] += __shfl_sync(0xffffffffu, rq[j], i);
+      }
+    }
   }
   __syncwarp();
-  const int64_t p0 = P.adjptr[n], p1 = P.adjptr[n + 1];
   const int L = P.rowlen[n];
   const int64_t vb = P.vbase[n];
-  for (int64_t p = p0 + lane; p < p1; p += 32) {
-    const int32_t c = P.adjcol[p];
-    double blk[9], r[3] = {0.0, 0.0, 0.0};
+  while (p < p1) {
+    if (c >= n) {                                // lower blocks: the transposes of c's upper blocks
+      double blk[9];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) blk[i] = 0.0;
-    const int64_t t1 = P.blkptr[p + 1];
-    for (int64_t t = P.blkptr[p]; t < t1; ++t) {
-      const int32_t code = P.blkcon[t];
-      if ((code >> 3) >= cnt) continue;          // never taken: codes index the node's incidences
-      const double* sb = S + (code >> 3) * HX_REC + (code & 7) * 9;
+      for (int i = 0; i < 9; ++i) blk[i] = 0.0;
+      for (int64_t t = t0; t < t1; ++t) {
+        const int32_t code = P.blkcon[t];
+        if (code >= nbk) continue;               // never taken: codes index the node's region
+        const double* sb = S + code * 9;
 #pragma unroll
-      for (int i = 0; i < 9; ++i) blk[i] += sb[i];
-      if (WR && c == n) {
-        const double* sr = S + (code >> 3) * HX_REC + 72;
-#pragma unroll
-        for (int j = 0; j < 3; ++j) r[j] += sr[j];
+        for (int i = 0; i < 9; ++i) blk[i] += sb[i];
       }
-    }
-    const unsigned mc = P.mask[c];
-    const int off = P.adjoff[p];
-    int rj = 0;
+      int rj = 0;
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      if (!(mn >> j & 1u)) continue;
-      double* row = P.K + vb + (int64_t)rj * L + off;
-      int rk = 0;
+      for (int j = 0; j < 3; ++j) {
+        if (!(mn >> j & 1u)) continue;
+        double* row = P.K + vb + (int64_t)rj * L + off;
+        int rk = 0;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        if (!(mc >> k & 1u)) continue;
-        row[rk] = ACC ? row[rk] + blk[3 * j + k] : blk[3 * j + k];
-        ++rk;
-      }
-      ++rj;
-    }
-    if (WR && c == n) {
-      double* Rout = P.R + P.rdof[n];
-      int rr = 0;
-#pragma unroll
-      for (int j = 0; j < 3; ++j)
-        if (mn >> j & 1u) {
-          Rout[rr] = ACC ? Rout[rr] + r[j] : r[j];
-          ++rr;
+        for (int k = 0; k < 3; ++k) {
+          if (!(mc >> k & 1u)) continue;
+          row[rk] = ACC ? row[rk] + blk[3 * j + k] : blk[3 * j + k];
+          ++rk;
         }
+        ++rj;
+      }
+      if (c != n) {
+        int rk = 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          if (!(mc >> k & 1u)) continue;
+          double* row = P.K + vbc + (int64_t)rk * Lc + om;
+          int cj = 0;
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            if (!(mn >> j & 1u)) continue;
+            row[cj] = ACC ? row[cj] + blk[3 * j + k] : blk[3 * j + k];
+            ++cj;
+          }
+          ++rk;
+        }
+      } else if (WR) {
+        double* Rout = P.R + P.rdof[n];
+        int rr = 0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          if (mn >> j & 1u) {
+            Rout[rr] = ACC ? Rout[rr] + r[j] : r[j];
+            ++rr;
+          }
+      }
+    }
+    p += 32;                                     // rows of more than 32 blocks
+    c = -1;
+    if (p < p1) {
+      c = P.adjcol[p];
+      if (c >= n) {
+        t0 = P.blkptr[p];
+        t1 = P.blkptr[p + 1];
+        off = P.adjoff[p];
+        om = P.moff[p];
+        mc = P.mask[c];
+        vbc = P.vbase[c];
+        Lc = P.rowlen[c];
+      }
     }
   }
 }
@@ -967,6 +1034,9 @@ static VolParams vol_params(const fea_nodes_t* N, const fea_group_t* G, double m
   P.blkptr = G->blkptr_dev;
   P.blkcon = G->blkcon_dev;
   P.incpos = G->incpos_dev;
+  P.recbase = G->recbase_dev;
+  P.nodeblk = G->nodeblk_dev;
+  P.moff = N->moff_dev;
   P.gc = gc;
   P.K = P.R = P.elemR = nullptr;
   P.mu = mu;
@@ -1017,8 +1087,8 @@ using namespace fea;
 extern "C" int64_t fea_reduce_scratch_len(int64_t n_items) { return (n_items + 255) / 256 + 1; }
 
 extern "C" int64_t fea_assemble_work_len(const fea_group_t* G) {
-  if (!G) return 0;
-  return G->kind == FEA_C3D8 ? G->ne * 8 * (int64_t)HX_REC : 0;
+  if (!G || G->kind != FEA_C3D8) return 0;
+  return hx_rslot_base(G->nblk) + G->ne * 8 * 4;
 }
 
 extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, double mu, double kappa,
@@ -1040,28 +1110,28 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
     if (hex) {
       if (!work || work_len < fea_assemble_work_len(G)) return FEA_EWORK;
       if (((uintptr_t)work & 15) != 0) return FEA_EINVAL;
-      if (!G->incpos_dev || !G->blkptr_dev || !G->blkcon_dev || !N->adjptr_dev || !N->adjcol_dev ||
-          !N->adjoff_dev)
+      if (!G->incpos_dev || !G->recbase_dev || !G->nodeblk_dev || !G->blkptr_dev || !G->blkcon_dev ||
+          !N->adjptr_dev || !N->adjcol_dev || !N->adjoff_dev || !N->moff_dev || G->nblk < 0 || G->maxblk < 0)
         return FEA_EINVAL;
-      const int cap = std::max<int>(G->maxval, 1);
-      const size_t gbytes = (size_t)HX_GW * cap * HX_REC * sizeof(double);
+      const int capb = std::max<int>(G->maxblk, 1);
+      const size_t gbytes = (size_t)HX_GW * capb * 9 * sizeof(double);
       if (gbytes > (size_t)smem_limit()) return FEA_ESMEM;
+      double* rslot = work + hx_rslot_base(G->nblk);
       const unsigned grid = (unsigned)((G->ne + HX_EPB - 1) / HX_EPB);
       if (grid) {
-        if (er) k_hex_elem<true><<<grid, HX_TPB, 0, st>>>(P, work);
-        else k_hex_elem<false><<<grid, HX_TPB, 0, st>>>(P, work);
+        if (er) k_hex_elem<true><<<grid, HX_TPB, 0, st>>>(P, work, rslot);
+        else k_hex_elem<false><<<grid, HX_TPB, 0, st>>>(P, work, rslot);
         count_launch();
         if (cudaError_t ce = cudaGetLastError()) return (int)ce;
       }
       const unsigned g2 = (unsigned)((N->n_nodes + HX_GW - 1) / HX_GW);
       if (g2) {
-        const double* cw = work;
-        void (*gk)(VolParams, const double*, int) =
+        void (*gk)(VolParams, const double*, const double*, int) =
             wr ? (acc ? k_hex_gat<true, true> : k_hex_gat<true, false>)
                : (acc ? k_hex_gat<false, true> : k_hex_gat<false, false>);
         if (cudaError_t ce = cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gbytes))
           return (int)ce;
-        gk<<<g2, HX_GW * 32, gbytes, st>>>(P, cw, cap);
+        gk<<<g2, HX_GW * 32, gbytes, st>>>(P, work, rslot, capb);
         count_launch();
       }
       return (int)cudaGetLastError();

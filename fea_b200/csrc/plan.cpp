@@ -49,9 +49,11 @@ struct GatherList {            // one element group or one face group
   std::vector<int32_t> chunkdim;   // [nchunk*3]: values, residual entries, contiguous flag
   std::vector<int32_t> soff;       // [N] shared-memory offset of the node's values in its chunk
   std::vector<int32_t> roff;       // [N] offset of its residual entries (after the chunk's values)
-  std::vector<int64_t> blkptr;     // [nnzb+1] contributors of every (row node, column node) block
-  std::vector<int32_t> blkcon;     // i*8 + b: the row node's i-th incidence, column node b of its element
+  std::vector<int64_t> blkptr;     // [nnzb+1] contributors of every upper (row node n, column node c >= n) block
+  std::vector<int32_t> blkcon;     // block index of each contributor within the row node's record region
   std::vector<int32_t> incpos;     // [ne*nn] incidence index of (e, a), -1 for a node without rows
+  std::vector<int32_t> recbase;    // [ne*nn] first staged block of (e, a)'s record, -1 for a node without rows
+  std::vector<int64_t> nodeblk;    // [N+1] first staged block of each node's record region
   std::vector<int32_t> allptr;     // [N+1] incidences of every node (constrained ones included)
   std::vector<int32_t> allinc;     // e*16 + a, element order ascending
   int64_t maxval = 0, threads = 0, smem = 0;
@@ -79,6 +81,7 @@ struct fea_plan {
   std::vector<uint8_t> mask;
   std::vector<int64_t> vbase, indptr, adjptr;
   std::vector<int32_t> indices, adjcol, adjoff;
+  std::vector<int32_t> moff;       // [nnzb] value offset of n in row c, for entry (n, c)
   std::vector<GatherList> groups, faces;
 };
 
@@ -204,12 +207,42 @@ int build_gather(const fea_plan& P, int kind, int64_t ne, const int32_t* conn, c
   return FEA_OK;
 }
 
-// Contributors of every node-level block (n, c): the (element, a, b) with
-// conn[e][a] = n and conn[e][b] = c, in ascending element order, each coded
-// as i*8 + b with i the position of (e, a) among n's incidences (the record
-// of the staged block row in the C3D8 assembly).
+// Upper-block records of a C3D8 group.  The record of incidence (e, a) of
+// node n = conn[e][a] holds the blocks (a, b) whose column node c =
+// conn[e][b] is active and c >= n, in ascending b; the records of a node are
+// contiguous and in element order (its record region).  Every upper block
+// (n, c >= n) lists its contributors' positions in n's region, in ascending
+// element order; lower blocks have none (they are the transposes of upper
+// ones, written by the column node's gather).
 int build_blocks(const fea_plan& P, int nn, const int32_t* conn, const Incidence& I, GatherList& G) {
   const int64_t N = P.N;
+  auto included = [&](int64_t e, int a, int b) {
+    const int32_t na = conn[e * nn + a], nb = conn[e * nn + b];
+    return P.mask[na] && P.mask[nb] && nb >= na;
+  };
+  G.nodeblk.assign(N + 1, 0);
+  for (int64_t n = 0; n < N; ++n) {
+    int64_t c = 0;
+    if (P.mask[n])
+      for (int64_t q = I.ptr[n]; q < I.ptr[n + 1]; ++q) {
+        const int64_t e = I.ent[q] >> 4;
+        const int a = (int)(I.ent[q] & 15);
+        for (int b = 0; b < nn; ++b) c += included(e, a, b);
+      }
+    G.nodeblk[n + 1] = G.nodeblk[n] + c;
+  }
+  if (G.nodeblk[N] >= INT32_MAX) return FEA_ERANGE;
+  G.recbase.assign((size_t)G.ne * nn, -1);
+  for (int64_t n = 0; n < N; ++n) {
+    if (!P.mask[n]) continue;
+    int64_t off = G.nodeblk[n];
+    for (int64_t q = I.ptr[n]; q < I.ptr[n + 1]; ++q) {
+      const int64_t e = I.ent[q] >> 4;
+      const int a = (int)(I.ent[q] & 15);
+      G.recbase[e * nn + a] = (int32_t)off;
+      for (int b = 0; b < nn; ++b) off += included(e, a, b);
+    }
+  }
   std::vector<int32_t> cnt(P.nnzb, 0);
   int err = FEA_OK;
   parallel_for(N, [&](int64_t a0, int64_t a1) {
@@ -218,10 +251,11 @@ int build_blocks(const fea_plan& P, int nn, const int32_t* conn, const Incidence
       const int32_t* col = P.adjcol.data() + P.adjptr[n];
       int64_t ncol = P.adjptr[n + 1] - P.adjptr[n];
       for (int64_t q = I.ptr[n]; q < I.ptr[n + 1]; ++q) {
-        int64_t e = I.ent[q] >> 4;
+        const int64_t e = I.ent[q] >> 4;
+        const int a = (int)(I.ent[q] & 15);
         for (int b = 0; b < nn; ++b) {
-          int32_t c = conn[e * nn + b];
-          if (!P.mask[c]) continue;
+          if (!included(e, a, b)) continue;
+          const int32_t c = conn[e * nn + b];
           const int32_t* it = std::lower_bound(col, col + ncol, c);
           if (it == col + ncol || *it != c) { err = FEA_ERANGE; continue; }
           cnt[P.adjptr[n] + (it - col)]++;
@@ -232,7 +266,6 @@ int build_blocks(const fea_plan& P, int nn, const int32_t* conn, const Incidence
   if (err) return err;
   G.blkptr.assign(P.nnzb + 1, 0);
   for (int64_t p = 0; p < P.nnzb; ++p) G.blkptr[p + 1] = G.blkptr[p] + cnt[p];
-  if (G.blkptr[P.nnzb] > 0 && (int64_t)I.ent.size() * nn >= INT64_MAX / 2) return FEA_ERANGE;
   G.blkcon.resize(G.blkptr[P.nnzb]);
   parallel_for(N, [&](int64_t a0, int64_t a1) {
     std::vector<int64_t> fill;
@@ -242,13 +275,14 @@ int build_blocks(const fea_plan& P, int nn, const int32_t* conn, const Incidence
       int64_t ncol = P.adjptr[n + 1] - P.adjptr[n];
       fill.assign(G.blkptr.begin() + P.adjptr[n], G.blkptr.begin() + P.adjptr[n + 1]);
       for (int64_t q = I.ptr[n]; q < I.ptr[n + 1]; ++q) {
-        int64_t e = I.ent[q] >> 4;
-        const int64_t i = q - I.ptr[n];
+        const int64_t e = I.ent[q] >> 4;
+        const int a = (int)(I.ent[q] & 15);
+        int32_t pos = (int32_t)(G.recbase[e * nn + a] - G.nodeblk[n]);
         for (int b = 0; b < nn; ++b) {
-          int32_t c = conn[e * nn + b];
-          if (!P.mask[c]) continue;
+          if (!included(e, a, b)) continue;
+          const int32_t c = conn[e * nn + b];
           int64_t k = std::lower_bound(col, col + ncol, c) - col;
-          G.blkcon[fill[k]++] = (int32_t)(i * 8 + b);
+          G.blkcon[fill[k]++] = pos++;
         }
       }
     }
@@ -367,6 +401,21 @@ extern "C" int fea_plan_build(int64_t n_nodes, const uint8_t* free_mask, int32_t
   });
   P->indptr[P->ndof] = P->nnz;
   { std::vector<std::vector<int32_t>>().swap(adj); }
+  // mirrored offsets: for entry (n, c), the value offset of n in row c
+  P->moff.assign(P->nnzb, -1);
+  int merr = FEA_OK;
+  parallel_for(N, [&](int64_t a0, int64_t a1) {
+    for (int64_t n = a0; n < a1; ++n)
+      for (int64_t p = P->adjptr[n]; p < P->adjptr[n + 1]; ++p) {
+        const int32_t c = P->adjcol[p];
+        const int32_t* col = P->adjcol.data() + P->adjptr[c];
+        const int64_t ncol = P->adjptr[c + 1] - P->adjptr[c];
+        const int32_t* it = std::lower_bound(col, col + ncol, (int32_t)n);
+        if (it == col + ncol || *it != n) { merr = FEA_ERANGE; continue; }
+        P->moff[p] = P->adjoff[P->adjptr[c] + (it - col)];
+      }
+  });
+  if (merr) return merr;
   // gather lists
   P->groups.resize(n_groups);
   P->faces.resize(n_faces);
@@ -375,7 +424,6 @@ extern "C" int fea_plan_build(int64_t n_nodes, const uint8_t* free_mask, int32_t
     int th = vol_threads > 0 ? vol_threads : (group_kind[g] == FEA_C3D8 ? 32 : 256);
     int r = build_gather(*P, group_kind[g], group_ne[g], group_conn[g], ginc[g], th, budget, P->groups[g]);
     if (r) return r;
-    if (group_ne[g] >= (int64_t)1 << 25) return FEA_ERANGE;   // e*64 + a*8 + b must fit int32
     if (group_kind[g] == FEA_C3D8 && (r = build_blocks(*P, 8, group_conn[g], ginc[g], P->groups[g]))) return r;
   }
   for (int g = 0; g < n_faces; ++g) {
@@ -434,6 +482,8 @@ extern "C" int fea_plan_get(const fea_plan* P, int32_t id, int32_t group, void* 
       case 15: return put(G->allptr, dst, count);
       case 16: return put(G->allinc, dst, count);
       case 17: return put(G->incpos, dst, count);
+      case 18: return put(G->recbase, dst, count);
+      case 19: return put(G->nodeblk, dst, count);
       default: return FEA_EINVAL;
     }
   }
@@ -451,6 +501,7 @@ extern "C" int fea_plan_get(const fea_plan* P, int32_t id, int32_t group, void* 
     case FEA_A_ADJPTR: return put(P->adjptr, dst, count);
     case FEA_A_ADJCOL: return put(P->adjcol, dst, count);
     case FEA_A_ADJOFF: return put(P->adjoff, dst, count);
+    case FEA_A_MOFF: return put(P->moff, dst, count);
     default: return FEA_EINVAL;
   }
 }

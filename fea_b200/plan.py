@@ -32,11 +32,12 @@ class HostPlan:
 
     _DT = {L.FEA_A_RDOF: np.int32, L.FEA_A_MASK: np.uint8, L.FEA_A_DBASE: np.int32, L.FEA_A_VBASE: np.int64,
            L.FEA_A_ROWLEN: np.int32, L.FEA_A_INDPTR: np.int64, L.FEA_A_INDICES: np.int32,
-           L.FEA_A_ADJPTR: np.int64, L.FEA_A_ADJCOL: np.int32, L.FEA_A_ADJOFF: np.int32}
+           L.FEA_A_ADJPTR: np.int64, L.FEA_A_ADJCOL: np.int32, L.FEA_A_ADJOFF: np.int32,
+           L.FEA_A_MOFF: np.int32}
     _GDT = {L.A_INC: np.int32, L.A_BOFF: np.uint16, L.A_NODEINC: np.int32, L.A_CHUNKPTR: np.int32,
             L.A_CHUNKINC: np.int32, L.A_CHUNKLIST: np.int32, L.A_CHUNKDIM: np.int32, L.A_SOFF: np.int32,
             L.A_ROFF: np.int32, L.A_BLKPTR: np.int64, L.A_BLKCON: np.int32, L.A_ALLPTR: np.int32,
-            L.A_ALLINC: np.int32, L.A_INCPOS: np.int32}
+            L.A_ALLINC: np.int32, L.A_INCPOS: np.int32, L.A_RECBASE: np.int32, L.A_NODEBLK: np.int64}
 
     def __init__(self, n_nodes, free_mask, groups, faces, vol_threads=0, smem_doubles=0):
         self._h = None
@@ -103,6 +104,11 @@ class GatherGroup:
         self.blkptr = dev(blkptr) if blkptr.size else None
         self.blkcon = dev(hp.array(base + L.A_BLKCON, index)) if blkptr.size else None
         self.incpos = dev(hp.array(base + L.A_INCPOS, index)) if blkptr.size else None
+        self.recbase = dev(hp.array(base + L.A_RECBASE, index)) if blkptr.size else None
+        nodeblk = hp.array(base + L.A_NODEBLK, index) if blkptr.size else np.zeros(1, np.int64)
+        self.nodeblk = dev(nodeblk) if blkptr.size else None
+        nblk = int(nodeblk[-1])
+        maxblk = int(np.diff(nodeblk).max()) if nodeblk.size > 1 else 0
         self.allptr = dev(hp.array(base + L.A_ALLPTR, index))
         self.allinc = dev(hp.array(base + L.A_ALLINC, index))
         self.ne = int(self.conn.shape[0])
@@ -117,7 +123,9 @@ class GatherGroup:
                             hp.scalar(base + L.S_NCHUNK, index),
                             hp.scalar(base + L.S_MAXVAL, index), hp.scalar(base + L.S_THREADS, index),
                             hp.scalar(base + L.S_SMEM, index),
-                            self.incpos.data_ptr() if self.incpos is not None else None)
+                            self.incpos.data_ptr() if self.incpos is not None else None,
+                            self.recbase.data_ptr() if self.recbase is not None else None,
+                            self.nodeblk.data_ptr() if self.nodeblk is not None else None, nblk, maxblk, 0)
         self.nchunk = int(self.desc.nchunk)
 
 
@@ -153,10 +161,11 @@ class DevicePlan:
             self.adjptr = dev(hp.array(L.FEA_A_ADJPTR))
             self.adjcol = dev(hp.array(L.FEA_A_ADJCOL))
             self.adjoff = dev(hp.array(L.FEA_A_ADJOFF))
+            self.moff = dev(hp.array(L.FEA_A_MOFF))
             self.nodes = L.Nodes(self.n_nodes, self.ndof, self.nnz, self.X.data_ptr(), self.rdof.data_ptr(),
                                  self.mask.data_ptr(), self.vbase.data_ptr(), self.rowlen.data_ptr(),
                                  self.dbase.data_ptr(), self.adjptr.data_ptr(), self.adjcol.data_ptr(),
-                                 self.adjoff.data_ptr())
+                                 self.adjoff.data_ptr(), self.moff.data_ptr())
             self.groups = [GatherGroup(hp, L.G_BASE, i, k, c, self.device) for i, (k, c) in enumerate(gl)]
             self.faces = [GatherGroup(hp, L.F_BASE, i, k, c, self.device) for i, (k, c) in enumerate(fl)]
         self._scratch = None
@@ -181,7 +190,7 @@ class DevicePlan:
 
     # -- element / load kernels ---------------------------------------------
     def stage(self, gi):
-        """Scratch of the element kernels of group gi (C3D8: staged block rows, one record per incidence)."""
+        """Scratch of the element kernels of group gi (C3D8: staged upper block rows and residual slots)."""
         g = self.groups[gi]
         n = int(L.fea_assemble_work_len(C.byref(g.desc)))
         if n == 0:

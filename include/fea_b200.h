@@ -100,6 +100,7 @@ enum {
   FEA_A_ADJPTR = 17,     /* int64 [N+1] node adjacency row pointer         */
   FEA_A_ADJCOL = 18,     /* int32 [nnzb] neighbour node                    */
   FEA_A_ADJOFF = 19,     /* int32 [nnzb] value offset of neighbour in row  */
+  FEA_A_MOFF = 20,       /* int32 [nnzb] value offset of the row node in the neighbour's row */
   FEA_A_G_INC = 30,      /* int32 [ninc] element*16 + local node           */
   FEA_A_G_BOFF = 31,     /* uint16 [ninc, nn] row offset per element node  */
   FEA_A_G_NODEINC = 32,  /* int32 [N+1] first incidence of each node       */
@@ -113,11 +114,13 @@ enum {
   FEA_A_G_CHUNKDIM = 40, /* int32 [nchunk,3] values, residual entries, contiguous */
   FEA_A_G_SOFF = 41,     /* int32 [N] shared offset of the node's values   */
   FEA_A_G_ROFF = 42,     /* int32 [N] offset of its residual entries       */
-  FEA_A_G_BLKPTR = 43,   /* int64 [nnzb+1] contributors of each node block (C3D8) */
-  FEA_A_G_BLKCON = 44,   /* int32 i*8 + b: i-th incidence of the row node, element order */
+  FEA_A_G_BLKPTR = 43,   /* int64 [nnzb+1] contributors of each upper node block (c >= n; C3D8) */
+  FEA_A_G_BLKCON = 44,   /* int32 staged block index within the row node's record region */
   FEA_A_G_ALLPTR = 45,   /* int32 [N+1] incidences of every node (all nodes) */
   FEA_A_G_ALLINC = 46,   /* int32 element*16 + a                           */
   FEA_A_G_INCPOS = 47,   /* int32 [ne, nn] incidence index of (e, a), -1: node without rows */
+  FEA_A_G_RECBASE = 48,  /* int32 [ne, nn] first staged block of (e, a)'s record, -1: none */
+  FEA_A_G_NODEBLK = 49,  /* int64 [N+1] first staged block of each node's record region */
   FEA_A_F_INC = 50,      /* the same arrays / scalars for face groups      */
   FEA_A_F_BOFF = 51,
   FEA_A_F_NODEINC = 52,
@@ -156,6 +159,7 @@ typedef struct {
   const int64_t* adjptr_dev;  /* FEA_A_ADJPTR */
   const int32_t* adjcol_dev;  /* FEA_A_ADJCOL */
   const int32_t* adjoff_dev;  /* FEA_A_ADJOFF */
+  const int32_t* moff_dev;    /* FEA_A_MOFF   */
 } fea_nodes_t;
 
 typedef struct {
@@ -181,6 +185,11 @@ typedef struct {
   int32_t threads;
   int64_t smem_doubles;
   const int32_t* incpos_dev;  /* FEA_A_G_INCPOS (C3D8 only) */
+  const int32_t* recbase_dev; /* FEA_A_G_RECBASE (C3D8 only) */
+  const int64_t* nodeblk_dev; /* FEA_A_G_NODEBLK (C3D8 only) */
+  int64_t nblk;               /* staged blocks: NODEBLK[N] (C3D8 only)        */
+  int32_t maxblk;             /* most staged blocks of one node (C3D8 only)   */
+  int32_t reserved;
 } fea_group_t;
 
 /* Element residual and tangent of one Neo-Hookean group, gathered per node
@@ -190,9 +199,9 @@ typedef struct {
  * element residual in the reference's (a, j, e) order [nn*3*ne]; it is only
  * meaningful for a plan whose every element node is active.
  * work_dev: fea_assemble_work_len(group) doubles of scratch, 16-byte
- * aligned (C3D8 stages there, for every incidence (element, node a), the
- * element's block row (a, 0..7) and R_a: 76 doubles, ne*8*76 in all; C3D4
- * needs none). */
+ * aligned (C3D8 stages there the upper blocks of every element row, 9
+ * doubles each, node by node (nblk blocks), then R_a of every incidence, 4
+ * doubles each; C3D4 needs none). */
 int64_t fea_assemble_work_len(const fea_group_t* group);
 int fea_assemble_volume(const fea_nodes_t* nodes, const fea_group_t* group, double mu, double kappa,
                         const double* gc_dev, double* K_dev, double* R_dev, double* elemR_dev,

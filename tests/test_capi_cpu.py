@@ -179,43 +179,58 @@ def test_product_meshes_match_oracle_meshes():
     np.testing.assert_array_equal(faces, torch.cat([f for _, _, f in ref]).numpy())
 
 
-def test_block_contributor_lists(golden):
-    """Every (row node, column node) block lists exactly the (element, a, b) that
-    couple the two nodes, in ascending element order, coded as i*8 + b with i
-    the position of (e, a) among the row node's incidences; INCPOS maps every
-    (e, a) of a node with rows to that incidence's record."""
+def _upper_staging(hp, el, mask):
+    """The C3D8 staging arrays of a plan and the rule they follow: the record
+    of incidence (e, a) holds the blocks (a, b) of active column nodes
+    numbered >= the row node, in ascending b; a node's records are
+    contiguous, in element order."""
     from fea_b200 import _lib as L
+    arr = lambda i: hp.array(L.G_BASE + i)
+    return dict(nodeinc=arr(L.A_NODEINC), inc=arr(L.A_INC), incpos=arr(L.A_INCPOS).reshape(-1, 8),
+                recbase=arr(L.A_RECBASE).reshape(-1, 8), nodeblk=arr(L.A_NODEBLK), bp=arr(L.A_BLKPTR),
+                bc=arr(L.A_BLKCON), adjptr=hp.array(L.FEA_A_ADJPTR), adjcol=hp.array(L.FEA_A_ADJCOL),
+                adjoff=hp.array(L.FEA_A_ADJOFF), moff=hp.array(L.FEA_A_MOFF))
+
+
+def _included(el, mask, e, a):
+    na = el[e, a]
+    return [b for b in range(8) if mask[el[e, b]] and el[e, b] >= na] if mask[na] else []
+
+
+def test_block_contributor_lists(golden):
+    """Records, regions and contributor lists of the C3D8 staging: every upper
+    block (n, c >= n) lists the positions, in n's record region, of the (e, a,
+    b) that couple the two nodes, in ascending element order; lower blocks
+    list none; MOFF is n's value offset in row c."""
     g = golden("hex5")
     N, el = g["X"].shape[0], g["elems"]
     mask = np.full(N, 7, np.uint8)
     mask[g["fixed"]] = 0
-    hp = _plan(N, mask, [("C3D8", el)])
-    adjptr, adjcol = hp.array(L.FEA_A_ADJPTR), hp.array(L.FEA_A_ADJCOL)
-    bp, bc = hp.array(L.G_BASE + L.A_BLKPTR), hp.array(L.G_BASE + L.A_BLKCON)
-    nodeinc, inc = hp.array(L.G_BASE + L.A_NODEINC), hp.array(L.G_BASE + L.A_INC)
-    incpos = hp.array(L.G_BASE + L.A_INCPOS).reshape(-1, 8)
-    assert bp.size == adjcol.size + 1
-    rank = {}
-    for e in range(el.shape[0]):                       # incidences in element order
+    mask[g["fixed"][:3]] = 5                          # partial masks too
+    st = _upper_staging(_plan(N, mask, [("C3D8", el)]), el, mask)
+    nodeblk, recbase = st["nodeblk"], st["recbase"]
+    assert st["bp"].size == st["adjcol"].size + 1
+    pos = {n: int(nodeblk[n]) for n in range(N)}
+    expect = {}
+    for e in range(el.shape[0]):                       # element order = incidence order per node
         for a in range(8):
             n = el[e, a]
-            if mask[n]:
-                rank[(e, a)] = sum(1 for (e2, _a2) in rank if el[e2, _a2] == n)
-                assert incpos[e, a] == nodeinc[n] + rank[(e, a)]
-                assert inc[incpos[e, a]] == e * 16 + a
-            else:
-                assert incpos[e, a] == -1
-    expect = {}
-    for e in range(el.shape[0]):
-        for a in range(8):
-            for b in range(8):
-                n, c = el[e, a], el[e, b]
-                if mask[n] and mask[c]:
-                    expect.setdefault((n, c), []).append(rank[(e, a)] * 8 + b)
+            if not mask[n]:
+                assert recbase[e, a] == -1 and st["incpos"][e, a] == -1
+                continue
+            assert recbase[e, a] == pos[n]
+            for b in _included(el, mask, e, a):
+                expect.setdefault((n, el[e, b]), []).append(pos[n] - nodeblk[n])
+                pos[n] += 1
     for n in range(N):
-        for p in range(adjptr[n], adjptr[n + 1]):
-            assert list(bc[bp[p]:bp[p + 1]]) == expect[(n, adjcol[p])]
-    assert bp[-1] == sum(len(v) for v in expect.values())
+        assert pos[n] == nodeblk[n + 1]
+        for p in range(st["adjptr"][n], st["adjptr"][n + 1]):
+            c = st["adjcol"][p]
+            assert list(st["bc"][st["bp"][p]:st["bp"][p + 1]]) == expect.get((n, c), [])
+            if c < n:
+                assert st["bp"][p] == st["bp"][p + 1]
+            q = np.nonzero(st["adjcol"][st["adjptr"][c]:st["adjptr"][c + 1]] == n)[0][0] + st["adjptr"][c]
+            assert st["moff"][p] == st["adjoff"][q]
 
 
 def test_serving_requests_are_seeded_and_bounded():
@@ -284,3 +299,69 @@ def test_csr_of_eight_hex_mesh_by_hand(clamp):
     _, (oip, oix, _) = m.assemble(torch.zeros(int(m.free_mask().sum()), dtype=torch.float64))
     np.testing.assert_array_equal(oip.numpy(), ip)
     np.testing.assert_array_equal(oix.numpy(), ix)
+
+
+@pytest.mark.parametrize("dofs", [(0, 1, 2), (1,)])
+def test_upper_staging_emulated_gives_reference_K(dofs):
+    """The C3D8 assembly as the kernels perform it, emulated on the CPU with
+    the oracle's element blocks: upper records written per incidence, then
+    per node the upper block sums into the node's rows and their transposes
+    into the column nodes' rows.  The CSR values equal the oracle's reduced K
+    and R."""
+    from fea_b200 import _lib as L
+    X, el = O.hex_block(3, jitter=0.1, seed=5)
+    fixed = torch.nonzero(X[:, 0] < 1e-9).flatten().numpy()
+    m = O.Model(X, [O.Group("C3D8", el, 1.0, 10.0)], [], [(fixed, dofs)])
+    nfree = int(m.free_mask().sum())
+    gc = 0.01 * torch.randn(nfree, generator=torch.Generator().manual_seed(2), dtype=torch.float64)
+    Rref, (ip, ix, vref) = m.assemble(gc)
+    N = X.shape[0]
+    mask = np.full(N, 7, np.uint8)
+    for d in dofs:
+        mask[fixed] &= ~np.uint8(1 << d)
+    el = el.numpy()
+    hp = _plan(N, mask, [("C3D8", el)])
+    st = _upper_staging(hp, el, mask)
+    vbase, rowlen, rdof = hp.array(L.FEA_A_VBASE), hp.array(L.FEA_A_ROWLEN), hp.array(L.FEA_A_RDOF)
+    Re, Ke = O.element_residual_tangent("C3D8", X, torch.from_numpy(el), m.gc_to_u(gc), 1.0, 10.0)
+    Re, Ke = Re.numpy(), Ke.numpy()                    # [a,j,e], [a,j,b,k,e]
+    blocks = np.full((int(st["nodeblk"][-1]), 3, 3), np.nan)
+    rslot = np.full((int(st["nodeinc"][-1]), 3), np.nan)
+    for e in range(el.shape[0]):                       # element kernel, phase 3
+        for a in range(8):
+            rb = st["recbase"][e, a]
+            if rb < 0:
+                continue
+            for b in _included(el, mask, e, a):
+                blocks[rb] = Ke[a, :, b, :, e]
+                rb += 1
+            rslot[st["incpos"][e, a]] = Re[a, :, e]
+    K = np.full(int(vbase[-1]), np.nan)
+    R = np.full(nfree, np.nan)
+    free = lambda mk: [j for j in range(3) if mk >> j & 1]
+    for n in range(N):                                  # gather, one warp per node
+        if not mask[n]:
+            continue
+        S = blocks[st["nodeblk"][n]:st["nodeblk"][n + 1]]
+        for p in range(st["adjptr"][n], st["adjptr"][n + 1]):
+            c = st["adjcol"][p]
+            if c < n:
+                continue
+            blk = np.zeros((3, 3))
+            for t in range(st["bp"][p], st["bp"][p + 1]):
+                blk = blk + S[st["bc"][t]]
+            for rj, j in enumerate(free(mask[n])):
+                for rk, k in enumerate(free(mask[c])):
+                    K[vbase[n] + rj * rowlen[n] + st["adjoff"][p] + rk] = blk[j, k]
+            if c != n:
+                for rk, k in enumerate(free(mask[c])):
+                    for cj, j in enumerate(free(mask[n])):
+                        K[vbase[c] + rk * rowlen[c] + st["moff"][p] + cj] = blk[j, k]
+            else:
+                r = rslot[st["nodeinc"][n]:st["nodeinc"][n + 1]].sum(0)
+                for rr, j in enumerate(free(mask[n])):
+                    R[rdof[n] + rr] = r[j]
+    assert not np.isnan(K).any() and not np.isnan(R).any()
+    np.testing.assert_array_equal(hp.array(L.FEA_A_INDPTR), ip.numpy())
+    np.testing.assert_allclose(K, vref.numpy(), rtol=0, atol=1e-13 * np.abs(vref.numpy()).max())
+    np.testing.assert_allclose(R, Rref.numpy(), rtol=0, atol=1e-13 * np.abs(Rref.numpy()).max())
