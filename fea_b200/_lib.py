@@ -102,6 +102,8 @@ fea_energy_pressure = _sig("fea_energy_pressure", I32, NP, GP, P, P, P, P, I64, 
 fea_energy_volume_noalloc = _sig("fea_energy_volume_noalloc", I32, NP, GP, D, D, P, P, P)
 fea_lumped_mass = _sig("fea_lumped_mass", I32, NP, GP, D, P, P)
 fea_invert_mass = _sig("fea_invert_mass", I32, I64, P, P)
+fea_mass_csr = _sig("fea_mass_csr", I32, NP, GP, D, P, P)
+fea_axpy = _sig("fea_axpy", I32, I64, D, P, P, P)
 fea_pcg_work_len = _sig("fea_pcg_work_len", I64, I64)
 fea_pcg_solve = _sig("fea_pcg_solve", I32, I64, P, P, P, P, P, D, I32, I32, I32, P, I64,
                      C.POINTER(I32), C.POINTER(D), P)
@@ -131,7 +133,7 @@ fea_launch_count = _sig("fea_launch_count", I64)
 # every symbol the header declares (checked by the CPU test suite)
 EXPORTED = ["fea_plan_build", "fea_plan_free", "fea_plan_get", "fea_assemble_work_len", "fea_assemble_volume", "fea_assemble_pressure",
             "fea_reduce_scratch_len", "fea_energy_volume", "fea_energy_volume_noalloc", "fea_energy_pressure", "fea_lumped_mass",
-            "fea_invert_mass", "fea_pcg_work_len", "fea_pcg_solve", "fea_pcg_mixed_work_len",
+            "fea_invert_mass", "fea_mass_csr", "fea_axpy", "fea_pcg_work_len", "fea_pcg_solve", "fea_pcg_mixed_work_len",
             "fea_pcg_solve_mixed", "fea_spmv", "fea_spmv_nodes", "fea_pcg_solve_nodes", "fea_pcg_solve_mixed_nodes", "fea_convert_f32", "fea_pcgb_work_len", "fea_pcgb_table_bytes", "fea_pcgb_set", "fea_pcgb_start",
             "fea_pcgb_iterate", "fea_pcgb_state", "fea_explicit_work_len", "fea_explicit_run",
             "fea_adjoint_vjp_volume", "fea_adjoint_hvp_pressure", "fea_version", "fea_launch_count"]

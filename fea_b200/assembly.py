@@ -282,7 +282,22 @@ class Assembly:
 
     # -- dynamics (assembly.py:187-206, 421-443) -----------------------------------
     def initialize_dynamic(self):
-        self._minv = self.plan.lumped_mass_inv([float(e.density) for e in self._mat_elems])
+        rhos = [float(e.density) for e in self._mat_elems]
+        self._minv = self.plan.lumped_mass_inv(rhos)
+        self._mass_values = self.plan.mass_csr(rhos)
+
+    def mass_csr(self):
+        """Consistent mass as values of the reduced CSR pattern [nnz] (constant)."""
+        if getattr(self, "_mass_values", None) is None:
+            self.initialize_dynamic()
+        return self._mass_values
+
+    def assemble_mass_matrix(self, GC_now=None):
+        """(indices int64 [2, nnz], values [nnz]) of the reduced consistent mass
+        (assembly.py:421-443): the same sparse matrix as the reference's
+        duplicate COO, given on the stiffness pattern (entries that couple
+        unlike directions are zero).  The mass does not depend on GC_now."""
+        return self.plan.coo_indices(), self.mass_csr()
 
     def lumped_mass_inv(self):
         if getattr(self, "_minv", None) is None:

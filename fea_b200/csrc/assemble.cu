@@ -1000,6 +1000,68 @@ __global__ void __launch_bounds__(128) k_lumped_mass(VolParams P, double rho, do
     if (mn >> d & 1u) out[rj++] += acc[d];
 }
 
+// Consistent mass in the reduced CSR values: one thread per row node n,
+// incidences in element order; M_ab = sum_g rho N_a N_b w detJ0 of every
+// incident element goes to the entries ((n, d), (c_b, d)) of the DOFs d free
+// at both nodes (the mass couples like directions only), added to Mv.
+// Follows Element_3D.get_mass_matrix (C3base.py:348-384) with the reduction
+// of Assembly.assemble_mass_matrix (assembly.py:421-443).
+template <int NN>
+__global__ void __launch_bounds__(128) k_mass_csr(VolParams P, double rho, double* __restrict__ Mv) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= P.n_nodes) return;
+  const unsigned mn = P.mask[n];
+  if (!mn) return;
+  const int L = P.rowlen[n];
+  const int64_t vb = P.vbase[n];
+  for (int q = P.nodeinc[n]; q < P.nodeinc[n + 1]; ++q) {
+    const int ea = P.inc[q];
+    const int64_t e = ea >> 4;
+    const int a = ea & 15;
+    int32_t cn[NN];
+#pragma unroll
+    for (int b = 0; b < NN; ++b) cn[b] = P.conn[e * NN + b];
+    double mab[NN];
+#pragma unroll
+    for (int b = 0; b < NN; ++b) mab[b] = 0.0;
+#pragma unroll
+    for (int g = 0; g < Elem<NN>::NG; ++g) {
+      double J0[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) J0[i] = 0.0;
+#pragma unroll
+      for (int b = 0; b < NN; ++b)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          double d = Elem<NN>::dxi(g, b, m);
+#pragma unroll
+          for (int i = 0; i < 3; ++i) J0[3 * i + m] += P.X[3 * (int64_t)cn[b] + i] * d;
+        }
+      const double w = det3(J0) * Elem<NN>::wq(g) * rho * Elem<NN>::N(g, a);
+#pragma unroll
+      for (int b = 0; b < NN; ++b) mab[b] += w * Elem<NN>::N(g, b);
+    }
+#pragma unroll
+    for (int b = 0; b < NN; ++b) {
+      const unsigned bo = P.boff[(int64_t)q * NN + b];
+      if (bo == 0xFFFFu) continue;                   // column node without free DOFs
+      const unsigned mc = P.mask[cn[b]];
+      int rd = 0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        if (!(mn >> d & 1u)) continue;
+        if (mc >> d & 1u) Mv[vb + (int64_t)rd * L + bo + __popc(mc & ((1u << d) - 1u))] += mab[b];
+        ++rd;
+      }
+    }
+  }
+}
+
+__global__ void k_axpy(int64_t n, double alpha, const double* __restrict__ x, double* __restrict__ y) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] += alpha * x[i];
+}
+
 __global__ void k_invert_mass(int64_t n, double* m) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {
@@ -1249,6 +1311,28 @@ extern "C" int fea_lumped_mass(const fea_nodes_t* N, const fea_group_t* G, doubl
   const int grid = grid_for(N->n_nodes, 128);
   if (G->kind == FEA_C3D8) k_lumped_mass<8><<<grid, 128, 0, st>>>(P, rho, m);
   else k_lumped_mass<4><<<grid, 128, 0, st>>>(P, rho, m);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+extern "C" int fea_mass_csr(const fea_nodes_t* N, const fea_group_t* G, double rho, double* Mv,
+                            cudaStream_t st) {
+  if (!N || !G || !Mv || (G->kind != FEA_C3D4 && G->kind != FEA_C3D8) || !G->boff_dev) return FEA_EINVAL;
+  if (int r = ensure_tables()) return r;
+  if (N->n_nodes == 0) return FEA_OK;
+  VolParams P = vol_params(N, G, 0.0, 0.0, nullptr);
+  const int grid = grid_for(N->n_nodes, 128);
+  if (G->kind == FEA_C3D8) k_mass_csr<8><<<grid, 128, 0, st>>>(P, rho, Mv);
+  else k_mass_csr<4><<<grid, 128, 0, st>>>(P, rho, Mv);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+extern "C" int fea_axpy(int64_t n, double alpha, const double* x, double* y, cudaStream_t st) {
+  if (n < 0 || (n > 0 && (!x || !y))) return FEA_EINVAL;
+  if (n == 0) return FEA_OK;
+  const int64_t g = std::min<int64_t>((n + 255) / 256, 148 * 16);
+  k_axpy<<<(unsigned)g, 256, 0, st>>>(n, alpha, x, y);
   count_launch();
   return (int)cudaGetLastError();
 }

@@ -246,6 +246,21 @@ class DevicePlan:
         L.check(L.fea_invert_mass(self.ndof, vptr(m), stream()), "fea_invert_mass")
         return m
 
+    def mass_csr(self, rhos):
+        """Consistent mass in the values of the reduced CSR pattern [nnz]."""
+        Mv = self.zeros(self.nnz)
+        for gi, rho in enumerate(rhos):
+            L.check(L.fea_mass_csr(C.byref(self.nodes), C.byref(self.groups[gi].desc), float(rho), vptr(Mv),
+                                   stream()), "fea_mass_csr")
+        return Mv
+
+    def axpy(self, alpha, x, y):
+        """y += alpha x (float64 device vectors of one length), in place."""
+        if x.numel() != y.numel() or x.dtype != torch.float64 or y.dtype != torch.float64:
+            raise ValueError("axpy: float64 vectors of one length")
+        L.check(L.fea_axpy(int(y.numel()), float(alpha), vptr(x), vptr(y), stream()), "fea_axpy")
+        return y
+
     # -- linear algebra --------------------------------------------------------
     def spmv(self, values, x, y=None, generic=False):
         """y = K x on the plan's reduced matrix (node-row kernel; generic=True

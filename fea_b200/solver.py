@@ -11,6 +11,10 @@ adds a relative stop test ||R|| / ||R_first|| <= rtol; in that mode a
 residual that has stopped falling below ``floor_rtol`` (1e-9) of the first
 one is the round-off floor and also ends the iteration.
 
+DynamicImplicitSolver keeps the reference's Newmark time loop and per-step
+Newton (dynamic_implicit.py) on the same device kernels, with the consistent
+mass in the stiffness pattern.
+
 DynamicExplicitSolver keeps the reference's time and storage bookkeeping
 (dynamic_explicit.py:66-145) and advances the state with the fused
 explicit kernel between storage points.
@@ -254,6 +258,210 @@ class StaticImplicitSolver(BaseSolver):
             self._diag_pos = torch.nonzero(rows[0] == rows[1]).flatten()
         d = K_values[self._diag_pos]
         return torch.where(d == 0, torch.ones_like(d), d)
+
+
+class DynamicImplicitSolver(StaticImplicitSolver):
+    """Implicit Newmark dynamics (dynamic_implicit.py:15-501).
+
+    Average acceleration (beta = 1/4, gamma = 1/2).  Each step predicts
+    GC_pre = GC + dt GV + dt^2 GA / 4 and minimises the incremental energy
+    Pi(x) + (x - GC_pre) M (x - GC_pre) / (2 beta dt^2) by Newton with the
+    reference's Armijo line search and stop test; the tangent K + M /
+    (beta dt^2) and the consistent mass M share the plan's CSR pattern, so
+    the effective tangent is one axpy on the values and M x one node-row
+    SpMV.  The linear solves are the device Jacobi-PCG of
+    StaticImplicitSolver (tight where the reference takes its direct
+    solver).  The initial acceleration solves M a0 = R(GC0) with the
+    assembled residual R, as the reference does (dynamic_implicit.py:290-302).
+    """
+
+    def __init__(self, maximum_iteration: int = 10000, deltaT: float = 1e-2, time_end: float = 1.0,
+                 tol_error: float = 1e-5, pcg_tol: float = 1e-5, pcg_max_iter: int = 1500,
+                 tight_pcg_tol: float = 1e-22, tight_pcg_max_iter: int = 20000, verbose: bool = False) -> None:
+        super().__init__(maximum_iteration=maximum_iteration, tol_error=tol_error, pcg_tol=pcg_tol,
+                         pcg_max_iter=pcg_max_iter, tight_pcg_tol=tight_pcg_tol,
+                         tight_pcg_max_iter=tight_pcg_max_iter, verbose=verbose)
+        self._deltaT = deltaT
+        self._time_end = time_end
+        self._gamma = 0.5
+        self._beta = 0.25
+        self._GC_list = None
+        self._GV_list = None
+        self._GA_list = None
+        self._time_list = []
+        self._deltaT_list = []
+
+    def initialize(self, assembly, *args, **kwargs):
+        super().initialize(assembly)
+        self.assembly.initialize_dynamic()
+        self._GC_list, self._GV_list, self._GA_list = [], [], []
+        self._time_list, self._deltaT_list = [], []
+
+    def set_deltaT(self, deltaT: float):
+        self._deltaT = deltaT
+
+    # -- energies and the incremental system (dynamic_implicit.py:88-146) --------
+    def _mass_dot(self, x):
+        return self.assembly.plan.spmv(self.assembly.mass_csr(), x.contiguous())
+
+    def get_total_energy(self, GC_now, GC0=None, GV0=None, GA0=None, deltaT=None):
+        """Pi(GC_now) + v M v / 2 with v the Newmark velocity at GC_now."""
+        if GC0 is None:
+            return self.assembly._total_Potential_Energy(GC=GC_now)
+        deltaT = self._deltaT if deltaT is None else deltaT
+        v = self.get_next_velocity(GC_now, GC0, GV0, GA0, deltaT)[0]
+        return self.assembly._total_Potential_Energy(GC=GC_now) + 0.5 * torch.dot(v, self._mass_dot(v))
+
+    def get_incremental_energy(self, GC_now, GC_pre, deltaT=None):
+        deltaT = self._deltaT if deltaT is None else deltaT
+        d = GC_now - GC_pre
+        return (self.assembly._total_Potential_Energy(GC=GC_now)
+                + torch.dot(d, self._mass_dot(d)) / (2 * self._beta * deltaT ** 2))
+
+    def _incremental_csr(self, GC_now, GC_pre):
+        """(R + M (x - x_pre) / (beta dt^2), CSR values of K + M / (beta dt^2))."""
+        c = 1.0 / (self._beta * self._deltaT ** 2)
+        R, Kv = self.assembly.assemble_csr(GC_now)
+        P = self.assembly.plan
+        P.axpy(c, self._mass_dot(GC_now - GC_pre), R)
+        P.axpy(c, self.assembly.mass_csr(), Kv)
+        return R, Kv
+
+    def get_incremental_stiffness_matrix(self, GC_now, GC_pre):
+        """(R, K_indices int64 [2, nnz], K_values) of the step's Newton system."""
+        R, Kv = self._incremental_csr(GC_now, GC_pre)
+        return R, self.assembly.plan.coo_indices(), Kv
+
+    def get_next_velocity(self, GC_now, GC0, GV0, GA0, deltaT):
+        """Newmark velocity and acceleration at GC_now (dynamic_implicit.py:269-289)."""
+        g, b = self._gamma, self._beta
+        GV_now = g / (b * deltaT) * (GC_now - GC0) + (1 - g / b) * GV0 + deltaT * (1 - g / (2 * b)) * GA0
+        GA_now = 1 / (b * deltaT ** 2) * (GC_now - GC0) - 1 / (b * deltaT) * GV0 - (1 / (2 * b) - 1) * GA0
+        return GV_now, GA_now
+
+    def get_current_acceleration(self, GC0, GV0=None):
+        """M a = R(GC0), the assembled residual, as in the reference
+        (dynamic_implicit.py:290-302); M by device PCG to round-off."""
+        P = self.assembly.plan
+        R = self.assembly.assemble_force(GC=GC0).contiguous()
+        a = torch.zeros_like(R)
+        P.pcg(self.assembly.mass_csr(), R, a, 1e-26, 10000, raise_on_breakdown=True)
+        return a
+
+    # -- time loop (dynamic_implicit.py:148-226) ---------------------------------
+    def solve(self, GC0=None, GV0=None, *args, **kwargs):
+        t0 = time.time()
+        if GC0 is None:
+            GC0 = self.assembly.GC.clone()
+        GC0 = self.assembly._gc(GC=GC0)
+        GV0 = torch.zeros_like(GC0) if GV0 is None else GV0.to(GC0.device, torch.float64)
+        self._GC_list = [GC0]
+        self._GV_list = [GV0]
+        self._GA_list = [self.get_current_acceleration(GC0=GC0, GV0=GV0)]
+        self._time_list = [0.0]
+        self._deltaT_list = []
+        self.E_history = [float(self.get_total_energy(GC0, GC0, GV0, self._GA_list[-1]))]
+        step = 0
+        while True:
+            dt = self._deltaT
+            GC_pre = self._GC_list[-1] + dt * self._GV_list[-1] + 0.25 * dt ** 2 * self._GA_list[-1]
+            GC_now = self._solve_iteration(GC0=self._GC_list[-1], GC_pre=GC_pre, deltaT=dt, tol_error=self.tol_error)
+            if isinstance(GC_now, bool):
+                raise RuntimeError("Newton iteration of time step %d did not converge" % (step + 1))
+            GV, GA = self.get_next_velocity(GC_now, self._GC_list[-1], self._GV_list[-1], self._GA_list[-1], dt)
+            self.E_history.append(float(self.get_total_energy(GC_now, self._GC_list[-1], self._GV_list[-1],
+                                                              self._GA_list[-1], dt)))
+            self._GC_list.append(GC_now)
+            self._GV_list.append(GV)
+            self._GA_list.append(GA)
+            self._deltaT_list.append(dt)
+            self._time_list.append(self._time_list[-1] + dt)
+            step += 1
+            if self.verbose:
+                print("step %d  time %.6g  newton %d" % (step, self._time_list[-1], self._iter_now))
+            if self._time_list[-1] >= self._time_end:
+                break
+        self.GC = self._GC_list[-1]
+        self.assembly.RGC = self.assembly.refine_RGC(self.assembly._GC2RGC(self.assembly.GC))
+        if self.verbose:
+            print("total_time:%.2f" % (time.time() - t0))
+        return True
+
+    # -- Newton per step (dynamic_implicit.py:304-460) ---------------------------
+    def _dyn_line_search(self, GC_now, GC_pre, dGC, R, energy0, deltaT):
+        """Armijo backtracking on the incremental energy (c1 = 0.3, halving,
+        alpha < 1e-12 -> 0).  As in StaticImplicitSolver, where the predicted
+        decrease is below the energy's round-off the trial step is accepted
+        when it reduces the residual norm instead."""
+        alpha, c1 = 1.0, 0.3
+        deltaE = float((dGC * R).sum())
+        if deltaE > 0:
+            dGC, deltaE = -dGC, -deltaE
+        if not bool(torch.isfinite(dGC).all()):
+            raise ValueError("dGC has nan or inf")
+        e0 = float(energy0)
+        step_max = float(dGC.abs().max())
+        roundoff = abs(deltaE) <= 1e-10 * abs(e0)
+        r0 = float(R.norm())
+        while True:
+            GCnew = GC_now + alpha * dGC
+            if roundoff:
+                rn = float(self._incremental_csr(GCnew, GC_pre)[0].norm())
+                ok = math.isfinite(rn) and rn < r0
+                e_new = float(self.get_incremental_energy(GCnew, GC_pre, deltaT)) if ok else e0
+            else:
+                e_new = float(self.get_incremental_energy(GCnew, GC_pre, deltaT))
+                ok = math.isfinite(e_new) and e_new <= e0 + c1 * deltaE * alpha
+            if ok and alpha * step_max <= self._maximum_step_length:
+                return alpha, GCnew, e_new
+            alpha *= 0.5
+            if alpha < 1e-12:
+                return 0.0, GC_now.clone(), e0
+
+    def _solve_iteration(self, GC0, GC_pre=None, deltaT=None, tol_error=None):
+        """Newton on the step's incremental energy; returns GC or False."""
+        if GC_pre is None:                        # the static signature (GC, tol_error)
+            return super()._solve_iteration(GC0, tol_error)
+        deltaT = self._deltaT if deltaT is None else deltaT
+        tol_error = self.tol_error if tol_error is None else tol_error
+        GC_now = GC0.clone()
+        self._iter_now = 0
+        self.history = []
+        energy = float(self.get_incremental_energy(GC_now, GC_pre, deltaT))
+        dGC = torch.zeros_like(GC0)
+        low_alpha, alpha = 0, 0.0
+        while True:
+            if self._iter_now > self.maximum_iteration:
+                self.assembly.GC = GC_now
+                return False
+            R, Kv = self._incremental_csr(GC_now, GC_pre)
+            self._iter_now += 1
+            rmax = float(R.abs().max()) if R.numel() else 0.0
+            self.history.append(dict(iter=self._iter_now, rmax=rmax, rnorm=float(R.norm())))
+            req = self._linear_request(Kv, -R, self._iter_now, alpha, dGC)
+            self._run_linear(req)
+            dGC = self._linear_finish(req, Kv, -R)
+            alpha, GCnew, energy_new = self._dyn_line_search(GC_now, GC_pre, dGC, R, energy, deltaT)
+            self.history[-1].update(alpha=alpha)
+            if alpha == 0 and rmax > tol_error:
+                self.assembly.GC = GC_now
+                return False
+            if alpha == 0:
+                break
+            if alpha < 0.01:
+                low_alpha += 1
+            else:
+                low_alpha = max(0, low_alpha - 5)
+            if low_alpha > 10:
+                if rmax < 1e-3:
+                    self.assembly.GC = GC_now
+                    break
+                return False
+            energy = float(self.get_incremental_energy(GCnew, GC_pre, deltaT))
+            GC_now = GCnew
+            if float(dGC.abs().max()) < tol_error and rmax < tol_error:
+                break
+        return GC_now
 
 
 class DynamicExplicitSolver(BaseSolver):

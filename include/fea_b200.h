@@ -249,6 +249,19 @@ int fea_lumped_mass(const fea_nodes_t* nodes, const fea_group_t* group, double r
                     double* m_dev, cudaStream_t stream);
 int fea_invert_mass(int64_t ndof, double* m_dev, cudaStream_t stream);
 
+/* Consistent mass of one element group added into Mv_dev [nnz], the values
+ * of the plan's reduced CSR pattern (the mass couples like directions of two
+ * nodes, a subset of the stiffness pattern; other entries are left as they
+ * are).  Replaces Element_3D.get_mass_matrix (FEA/assemble/elements/C3/
+ * C3base.py:348-384) with the reduction of Assembly.assemble_mass_matrix
+ * (FEA/assemble/assembly.py:421-443), whose duplicates this sums. */
+int fea_mass_csr(const fea_nodes_t* nodes, const fea_group_t* group, double rho, double* Mv_dev,
+                 cudaStream_t stream);
+
+/* y += alpha x over n doubles (the effective tangent K + M / (beta dt^2) of
+ * FEA/solver/dynamic_implicit.py:120-146 on CSR values of one pattern). */
+int fea_axpy(int64_t n, double alpha, const double* x_dev, double* y_dev, cudaStream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Jacobi-preconditioned CG on the reduced CSR matrix.
  *   stop test: (r.D^-1 r) / (b.D^-1 b) < tol  — the reference's

@@ -438,6 +438,38 @@ class Model:
         m[m.abs() < 1e-12] = 1.0
         return 1.0 / m
 
+    def mass_coo(self):
+        """Reduced consistent mass as duplicate COO (rows, cols, values).
+
+        Follows Element_3D.get_mass_matrix (C3base.py:348-384: M_ab times the
+        3x3 identity of every element, stored as full 3x3 blocks on the
+        stiffness pattern, zeros included) and Assembly.assemble_mass_matrix
+        (assembly.py:421-443: entries of fixed DOFs dropped, rows and columns
+        relabelled in GC order).
+        """
+        free = self.free_mask()
+        rid = torch.cumsum(free.to(torch.int64), 0) - 1
+        rows, cols, vals = [], [], []
+        for g in self.groups:
+            Me = element_mass(g.kind, self.X, g.elems, g.rho)         # [nn,nn,E]
+            nn = g.elems.shape[1]
+            for j in range(3):
+                for k in range(3):
+                    ra = (3 * g.elems.T[:, None, :] + j).expand(nn, nn, -1)
+                    cb = (3 * g.elems.T[None, :, :] + k).expand(nn, nn, -1)
+                    rows.append(ra.reshape(-1)); cols.append(cb.reshape(-1))
+                    vals.append(Me.reshape(-1) if j == k else torch.zeros(Me.numel(), dtype=DT))
+        rows = torch.cat(rows); cols = torch.cat(cols); vals = torch.cat(vals)
+        keep = free[rows] & free[cols]
+        return rid[rows[keep]], rid[cols[keep]], vals[keep]
+
+    def mass_matrix(self):
+        """The reduced consistent mass as a scipy CSR matrix (duplicates summed)."""
+        import scipy.sparse as sp
+        r, c, v = self.mass_coo()
+        n = int(self.free_mask().sum())
+        return sp.coo_matrix((v.numpy(), (r.numpy(), c.numpy())), shape=(n, n)).tocsr()
+
 
 # ---------------------------------------------------------------------------
 # Solvers
@@ -566,6 +598,85 @@ def explicit_run(model: Model, gc0, gv0, dt, steps):
         v = 0.5 * (vh + vh_prev)
         vh_prev = vh
     return u, v, a
+
+
+def newmark_run(model: Model, gc0, gv0, dt, steps, tol_error=1e-5, max_iter=10000, beta=0.25, gamma=0.5):
+    """Implicit Newmark dynamics with Newton per step and direct solves.
+
+    Follows DynamicImplicitSolver (dynamic_implicit.py): the initial
+    acceleration solves M a0 = R(gc0) with R the assembled residual, as
+    written there (:300-302); each step predicts gc_pre = gc + dt v +
+    dt^2 a / 4 (:180) and minimises the incremental energy
+    Pi(x) + (x - gc_pre) M (x - gc_pre) / (2 beta dt^2) (:103-114) by Newton
+    on R + M (x - gc_pre) / (beta dt^2) with tangent K + M / (beta dt^2)
+    (:116-146) and Armijo backtracking (c1 = 0.3, halving, alpha < 1e-12 ->
+    0, :304-351); the Newton loop (:353-460) stops when max|dx| < tol and
+    max|R| < tol.  The CPU direct solve stands for its solver on the CPU
+    (:487-493).  Velocity and acceleration follow :269-289.
+    Returns the lists (GC, GV, GA), one entry per stored time.
+    """
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    Mm = model.mass_matrix()
+    c = 1.0 / (beta * dt * dt)
+
+    def inc_energy(x, pre):
+        d = (x - pre).numpy()
+        return float(model.energy(x)) + float(d @ (Mm @ d)) * c / 2
+
+    def next_va(x, x0, v0, a0):
+        v = gamma / (beta * dt) * (x - x0) + (1 - gamma / beta) * v0 + dt * (1 - gamma / (2 * beta)) * a0
+        a = c * (x - x0) - v0 / (beta * dt) - (1 / (2 * beta) - 1) * a0
+        return v, a
+
+    R0 = model.assemble(gc0, want_K=False)[0]
+    a0 = torch.from_numpy(spla.spsolve(Mm.tocsc(), R0.numpy()))
+    GC, GV, GA = [gc0.clone()], [gv0.clone()], [a0]
+    for _ in range(steps):
+        pre = GC[-1] + dt * GV[-1] + 0.25 * dt * dt * GA[-1]
+        x = GC[-1].clone()
+        energy = inc_energy(x, pre)
+        low_alpha, it = 0, 0
+        while True:
+            if it > max_iter:
+                raise RuntimeError("Newton did not converge")
+            Rv, (ip, ix, vv) = model.assemble(x)
+            d = (x - pre).numpy()
+            R = Rv + torch.from_numpy(Mm @ d) * c
+            n = R.shape[0]
+            K = sp.csr_matrix((vv.numpy(), ix.numpy(), ip.numpy()), shape=(n, n)) + Mm * c
+            it += 1
+            dx = torch.from_numpy(spla.spsolve(K.tocsc(), -R.numpy()))
+            alpha, c1 = 1.0, 0.3
+            dE = float((dx * R).sum())
+            if dE > 0:
+                dx, dE = -dx, -dE
+            while True:
+                trial = x + alpha * dx
+                e_new = inc_energy(trial, pre)
+                if not math.isfinite(e_new) or e_new > energy + c1 * dE * alpha:
+                    alpha *= 0.5
+                    if alpha < 1e-12:
+                        alpha, trial, e_new = 0.0, x.clone(), energy
+                        break
+                else:
+                    break
+            rmax = float(R.abs().max())
+            if alpha == 0.0 and rmax > tol_error:
+                raise RuntimeError("line search failed")
+            if alpha == 0.0:
+                break
+            low_alpha = low_alpha + 1 if alpha < 0.01 else max(0, low_alpha - 5)
+            if low_alpha > 10:
+                if rmax < 1e-3:
+                    break
+                raise RuntimeError("Newton stalled")
+            x, energy = trial, inc_energy(trial, pre)
+            if float(dx.abs().max()) < tol_error and rmax < tol_error:
+                break
+        v, a = next_va(x, GC[-1], GV[-1], GA[-1])
+        GC.append(x); GV.append(v); GA.append(a)
+    return GC, GV, GA
 
 
 # ---------------------------------------------------------------------------

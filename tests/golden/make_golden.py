@@ -240,18 +240,58 @@ def case_explicit(FEA, O, out, n=4, mu=1.0, kappa=10.0, rho=1.0, steps=40, name=
     print(name, "dt", dt, "stored", len(c.solver._GC_list), "t", c.solver._time_list[-1])
 
 
+def case_implicit_dynamic(FEA, O, out, n=2, mu=1.0, kappa=10.0, rho=1.0, p=0.05, dt=0.05, steps=4, tol=1e-8,
+                          name="newmark_tet2"):
+    """Implicit Newmark run (DynamicImplicitSolver) on a small Kuhn-tet cube:
+    bottom clamped, top pressure, from rest; the stored GC/GV/GA histories and
+    the reduced consistent mass."""
+    X, el = O.tet_block(n)
+    bottom = torch.nonzero(X[:, 2].abs() < 1e-9).flatten().numpy()
+    sets = O.boundary_faces("C3D4", el, X, 2, 1.0)
+    surf = [(idx.numpy(), fid) for idx, fid, _ in sets]
+    c, part, (e,), (ld,) = build_reference(FEA, X, [("C3D4", el, mu, kappa, rho)], [(surf, p)], [(bottom, (0, 1, 2))])
+    c.solver = FEA.solver.DynamicImplicitSolver(deltaT=dt, time_end=steps * dt * (1 - 1e-9), tol_error=tol)
+    c.initialize()
+    gc0 = torch.zeros_like(c.assembly.GC)
+    import contextlib
+    import io
+    with contextlib.redirect_stdout(io.StringIO()):
+        ok = c.solver.solve(GC0=gc0)
+    if ok is not True or len(c.solver._GC_list) != steps + 1:
+        raise RuntimeError("reference implicit dynamics did not finish")
+    mi, mv = c.assembly.assemble_mass_matrix(GC_now=gc0)
+    ip, ix, vv = coalesced_csr(gc0, mi, mv)
+    res = dict(X=X.numpy(), elems=el.numpy(), mu=mu, kappa=kappa, rho=rho, p=p, dt=dt, steps=steps, tol=tol,
+               fixed=bottom, pressure_faces=torch.cat([s_._elems for s_ in ld.surface_element]).numpy(),
+               face_elem=np.concatenate([i for i, _ in surf]),
+               face_id=np.concatenate([np.full(len(i), f) for i, f in surf]),
+               GC=torch.stack(c.solver._GC_list).numpy(), GV=torch.stack(c.solver._GV_list).numpy(),
+               GA=torch.stack(c.solver._GA_list).numpy(), time=np.array(c.solver._time_list),
+               mass_indptr=ip, mass_indices=ix, mass_values=vv)
+    np.savez_compressed(os.path.join(out, "%s.npz" % name), **res)
+    print(name, "E", el.shape[0], "n", gc0.shape[0], "steps", steps, "max|GC|", float(res["GC"][-1].__abs__().max()))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", default=HERE)
+    ap.add_argument("--case", default="all", help="all, or one of: cfg1 tet3 hex5 explicit newmark")
     a = ap.parse_args()
     FEA = import_reference(a.ref)
     from oracle import fea_oracle as O  # mesh generators only
     torch.set_num_threads(os.cpu_count())
-    case_tet_cube(FEA, O, a.out, n=10, name="cfg1")
-    case_tet_cube(FEA, O, a.out, n=3, full_element=True, name="tet3")
-    case_hex_block(FEA, O, a.out)
-    case_explicit(FEA, O, a.out)
+    run = lambda name: a.case in ("all", name)
+    if run("cfg1"):
+        case_tet_cube(FEA, O, a.out, n=10, name="cfg1")
+    if run("tet3"):
+        case_tet_cube(FEA, O, a.out, n=3, full_element=True, name="tet3")
+    if run("hex5"):
+        case_hex_block(FEA, O, a.out)
+    if run("explicit"):
+        case_explicit(FEA, O, a.out)
+    if run("newmark"):
+        case_implicit_dynamic(FEA, O, a.out)
 
 
 if __name__ == "__main__":

@@ -143,3 +143,37 @@ def test_cg_matches_reference_semantics(golden):
     assert r.norm() / b.norm() < 1e-10
     xd = O.direct_solve(ip, ix, vv, b)
     assert rel(x, xd) < 1e-9
+
+
+def newmark_model(g):
+    X = torch.from_numpy(g["X"])
+    el = torch.from_numpy(g["elems"])
+    faces = torch.from_numpy(g["pressure_faces"])
+    return O.Model(X, [O.Group("C3D4", el, float(g["mu"]), float(g["kappa"]), float(g["rho"]))],
+                   [O.PressureLoad(faces, float(g["p"]))], [(g["fixed"], (0, 1, 2))])
+
+
+def test_consistent_mass(golden):
+    """Reduced consistent mass of the reference (assembly.py:421-443), summed."""
+    g = golden("newmark_tet2")
+    M = newmark_model(g).mass_matrix()
+    M.sum_duplicates()
+    M.sort_indices()
+    np.testing.assert_array_equal(M.indptr, g["mass_indptr"])
+    np.testing.assert_array_equal(M.indices, g["mass_indices"])
+    assert rel(M.data, g["mass_values"]) < 1e-14
+
+
+def test_newmark_run(golden):
+    """Implicit Newmark histories of the reference's DynamicImplicitSolver,
+    including its initial acceleration M a0 = R(gc0)."""
+    g = golden("newmark_tet2")
+    m = newmark_model(g)
+    n = g["GC"].shape[1]
+    z = torch.zeros(n, dtype=DT)
+    GC, GV, GA = O.newmark_run(m, z, z, float(g["dt"]), int(g["steps"]), tol_error=float(g["tol"]))
+    assert len(GC) == g["GC"].shape[0]
+    for k in range(len(GC)):
+        assert rel(GC[k], g["GC"][k]) < 1e-10 or np.abs(g["GC"][k]).max() < 1e-15
+        assert rel(GV[k], g["GV"][k]) < 1e-10 or np.abs(g["GV"][k]).max() < 1e-15
+        assert rel(GA[k], g["GA"][k]) < 1e-10
