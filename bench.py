@@ -53,12 +53,15 @@ def args_():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
-    ap.add_argument("--workload", default="assembly", choices=["assembly", "pcg", "explicit", "newton", "adjoint", "serving"],
+    ap.add_argument("--workload", default="assembly", choices=["assembly", "pcg", "explicit", "newton", "adjoint", "serving", "newmark"],
                     help="assembly (default, the headline line) or one of the other measured forms")
     ap.add_argument("--explicit-n", type=int, default=70, help="cells per side of the Kuhn-tet cube")
     ap.add_argument("--explicit-steps", type=int, default=10000)
     ap.add_argument("--pcg-max-iter", type=int, default=50000, help="iteration cap of each PCG solve")
     ap.add_argument("--adjoint-n", type=int, default=40, help="elements per side of the compliance block")
+    ap.add_argument("--newmark-n", type=int, default=48, help="elements per side of the Newmark block")
+    ap.add_argument("--newmark-dt", type=float, default=0.01)
+    ap.add_argument("--newmark-steps", type=int, default=10)
     ap.add_argument("--fd-samples", type=int, default=200, help="coordinates checked by central differences")
     ap.add_argument("--serve-requests", type=int, default=512)
     ap.add_argument("--serve-rates", default="inf", help="comma-separated Poisson arrival rates (requests/s)")
@@ -210,12 +213,14 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
-def build_block_model(n, p=0.02):
+def build_block_model(n, p=0.02, rho=None):
     import fea_b200 as F
     X, el, clamp, end, faces = workload(n)
     part = F.Part(X)
     e = F.elements.C3D8(elems=el, elems_index=np.arange(el.shape[0]), part=part)
     e.set_materials(F.materials.NeoHookean(1.0, 50.0))
+    if rho is not None:
+        e.set_density(rho)
     part.add_element(e)
     part.set_nodes["clamp"] = clamp
     part.add_surface_set("end", [(end, 3)])
@@ -380,6 +385,47 @@ def run_newton(a):
     print(json.dumps(line), flush=True)
 
 
+def run_newmark(a):
+    """Implicit Newmark dynamics (DynamicImplicitSolver) of the jittered n^3
+    C3D8 block, rho = 1, clamped at x = 0, pressure 0.02 on x = 1 from t = 0,
+    from rest: ``--newmark-steps`` steps of dt = ``--newmark-dt``, Newton to
+    max|R| < 1e-11 per step."""
+    import torch
+    import fea_b200 as F
+    asm, el, X, _ = build_block_model(a.newmark_n, rho=1.0)
+    sol = F.solver.DynamicImplicitSolver(deltaT=a.newmark_dt, time_end=a.newmark_steps * a.newmark_dt * (1 - 1e-9),
+                                         tol_error=1e-11)
+    sol.initialize(asm)
+    gc0 = torch.zeros_like(asm.GC)
+    newton, pcg = [], []
+    orig = sol._solve_iteration
+
+    def counted(*args, **kw):
+        r = orig(*args, **kw)
+        newton.append(sol._iter_now)
+        pcg.append(sum(h.get("pcg_iters", 0) for h in sol.history))
+        return r
+
+    sol._solve_iteration = counted
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    sol.solve(GC0=gc0)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    steps = len(sol._GC_list) - 1
+    R = sol._incremental_csr(sol._GC_list[-1], sol._GC_list[-2] + a.newmark_dt * sol._GV_list[-2]
+                             + 0.25 * a.newmark_dt ** 2 * sol._GA_list[-2])[0]
+    line = {"metric": "implicit Newmark steps/s (%d^3 C3D8, dt %g)" % (a.newmark_n, a.newmark_dt),
+            "unit": "steps/s", "value": steps / (ms * 1e-3), "higher_is_better": True, "workload": "newmark",
+            "ms_per_step": ms / steps, "steps": steps, "elements": int(el.shape[0]), "ndof": int(asm.plan.ndof),
+            "newton_iters_per_step": newton, "pcg_iters_per_step": pcg,
+            "last_step_max_residual": float(R.abs().max()), "max_displacement": float(sol._GC_list[-1].abs().max()),
+            "energy_history": sol.E_history, "timing": "CUDA events around solve(), initial acceleration included"}
+    print(json.dumps(line), flush=True)
+
+
 def run_adjoint(a):
     """Compliance f.u of an n^3 C3D8 block (nodes jittered as in the assembly
     workload, mu = 1, kappa = 50, bottom node plane clamped, pressure 0.03 on
@@ -533,7 +579,7 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         {"pcg": run_pcg, "explicit": run_explicit, "newton": run_newton, "adjoint": run_adjoint,
-         "serving": run_serving}[a.workload](a)
+         "serving": run_serving, "newmark": run_newmark}[a.workload](a)
         return
     import torch
     import torch.distributed as dist
