@@ -843,7 +843,10 @@ static int read_nnz(const int64_t* ip, int64_t n, int64_t* nnz, cudaStream_t s) 
 // order with no block-level barrier.  A slot's arithmetic depends only on
 // its own items, so its iterates are the same bits alone or batched.
 constexpr int PCGB_ROWS = 256;      // rows per update item and per start chunk
-constexpr int PCGB_GROUP = 16;      // nodes (plan layout) or rows (CSR) per SpMV item
+#ifndef FEA_PCGB_GROUP
+#define FEA_PCGB_GROUP 16
+#endif
+constexpr int PCGB_GROUP = FEA_PCGB_GROUP;   // nodes (plan layout) or rows (CSR) per SpMV item
 
 struct PcgbSlotDev {
   const int64_t* ptr;
@@ -894,6 +897,17 @@ static int64_t pcgb_items_s(int64_t n, int64_t n_nodes) {
 }
 static int64_t pcgb_items_u(int64_t n) { return (n + PCGB_ROWS - 1) / PCGB_ROWS; }
 
+// As pcgb_warp_last, for a warp that finished `add` items of the slot at once.
+__device__ __forceinline__ bool pcgb_warp_last_n(unsigned* counter, unsigned add, int total, int lane) {
+  unsigned old = 0u;
+  if (lane == 0) {
+    __threadfence();
+    old = atomicAdd(counter, add);
+  }
+  old = __shfl_sync(0xffffffffu, old, 0);
+  return old + add == (unsigned)total;
+}
+
 __device__ __forceinline__ bool pcgb_warp_last(unsigned* counter, int total, int lane) {
   unsigned old = 0u;
   if (lane == 0) {
@@ -923,30 +937,39 @@ __device__ __forceinline__ double pcgb_warp_sum(const double* part, int n, int s
   return v;
 }
 
-// q = A p over nodes [n0, n1) of a plan-layout slot: half-warp h takes nodes
-// n0 + 2i + h (16 lanes, 48 columns per pass); the next pair's metadata and
-// first column indices are prefetched.  Returns p.q over those rows (lane 0).
-__device__ __forceinline__ double pcgb_nodes_spmv(const PcgbSlotDev& S, int64_t n0, int64_t n1, int lane) {
+// q = A p over the node items g0 .. g0 + cnt - 1 of slot S (PCGB_GROUP nodes
+// each), two nodes at a time per warp (16 lanes each, 48 columns per pass).
+// The next pair's metadata and first-pass column indices are loaded while
+// the current pair is processed, across item boundaries, so a run of items
+// streams like one long item; each item's p.q is reduced by the same fixed
+// tree over the warp and written to part_s[g] when the item ends: an item's
+// sums do not depend on the run it is processed in.  (With the register
+// count capped for 4 CTAs per SM the kernel ran 24% slower.)
+__device__ __forceinline__ void pcgb_nodes_spmv_run(const PcgbSlotDev& S, int g0, int cnt, int lane) {
   const int h = lane >> 4, hl = lane & 15;
+  const int64_t nbeg = (int64_t)g0 * PCGB_GROUP;
+  const int64_t nend = min((int64_t)(g0 + cnt) * PCGB_GROUP, S.n_nodes);
   double contrib = 0.0;
-  int64_t nd = n0 + h;
+  int64_t nd = nbeg + h;
   unsigned m = 0;
   int L = 0;
   int64_t vb = 0;
   int32_t jn[3] = {0, 0, 0};
-  if (nd < n1) {
+  if (nd < nend) {
     m = S.mask[nd];
     L = m ? S.rowlen[nd] : 0;
     vb = S.vbase[nd];
 #pragma unroll
     for (int k = 0; k < 3; ++k) jn[k] = hl + 16 * k < L ? __ldg(S.idx + vb + hl + 16 * k) : 0;
   }
-  for (int64_t base = n0; base < n1; base += 2) {          // warp-uniform
+  int g = g0;
+  int64_t item_end = min(nbeg + PCGB_GROUP, nend);
+  for (int64_t base = nbeg; base < nend; base += 2) {          // warp-uniform
     const int64_t nx = nd + 2;
     unsigned m2 = 0;
     int L2 = 0;
     int64_t vb2 = 0;
-    if (nx < n1) {
+    if (nx < nend) {
       m2 = S.mask[nx];
       L2 = S.rowlen[nx];
       vb2 = S.vbase[nx];
@@ -999,11 +1022,15 @@ __device__ __forceinline__ double pcgb_nodes_spmv(const PcgbSlotDev& S, int64_t 
     m = m2;
     L = Ln;
     vb = vb2;
-  }
-  // lanes 0-2 and 16-18 hold the sums: fixed tree over the warp
+    if (base + 2 >= item_end) {                                 // the item's last pair
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, o);
-  return lane == 0 ? contrib : 0.0;
+      for (int o = 16; o > 0; o >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, o);
+      if (lane == 0) S.part_s[g] = contrib;
+      contrib = 0.0;
+      ++g;
+      item_end = min(item_end + PCGB_GROUP, nend);
+    }
+  }
 }
 
 // q = A p over CSR rows [r0, r1), LANES lanes per row; returns p.q (lane 0)
@@ -1031,25 +1058,35 @@ __device__ __forceinline__ double pcgb_rows_spmv(const PcgbSlotDev& S, int64_t r
   return lane == 0 ? contrib : 0.0;
 }
 
+// Each warp takes a contiguous range of the item list (items of one slot are
+// consecutive in it) and processes it slot run by slot run: the node-row
+// SpMV streams through a run's items without stopping at their boundaries,
+// and the slot's completion counter advances once per run.
 __global__ void __launch_bounds__(PCG_TPB) k_pcgb_spmv(PcgbView V) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * PCG_WARPS;
   const int64_t nit = V.hdr->nitem_s;
-  for (int64_t it = (int64_t)blockIdx.x * PCG_WARPS + (threadIdx.x >> 5); it < nit; it += nw) {
+  const int64_t per = (nit + nw - 1) / nw;
+  int64_t it = ((int64_t)blockIdx.x * PCG_WARPS + (threadIdx.x >> 5)) * per;
+  const int64_t it_end = min(nit, it + per);
+  while (it < it_end) {                           // warp-uniform
     const PcgbSlotDev& S = V.slots[V.s_slot[it]];
-    if (S.st[S_DONE] != 0.0) continue;            // warp-uniform
-    const int g = V.s_local[it];
-    double c;
+    const int g0 = V.s_local[it];
+    const int cnt = (int)min(it_end - it, (int64_t)S.nitem_s - g0);
+    it += cnt;
+    if (S.st[S_DONE] != 0.0) continue;
     if (S.vbase) {
-      const int64_t n0 = (int64_t)g * PCGB_GROUP;
-      c = pcgb_nodes_spmv(S, n0, min(n0 + PCGB_GROUP, S.n_nodes), lane);
+      pcgb_nodes_spmv_run(S, g0, cnt, lane);
     } else {
-      const int64_t r0 = (int64_t)g * PCGB_GROUP, r1 = min(r0 + PCGB_GROUP, S.n);
-      c = S.lanes == 32 ? pcgb_rows_spmv<32>(S, r0, r1, lane)
-                        : (S.lanes == 16 ? pcgb_rows_spmv<16>(S, r0, r1, lane) : pcgb_rows_spmv<8>(S, r0, r1, lane));
+      for (int g = g0; g < g0 + cnt; ++g) {
+        const int64_t r0 = (int64_t)g * PCGB_GROUP, r1 = min(r0 + PCGB_GROUP, S.n);
+        const double c = S.lanes == 32 ? pcgb_rows_spmv<32>(S, r0, r1, lane)
+                                       : (S.lanes == 16 ? pcgb_rows_spmv<16>(S, r0, r1, lane)
+                                                        : pcgb_rows_spmv<8>(S, r0, r1, lane));
+        if (lane == 0) S.part_s[g] = c;
+      }
     }
-    if (lane == 0) S.part_s[g] = c;
-    if (pcgb_warp_last(S.counter + 0, S.nitem_s, lane)) {
+    if (pcgb_warp_last_n(S.counter + 0, (unsigned)cnt, S.nitem_s, lane)) {
       const double pq = pcgb_warp_sum(S.part_s, S.nitem_s, 1, 0, lane);
       if (lane == 0) {
         S.st[S_PQ] = pq;

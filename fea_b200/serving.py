@@ -351,6 +351,8 @@ def serve(requests, max_slots=32, round_iters=32, mem_budget=32 << 30, use_graph
     slots = [None] * max_slots
     finished = []                      # jobs whose solve ended in the last polled round
     in_flight = False
+    ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    timing.update(round_gpu_s=0.0, slot_rounds=0)
     while waiting or preparing or ready or queue_slot or finished or in_flight or any(j is not None for j in slots):
         now = time.perf_counter() - t0
         # admit arrived requests into preparation while memory allows
@@ -379,6 +381,7 @@ def serve(requests, max_slots=32, round_iters=32, mem_budget=32 << 30, use_graph
             t_w = time.perf_counter()
             state = eng.wait()
             timing["wait_s"] += time.perf_counter() - t_w
+            timing["round_gpu_s"] += ev_a.elapsed_time(ev_b) * 1e-3
             in_flight = False
             busy_rounds += 1
             for k, job in enumerate(slots):
@@ -410,7 +413,10 @@ def serve(requests, max_slots=32, round_iters=32, mem_budget=32 << 30, use_graph
             main.wait_stream(work_stream)
             for k in fresh:
                 eng.start(k)
+        timing["slot_rounds"] += sum(j is not None for j in slots)
+        ev_a.record()
         eng.run_round()
+        ev_b.record()
         eng.poll_async()
         in_flight = True
     pool.shutdown()
