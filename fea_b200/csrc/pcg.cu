@@ -1103,14 +1103,22 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcgb_spmv(PcgbView V) {
   }
 }
 
+// The vector kernels take contiguous runs of the update item list as the
+// SpMV does: the slot's pointers and scalars are read once per run and its
+// completion counter advances once per run.
 __global__ void __launch_bounds__(PCG_TPB) k_pcgb_update(PcgbView V) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * PCG_WARPS;
   const int64_t nit = V.hdr->nitem_u;
-  for (int64_t it = (int64_t)blockIdx.x * PCG_WARPS + (threadIdx.x >> 5); it < nit; it += nw) {
+  const int64_t per = (nit + nw - 1) / nw;
+  int64_t it = ((int64_t)blockIdx.x * PCG_WARPS + (threadIdx.x >> 5)) * per;
+  const int64_t it_end = min(nit, it + per);
+  while (it < it_end) {                           // warp-uniform
     const PcgbSlotDev& S = V.slots[V.u_slot[it]];
+    const int l0 = V.u_local[it];
+    const int cnt = (int)min(it_end - it, (int64_t)S.nitem_u - l0);
+    it += cnt;
     if (S.st[S_DONE] != 0.0) continue;
-    const int l = V.u_local[it];
     const double alpha = S.st[S_ALPHA];
     double* __restrict__ x = S.x;
     double* __restrict__ r = S.r;
@@ -1118,36 +1126,39 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcgb_update(PcgbView V) {
     const double* __restrict__ p = S.p;
     const double* __restrict__ q = S.q;
     const double* __restrict__ dinv = S.dinv;
-    constexpr int K = PCGB_ROWS / 32;
-    double xv[K], pv[K], rv[K], qv[K], dv[K];
-    const int64_t i0 = (int64_t)l * PCGB_ROWS + lane;
+    const int64_t n = S.n;
+    for (int l = l0; l < l0 + cnt; ++l) {
+      constexpr int K = PCGB_ROWS / 32;
+      double xv[K], pv[K], rv[K], qv[K], dv[K];
+      const int64_t i0 = (int64_t)l * PCGB_ROWS + lane;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {              // all loads of the item first
-      const int64_t i = i0 + 32 * k;
-      const bool in = i < S.n;
-      xv[k] = in ? x[i] : 0.0;
-      pv[k] = in ? p[i] : 0.0;
-      rv[k] = in ? r[i] : 0.0;
-      qv[k] = in ? q[i] : 0.0;
-      dv[k] = in ? dinv[i] : 0.0;
-    }
-    double c = 0.0;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int64_t i = i0 + 32 * k;
-      if (i < S.n) {
-        x[i] = xv[k] + alpha * pv[k];
-        const double ri = rv[k] - alpha * qv[k];
-        r[i] = ri;
-        const double zi = ri * dv[k];
-        z[i] = zi;
-        c += ri * zi;
+      for (int k = 0; k < K; ++k) {            // all loads of the item first
+        const int64_t i = i0 + 32 * k;
+        const bool in = i < n;
+        xv[k] = in ? x[i] : 0.0;
+        pv[k] = in ? p[i] : 0.0;
+        rv[k] = in ? r[i] : 0.0;
+        qv[k] = in ? q[i] : 0.0;
+        dv[k] = in ? dinv[i] : 0.0;
       }
-    }
+      double c = 0.0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if (lane == 0) S.part_u[l] = c;
-    if (pcgb_warp_last(S.counter + 1, S.nitem_u, lane)) {
+      for (int k = 0; k < K; ++k) {
+        const int64_t i = i0 + 32 * k;
+        if (i < n) {
+          x[i] = xv[k] + alpha * pv[k];
+          const double ri = rv[k] - alpha * qv[k];
+          r[i] = ri;
+          const double zi = ri * dv[k];
+          z[i] = zi;
+          c += ri * zi;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+      if (lane == 0) S.part_u[l] = c;
+    }
+    if (pcgb_warp_last_n(S.counter + 1, (unsigned)cnt, S.nitem_u, lane)) {
       const double rz = pcgb_warp_sum(S.part_u, S.nitem_u, 1, 0, lane);
       if (lane == 0) {
         const double iter = S.st[S_ITER] + 1.0;
@@ -1173,26 +1184,34 @@ __global__ void __launch_bounds__(PCG_TPB) k_pcgb_p(PcgbView V) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * PCG_WARPS;
   const int64_t nit = V.hdr->nitem_u;
-  for (int64_t it = (int64_t)blockIdx.x * PCG_WARPS + (threadIdx.x >> 5); it < nit; it += nw) {
+  const int64_t per = (nit + nw - 1) / nw;
+  int64_t it = ((int64_t)blockIdx.x * PCG_WARPS + (threadIdx.x >> 5)) * per;
+  const int64_t it_end = min(nit, it + per);
+  while (it < it_end) {                           // warp-uniform
     const PcgbSlotDev& S = V.slots[V.u_slot[it]];
+    const int l0 = V.u_local[it];
+    const int cnt = (int)min(it_end - it, (int64_t)S.nitem_u - l0);
+    it += cnt;
     if (S.st[S_DONE] != 0.0) continue;
     const double beta = S.st[S_BETA];
-    const int l = V.u_local[it];
     double* __restrict__ p = S.p;
     const double* __restrict__ z = S.z;
-    constexpr int K = PCGB_ROWS / 32;
-    double zv[K], pv[K];
-    const int64_t i0 = (int64_t)l * PCGB_ROWS + lane;
+    const int64_t n = S.n;
+    for (int l = l0; l < l0 + cnt; ++l) {
+      constexpr int K = PCGB_ROWS / 32;
+      double zv[K], pv[K];
+      const int64_t i0 = (int64_t)l * PCGB_ROWS + lane;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int64_t i = i0 + 32 * k;
-      zv[k] = i < S.n ? z[i] : 0.0;
-      pv[k] = i < S.n ? p[i] : 0.0;
-    }
+      for (int k = 0; k < K; ++k) {
+        const int64_t i = i0 + 32 * k;
+        zv[k] = i < n ? z[i] : 0.0;
+        pv[k] = i < n ? p[i] : 0.0;
+      }
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int64_t i = i0 + 32 * k;
-      if (i < S.n) p[i] = zv[k] + beta * pv[k];
+      for (int k = 0; k < K; ++k) {
+        const int64_t i = i0 + 32 * k;
+        if (i < n) p[i] = zv[k] + beta * pv[k];
+      }
     }
   }
 }
