@@ -53,12 +53,14 @@ def args_():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
-    ap.add_argument("--workload", default="assembly", choices=["assembly", "pcg", "explicit", "newton", "adjoint", "serving", "newmark"],
+    ap.add_argument("--workload", default="assembly", choices=["assembly", "pcg", "explicit", "newton", "adjoint", "serving", "newmark", "pcgb"],
                     help="assembly (default, the headline line) or one of the other measured forms")
     ap.add_argument("--explicit-n", type=int, default=70, help="cells per side of the Kuhn-tet cube")
     ap.add_argument("--explicit-steps", type=int, default=10000)
     ap.add_argument("--pcg-max-iter", type=int, default=50000, help="iteration cap of each PCG solve")
     ap.add_argument("--adjoint-n", type=int, default=40, help="elements per side of the compliance block")
+    ap.add_argument("--pcgb-slots", type=int, default=24)
+    ap.add_argument("--pcgb-rounds", type=int, default=10)
     ap.add_argument("--newmark-n", type=int, default=48, help="elements per side of the Newmark block")
     ap.add_argument("--newmark-dt", type=float, default=0.01)
     ap.add_argument("--newmark-steps", type=int, default=10)
@@ -426,6 +428,53 @@ def run_newmark(a):
     print(json.dumps(line), flush=True)
 
 
+def run_pcgb(a):
+    """Batched PCG kernels of the serving engine alone: ``--pcgb-slots``
+    resident C3D4 cantilever systems (60k-120k elements, seeded, K at rest),
+    PCG with a tolerance no slot reaches in the timed rounds; device time per
+    batched iteration (CUDA events over ``--pcgb-rounds`` graph replays of 32
+    iterations) and the bytes it streams (values, column lists once per
+    node, 13 vector passes)."""
+    import torch
+    from fea_b200 import serving, solver as S
+    reqs = serving.make_requests(a.pcgb_slots, float("inf"), seed=1, min_elems=60000, max_elems=120000)
+    asms, lins, works = [], [], []
+    for r in reqs:
+        asm = serving.build_assembly(r)
+        R, K = asm.assemble_csr(asm.GC)
+        b = (-R).contiguous()
+        lins.append(S.LinearSolve(K, b, torch.zeros_like(b), 1e-300, 10 ** 8, False))
+        asms.append(asm)
+    max_items = a.pcgb_slots * max((serving.request_rows(r) // 3 + 15) // 16 + 1 for r in reqs)
+    eng = serving.BatchedPCG(a.pcgb_slots, max_items, 32, True)
+    for k, (asm, lin) in enumerate(zip(asms, lins)):
+        w = torch.empty(serving.BatchedPCG.work_len(asm.plan), dtype=torch.float64, device="cuda")
+        works.append(w)
+        eng.assign(k, asm.plan, lin, w)
+    eng.sync()
+    for k in range(a.pcgb_slots):
+        eng.start(k)
+    for _ in range(3):
+        eng.run_round()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.pcgb_rounds):
+        eng.run_round()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / (a.pcgb_rounds * 32)
+    active = int((eng.poll()[:, 0] == 0).sum())
+    nnz = sum(x.plan.nnz for x in asms)
+    n = sum(x.plan.ndof for x in asms)
+    idx = sum(int(x.plan.rowlen[x.plan.mask != 0].to(torch.int64).sum()) for x in asms)
+    byt = 8 * nnz + 4 * idx + 8 * 13 * n
+    print(json.dumps({"metric": "batched PCG iteration (%d resident C3D4 slots)" % a.pcgb_slots, "unit": "ms",
+                      "value": ms, "higher_is_better": False, "workload": "pcgb", "slots_active": active,
+                      "ndof_total": n, "nnz_total": nnz, "bytes_per_iter": byt,
+                      "achieved_GBs": byt / (ms * 1e-3) / 1e9}), flush=True)
+
+
 def run_adjoint(a):
     """Compliance f.u of an n^3 C3D8 block (nodes jittered as in the assembly
     workload, mu = 1, kappa = 50, bottom node plane clamped, pressure 0.03 on
@@ -579,7 +628,7 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         {"pcg": run_pcg, "explicit": run_explicit, "newton": run_newton, "adjoint": run_adjoint,
-         "serving": run_serving, "newmark": run_newmark}[a.workload](a)
+         "serving": run_serving, "newmark": run_newmark, "pcgb": run_pcgb}[a.workload](a)
         return
     import torch
     import torch.distributed as dist
