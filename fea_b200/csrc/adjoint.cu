@@ -75,7 +75,7 @@ __device__ __forceinline__ void adj_gauss(const AdjParams& P, const int32_t* cn,
 // M of the formula above (row-major M[p][k]) and dPhi/dmu at one Gauss point.
 __device__ __forceinline__ void adj_M(const double F[9], const double iF[9], double J, const double Lam[9], double mu,
                                       double kappa, double M[9], double& dmu) {
-  const double Jm = pow(J, -2.0 / 3.0);
+  const double Jm = jm23(J);
   double sF2 = 0.0;
 #pragma unroll
   for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];

@@ -121,7 +121,7 @@ __device__ __forceinline__ void element_strip(const VolParams& P, const int32_t*
   for (int g = 0; g < Elem<NN>::NG; ++g) {
     double w, F[9], iF[9], J, iJ[9];
     gauss_kin<NN>(P, cn, mk, rd, g, w, F, iF, J, iJ);
-    double Jm = pow(J, -2.0 / 3.0);
+    double Jm = jm23(J);
     double sF2 = 0.0;
 #pragma unroll
     for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
         F[3 * I + i] = (I == i ? 1.0 : 0.0) + Ju[3 * I] * iJ[i] + Ju[3 * I + 1] * iJ[3 + i] + Ju[3 * I + 2] * iJ[6 + i];
     const double J = inv3(F, iF);
     const double mu = P.mu, kappa = P.kappa;
-    const double Jm = pow(J, -2.0 / 3.0);
+    const double Jm = jm23(J);
     double sF2 = 0.0;
 #pragma unroll
     for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];
@@ -725,7 +725,7 @@ __global__ void __launch_bounds__(256) k_vol_energy(VolParams P, double* partial
       double sF2 = 0.0;
 #pragma unroll
       for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];
-      double I1 = sF2 * pow(J, -2.0 / 3.0);
+      double I1 = sF2 * jm23(J);
       double W = P.mu / 2.0 * (I1 - 3.0) + P.kappa / 2.0 * (J - 1.0) * (J - 1.0);
       acc += W * w;
     }

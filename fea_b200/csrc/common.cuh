@@ -99,6 +99,14 @@ struct Elem<8> {
 };
 
 // ---- 3x3 (row-major m[3*r+c]) --------------------------------------------
+// J^(-2/3) of the Neo-Hookean isochoric part from the reciprocal cube root
+// (CUDA's rcbrt, 1 ulp) squared: one special function instead of a general
+// power.  J < 0 gives NaN and J = 0 gives +inf, as pow(J, -2/3) does.
+__device__ __forceinline__ double jm23(double J) {
+  const double r = rcbrt(J);
+  return J < 0.0 ? __longlong_as_double(0x7ff8000000000000LL) : r * r;
+}
+
 template <class T>
 __device__ __forceinline__ T det3(const T m[9]) {
   return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +

@@ -79,7 +79,7 @@ __device__ __forceinline__ void elem_force(const ExParams& P, const int32_t* cn,
       for (int i = 0; i < 3; ++i)
         F[3 * I + i] = (I == i ? T(1) : T(0)) + Ju[3 * I] * iJ[i] + Ju[3 * I + 1] * iJ[3 + i] + Ju[3 * I + 2] * iJ[6 + i];
     T J = inv3(F, iF);
-    T Jm = (T)pow((double)J, -2.0 / 3.0);
+    T Jm = (T)jm23((double)J);
     T sF2 = T(0);
 #pragma unroll
     for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];
