@@ -518,7 +518,7 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
       ro[1] = make_double2(racc[2], 0.0);
     }
   }
-  if (ER) {
+  if (ER && act) {
 #pragma unroll
     for (int j = 0; j < 3; ++j) P.elemR[(int64_t)(3 * a + j) * P.ne + e] = racc[j];
   }

@@ -132,6 +132,29 @@ __device__ __forceinline__ T inv3(const T m[9], T r[9]) {
   return d;
 }
 
+// Inverse of the deformation gradient with J^(-2/3) from one reciprocal cube
+// root r = rcbrt(J): 1/J = r^3 replaces the division of inv3.  Returns J;
+// *jm = J^(-2/3) (NaN for J < 0, as pow gives).
+__device__ __forceinline__ double inv3_jm(const double m[9], double r[9], double* jm) {
+  const double c00 = m[4] * m[8] - m[5] * m[7];
+  const double c01 = m[5] * m[6] - m[3] * m[8];
+  const double c02 = m[3] * m[7] - m[4] * m[6];
+  const double d = m[0] * c00 + m[1] * c01 + m[2] * c02;
+  const double cr = rcbrt(d);
+  const double id = cr * cr * cr;
+  *jm = d < 0.0 ? __longlong_as_double(0x7ff8000000000000LL) : cr * cr;
+  r[0] = c00 * id;
+  r[1] = (m[2] * m[7] - m[1] * m[8]) * id;
+  r[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+  r[3] = c01 * id;
+  r[4] = (m[0] * m[8] - m[2] * m[6]) * id;
+  r[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+  r[6] = c02 * id;
+  r[7] = (m[1] * m[6] - m[0] * m[7]) * id;
+  r[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+  return d;
+}
+
 __device__ __forceinline__ int popc3(unsigned m) { return __popc(m & 7u); }
 __device__ __forceinline__ int rank3(unsigned m, int k) { return __popc(m & ((1u << k) - 1u)); }
 

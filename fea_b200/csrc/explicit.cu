@@ -78,8 +78,15 @@ __device__ __forceinline__ void elem_force(const ExParams& P, const int32_t* cn,
 #pragma unroll
       for (int i = 0; i < 3; ++i)
         F[3 * I + i] = (I == i ? T(1) : T(0)) + Ju[3 * I] * iJ[i] + Ju[3 * I + 1] * iJ[3 + i] + Ju[3 * I + 2] * iJ[6 + i];
-    T J = inv3(F, iF);
-    T Jm = (T)jm23((double)J);
+    T J, Jm;
+    if constexpr (sizeof(T) == 8 && NN == 4) {       // (C3D8: 222 instead of 168 registers)
+      double jmd;
+      J = inv3_jm(F, iF, &jmd);
+      Jm = jmd;
+    } else {
+      J = inv3(F, iF);
+      Jm = (T)jm23((double)J);
+    }
     T sF2 = T(0);
 #pragma unroll
     for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];

@@ -360,3 +360,25 @@ def test_lumped_mass_totals_rho_volume(kind):
         assert abs(float(m[:, d].sum()) - rho * vol) < 1e-12 * rho * vol
     ref = O.Model(X, [O.Group(kind, el, 1.0, 1.0, rho)], [], []).lumped_mass_inv()
     assert rel(asm.lumped_mass_inv(), ref) < 1e-14
+
+
+def test_hex_element_residual_stays_in_bounds(golden):
+    """hex5 has 125 elements, not a multiple of the 8 elements of a C3D8 CTA:
+    the element residual output must hold exactly the golden values and the
+    memory after it must stay untouched, on every one of repeated calls."""
+    g = golden("hex5")
+    c, e, _ = fea_model(g, "C3D8")
+    c.initialize()
+    U = c.assembly._GC2RGC(torch.from_numpy(g["state"]).cuda())[0]
+    P = e._group_plan()
+    mu, kappa = e.materials.parameters()
+    gc = e._gc(U)
+    n = 8 * 3 * e._elems.shape[0]
+    assert e._elems.shape[0] % 8 != 0
+    for _ in range(20):
+        buf = torch.full((n + 256,), -7.0, dtype=torch.float64, device="cuda")
+        K = torch.full((P.nnz,), float("nan"), dtype=torch.float64, device="cuda")
+        P.assemble_volume(0, mu, kappa, gc, K=K, elemR=buf[:n])
+        assert bool((buf[n:] == -7.0).all())
+        assert rel(buf[:n], g["elem_R"]) < TOL
+        assert rel(K, g["elem_K_values"]) < TOL
