@@ -308,22 +308,28 @@ __global__ void __launch_bounds__(PCG_TPB) k_spmv_node_sub(NodeOp<V> A, const X*
         h[k] = q < L;
         j[k] = q0 == 0 ? jn[k] : (h[k] ? __ldg(A.idx + vb + q) : 0);
       }
-      V va[3][CPL];
+      double va[3][CPL];
 #pragma unroll
       for (int r = 0; r < 3; ++r)
 #pragma unroll
         for (int k = 0; k < CPL; ++k) {
           const int q = q0 + hl + LPN * k;
-          va[r][k] = (r < f && h[k]) ? __ldcs(v0 + (int64_t)r * L + q) : (V)0;
+          va[r][k] = (r < f && h[k]) ? (double)__ldcs(v0 + (int64_t)r * L + q) : 0.0;
         }
-      X xv[CPL];
+      double xv[CPL];
 #pragma unroll
-      for (int k = 0; k < CPL; ++k) xv[k] = h[k] ? x[j[k]] : (X)0;
+      for (int k = 0; k < CPL; ++k) xv[k] = h[k] ? (double)x[j[k]] : 0.0;
+      if constexpr (CPL == 3) {
+        s0 += va[0][0] * xv[0] + va[0][1] * xv[1] + va[0][2] * xv[2];
+        s1 += va[1][0] * xv[0] + va[1][1] * xv[1] + va[1][2] * xv[2];
+        s2 += va[2][0] * xv[0] + va[2][1] * xv[1] + va[2][2] * xv[2];
+      } else {
 #pragma unroll
-      for (int k = 0; k < CPL; ++k) {
-        s0 += (double)va[0][k] * (double)xv[k];
-        s1 += (double)va[1][k] * (double)xv[k];
-        s2 += (double)va[2][k] * (double)xv[k];
+        for (int k = 0; k < CPL; ++k) {
+          s0 += va[0][k] * xv[k];
+          s1 += va[1][k] * xv[k];
+          s2 += va[2][k] * xv[k];
+        }
       }
     }
     const int Ln = m2 ? L2 : 0;
