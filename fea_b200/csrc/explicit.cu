@@ -116,13 +116,37 @@ __global__ void __launch_bounds__(128) k_explicit(ExParams P, int flags) {
   const unsigned mn = P.mask[n];
   if (!mn) return;
   double r[3] = {0.0, 0.0, 0.0};
-  if (flags & 1) {
+  if ((flags & 1) && NN == 8) {
     for (int q = P.nodeinc[n]; q < P.nodeinc[n + 1]; ++q) {
       const int ea = P.inc[q];
       const int64_t e = ea >> 4;
       int32_t cn[NN];
 #pragma unroll
       for (int b = 0; b < NN; ++b) cn[b] = P.conn[e * NN + b];
+      elem_force<NN, T>(P, cn, ea & 15, r);
+    }
+  } else if (flags & 1) {
+    // C3D4: the next incidence and its element's nodes are loaded while the
+    // current element is evaluated (for C3D8 the extra registers cost a CTA
+    // per SM)
+    const int q0 = P.nodeinc[n], q1 = P.nodeinc[n + 1];
+    int ea_n = 0;
+    int32_t cn_n[NN];
+    if (q0 < q1) {
+      ea_n = P.inc[q0];
+#pragma unroll
+      for (int b = 0; b < NN; ++b) cn_n[b] = P.conn[(int64_t)(ea_n >> 4) * NN + b];
+    }
+    for (int q = q0; q < q1; ++q) {
+      const int ea = ea_n;
+      int32_t cn[NN];
+#pragma unroll
+      for (int b = 0; b < NN; ++b) cn[b] = cn_n[b];
+      if (q + 1 < q1) {
+        ea_n = P.inc[q + 1];
+#pragma unroll
+        for (int b = 0; b < NN; ++b) cn_n[b] = P.conn[(int64_t)(ea_n >> 4) * NN + b];
+      }
       elem_force<NN, T>(P, cn, ea & 15, r);
     }
   }
