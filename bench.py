@@ -69,7 +69,7 @@ def args_():
     ap.add_argument("--serve-rates", default="inf", help="comma-separated Poisson arrival rates (requests/s)")
     ap.add_argument("--serve-min-elems", type=int, default=2000)
     ap.add_argument("--serve-max-elems", type=int, default=200000)
-    ap.add_argument("--serve-slots", type=int, default=32)
+    ap.add_argument("--serve-slots", type=int, default=48)
     ap.add_argument("--serve-round", type=int, default=32, help="PCG iterations per captured round")
     ap.add_argument("--serve-plain", type=int, default=1, help="also time the one-at-a-time path")
     return ap.parse_args()

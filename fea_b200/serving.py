@@ -293,7 +293,7 @@ def _prepare(req, stream_):
     return asm, sol
 
 
-def serve(requests, max_slots=32, round_iters=32, mem_budget=32 << 30, use_graph=True, prep_threads=2,
+def serve(requests, max_slots=48, round_iters=32, mem_budget=32 << 30, use_graph=True, prep_threads=2,
           keep=True):
     """Serve `requests` (arrival times honoured) with continuous batching.
     Returns (results in request order, server statistics)."""
