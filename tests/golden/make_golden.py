@@ -241,15 +241,15 @@ def case_explicit(FEA, O, out, n=4, mu=1.0, kappa=10.0, rho=1.0, steps=40, name=
 
 
 def case_implicit_dynamic(FEA, O, out, n=2, mu=1.0, kappa=10.0, rho=1.0, p=0.05, dt=0.05, steps=4, tol=1e-8,
-                          name="newmark_tet2"):
-    """Implicit Newmark run (DynamicImplicitSolver) on a small Kuhn-tet cube:
-    bottom clamped, top pressure, from rest; the stored GC/GV/GA histories and
-    the reduced consistent mass."""
-    X, el = O.tet_block(n)
+                          name="newmark_tet2", kind="C3D4"):
+    """Implicit Newmark run (DynamicImplicitSolver) on a small block of Kuhn
+    tets (or hexes): bottom clamped, top pressure, from rest; the stored
+    GC/GV/GA histories and the reduced consistent mass."""
+    X, el = O.tet_block(n) if kind == "C3D4" else O.hex_block(n)
     bottom = torch.nonzero(X[:, 2].abs() < 1e-9).flatten().numpy()
-    sets = O.boundary_faces("C3D4", el, X, 2, 1.0)
+    sets = O.boundary_faces(kind, el, X, 2, 1.0)
     surf = [(idx.numpy(), fid) for idx, fid, _ in sets]
-    c, part, (e,), (ld,) = build_reference(FEA, X, [("C3D4", el, mu, kappa, rho)], [(surf, p)], [(bottom, (0, 1, 2))])
+    c, part, (e,), (ld,) = build_reference(FEA, X, [(kind, el, mu, kappa, rho)], [(surf, p)], [(bottom, (0, 1, 2))])
     c.solver = FEA.solver.DynamicImplicitSolver(deltaT=dt, time_end=steps * dt * (1 - 1e-9), tol_error=tol)
     c.initialize()
     gc0 = torch.zeros_like(c.assembly.GC)
@@ -261,7 +261,7 @@ def case_implicit_dynamic(FEA, O, out, n=2, mu=1.0, kappa=10.0, rho=1.0, p=0.05,
         raise RuntimeError("reference implicit dynamics did not finish")
     mi, mv = c.assembly.assemble_mass_matrix(GC_now=gc0)
     ip, ix, vv = coalesced_csr(gc0, mi, mv)
-    res = dict(X=X.numpy(), elems=el.numpy(), mu=mu, kappa=kappa, rho=rho, p=p, dt=dt, steps=steps, tol=tol,
+    res = dict(X=X.numpy(), elems=el.numpy(), kind=kind, mu=mu, kappa=kappa, rho=rho, p=p, dt=dt, steps=steps, tol=tol,
                fixed=bottom, pressure_faces=torch.cat([s_._elems for s_ in ld.surface_element]).numpy(),
                face_elem=np.concatenate([i for i, _ in surf]),
                face_id=np.concatenate([np.full(len(i), f) for i, f in surf]),
@@ -276,7 +276,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", default=HERE)
-    ap.add_argument("--case", default="all", help="all, or one of: cfg1 tet3 hex5 explicit newmark")
+    ap.add_argument("--case", default="all", help="all, or one of: cfg1 tet3 hex5 explicit newmark newmark_hex")
     a = ap.parse_args()
     FEA = import_reference(a.ref)
     from oracle import fea_oracle as O  # mesh generators only
@@ -292,6 +292,8 @@ def main():
         case_explicit(FEA, O, a.out)
     if run("newmark"):
         case_implicit_dynamic(FEA, O, a.out)
+    if run("newmark_hex"):
+        case_implicit_dynamic(FEA, O, a.out, n=2, kappa=20.0, p=0.05, dt=0.05, name="newmark_hex2", kind="C3D8")
 
 
 if __name__ == "__main__":

@@ -18,17 +18,21 @@ from tests.helpers import fea_model, rel
 pytestmark = pytest.mark.gpu
 
 
+NEWMARK = ["newmark_tet2", "newmark_hex2"]
+
+
 def _newmark_model(g):
     import fea_b200 as F
     dt, steps = float(g["dt"]), int(g["steps"])
     sol = F.solver.DynamicImplicitSolver(deltaT=dt, time_end=steps * dt * (1 - 1e-9), tol_error=float(g["tol"]))
-    c, e, load = fea_model(g, "C3D4", solver=sol)
+    c, e, load = fea_model(g, str(g["kind"]), solver=sol)
     c.initialize()
     return c
 
 
-def test_consistent_mass_vs_golden(golden):
-    g = golden("newmark_tet2")
+@pytest.mark.parametrize("name", NEWMARK)
+def test_consistent_mass_vs_golden(golden, name):
+    g = golden(name)
     c = _newmark_model(g)
     idx, vals = c.assembly.assemble_mass_matrix(GC_now=None)
     n = g["GC"].shape[1]
@@ -43,8 +47,9 @@ def test_consistent_mass_vs_golden(golden):
     np.testing.assert_array_equal(c.assembly.plan.indices.cpu().numpy(), ix)
 
 
-def test_newmark_histories_vs_reference(golden):
-    g = golden("newmark_tet2")
+@pytest.mark.parametrize("name", NEWMARK)
+def test_newmark_histories_vs_reference(golden, name):
+    g = golden(name)
     c = _newmark_model(g)
     n = g["GC"].shape[1]
     z = torch.zeros(n, dtype=torch.float64, device="cuda")
@@ -61,11 +66,12 @@ def test_newmark_histories_vs_reference(golden):
     assert s.history[-1]["rmax"] < float(g["tol"])
 
 
-def test_newmark_energy_and_incremental_system(golden):
+@pytest.mark.parametrize("name", NEWMARK)
+def test_newmark_energy_and_incremental_system(golden, name):
     """The incremental system is the gradient and Hessian of the incremental
     energy: central differences of the energy along a random direction match
     R . d, and of R match K d."""
-    g = golden("newmark_tet2")
+    g = golden(name)
     c = _newmark_model(g)
     s = c.solver
     n = g["GC"].shape[1]

@@ -1,5 +1,6 @@
 """The CPU oracle against fixtures produced by running the reference itself."""
 import numpy as np
+import pytest
 import torch
 
 from oracle import fea_oracle as O
@@ -149,13 +150,17 @@ def newmark_model(g):
     X = torch.from_numpy(g["X"])
     el = torch.from_numpy(g["elems"])
     faces = torch.from_numpy(g["pressure_faces"])
-    return O.Model(X, [O.Group("C3D4", el, float(g["mu"]), float(g["kappa"]), float(g["rho"]))],
+    return O.Model(X, [O.Group(str(g["kind"]), el, float(g["mu"]), float(g["kappa"]), float(g["rho"]))],
                    [O.PressureLoad(faces, float(g["p"]))], [(g["fixed"], (0, 1, 2))])
 
 
-def test_consistent_mass(golden):
+NEWMARK = ["newmark_tet2", "newmark_hex2"]
+
+
+@pytest.mark.parametrize("name", NEWMARK)
+def test_consistent_mass(golden, name):
     """Reduced consistent mass of the reference (assembly.py:421-443), summed."""
-    g = golden("newmark_tet2")
+    g = golden(name)
     M = newmark_model(g).mass_matrix()
     M.sum_duplicates()
     M.sort_indices()
@@ -164,10 +169,11 @@ def test_consistent_mass(golden):
     assert rel(M.data, g["mass_values"]) < 1e-14
 
 
-def test_newmark_run(golden):
+@pytest.mark.parametrize("name", NEWMARK)
+def test_newmark_run(golden, name):
     """Implicit Newmark histories of the reference's DynamicImplicitSolver,
     including its initial acceleration M a0 = R(gc0)."""
-    g = golden("newmark_tet2")
+    g = golden(name)
     m = newmark_model(g)
     n = g["GC"].shape[1]
     z = torch.zeros(n, dtype=DT)
