@@ -87,6 +87,24 @@ def workload(n):
     return X, el, clamp, end, faces
 
 
+FP64_NOMINAL_TFLOPS = 37.0   # B200 FP64 (vector and tensor alike), NVIDIA's nominal figure
+
+
+def fp64_roofline(E, B, hbm_gbs, kern_ms, nn=8, ng=8):
+    """The assembly's flop side: F = E g (60 nn^2 + 108 nn + 300) FP64 flops
+    for the full element tangent in the reference's formulation (1.05e10 at
+    64^3), its rate over the volume kernels' time against the nominal FP64
+    peak, and the combined roofline max(B / BW, F / FP64) of the two bounds."""
+    F = float(E) * ng * (60 * nn * nn + 108 * nn + 300)
+    t = kern_ms * 1e-3
+    t_hbm = B / (hbm_gbs * 1e9)
+    t_fp64 = F / (FP64_NOMINAL_TFLOPS * 1e12)
+    return {"bound": "fp64", "flops": F, "achieved_tflops": F / t / 1e12, "peak_tflops": FP64_NOMINAL_TFLOPS,
+            "frac": F / t / 1e12 / FP64_NOMINAL_TFLOPS,
+            "peak_source": "nominal B200 FP64 (no measured FP64 peak on this pool)",
+            "combined_roofline_ms": 1e3 * max(t_hbm, t_fp64), "combined_frac": max(t_hbm, t_fp64) / t}
+
+
 def algorithmic_bytes(E, nn, nnz, N, n):
     """Per-assembly algorithmic bytes: connectivity, the reference's int32
     element-to-slot map, K values, coordinates + displacement, residual."""
@@ -786,6 +804,7 @@ def main():
                      "traffic": traffic, "algorithmic_bytes": B, "kernel_ms": kern_ms,
                      "kernel": "k_hex_elem + k_hex_gat (C3D8 upper block rows staged node by node, then node-row gather with transposed writes into CSR)",
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650"},
+        "roofline_fp64": fp64_roofline(E, B, hbm, kern_ms),
         "e2e": {"value": job_rate(world, E, e2e_ms), "unit": UNIT, "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": 8 * ndof, "d2h_bytes_per_step": 8 * ndof,
                 "api": "Assembly.assemble_Stiffness_Matrix",
