@@ -148,3 +148,34 @@ def test_explicit_and_adjoint_stay_in_bounds(golden, name, kind):
     for buf, m in ((ub, n), (vhb, n), (ab, n), (vb, n), (wb, wl), (dXb, 3 * N), (dmb, 1), (sb, ns)):
         assert intact(buf, m)
     assert bool(torch.isfinite(u).all()) and bool(torch.isfinite(dX).all())
+
+
+def test_batched_pcg_stays_in_bounds():
+    """Three cantilever systems in the batched PCG with their work buffers and
+    iterates as guarded views; the right-hand sides and matrices unchanged."""
+    from fea_b200 import serving, solver as S
+    reqs = serving.make_requests(3, float("inf"), seed=5, min_elems=2000, max_elems=6000)
+    eng = serving.BatchedPCG(4, 4 * max((serving.request_rows(r) // 3 + 15) // 16 + 1 for r in reqs), 8, True)
+    keep = []
+    for k, r in enumerate(reqs):
+        asm = serving.build_assembly(r)
+        R, K = asm.assemble_csr(asm.GC)
+        b = (-R).contiguous()
+        xb, x = guarded(b.numel())
+        x.zero_()
+        wl = serving.BatchedPCG.work_len(asm.plan)
+        wb, w = guarded(wl)
+        lin = S.LinearSolve(K, b, x, 1e-20, 100000, False)
+        lin.x = x
+        eng.assign(k, asm.plan, lin, w)
+        keep.append((asm, K.clone(), b.clone(), K, b, xb, x, wb, wl))
+    eng.sync()
+    for k in range(len(reqs)):
+        eng.start(k)
+    for _ in range(5):
+        eng.run_round()
+    torch.cuda.synchronize()
+    for asm, K0, b0, K, b, xb, x, wb, wl in keep:
+        assert intact(xb, x.numel()) and intact(wb, wl)
+        assert torch.equal(K, K0) and torch.equal(b, b0)
+        assert bool(torch.isfinite(x).all())
