@@ -609,9 +609,10 @@ def run_serving(a):
                 r.arrival = 0.0
 
         def summary(res, wall):
-            lat = np.array([r.latency for r in res])
+            ok = [r for r in res if r.error is None]
+            lat = np.array([r.latency for r in ok])
             span = max(r.done for r in res) - min(r.arrival for r in res)
-            return {"solves_per_s": len(res) / span, "p50_s": float(np.percentile(lat, 50)),
+            return {"solves_per_s": len(ok) / span, "rejected": len(res) - len(ok), "p50_s": float(np.percentile(lat, 50)),
                     "p99_s": float(np.percentile(lat, 99)), "makespan_s": span, "wall_s": wall,
                     "newton_iters": int(sum(r.newton_iters for r in res)), "pcg_iters": int(sum(r.pcg_iters for r in res))}
         # warm-up: one small request through both paths
@@ -629,7 +630,8 @@ def run_serving(a):
             rec["plain"] = summary(plain, time.perf_counter() - t0)
             rec["speedup_solves_per_s"] = rec["served"]["solves_per_s"] / rec["plain"]["solves_per_s"]
             rec["max_rel_diff_served_vs_plain"] = max(float((x.gc - y.gc).norm() / y.gc.norm())
-                                                      for x, y in zip(served, plain))
+                                                      for x, y in zip(served, plain)
+                                                      if x.gc is not None and y.gc is not None)
         out.append(rec)
     line = {"metric": "served static solves/s (C3D4 cantilevers, Newton to 1e-8)", "unit": "solves/s",
             "value": out[0]["served"]["solves_per_s"], "higher_is_better": True, "workload": "serving",

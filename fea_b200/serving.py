@@ -136,12 +136,13 @@ def estimate_bytes(req: BeamRequest):
 @dataclasses.dataclass
 class Result:
     rid: int
-    gc: torch.Tensor
+    gc: torch.Tensor         # None for a rejected request
     newton_iters: int
     pcg_iters: int
     arrival: float
     admitted: float
     done: float
+    error: str = None        # why the request was rejected (its solve failed)
 
     @property
     def latency(self):
@@ -159,15 +160,19 @@ def solve_plain(requests, clock=None, keep=True):
         if now < req.arrival:
             time.sleep(req.arrival - now)
         start = time.perf_counter() - t0
-        asm = build_assembly(req)
-        sol = make_solver(asm)
-        gc = sol.solve(GC0=asm.GC.clone())
-        if isinstance(gc, bool):
-            raise RuntimeError("request %d did not converge" % req.rid)
+        asm = sol = gc = None
+        try:
+            asm = build_assembly(req)
+            sol = make_solver(asm)
+            gc = sol.solve(GC0=asm.GC.clone())
+            err = "Newton did not converge" if isinstance(gc, bool) else None
+        except Exception as ex:              # the request is rejected; the others go on
+            err = "%s: %s" % (type(ex).__name__, ex)
         torch.cuda.synchronize()
         done = time.perf_counter() - t0
-        out.append(Result(req.rid, gc.cpu() if keep else None, len(sol.history),
-                          sum(h.get("pcg_iters", 0) for h in sol.history), req.arrival, start, done))
+        hist = sol.history if sol is not None else []
+        out.append(Result(req.rid, gc.cpu() if (keep and err is None) else None, len(hist),
+                          sum(h.get("pcg_iters", 0) for h in hist), req.arrival, start, done, err))
         del asm, sol, gc
     return sorted(out, key=lambda r: r.rid)
 
@@ -315,14 +320,16 @@ def serve(requests, max_slots=48, round_iters=32, mem_budget=32 << 30, use_graph
     work_stream = torch.cuda.Stream()
     main = torch.cuda.current_stream()
 
-    def finish(job, value):
+    def finish(job, value, error=None):
+        """Record the job's result (value: GC, or False when Newton failed)."""
         nonlocal mem_used
-        if isinstance(value, bool):
-            raise RuntimeError("request %d did not converge" % job.req.rid)
+        if error is None and isinstance(value, bool):
+            error = "Newton did not converge"
         work_stream.synchronize()
-        results[job.req.rid] = Result(job.req.rid, value.cpu() if keep else None, len(job.solver.history),
+        results[job.req.rid] = Result(job.req.rid, value.cpu() if (keep and error is None) else None,
+                                      len(job.solver.history),
                                       sum(h.get("pcg_iters", 0) for h in job.solver.history), job.req.arrival,
-                                      job.admitted, time.perf_counter() - t0)
+                                      job.admitted, time.perf_counter() - t0, error)
         mem_used -= job.bytes
 
     timing = {"newton_host_s": 0.0, "wait_s": 0.0, "prep_s": 0.0}
@@ -333,6 +340,9 @@ def serve(requests, max_slots=48, round_iters=32, mem_budget=32 << 30, use_graph
         t_a = time.perf_counter()
         try:
             return _advance(job, first)
+        except Exception as ex:              # a failing request is rejected; the others go on
+            finish(job, False, "%s: %s" % (type(ex).__name__, ex))
+            return False
         finally:
             timing["newton_host_s"] += time.perf_counter() - t_a
 
@@ -367,7 +377,13 @@ def serve(requests, max_slots=48, round_iters=32, mem_budget=32 << 30, use_graph
         for fut in [f for f in preparing if f.done()]:
             req, st_, nb, adm = preparing.pop(fut)
             free_streams.append(st_)
-            asm, sol = fut.result()
+            try:
+                asm, sol = fut.result()
+            except Exception as ex:          # the model could not be built: rejected
+                results[req.rid] = Result(req.rid, None, 0, 0, req.arrival, adm, time.perf_counter() - t0,
+                                          "%s: %s" % (type(ex).__name__, ex))
+                mem_used -= nb
+                continue
             with torch.cuda.stream(work_stream):
                 ready.append(_Job(req, asm, sol, adm, nb))
         # host work of the jobs that left the batch, overlapping the round in flight
