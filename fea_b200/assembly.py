@@ -18,6 +18,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
+from ._trace import nvtx
 from .boundarys import Boundary_Condition
 from .loads import Pressure
 from .part import Instance, Part
@@ -236,6 +237,10 @@ class Assembly:
     # -- assembly ------------------------------------------------------------------
     def assemble_csr(self, GC, want_K=True, K=None, R=None):
         """Reduced residual R [n] and K values [nnz] in the plan's CSR order."""
+        with nvtx("fea.assemble_csr" if want_K else "fea.assemble_force"):
+            return self._assemble_csr(GC, want_K, K, R)
+
+    def _assemble_csr(self, GC, want_K, K, R):
         P = self.plan
         gc = self._gc(GC=GC)
         R = P.zeros(P.ndof) if R is None else R

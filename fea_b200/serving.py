@@ -36,6 +36,7 @@ import numpy as np
 import torch
 
 from . import _lib as L
+from ._trace import nvtx
 from .plan import stream, vptr
 
 
@@ -253,11 +254,12 @@ class BatchedPCG:
                 "fea_pcgb_iterate")
 
     def run_round(self):
-        self.sync()
-        if self.graph is not None:
-            self.graph.replay()
-        else:
-            self._iterate()
+        with nvtx("fea.pcgb_round"):
+            self.sync()
+            if self.graph is not None:
+                self.graph.replay()
+            else:
+                self._iterate()
         self.rounds += 1
 
     def poll(self):

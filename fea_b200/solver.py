@@ -27,6 +27,7 @@ import time
 import torch
 
 from . import _lib as L
+from ._trace import nvtx
 
 
 class LinearSolve:
@@ -227,6 +228,10 @@ class StaticImplicitSolver(BaseSolver):
         return LinearSolve(K_values, R.contiguous(), x, tol, cap, tight)
 
     def _run_linear(self, req):
+        with nvtx("fea.pcg"):
+            self._run_linear_inner(req)
+
+    def _run_linear_inner(self, req):
         P = self.assembly.plan
         if self.precision == "mixed":
             v32 = P.to_f32(req.K)
@@ -365,7 +370,9 @@ class DynamicImplicitSolver(StaticImplicitSolver):
         while True:
             dt = self._deltaT
             GC_pre = self._GC_list[-1] + dt * self._GV_list[-1] + 0.25 * dt ** 2 * self._GA_list[-1]
-            GC_now = self._solve_iteration(GC0=self._GC_list[-1], GC_pre=GC_pre, deltaT=dt, tol_error=self.tol_error)
+            with nvtx("fea.newmark_step"):
+                GC_now = self._solve_iteration(GC0=self._GC_list[-1], GC_pre=GC_pre, deltaT=dt,
+                                               tol_error=self.tol_error)
             if isinstance(GC_now, bool):
                 raise RuntimeError("Newton iteration of time step %d did not converge" % (step + 1))
             GV, GA = self.get_next_velocity(GC_now, self._GC_list[-1], self._GV_list[-1], self._GA_list[-1], dt)

@@ -365,3 +365,20 @@ def test_upper_staging_emulated_gives_reference_K(dofs):
     np.testing.assert_array_equal(hp.array(L.FEA_A_INDPTR), ip.numpy())
     np.testing.assert_allclose(K, vref.numpy(), rtol=0, atol=1e-13 * np.abs(vref.numpy()).max())
     np.testing.assert_allclose(R, Rref.numpy(), rtol=0, atol=1e-13 * np.abs(Rref.numpy()).max())
+
+
+def test_nvtx_ranges_are_opt_in():
+    """FEA_B200_NVTX=1 turns the host-side NVTX ranges on; unset, they cost
+    nothing and push nothing."""
+    import subprocess
+    import sys
+    code = ("import fea_b200._trace as t\n"
+            "with t.nvtx('fea.test'):\n"
+            "    pass\n"
+            "print(int(t.ENABLED))\n")
+    env = dict(os.environ, FEA_B200_NVTX="1")
+    on = subprocess.run([sys.executable, "-c", code], env=env, cwd=ROOT, capture_output=True, text=True)
+    env.pop("FEA_B200_NVTX")
+    off = subprocess.run([sys.executable, "-c", code], env=env, cwd=ROOT, capture_output=True, text=True)
+    assert on.returncode == 0 and on.stdout.strip() == "1"
+    assert off.returncode == 0 and off.stdout.strip() == "0"

@@ -382,3 +382,26 @@ def test_hex_element_residual_stays_in_bounds(golden):
         assert bool((buf[n:] == -7.0).all())
         assert rel(buf[:n], g["elem_R"]) < TOL
         assert rel(K, g["elem_K_values"]) < TOL
+
+
+def test_nvtx_ranges_do_not_change_results(golden):
+    """The optional NVTX ranges wrap host calls only: the assembly and PCG
+    give the same bits with them on."""
+    import fea_b200._trace as T
+    g = golden("hex5")
+    c, e, _ = fea_model(g, "C3D8")
+    c.initialize()
+    asm = c.assembly
+    st = torch.from_numpy(g["state"]).cuda()
+    R0, K0 = asm.assemble_csr(st)
+    x0 = torch.zeros_like(R0)
+    asm.plan.pcg(K0, -R0, x0, 1e-20, 3000)
+    old = T.ENABLED
+    T.ENABLED = True
+    try:
+        R1, K1 = asm.assemble_csr(st)
+        x1 = torch.zeros_like(R1)
+        asm.plan.pcg(K1, -R1, x1, 1e-20, 3000)
+    finally:
+        T.ENABLED = old
+    assert torch.equal(R0, R1) and torch.equal(K0, K1) and torch.equal(x0, x1)
