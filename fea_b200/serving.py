@@ -370,6 +370,11 @@ def serve(requests, max_slots=48, round_iters=32, mem_budget=32 << 30, use_graph
         # admit arrived requests into preparation while memory allows
         while waiting and waiting[0].arrival <= now and free_streams:
             nb = estimate_bytes(waiting[0])
+            if nb > mem_budget:               # could never be admitted: rejected at admission
+                req = waiting.pop(0)
+                results[req.rid] = Result(req.rid, None, 0, 0, req.arrival, now, time.perf_counter() - t0,
+                                          "needs %d bytes, more than the memory budget %d" % (nb, mem_budget))
+                continue
             if mem_used + nb > mem_budget and (preparing or ready or queue_slot or any(slots)):
                 break
             req = waiting.pop(0)

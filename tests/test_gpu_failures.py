@@ -91,3 +91,18 @@ def test_serving_rejects_a_poisoned_request_and_keeps_the_others():
     plain = serving.solve_plain(reqs)
     assert plain[2].error is not None and all(p.error is None for p in plain if p.rid != 2)
     assert all(math.isfinite(p.latency) for p in plain)
+
+
+def test_serving_rejects_a_request_beyond_the_memory_budget():
+    from fea_b200 import serving
+    reqs = serving.make_requests(3, float("inf"), seed=12, min_elems=2000, max_elems=4000)
+    for r in reqs:
+        r.arrival = 0.0
+    reqs[1].n_elems = 40000
+    budget = max(serving.estimate_bytes(r) for r in (reqs[0], reqs[2])) * 2
+    assert serving.estimate_bytes(reqs[1]) > budget
+    res, _ = serving.serve(reqs, max_slots=4, round_iters=16, mem_budget=budget)
+    assert res[1].error is not None and "memory budget" in res[1].error and res[1].gc is None
+    assert res[0].error is None and res[2].error is None
+    alone, _ = serving.serve([reqs[0], reqs[2]], max_slots=4, round_iters=16)
+    assert torch.equal(alone[0].gc, res[0].gc) and torch.equal(alone[1].gc, res[2].gc)
