@@ -903,7 +903,9 @@ static int64_t pcgb_items_s(int64_t n, int64_t n_nodes) {
 }
 static int64_t pcgb_items_u(int64_t n) { return (n + PCGB_ROWS - 1) / PCGB_ROWS; }
 
-// As pcgb_warp_last, for a warp that finished `add` items of the slot at once.
+// A warp that finished `add` items of a slot counts them in the slot's
+// completion counter (after a fence that publishes its partial sums) and
+// learns whether it completed the slot's last items.
 __device__ __forceinline__ bool pcgb_warp_last_n(unsigned* counter, unsigned add, int total, int lane) {
   unsigned old = 0u;
   if (lane == 0) {
@@ -914,15 +916,6 @@ __device__ __forceinline__ bool pcgb_warp_last_n(unsigned* counter, unsigned add
   return old + add == (unsigned)total;
 }
 
-__device__ __forceinline__ bool pcgb_warp_last(unsigned* counter, int total, int lane) {
-  unsigned old = 0u;
-  if (lane == 0) {
-    __threadfence();
-    old = atomicAdd(counter, 1u);
-  }
-  old = __shfl_sync(0xffffffffu, old, 0);
-  return old == (unsigned)(total - 1);
-}
 
 __device__ __forceinline__ double pcgb_warp_sum(const double* part, int n, int stride, int off, int lane) {
   // 8 independent L2 loads per lane in flight per batch, fixed order
