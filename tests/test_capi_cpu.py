@@ -301,15 +301,19 @@ def test_csr_of_eight_hex_mesh_by_hand(clamp):
     np.testing.assert_array_equal(oix.numpy(), ix)
 
 
-@pytest.mark.parametrize("dofs", [(0, 1, 2), (1,)])
-def test_upper_staging_emulated_gives_reference_K(dofs):
+@pytest.mark.parametrize("dofs,collapse", [((0, 1, 2), False), ((1,), False), ((0, 1, 2), True)])
+def test_upper_staging_emulated_gives_reference_K(dofs, collapse):
     """The C3D8 assembly as the kernels perform it, emulated on the CPU with
     the oracle's element blocks: upper records written per incidence, then
     per node the upper block sums into the node's rows and their transposes
     into the column nodes' rows.  The CSR values equal the oracle's reduced K
-    and R."""
+    and R; also with a collapsed element (two of its corners one node), whose
+    repeated node puts two blocks of the element on the diagonal."""
     from fea_b200 import _lib as L
     X, el = O.hex_block(3, jitter=0.1, seed=5)
+    if collapse:
+        el = el.clone()
+        el[13, 6] = el[13, 7]                   # the centre element's top edge 6-7 collapsed
     fixed = torch.nonzero(X[:, 0] < 1e-9).flatten().numpy()
     m = O.Model(X, [O.Group("C3D8", el, 1.0, 10.0)], [], [(fixed, dofs)])
     nfree = int(m.free_mask().sum())
