@@ -405,3 +405,32 @@ def test_nvtx_ranges_do_not_change_results(golden):
     finally:
         T.ENABLED = old
     assert torch.equal(R0, R1) and torch.equal(K0, K1) and torch.equal(x0, x1)
+
+
+def test_collapsed_c3d8_element_matches_oracle():
+    """A C3D8 element with two corners on one node (its top edge collapsed):
+    the element kernel stages both blocks the repeated node puts on the
+    diagonal, and R, K equal the oracle's."""
+    import fea_b200 as F
+    X, el = O.hex_block(3, jitter=0.1, seed=5)
+    el = el.clone()
+    el[13, 6] = el[13, 7]
+    fixed = torch.nonzero(X[:, 0] < 1e-9).flatten().numpy()
+    m = O.Model(X, [O.Group("C3D8", el, 1.0, 10.0)], [], [(fixed, (0, 1, 2))])
+    nfree = int(m.free_mask().sum())
+    gc = 0.01 * torch.randn(nfree, generator=torch.Generator().manual_seed(2), dtype=torch.float64)
+    Rref, (ip, ix, vref) = m.assemble(gc)
+    part = F.Part(X)
+    e = F.elements.C3D8(elems=el, elems_index=torch.arange(el.shape[0]), part=part)
+    e.set_materials(F.materials.NeoHookean(1.0, 10.0))
+    part.add_element(e)
+    part.set_nodes["fix"] = fixed
+    asm = F.Assembly()
+    asm.add_part(part, "p")
+    asm.add_instance(F.Instance(part), "p")
+    asm.add_boundary(F.boundarys.Boundary_Condition(instance_name="p", set_nodes_name="fix"), "bc")
+    asm.initialize()
+    R, K = asm.assemble_csr(gc.cuda())
+    np.testing.assert_array_equal(asm.plan.indptr.cpu().numpy(), ip.numpy())
+    assert rel(R, Rref) < TOL
+    assert rel(K, vref) < TOL
