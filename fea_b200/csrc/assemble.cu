@@ -1158,23 +1158,30 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
                                    double* work, int64_t work_len, cudaStream_t st) {
   if (!N || !G || !gc || (G->kind != FEA_C3D4 && G->kind != FEA_C3D8)) return FEA_EINVAL;
   if (G->nn != (G->kind == FEA_C3D8 ? 8 : 4)) return FEA_EINVAL;
+  const bool hex = G->kind == FEA_C3D8;
+  const int tpb = hex ? HX_GINC : VolTPB<4>::v;
+  if (G->threads != tpb) return FEA_ECHUNK;
+  // every argument check comes before the first device call
+  if (K && hex) {
+    if (!work || work_len < fea_assemble_work_len(G)) return FEA_EWORK;
+    if (((uintptr_t)work & 15) != 0) return FEA_EINVAL;
+    if (!G->incpos_dev || !G->recbase_dev || !G->nodeblk_dev || !G->blkptr_dev || !G->blkcon_dev ||
+        !N->adjptr_dev || !N->adjcol_dev || !N->adjoff_dev || !N->moff_dev || G->nblk < 0 || G->maxblk < 0)
+      return FEA_EINVAL;
+  }
+  if (!K) {
+    if (!R && !elemR) return FEA_OK;
+    if (!R) return FEA_EINVAL;  // the residual-only path writes R
+  }
   if (int r = ensure_tables()) return r;
   VolParams P = vol_params(N, G, mu, kappa, gc);
   P.K = K;
   P.R = R;
   P.elemR = elemR;
-  const bool hex = G->kind == FEA_C3D8;
-  const int tpb = hex ? HX_GINC : VolTPB<4>::v;
-  if (G->threads != tpb) return FEA_ECHUNK;
   if (K) {
     int64_t smem = G->smem_doubles;
     const bool acc = accumulate != 0, wr = R != nullptr, er = elemR != nullptr;
     if (hex) {
-      if (!work || work_len < fea_assemble_work_len(G)) return FEA_EWORK;
-      if (((uintptr_t)work & 15) != 0) return FEA_EINVAL;
-      if (!G->incpos_dev || !G->recbase_dev || !G->nodeblk_dev || !G->blkptr_dev || !G->blkcon_dev ||
-          !N->adjptr_dev || !N->adjcol_dev || !N->adjoff_dev || !N->moff_dev || G->nblk < 0 || G->maxblk < 0)
-        return FEA_EINVAL;
       const int capb = std::max<int>(G->maxblk, 1);
       const size_t gbytes = (size_t)HX_GW * capb * 9 * sizeof(double);
       if (gbytes > (size_t)smem_limit()) return FEA_ESMEM;
@@ -1207,10 +1214,6 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
 #undef FEA_RK
     return FEA_EINVAL;
   }
-  if (!R && !elemR) return FEA_OK;
-  double* Rtmp = R;
-  if (!R) return FEA_EINVAL;  // the residual-only path writes R
-  P.R = Rtmp;
   const int grid = grid_for(N->n_nodes, 128);
   if (N->n_nodes == 0) return FEA_OK;
   if (hex) {
@@ -1255,8 +1258,8 @@ extern "C" int fea_assemble_pressure(const fea_nodes_t* N, const fea_group_t* G,
                                      const double* gc, double* K, double* R, cudaStream_t st) {
   if (!N || !G || !Xi || !gc || (G->kind != FEA_T3 && G->kind != FEA_Q4)) return FEA_EINVAL;
   if (G->nn != (G->kind == FEA_T3 ? 3 : 4) || G->threads != 128) return FEA_EINVAL;
-  if (int r = ensure_tables()) return r;
   if (!K && !R) return FEA_OK;
+  if (int r = ensure_tables()) return r;
   FaceParams P = face_params(N, G, p, Xi, gc);
   P.K = K;
   P.R = R;

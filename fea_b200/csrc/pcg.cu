@@ -1232,7 +1232,11 @@ __device__ __forceinline__ double pcgb_row_ax(const PcgbSlotDev& S, int64_t row,
 template <int LANES>
 __global__ void __launch_bounds__(PCG_TPB) k_pcgb_start(PcgbView V, int32_t slot) {
   __shared__ double sh[PCG_WARPS];
+  static_assert(PCGB_ROWS == PCG_TPB, "the second phase takes one thread per row of the chunk");
   const PcgbSlotDev& S = V.slots[slot];
+  // the grid comes from the caller's row count: chunks beyond the slot's own
+  // (whose partials would land past its work buffer) leave at once
+  if ((int64_t)blockIdx.x >= (int64_t)S.nchunk0) return;
   constexpr int RPP = PCG_TPB / LANES;
   const int lane = threadIdx.x % LANES, sub = threadIdx.x / LANES;
   const int64_t row0 = (int64_t)blockIdx.x * PCGB_ROWS;
@@ -1443,10 +1447,14 @@ extern "C" int fea_pcgb_set(void* table, int32_t max_slots, int64_t max_items, i
       for (int32_t c = 0; c < d.nitem_s; ++c) { ss.push_back(k); sl.push_back(c); }
       for (int32_t c = 0; c < d.nitem_u; ++c) { us.push_back(k); ul.push_back(c); }
     }
-    // completion counters are zero between kernels; a new work buffer starts so
-    if (cudaError_t e = cudaMemsetAsync(d.counter, 0, 4 * sizeof(unsigned), s)) return (int)e;
   }
   if ((int64_t)ss.size() > max_items || (int64_t)us.size() > max_items) return FEA_ERANGE;
+  // all slots checked: a rejected call has touched no device memory
+  for (int32_t k = 0; k < nslots; ++k) {
+    // completion counters are zero between kernels; a new work buffer starts so
+    if (dev[k].counter)
+      if (cudaError_t e = cudaMemsetAsync(dev[k].counter, 0, 4 * sizeof(unsigned), s)) return (int)e;
+  }
   PcgbView V = pcgb_view(table, max_slots, max_items);
   PcgbHeader hdr{(int64_t)ss.size(), (int64_t)us.size(), (int64_t)nslots};
   if (cudaError_t e = cudaMemcpyAsync(V.hdr, &hdr, sizeof(hdr), cudaMemcpyHostToDevice, s)) return (int)e;

@@ -331,9 +331,12 @@ int fea_pcg_solve_mixed_nodes(const fea_nodes_t* nodes, const int32_t* indices_d
  *     max_items bounds the items of all active slots in each list.
  *   fea_pcgb_set: loads the slot table (host array of nslots descriptors;
  *     work == NULL marks an empty slot) and the item lists of the active
- *     slots; synchronises `stream`.
+ *     slots; synchronises `stream`.  Every descriptor is checked before
+ *     the first device call: a call that returns FEA_EINVAL, FEA_EWORK or
+ *     FEA_ERANGE has changed neither the table nor any work buffer.
  *   fea_pcgb_start: initial residual, Jacobi scaling and state of one slot
- *     (x holds the initial guess).
+ *     (x holds the initial guess).  n and nnz are the slot's own (they size
+ *     the launch; chunks beyond the slot's rows exit without writing).
  *   fea_pcgb_iterate: `iters` iterations of every active, unfinished slot;
  *     a fixed launch sequence that reads the table from device memory, so it
  *     can be captured once and replayed while slots come and go.
