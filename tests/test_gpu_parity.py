@@ -181,10 +181,12 @@ def test_assembly_deterministic_and_symmetric(golden):
     assert float((A - A.T).abs().max()) <= 1e-12 * float(A.abs().max())
 
 
-def test_tangent_is_derivative_of_residual(golden):
-    """Central differences of R along a random direction reproduce K d."""
-    g = golden("tet3")
-    c, e, _ = fea_model(g, "C3D4")
+@pytest.mark.parametrize("name,kind", [("tet3", "C3D4"), ("hex5", "C3D8")])
+def test_tangent_is_derivative_of_residual(golden, name, kind):
+    """Central differences of R along a random direction reproduce K d
+    (follower pressure included)."""
+    g = golden(name)
+    c, e, _ = fea_model(g, kind)
     c.initialize()
     A = c.assembly
     x = torch.from_numpy(g["state"]).cuda()

@@ -1,7 +1,8 @@
 """Known-answer checks of the oracle itself (CPU): rigid rotation, the
 closed-form uniaxial Neo-Hookean stress, the patch test on a jittered C3D8
-block, and the lumped mass total rho * volume.  The same checks run through
-the CUDA path in test_gpu_parity.py."""
+block, the lumped mass total rho * volume, and R and K as central
+differences of the energy and of R.  The same checks run through the CUDA
+path in test_gpu_parity.py."""
 import numpy as np
 import pytest
 import torch
@@ -88,3 +89,36 @@ def test_lumped_mass_totals_rho_volume(kind):
     assert abs(vol - 1.0) < 0.05
     for d in range(3):
         assert abs(float(mass[:, d].sum()) - rho * vol) < 1e-12 * rho * vol
+
+
+@pytest.mark.parametrize("kind", ["C3D8", "C3D4"])
+def test_residual_and_tangent_are_derivatives(kind):
+    """At a finite-strain state, the central difference (h = 1e-6) of the
+    energy along a random direction d equals R . d, and that of R equals K d."""
+    m = _block(kind, 2, jitter=0.1 if kind == "C3D8" else 0.0)
+    g = torch.Generator().manual_seed(3)
+    u = 0.05 * torch.randn(m.X.shape, generator=g, dtype=torch.float64).reshape(-1)
+    d = torch.randn(u.shape, generator=g, dtype=torch.float64)
+    R, (ip, ix, v) = m.assemble(u)
+    h = 1e-6
+    dE = float(m.energy(u + h * d) - m.energy(u - h * d)) / (2 * h)
+    assert abs(dE - float((R * d).sum())) < 1e-8 * abs(dE)
+    Kd = O.csr_matvec(ip, ix, v, d)
+    fd = (m.assemble(u + h * d, want_K=False)[0] - m.assemble(u - h * d, want_K=False)[0]) / (2 * h)
+    assert float((fd - Kd).norm()) < 1e-8 * float(Kd.norm())
+
+
+@pytest.mark.parametrize("name,kind", [("tet3", "C3D4"), ("hex5", "C3D8")])
+def test_tangent_with_follower_pressure_is_derivative(golden, name, kind):
+    """The same check on the committed fixtures, whose follower pressure adds
+    its own, unsymmetric, part to R and K."""
+    from tests.helpers import oracle_model
+    g = golden(name)
+    m = oracle_model(g, kind)
+    x = torch.from_numpy(g["state"])
+    d = torch.randn(x.shape, generator=torch.Generator().manual_seed(5), dtype=torch.float64)
+    _, (ip, ix, v) = m.assemble(x)
+    Kd = O.csr_matvec(ip, ix, v, d)
+    h = 1e-6
+    fd = (m.assemble(x + h * d, want_K=False)[0] - m.assemble(x - h * d, want_K=False)[0]) / (2 * h)
+    assert float((fd - Kd).norm()) < 1e-8 * float(Kd.norm())
