@@ -212,6 +212,64 @@ def cpu_baseline(n, seconds):
                       "%d reps in %.1f s" % (len(keep), slab, n, n, reps, reps * dt)}
 
 
+def _timed_difference(run, seconds, cap):
+    """Time `run(k)`, which returns (seconds, units done), at k = 1 and
+    k = 1 + m, m sized from the first call so that the second takes about
+    `seconds`: per-unit time with the set-up of each call cancelled (after
+    one untimed call that warms the thread pool and caches).  Returns
+    (seconds per unit, units timed, seconds of the long call)."""
+    run(1)
+    t1, u1 = run(1)
+    m = max(2, min(cap, int(seconds / max(t1 / 2, 1e-6))))
+    t2, u2 = run(1 + m)
+    return max(t2 - t1, 1e-9) / max(u2 - u1, 1), u2 - u1, t2
+
+
+def cpu_cg_iteration(indptr, indices, values, b, seconds):
+    """Oracle port of the reference's conjugate_gradient on the same reduced
+    system, on the host cores: time per iteration."""
+    import torch
+    from oracle import fea_oracle as O
+    torch.set_num_threads(os.cpu_count() or 1)
+    ip, ix, v, bb = indptr.cpu(), indices.cpu().to(torch.int64), values.cpu(), b.cpu()
+
+    def run(k):
+        # the stop test only ends a run whose residual would otherwise reach
+        # denormal values, which are slow on the host and not the reference's cost
+        t = time.perf_counter()
+        _, it = O.conjugate_gradient(ip, ix, v, bb, tol=1e-30, max_iter=k)
+        return time.perf_counter() - t, it
+
+    per, m, total = _timed_difference(run, seconds, 2000)
+    return {"value": per * 1e3, "unit": "ms per CG iteration", "cores": torch.get_num_threads(), "kind": "port",
+            "sample": "%d iterations of the reference's CG (CSR SpMV + vector updates) on the same %d-row, "
+                      "%d-nonzero system, minus a 1-iteration call; %.1f s" % (m, bb.shape[0], v.shape[0], total)}
+
+
+def cpu_explicit_step(X, el, dt, seconds):
+    """Oracle port of the reference's central-difference loop (lumped mass,
+    residual-only element pass with the residual index precomputed) on the
+    same mesh, on the host cores: time per step."""
+    import torch
+    from oracle import fea_oracle as O
+    torch.set_num_threads(os.cpu_count() or 1)
+    m = O.Model(torch.from_numpy(np.asarray(X)), [O.Group("C3D4", torch.from_numpy(np.asarray(el)), 1.0, 10.0, 1.0)],
+                [], [])
+    n = int(m.free_mask().sum())
+    gc0 = torch.zeros(n, dtype=torch.float64)
+    gv0 = 0.01 * torch.randn(n, generator=torch.Generator().manual_seed(0), dtype=torch.float64)
+
+    def run(k):
+        t = time.perf_counter()
+        O.explicit_run(m, gc0, gv0, dt, k)
+        return time.perf_counter() - t, k
+
+    per, steps, total = _timed_difference(run, seconds, 50)
+    return {"value": 1.0 / per, "unit": "steps/s", "cores": torch.get_num_threads(), "kind": "port",
+            "sample": "%d steps of the reference's loop on the same %d-element mesh, minus a 1-step run "
+                      "(lumped mass and first force pass cancel); %.1f s" % (steps, len(el), total)}
+
+
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -300,6 +358,8 @@ def run_pcg(a):
             "achieved_GBs": {"fp64": bytes64 / (out["fp64"]["ms_per_iter"] * 1e-3) / 1e9,
                              "fp64_csr": bytes64_csr / (out["fp64_csr"]["ms_per_iter"] * 1e-3) / 1e9,
                              "mixed": bytes32 / (out["mixed"]["ms_per_iter"] * 1e-3) / 1e9}}
+    if not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_cg_iteration(P.indptr, P.indices, K, b, a.cpu_seconds)
     print(json.dumps(line), flush=True)
 
 
@@ -371,6 +431,8 @@ def run_explicit(a):
             "elements": E, "nodes": N, "steps": a.explicit_steps, "dt": dt, "fp64": res["fp64"],
             "fp32": res["fp32"], "fp32_vs_fp64_disp_rel": du,
             "elements_per_s": E * 1e3 / res["fp64"]["ms_per_step"]}
+    if not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_explicit_step(X, el, dt, a.cpu_seconds)
     print(json.dumps(line), flush=True)
 
 

@@ -166,8 +166,16 @@ def element_pattern(elems: torch.Tensor):
     key = (row * S + col).reshape(-1)
     uniq, inverse = torch.unique(key, sorted=True, return_inverse=True)
     idx = torch.stack([uniq // S, uniq % S])
-    force = (3 * el[:, None, :] + j3[None, :, None]).reshape(-1)
-    return idx, inverse, force
+    return idx, inverse, element_force_index(elems)
+
+
+def element_force_index(elems: torch.Tensor):
+    """The residual index 3 n_a + j in (a, j, e) order alone: what
+    structural_Force(if_onlyforce=True) scatters with (C3base.py:413-426),
+    precomputed by Element_3D.initialize (C3base.py:109-153)."""
+    el = elems.to(torch.int64).T                         # [nn,E]
+    j3 = torch.arange(3, dtype=torch.int64)
+    return (3 * el[:, None, :] + j3[None, :, None]).reshape(-1)
 
 
 # ---------------------------------------------------------------------------
@@ -333,19 +341,24 @@ class Model:
 
     def __post_init__(self):
         self.X = self.X.to(DT)
+        self._free = None
 
     # DOF bookkeeping: assembly.py:157-183 and boundary_condition.py:35-41
     def free_mask(self):
-        N = self.X.shape[0]
-        m = torch.zeros(N, 3, dtype=torch.bool)
-        for g in self.groups:
-            m[torch.unique(g.elems)] = True
-        for pl in self.pressures:
-            m[torch.unique(pl.faces)] = True
-        for nodes, dofs in self.fixed:
-            for d in dofs:
-                m[torch.as_tensor(nodes, dtype=torch.int64), d] = False
-        return m.reshape(-1)
+        """Free DOFs in RGC order; computed once, like the reference's
+        reduction mask (the model is not changed after construction)."""
+        if self._free is None:
+            N = self.X.shape[0]
+            m = torch.zeros(N, 3, dtype=torch.bool)
+            for g in self.groups:
+                m[torch.unique(g.elems)] = True
+            for pl in self.pressures:
+                m[torch.unique(pl.faces)] = True
+            for nodes, dofs in self.fixed:
+                for d in dofs:
+                    m[torch.as_tensor(nodes, dtype=torch.int64), d] = False
+            self._free = m.reshape(-1)
+        return self._free.clone()
 
     def initial_gc(self):
         """GC0 with the 1e-5 seed on the last node (assembly.py:113)."""
@@ -378,7 +391,10 @@ class Model:
         rows, cols, vals = [], [], []
         for g in self.groups:
             Re, Ke = element_residual_tangent(g.kind, self.X, g.elems, u, g.mu, g.kappa, want_K)
-            idx, slot, force = element_pattern(g.elems)
+            if want_K:
+                idx, slot, force = element_pattern(g.elems)
+            else:
+                force = element_force_index(g.elems)
             R0.scatter_add_(0, force, Re.reshape(-1))
             if want_K:
                 v = torch.zeros(idx.shape[1], dtype=DT).scatter_add_(0, slot, Ke.reshape(-1))
