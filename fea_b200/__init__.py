@@ -12,6 +12,7 @@ from .assembly import Assembly
 from .controller import FEAController
 from . import solver
 from .plan import DevicePlan
+from .inp import FEA_INP, from_inp
 
 __all__ = ["Part", "Instance", "Assembly", "FEAController", "materials", "elements", "loads", "boundarys",
-           "solver", "DevicePlan"]
+           "solver", "DevicePlan", "FEA_INP", "from_inp"]

@@ -272,11 +272,65 @@ def case_implicit_dynamic(FEA, O, out, n=2, mu=1.0, kappa=10.0, rho=1.0, p=0.05,
     print(name, "E", el.shape[0], "n", gc0.shape[0], "steps", steps, "max|GC|", float(res["GC"][-1].__abs__().max()))
 
 
+def case_inp(FEA, out):
+    """The reference's FEA_INP.read_inp and from_inp on the sample INP files
+    of inp_samples.py: what it parses (nodes, element arrays, sets, surfaces,
+    sections, the element material table, materials, instances) and the
+    model it builds (per element group: type, labels, connectivity, mu,
+    kappa, density; per part: node sets)."""
+    import inp_samples
+    for name, path in inp_samples.write_samples(out).items():
+        inp = FEA.FEA_INP()
+        inp.read_inp(path)
+        d = {}
+        for pn, p in inp.part.items():
+            d["nodes:%s" % pn] = p.nodes.numpy()
+            d["elemtypes:%s" % pn] = np.array(list(p.elems.keys()))
+            for t, e in p.elems.items():
+                d["elems:%s:%s" % (pn, t)] = np.asarray(e, dtype=np.int64)
+            for sn, m in p.sets_nodes.items():
+                d["nset:%s:%s" % (pn, sn)] = np.array(sorted(m), dtype=np.int64)
+            for sn, m in p.sets_elems.items():
+                d["elset:%s:%s" % (pn, sn)] = np.array(sorted(m), dtype=np.int64)
+            d["surfaces:%s" % pn] = np.array(list(p.surfaces.keys()))
+            for sn, entries in p.surfaces.items():
+                d["surfn:%s:%s" % (pn, sn)] = np.array(len(entries))
+                for k, (labels, face) in enumerate(entries):
+                    d["surf:%s:%s:%d:labels" % (pn, sn, k)] = np.asarray(labels, dtype=np.int64)
+                    d["surf:%s:%s:%d:face" % (pn, sn, k)] = np.array(face)
+            d["sections:%s" % pn] = np.array(p.sections)
+            d["elems_material:%s" % pn] = p.elems_material.numpy()
+        for mn, m in inp.material.items():
+            d["material:%s" % mn] = np.array([m.type, m.mat_para[0], m.mat_para[1], m.density], dtype=np.float64)
+        for iname, (part_name, T) in getattr(inp.assemble, "instances", {}).items():
+            d["instance:%s" % iname] = np.asarray(T, dtype=np.float64)
+            d["instancepart:%s" % iname] = np.array(part_name)
+        for sn, m in getattr(inp.assemble, "sets_nodes", {}).items():
+            d["asm_nset:%s" % sn] = np.array(sorted(m), dtype=np.int64)
+        for sn, m in getattr(inp.assemble, "sets_elems", {}).items():
+            d["asm_elset:%s" % sn] = np.array(sorted(m), dtype=np.int64)
+        fe = FEA.from_inp(inp)
+        for pn, part in fe.assembly._parts.items():
+            for sn, m in part.set_nodes.items():
+                d["pset:%s:%s" % (pn, sn)] = np.asarray(m, dtype=np.int64)
+            for k, (en, e) in enumerate(part.elems.items()):
+                g = "group:%s:%d" % (pn, k)
+                d[g + ":type"] = np.array(type(e).__name__)
+                d[g + ":elems_index"] = e._elems_index.numpy().astype(np.int64)
+                d[g + ":elems"] = e._elems.numpy().astype(np.int64)
+                d[g + ":mu"] = np.array(float(e.materials.mu))
+                d[g + ":kappa"] = np.array(float(e.materials.kappa))
+                d[g + ":density"] = np.asarray(e.density, dtype=np.float64)
+            d["ngroups:%s" % pn] = np.array(len(part.elems))
+        np.savez_compressed(os.path.join(out, name + ".npz"), **d)
+        print("wrote", name, len(d), "arrays")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", default=HERE)
-    ap.add_argument("--case", default="all", help="all, or one of: cfg1 tet3 hex5 explicit newmark newmark_hex")
+    ap.add_argument("--case", default="all", help="all, or one of: cfg1 tet3 hex5 explicit newmark newmark_hex inp")
     a = ap.parse_args()
     FEA = import_reference(a.ref)
     from oracle import fea_oracle as O  # mesh generators only
@@ -292,6 +346,9 @@ def main():
         case_explicit(FEA, O, a.out)
     if run("newmark"):
         case_implicit_dynamic(FEA, O, a.out)
+    if run("inp"):
+        sys.path.insert(0, HERE)
+        case_inp(FEA, a.out)
     if run("newmark_hex"):
         case_implicit_dynamic(FEA, O, a.out, n=2, kappa=20.0, p=0.05, dt=0.05, name="newmark_hex2", kind="C3D8")
 
