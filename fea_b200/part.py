@@ -1,7 +1,6 @@
 """Part and Instance (mirrors FEA/assemble/part.py of sssnnn7119/FEA)."""
 from __future__ import annotations
 
-import numpy as np
 import torch
 
 from .elements import merge_surfaces

@@ -12,7 +12,6 @@ import numpy as np
 import pytest
 import torch
 
-from oracle import fea_oracle as O
 from tests.helpers import fea_model, rel
 
 pytestmark = pytest.mark.gpu

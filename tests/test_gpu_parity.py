@@ -8,7 +8,7 @@ import pytest
 import torch
 
 from oracle import fea_oracle as O
-from tests.helpers import csr_from_api, fea_model, oracle_model, rel
+from tests.helpers import csr_from_api, fea_model, rel
 
 pytestmark = pytest.mark.gpu
 

@@ -4,7 +4,6 @@ Tolerances: a slot of the batched PCG reaches the same solution as the
 single-system PCG to 1e-10 relative; a served request's result is
 bitwise identical alone and among others; served and plain converged
 displacements agree to 1e-6 relative (both are Newton solves to 1e-8)."""
-import numpy as np
 import pytest
 import torch
 
