@@ -136,10 +136,12 @@ class FEA_INP:
                                          % (etype, v.size, nn + 1))
                     arr = v.reshape(-1, nn + 1) - 1
                     self.elems[etype] = np.concatenate([self.elems[etype], arr]) if etype in self.elems else arr
+                    # counted in data lines, as the reference does (two per C3D20
+                    # element): they size elems_material
                     if etype in SHELL_TYPES:
-                        self.num_elems_2D += arr.shape[0]
+                        self.num_elems_2D += len(data)
                     else:
-                        self.num_elems_3D += arr.shape[0]
+                        self.num_elems_3D += len(data)
                     if "elset" in params:
                         self.sets_elems.setdefault(params["elset"], set()).update(arr[:, 0].tolist())
                 elif name == "nset":
@@ -187,9 +189,10 @@ class FEA_INP:
                     if model:
                         raise NotImplementedError("*Hyperelastic, %s: only neo hooke is on the B200 path"
                                                   % ", ".join(model))
-                    c10, d1 = [float(t) for t in data[0].split(",") if t.strip()][:2]
+                    # every number of the line, the first two as (mu, kappa) = (2 C10, 2 / D1)
+                    v = [float(t) for t in data[0].split(",") if t.strip()]
                     self.type = 1
-                    self.mat_para = [2.0 * c10, 2.0 / d1]
+                    self.mat_para = [2.0 * v[0], 2.0 / v[1]] + v[2:]
                 elif name == "elastic":
                     self.type = 0
                     self.mat_para = [float(t) for t in data[0].split(",") if t.strip()]
@@ -286,7 +289,11 @@ class FEA_INP:
                 continue
             i += 1
         for p in self.part.values():
+            # rows: the reference's count of element data lines, widened to
+            # every label an element block or a section set names (the
+            # reference fails on a section over elements it does not read)
             labels = [int(e[:, 0].max()) + 1 for e in p.elems.values() if e.size]
+            labels += [max(p.sets_elems[es]) + 1 for es, _ in p.sections if p.sets_elems.get(es)]
             n = max([p.num_elems_2D + p.num_elems_3D] + labels)
             p.elems_material = -torch.ones([n, 5])
             for elset, mat_name in p.sections:

@@ -195,7 +195,8 @@ def test_format_variants_the_reference_skips():
     assert p.sections == [["both", "m"]]
     m = inp.material["m"]
     assert (m.type, m.mat_para, m.density) == (1, [0.5, 4.0], 3.0)
-    assert p.elems_material[:, 1:].tolist() == [[3.0, 1.0, 0.5, 4.0]] * 2
+    # rows = element data lines (3: the first element takes two), as the reference counts them
+    assert p.elems_material[:, 1:].tolist() == [[3.0, 1.0, 0.5, 4.0]] * 2 + [[-1.0] * 4]
 
 
 def test_unsupported_inputs_raise():
