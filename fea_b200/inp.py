@@ -299,6 +299,8 @@ class FEA_INP:
             for elset, mat_name in p.sections:
                 index = torch.tensor(sorted(p.sets_elems[elset]), dtype=torch.int64)
                 mat = self.material[mat_name]
+                if mat.type is None:
+                    raise ValueError("material %s of section %s defines no elastic behaviour" % (mat_name, elset))
                 p.elems_material[index, 0] = index.to(p.elems_material.dtype)
                 p.elems_material[index, 1] = mat.density
                 p.elems_material[index, 2] = mat.type

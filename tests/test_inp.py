@@ -211,3 +211,8 @@ def test_unsupported_inputs_raise():
     assert inp.part["p"].elems["C3D10"].shape == (1, 11)
     with pytest.raises(NotImplementedError):
         F.from_inp(inp)
+    with pytest.raises(ValueError):
+        inp.read_lines(["*Part, name=p\n", "*Node\n", "1, 0., 0., 0.\n", "*Element, type=C3D4\n",
+                        "1, 1, 1, 1, 1\n", "*Elset, elset=all\n", "1\n",
+                        "*Solid Section, elset=all, material=m\n", "*End Part\n",
+                        "*Material, name=m\n", "*Density\n", "1.,\n"])
