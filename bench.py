@@ -208,7 +208,19 @@ def cpu_baseline(n, seconds):
     dt = (time.perf_counter() - t0) / reps
     return {"value": len(keep) / dt / 1e9, "unit": UNIT, "cores": torch.get_num_threads(), "kind": "port",
             "sample": "%d-element slab (%d x %d x %d C3D8) of the same mesh, R+K+slot scatter+reduction, "
-                      "%d reps in %.1f s" % (len(keep), slab, n, n, reps, reps * dt)}
+                      "%d reps in %.1f s; %s" % (len(keep), slab, n, n, reps, reps * dt, cpu_model())}
+
+
+def cpu_model():
+    """The host CPU's model name (first processor in /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.lower().startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown CPU"
 
 
 def _timed_difference(run, seconds, cap):
@@ -242,7 +254,8 @@ def cpu_cg_iteration(indptr, indices, values, b, seconds):
     per, m, total = _timed_difference(run, seconds, 2000)
     return {"value": per * 1e3, "unit": "ms per CG iteration", "cores": torch.get_num_threads(), "kind": "port",
             "sample": "%d iterations of the reference's CG (CSR SpMV + vector updates) on the same %d-row, "
-                      "%d-nonzero system, minus a 1-iteration call; %.1f s" % (m, bb.shape[0], v.shape[0], total)}
+                      "%d-nonzero system, minus a 1-iteration call; %.1f s; %s"
+                      % (m, bb.shape[0], v.shape[0], total, cpu_model())}
 
 
 def cpu_explicit_step(X, el, dt, seconds):
@@ -266,7 +279,7 @@ def cpu_explicit_step(X, el, dt, seconds):
     per, steps, total = _timed_difference(run, seconds, 50)
     return {"value": 1.0 / per, "unit": "steps/s", "cores": torch.get_num_threads(), "kind": "port",
             "sample": "%d steps of the reference's loop on the same %d-element mesh, minus a 1-step run "
-                      "(lumped mass and first force pass cancel); %.1f s" % (steps, len(el), total)}
+                      "(lumped mass and first force pass cancel); %.1f s; %s" % (steps, len(el), total, cpu_model())}
 
 
 def run_reference(a):
