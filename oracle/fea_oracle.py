@@ -317,6 +317,42 @@ def pressure_volume(x, faces):
 # ---------------------------------------------------------------------------
 
 
+def reduced_pattern_csr(elem_groups, free, n_nodes):
+    """Reduced coalesced CSR pattern (indptr int64 [n+1], indices int64 [nnz])
+    from the node-level restatement of the element pattern, for meshes too
+    large for the DOF-level sort of ``element_pattern``.
+
+    The reference's pattern (C3base.py:109-153) is the sorted set of DOF
+    pairs (3 n_a + j, 3 n_b + k) of every element; after the Dirichlet mask
+    and the relabelling (assembly.py:357-387) a free row (n, j) holds, in
+    ascending order, the free DOFs of every node sharing an element with n.
+    Here the distinct node pairs are found with one sort of E nn^2 keys and
+    expanded to DOFs with numpy.  ``free`` is the [3 N] free-DOF mask.
+    """
+    free = np.asarray(free, dtype=bool).reshape(n_nodes, 3)
+    keys = []
+    for el in elem_groups:
+        el = np.asarray(el, dtype=np.int64)
+        keys.append((el[:, :, None] * n_nodes + el[:, None, :]).reshape(-1))
+    pairs = np.unique(np.concatenate(keys))
+    pn, pc = pairs // n_nodes, pairs % n_nodes               # sorted by (n, c)
+    fc = free.sum(1)                                          # free DOFs per node
+    rdof = np.concatenate([[0], np.cumsum(fc)[:-1]])          # first reduced DOF of each node
+    # node column list: for every pair (n, c), the free DOFs of c in order
+    cnt = fc[pc]
+    start = np.repeat(rdof[pc] - np.concatenate([[0], np.cumsum(cnt)[:-1]]), cnt)
+    cols = start + np.arange(int(cnt.sum()))
+    L = np.bincount(pn, weights=cnt, minlength=n_nodes).astype(np.int64)   # columns per row of node n
+    seg = np.concatenate([[0], np.cumsum(L)[:-1]])
+    # every free row (n, j) repeats its node's column list
+    rown = np.repeat(np.arange(n_nodes), fc)
+    rl = L[rown]
+    indptr = np.concatenate([[0], np.cumsum(rl)]).astype(np.int64)
+    first = np.repeat(seg[rown] - indptr[:-1], rl)
+    indices = cols[first + np.arange(int(indptr[-1]))]
+    return indptr, indices
+
+
 @dataclass
 class Group:
     kind: str
@@ -423,6 +459,57 @@ class Model:
         Ac = A.to_sparse_csr()
         return R, (Ac.crow_indices(), Ac.col_indices(), Ac.values())
 
+    def stiffness_coo(self, gc, patterns, chunk=16384):
+        """One Assembly.assemble_Stiffness_Matrix call in the reference's own
+        output form: (R [n], K_indices [2, M], K_values [M]), an UNCOALESCED
+        reduced COO.
+
+        Follows assembly.py:283-387 step by step: per element group
+        structural_Force (C3base.py:413-452: element R and K, R scattered by
+        the force index, K scattered by the element-to-slot map into the
+        group's coalesced values), the loads' -f and -k as COO
+        (pressure.py:80-132), concatenation, the Dirichlet mask on rows and
+        columns (assembly.py:373-376) and the relabelling of each index row
+        by ``unique(return_inverse=True)`` (assembly.py:379-380).
+        ``patterns`` holds one ``element_pattern`` per group: the
+        reference's ``initialize`` builds them once per mesh.  The element
+        arithmetic runs over ``chunk`` elements at a time (the same values
+        as one pass; bounded host memory).
+        """
+        u = self.gc_to_u(gc)
+        ndof = self.X.shape[0] * 3
+        R0 = torch.zeros(ndof, dtype=DT)
+        rows, cols, vals = [], [], []
+        for g, (idx, slot, force) in zip(self.groups, patterns):
+            E, nn = g.elems.shape
+            v = torch.zeros(idx.shape[1], dtype=DT)
+            slot2 = slot.view(-1, E)                         # (a, j, b, k) x e, e fastest
+            force2 = force.view(-1, E)                       # (a, j) x e
+            for e0 in range(0, E, chunk):
+                e1 = min(E, e0 + chunk)
+                Re, Ke = element_residual_tangent(g.kind, self.X, g.elems[e0:e1], u, g.mu, g.kappa)
+                R0.scatter_add_(0, force2[:, e0:e1].reshape(-1), Re.reshape(-1))
+                v.scatter_add_(0, slot2[:, e0:e1].reshape(-1), Ke.reshape(-1))
+            rows.append(idx[0]); cols.append(idx[1]); vals.append(v)
+        x = self.X + u
+        for pl in self.pressures:
+            f, k = pressure_force_tangent(x, pl.faces, pl.p)
+            fi = torch.stack([3 * pl.faces, 3 * pl.faces + 1, 3 * pl.faces + 2], dim=1)
+            R0.scatter_add_(0, fi.reshape(-1), -f.reshape(-1))
+            E, nf = pl.faces.shape
+            ra = (3 * pl.faces[:, None, :, None, None] + torch.arange(3)[None, :, None, None, None])
+            cb = (3 * pl.faces[:, None, None, None, :] + torch.arange(3)[None, None, None, :, None])
+            rows.append(ra.expand(E, 3, nf, 3, nf).reshape(-1))
+            cols.append(cb.expand(E, 3, nf, 3, nf).reshape(-1))
+            vals.append(-k.reshape(-1))
+        free = self.free_mask()
+        rows = torch.cat(rows); cols = torch.cat(cols); vals = torch.cat(vals)
+        keep = free[rows] & free[cols]
+        rows, cols, vals = rows[keep], cols[keep], vals[keep]
+        rows = rows.unique(return_inverse=True)[1]
+        cols = cols.unique(return_inverse=True)[1]
+        return R0[free], torch.stack([rows, cols]), vals
+
     def energy(self, gc):
         """Assembly._total_Potential_Energy, assembly.py:389-415 (pressure.py:134-159)."""
         u = self.gc_to_u(gc)
@@ -485,6 +572,148 @@ class Model:
         r, c, v = self.mass_coo()
         n = int(self.free_mask().sum())
         return sp.coo_matrix((v.numpy(), (r.numpy(), c.numpy())), shape=(n, n)).tocsr()
+
+
+# ---------------------------------------------------------------------------
+# Couple constraint: nodes tied to a reference point's rigid motion
+# ---------------------------------------------------------------------------
+
+
+def _eps3():
+    e = torch.zeros(3, 3, 3, dtype=DT)
+    e[0, 1, 2] = e[1, 2, 0] = e[2, 0, 1] = 1.0
+    e[0, 2, 1] = e[2, 1, 0] = e[1, 0, 2] = -1.0
+    return e
+
+
+def couple_motion(z, y):
+    """Displacement of tied nodes by the rotation vector z of a reference
+    point, R(z) y - y for rows of y (offsets from the point), and its first
+    and second derivatives with respect to z: (Y [n,3], Ydot [n,3,3],
+    Ydot2 [n,3,3,3]).
+
+    Follows Couple._rotation3d and Couple._calculate_Ydotz
+    (FEA/assemble/constraints/couple.py:169-282): Rodrigues' formula in the
+    angle theta = |z| + 1e-20 and the axis w = z / theta, differentiated by
+    the chain rule through (theta, w) with dtheta/dz = w,
+    dw/dz = I/theta - z z^T/theta^3 and its derivative.
+    """
+    z = z.to(DT)
+    y = y.to(DT)
+    th = z.norm() + 1e-20
+    w = z / th
+    c, s = torch.cos(th), torch.sin(th)
+    E = _eps3()
+    wy = y @ w                                            # [n]
+    wxy = torch.einsum("ijk,j,nk->ni", E, w, y)           # w x y
+    Y = y * c + wxy * s + w[None, :] * wy[:, None] * (1 - c) - y
+    I3 = torch.eye(3, dtype=DT)
+    f_t = -y * s + wxy * c + w[None, :] * wy[:, None] * s                 # d/dtheta
+    f_tt = -y * c - wxy * s + w[None, :] * wy[:, None] * c
+    Ey = torch.einsum("ilk,nk->nil", E, y)                               # d(w x y)_i / dw_l
+    wxI = I3[None] * wy[:, None, None] + w[None, :, None] * y[:, None, :]  # d(w (w.y))_i / dw_l
+    f_w = s * Ey + (1 - c) * wxI
+    f_wt = c * Ey + s * wxI
+    f_ww = (1 - c) * (torch.einsum("il,nm->nilm", I3, y) + torch.einsum("im,nl->nilm", I3, y))
+    dw = I3 / th - torch.outer(z, z) / th ** 3                           # dw/dz = d2theta/dz2
+    d2w = 3 * torch.einsum("i,p,q->ipq", z, z, z) / th ** 5 - (
+        torch.einsum("ip,q->ipq", I3, z) + torch.einsum("iq,p->ipq", I3, z) + torch.einsum("pq,i->ipq", I3, z)) / th ** 3
+    Ydot = torch.einsum("nil,lp->nip", f_w, dw) + torch.einsum("ni,p->nip", f_t, w)
+    Ydot2 = (torch.einsum("ni,pq->nipq", f_t, dw) + torch.einsum("ni,p,q->nipq", f_tt, w, w)
+             + torch.einsum("nil,lq,p->nipq", f_wt, dw, w) + torch.einsum("nil,lp,q->nipq", f_wt, dw, w)
+             + torch.einsum("nilm,lp,mq->nipq", f_ww, dw, dw) + torch.einsum("nil,lpq->nipq", f_w, d2w))
+    return Y, Ydot, Ydot2
+
+
+@dataclass
+class CoupledModel:
+    """A Model whose ``coupled`` nodes follow a reference point at ``rp``
+    (Couple, couple.py), with a concentrated force and a moment on the point
+    (concentrate_force.py, moment.py).  Reduced DOFs: the base model's free
+    node DOFs minus the tied nodes, then the point's 6 DOFs (v, z), in the
+    reference's order (instances first, reference points after,
+    assembly.py:90-105)."""
+    base: Model
+    coupled: np.ndarray
+    rp: torch.Tensor
+    force: torch.Tensor
+    moment: torch.Tensor
+
+    def node_free(self):
+        m = self.base.free_mask().view(-1, 3).clone()
+        m[torch.as_tensor(np.asarray(self.coupled), dtype=torch.int64)] = False
+        return m.reshape(-1)
+
+    def split(self, gc):
+        nf = int(self.node_free().sum())
+        return gc[:nf], gc[nf:nf + 3], gc[nf + 3:nf + 6]
+
+    def offsets(self):
+        return self.base.X[torch.as_tensor(np.asarray(self.coupled), dtype=torch.int64)] - self.rp.to(DT)[None, :]
+
+    def node_u(self, gc):
+        """Couple.modify_RGC (couple.py:34-40): tied nodes at v + R(z) y - y."""
+        g, v, z = self.split(gc)
+        u = torch.zeros(self.base.X.shape[0] * 3, dtype=DT)
+        u[self.node_free()] = g
+        Y = couple_motion(z, self.offsets())[0]
+        u = u.view(-1, 3)
+        u[torch.as_tensor(np.asarray(self.coupled), dtype=torch.int64)] = v[None, :] + Y
+        return u.reshape(-1)
+
+    def assemble(self, gc):
+        """Reduced R and coalesced CSR: element and pressure R, K over every
+        node DOF at the tied displacement, condensed onto the point's DOFs
+        (couple.py:68-166) with P = d u / d gc, plus the point's loads."""
+        b = self.base
+        N = b.X.shape[0]
+        uall = self.node_u(gc)
+        full = Model(b.X, b.groups, b.pressures, [])
+        full._free = torch.ones(3 * N, dtype=torch.bool)
+        R0, (ip, ix, vv) = full.assemble(uall)
+        rows = torch.repeat_interleave(torch.arange(3 * N), ip[1:] - ip[:-1])
+        K = torch.sparse_coo_tensor(torch.stack([rows, ix]), vv, (3 * N, 3 * N))
+        g, v, z = self.split(gc)
+        _, Yd, Yd2 = couple_motion(z, self.offsets())
+        nf = self.node_free()
+        nfree = int(nf.sum())
+        n = nfree + 6
+        cols = torch.full((3 * N,), -1, dtype=torch.int64)
+        cols[nf] = torch.arange(nfree)
+        pr, pc, pv = [torch.nonzero(nf).flatten()], [cols[nf]], [torch.ones(nfree, dtype=DT)]
+        cn = torch.as_tensor(np.asarray(self.coupled), dtype=torch.int64)
+        for q in range(3):
+            pr.append(3 * cn + q); pc.append(torch.full_like(cn, nfree + q)); pv.append(torch.ones(cn.shape[0], dtype=DT))
+            for p_ in range(3):
+                pr.append(3 * cn + q); pc.append(torch.full_like(cn, nfree + 3 + p_)); pv.append(Yd[:, q, p_])
+        Pm = torch.sparse_coo_tensor(torch.stack([torch.cat(pr), torch.cat(pc)]), torch.cat(pv), (3 * N, n)).coalesce()
+        Pd = Pm.to_dense()
+        Kr = Pd.T @ (K.to_dense() @ Pd)
+        Rc = R0.view(-1, 3)[cn]
+        Kr[nfree + 3:, nfree + 3:] += torch.einsum("ai,aipq->pq", Rc, Yd2)
+        R = Pd.T @ R0
+        R[nfree:nfree + 3] -= self.force.to(DT)
+        R[nfree + 3:] -= self.moment.to(DT)
+        # structural pattern: the element pattern's entries (stored zeros
+        # included) with every tied DOF spread over all six point DOFs
+        Kp = torch.sparse_coo_tensor(torch.stack([rows, ix]), torch.ones_like(vv), (3 * N, 3 * N)).to_dense()
+        Ps = (Pd != 0).to(DT)
+        Ps[3 * cn[:, None] + torch.arange(3)[None, :], nfree:] = 1.0
+        pattern = (Ps.T @ (Kp @ Ps)) != 0
+        pattern[nfree:, nfree:] = True
+        idx = torch.nonzero(pattern).T
+        A = torch.sparse_coo_tensor(idx, Kr[idx[0], idx[1]], (n, n)).coalesce().to_sparse_csr()
+        return R, (A.crow_indices(), A.col_indices(), A.values())
+
+    def energy(self, gc):
+        """Element and pressure energy at the tied displacement minus the
+        point loads' work (assembly.py:389-415)."""
+        b = self.base
+        uall = self.node_u(gc)
+        full = Model(b.X, b.groups, b.pressures, [])
+        full._free = torch.ones(3 * b.X.shape[0], dtype=torch.bool)
+        g, v, z = self.split(gc)
+        return full.energy(uall) - (self.force.to(DT) * v).sum() - (self.moment.to(DT) * z).sum()
 
 
 # ---------------------------------------------------------------------------

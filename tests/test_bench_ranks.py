@@ -39,11 +39,11 @@ def test_max_over_ranks_and_job_rate_with_gloo():
 def test_reference_arm_prints_on_rank_zero_only():
     env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
     r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--n", "8", "--steps", "1", "--warmup", "0",
-                        "--cpu-seconds", "0.2"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+                        ], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip() == ""
     env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0")
     r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--n", "8", "--steps", "1", "--warmup", "0",
-                        "--cpu-seconds", "0.2"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+                        ], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
