@@ -2,7 +2,9 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cmath>
+#include <mutex>
 
 #include "../../include/fea_b200.h"
 
@@ -26,13 +28,20 @@ static __constant__ double c_w_t3[3];
 static __constant__ double c_sf_q4[4][3][4];
 static __constant__ double c_w_q4[4];
 
-static unsigned long long g_tables_ready = 0;  // per translation unit: one bit per device
+// Per translation unit: one bit per device whose tables are uploaded.  The
+// first call on a device uploads them with synchronous copies under a mutex
+// (host threads making their first calls at once wait for one upload), so
+// that first call should come before any stream capture on that device.
+static std::atomic<unsigned long long> g_tables_ready{0};
+static std::mutex g_tables_mu;
 
 static inline int ensure_tables() {
   int dev = 0;
   cudaError_t err = cudaGetDevice(&dev);
   if (err != cudaSuccess) return (int)err;
-  if (dev < 64 && (g_tables_ready >> dev & 1ull)) return 0;
+  if (dev < 64 && (g_tables_ready.load(std::memory_order_acquire) >> dev & 1ull)) return 0;
+  std::lock_guard<std::mutex> lock(g_tables_mu);
+  if (dev < 64 && (g_tables_ready.load(std::memory_order_acquire) >> dev & 1ull)) return 0;
   double tet[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
   const double s[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
                           {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
@@ -76,7 +85,7 @@ static inline int ensure_tables() {
   if ((err = cudaMemcpyToSymbol(c_w_t3, w3, sizeof(w3))) != cudaSuccess) return (int)err;
   if ((err = cudaMemcpyToSymbol(c_sf_q4, sf4, sizeof(sf4))) != cudaSuccess) return (int)err;
   if ((err = cudaMemcpyToSymbol(c_w_q4, w4, sizeof(w4))) != cudaSuccess) return (int)err;
-  if (dev < 64) g_tables_ready |= 1ull << dev;
+  if (dev < 64) g_tables_ready.fetch_or(1ull << dev, std::memory_order_release);
   return 0;
 }
 

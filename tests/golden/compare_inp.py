@@ -3,7 +3,7 @@
 fea_b200.FEA_INP) and, where all elements are C3D4 / C3D8, build both models
 with from_inp; write a per-file report of every difference.
 
-    python tests/golden/compare_inp.py [--ref /root/reference]
+    python tests/golden/compare_inp.py --ref <path of the reference source tree>
 
 The INP files are read where they lie and are not copied; the report
 (``inp_reference_report.json`` next to this script) is the record.
@@ -100,7 +100,7 @@ def model_diffs(fr, fo):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="path of the reference source tree (the directory holding FEA/)")
     a = ap.parse_args()
     from make_golden import import_reference
     FEA = import_reference(a.ref)

@@ -2,7 +2,7 @@
 
 Run in a container where the reference source tree is available:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <path of the reference source tree>
 
 The reference is imported unmodified, with three stub modules injected first:
 ``tkinter`` and ``turtle`` (stray imports at FEA/assemble/loads/contact.py:1-2)
@@ -206,6 +206,186 @@ def case_hex_block(FEA, O, out, n=5, mu=1.0, kappa=50.0, p=-0.02, seed=0, name="
     print(name, "E", el.shape[0], "n", gc0.shape[0], "nnz", vv.shape[0], "final max|R|", rm)
 
 
+def case_rotated(FEA, O, out, n=3, mu=1.0, kappa=50.0, p=0.02, name="rot_hex3"):
+    """Two instances of one jittered C3D8 block: 'a' in place, 'b' rotated
+    (rotation vector ROT) and translated (TRANS); each clamped on its x = 0
+    face and loaded by pressure on its x = 1 face (the part's frame).  The
+    reduced R, K and energy at a state, the converged GC, instance b's
+    element-level outputs (structural_Force with its rotation matrix), its
+    energy and mass through the Instance API, and autograd of (R . lam)
+    with respect to the part's nodes (both instances) and mu."""
+    rot, trans = [0.3, -0.5, 0.7], [1.5, -2.0, 0.5]
+    X, el = O.hex_block(n, jitter=0.1, seed=6)
+    h = 1.0 / n
+    clamp = torch.nonzero(X[:, 0] < 0.5 * h).flatten().numpy()
+    xe = X[el][:, [1, 2, 6, 5], 0]
+    endel = torch.nonzero(xe.min(dim=1).values > 1 - 0.5 * h).flatten().numpy()
+    part = FEA.Part(X.clone())
+    e = FEA.elements.C3D8(elems=el.clone(), elems_index=torch.arange(el.shape[0]), part=part)
+    e.set_materials(FEA.materials.NeoHookean(torch.tensor(mu), torch.tensor(kappa)))
+    e.set_density(torch.tensor([1.0]))
+    part.add_element(e)
+    part.set_nodes["clamp"] = clamp
+    part.add_surface_set("end", [(endel, 3)])
+    asm = FEA.Assembly()
+    asm.add_part(part, "p")
+    ia, ib = FEA.Instance(part), FEA.Instance(part)
+    ib._rotation = torch.tensor(rot)
+    ib._translation = torch.tensor(trans)
+    asm.add_instance(ia, "a")
+    asm.add_instance(ib, "b")
+    for nm in ("a", "b"):
+        asm.add_load(FEA.loads.Pressure(instance_name=nm, surface_set="end", pressure=p), "p_" + nm)
+        asm.add_boundary(FEA.boundarys.Boundary_Condition(instance_name=nm, set_nodes_name="clamp"), "bc_" + nm)
+    c = FEA.FEAController()
+    c.assembly = asm
+    c.solver = FEA.solver.StaticImplicitSolver(tol_error=1e-10)
+    c.initialize()
+    gc0 = c.assembly.GC.clone()
+    res = dict(X=X.numpy(), elems=el.numpy(), fixed=clamp, end_elems=endel, mu=mu, kappa=kappa, p=p,
+               rotation=np.array(rot), translation=np.array(trans), gc0=gc0.numpy(),
+               rotation_matrix=ib.rotation_matrix.numpy())
+    gc, rm = converge(FEA, c, gc0)
+    res.update(gc_converged=gc.numpy(), resid_converged=rm)
+    state = gc + 2e-3 * torch.randn(gc.shape, generator=torch.Generator().manual_seed(8))
+    R, Ki, Kv = c.assembly.assemble_Stiffness_Matrix(GC=state)
+    ip, ix, vv = coalesced_csr(R, Ki, Kv)
+    RGC = c.assembly._GC2RGC(state)
+    Ub = RGC[ib._RGC_index]
+    fi, Re, Kidx, Kval = e.structural_Force(Ub, ib.rotation_matrix)
+    Mi, Mv = ib.get_mass_matrix()
+    res.update(state=state.numpy(), R=R.numpy(), indptr=ip, indices=ix, values=vv,
+               energy=float(c.assembly._total_Potential_Energy(GC=state)),
+               force=c.assembly.assemble_force(GC=state).numpy(),
+               Ub=Ub.numpy(), elem_force_index=fi.numpy(), elem_R=Re.numpy(), elem_K_indices=Kidx.numpy(),
+               elem_K_values=Kval.numpy(), inst_energy=float(ib.potential_energy(RGC)),
+               inst_mass_indices=Mi.numpy(), inst_mass_values=Mv.numpy())
+    lam = torch.randn(gc.shape, generator=torch.Generator().manual_seed(9))
+    Xg = part.nodes.clone().requires_grad_(True)
+    part.nodes = Xg
+    mu_t = torch.tensor(mu, requires_grad=True)
+    e.materials.mu = mu_t
+    c.initialize()
+    Rg = c.assembly.assemble_Stiffness_Matrix(GC=gc)[0]
+    gX, gmu = torch.autograd.grad((Rg * lam).sum(), [Xg, mu_t])
+    res.update(adj_lambda=lam.numpy(), adj_gX=gX.numpy(), adj_gmu=float(gmu))
+    np.savez_compressed(os.path.join(out, "%s.npz" % name), **res)
+    print(name, "E", el.shape[0], "n", gc0.shape[0], "nnz", vv.shape[0], "final max|R|", rm)
+
+
+def case_couple(FEA, O, out, n=3, mu=1.0, kappa=50.0, name="couple_hex3"):
+    """A jittered C3D8 block, bottom (k = 0) clamped, its top nodes (k = n)
+    tied by a Couple constraint to a reference point above the block
+    (couple.py:34-198) that carries a concentrated force and a moment
+    (concentrate_force.py, moment.py).  Reduced R, K, energy and residual
+    at a seeded state with a finite RP rotation, and the converged GC."""
+    X, el = O.hex_block(n, jitter=0.1, seed=11)
+    k = torch.arange(X.shape[0]) % (n + 1)
+    bottom = torch.nonzero(k == 0).flatten().numpy()
+    top = torch.nonzero(k == n).flatten().numpy()
+    part = FEA.Part(X.clone())
+    e = FEA.elements.C3D8(elems=el.clone(), elems_index=torch.arange(el.shape[0]), part=part)
+    e.set_materials(FEA.materials.NeoHookean(torch.tensor(mu), torch.tensor(kappa)))
+    e.set_density(torch.tensor([1.0]))
+    part.add_element(e)
+    part.set_nodes["bottom"] = bottom
+    part.set_nodes["top"] = top
+    asm = FEA.Assembly()
+    asm.add_part(part, "p")
+    asm.add_instance(FEA.Instance(part), "p")
+    rp_xyz = [0.5, 0.5, 1.5]
+    force, moment = [0.01, 0.02, -0.05], [0.01, -0.02, 0.015]
+    rp = asm.add_reference_point(FEA.ReferencePoint(rp_xyz))
+    asm.add_constraint(FEA.constraints.Couple(instance_name="p", set_nodes_name="top", rp_name=rp))
+    asm.add_load(FEA.loads.Concentrate_Force(rp_name=rp, force=force), "f")
+    asm.add_load(FEA.loads.Moment(rp_name=rp, moment=moment), "m")
+    asm.add_boundary(FEA.boundarys.Boundary_Condition(instance_name="p", set_nodes_name="bottom"), "bc")
+    c = FEA.FEAController()
+    c.assembly = asm
+    c.solver = FEA.solver.StaticImplicitSolver(tol_error=1e-10)
+    c.initialize()
+    gc0 = c.assembly.GC.clone()
+    res = dict(X=X.numpy(), elems=el.numpy(), fixed=bottom, top=top, mu=mu, kappa=kappa, rp=np.array(rp_xyz),
+               force=np.array(force), moment=np.array(moment), gc0=gc0.numpy())
+    gc, rm = converge(FEA, c, gc0)
+    res.update(gc_converged=gc.numpy(), resid_converged=rm)
+    state = gc + 2e-3 * torch.randn(gc.shape, generator=torch.Generator().manual_seed(12))
+    state[-3:] += torch.tensor([0.05, -0.03, 0.04])            # a finite RP rotation
+    R, Ki, Kv = c.assembly.assemble_Stiffness_Matrix(GC=state)
+    ip, ix, vv = coalesced_csr(R, Ki, Kv)
+    res.update(state=state.numpy(), R=R.numpy(), indptr=ip, indices=ix, values=vv,
+               energy=float(c.assembly._total_Potential_Energy(GC=state)),
+               force_R=c.assembly.assemble_force(GC=state).numpy(),
+               rgc_state=torch.cat([r.reshape(-1) for r in c.assembly._GC2RGC(state)]).numpy())
+    np.savez_compressed(os.path.join(out, "%s.npz" % name), **res)
+    print(name, "E", el.shape[0], "n", gc0.shape[0], "nnz", vv.shape[0], "final max|R|", rm,
+          "rp", gc[-6:].numpy())
+
+
+def case_explicit_loaded(FEA, O, out, n=3, rho=1.0, p=0.05, steps=40, name="explicit_loaded"):
+    """DynamicExplicitSolver with a pressure load and two element groups: a
+    Kuhn-tet cube split into two C3D4 groups of different materials (even
+    and odd cells), bottom clamped, pressure on the top face, from rest with
+    a seeded initial velocity, a state stored every step."""
+    X, el = O.tet_block(n)
+    cell = torch.arange(el.shape[0]) // 6
+    g0, g1 = el[cell % 2 == 0], el[cell % 2 == 1]
+    bottom = torch.nonzero(X[:, 2].abs() < 1e-9).flatten().numpy()
+    sets = O.boundary_faces("C3D4", el, X, 2, 1.0)
+    part = FEA.Part(X.clone())
+    mats = [(1.0, 10.0), (2.0, 30.0)]
+    groups = []
+    for k, (g, (mu, kappa)) in enumerate(zip((g0, g1), mats)):
+        idx = torch.nonzero(cell % 2 == k).flatten()
+        e = FEA.elements.C3D4(elems=g.clone(), elems_index=idx, part=part)
+        e.set_materials(FEA.materials.NeoHookean(torch.tensor(mu), torch.tensor(kappa)))
+        e.set_density(torch.tensor([rho]))
+        part.add_element(e, "g%d" % k)
+        groups.append(e)
+    # the top faces as (element labels, face id) of the whole mesh
+    surf = [(idx.numpy(), fid) for idx, fid, _ in sets]
+    part.add_surface_set("top", surf)
+    part.set_nodes["bottom"] = bottom
+    asm = FEA.Assembly()
+    asm.add_part(part, "p")
+    asm.add_instance(FEA.Instance(part), "p")
+    ld = FEA.loads.Pressure(instance_name="p", surface_set="top", pressure=p)
+    asm.add_load(ld, "pressure")
+    asm.add_boundary(FEA.boundarys.Boundary_Condition(instance_name="p", set_nodes_name="bottom"), "bc")
+    c = FEA.FEAController()
+    c.assembly = asm
+    x = X[el]
+    vol = torch.einsum("ei,ei->e", torch.cross(x[:, 1] - x[:, 0], x[:, 2] - x[:, 0], dim=1), x[:, 3] - x[:, 0]).abs() / 6
+    fa = []
+    for tri in ([0, 1, 2], [0, 1, 3], [0, 2, 3], [1, 2, 3]):
+        a = x[:, tri]
+        fa.append(0.5 * torch.cross(a[:, 1] - a[:, 0], a[:, 2] - a[:, 0], dim=1).norm(dim=1))
+    hmin = (3 * vol / torch.stack(fa, 1).max(1).values).min()
+    cwave = np.sqrt((30.0 + 4 * 2.0 / 3) / rho)
+    dt = float(0.5 * hmin / cwave)
+    T = dt * steps
+    c.solver = FEA.solver.DynamicExplicitSolver(time_end=T * (1 - 1e-9), time_per_storage=0.5 * dt)
+    c.initialize()
+    c.solver._deltaT = dt
+    gc0 = torch.zeros_like(c.assembly.GC)
+    gv0 = 0.01 * torch.randn(gc0.shape, generator=torch.Generator().manual_seed(10))
+    minv = c.solver.get_lumped_mass_inv(gc0)
+    import contextlib
+    import io
+    with contextlib.redirect_stdout(io.StringIO()):
+        c.solver.solve(GC0=gc0, GV0=gv0)
+    res = dict(X=X.numpy(), elems0=g0.numpy(), elems1=g1.numpy(), cell=cell.numpy(),
+               mats=np.array(mats), rho=rho, p=p, dt=dt, steps=steps, fixed=bottom,
+               face_elem=np.concatenate([i for i, _ in surf]),
+               face_id=np.concatenate([np.full(len(i), f) for i, f in surf]),
+               pressure_faces=torch.cat([s._elems for s in ld.surface_element]).numpy(),
+               gv0=gv0.numpy(), minv=minv.numpy(), u_final=c.solver._GC_list[-1].numpy(),
+               v_final=c.solver._GV_list[-1].numpy(), a_final=c.solver._GA_list[-1].numpy(),
+               n_stored=len(c.solver._GC_list), time_final=c.solver._time_list[-1])
+    np.savez_compressed(os.path.join(out, "%s.npz" % name), **res)
+    print(name, "dt", dt, "stored", len(c.solver._GC_list), "max|u|", float(res["u_final"].__abs__().max()))
+
+
 def case_explicit(FEA, O, out, n=4, mu=1.0, kappa=10.0, rho=1.0, steps=40, name="explicit_tet4"):
     """Config-3 style explicit run on a small Kuhn-tet cube, no BCs."""
     X, el = O.tet_block(n)
@@ -328,9 +508,9 @@ def case_inp(FEA, out):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="path of the reference source tree (the directory holding FEA/)")
     ap.add_argument("--out", default=HERE)
-    ap.add_argument("--case", default="all", help="all, or one of: cfg1 tet3 hex5 explicit newmark newmark_hex inp")
+    ap.add_argument("--case", default="all", help="all, or one of: cfg1 tet3 hex5 explicit newmark newmark_hex inp rotated explicit_loaded couple")
     a = ap.parse_args()
     FEA = import_reference(a.ref)
     from oracle import fea_oracle as O  # mesh generators only
@@ -351,6 +531,12 @@ def main():
         case_inp(FEA, a.out)
     if run("newmark_hex"):
         case_implicit_dynamic(FEA, O, a.out, n=2, kappa=20.0, p=0.05, dt=0.05, name="newmark_hex2", kind="C3D8")
+    if run("rotated"):
+        case_rotated(FEA, O, a.out)
+    if run("explicit_loaded"):
+        case_explicit_loaded(FEA, O, a.out)
+    if run("couple"):
+        case_couple(FEA, O, a.out)
 
 
 if __name__ == "__main__":
