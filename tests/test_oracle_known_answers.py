@@ -122,3 +122,31 @@ def test_tangent_with_follower_pressure_is_derivative(golden, name, kind):
     h = 1e-6
     fd = (m.assemble(x + h * d, want_K=False)[0] - m.assemble(x - h * d, want_K=False)[0]) / (2 * h)
     assert float((fd - Kd).norm()) < 1e-8 * float(Kd.norm())
+
+
+@pytest.mark.parametrize("name", ["cfg1", "tet3", "hex5"])
+def test_node_level_pattern_matches_reference_csr(golden, name):
+    """The node-level restatement of the pattern (used where the DOF-level
+    sort is too large) gives the reference's reduced CSR bit for bit."""
+    g = golden(name)
+    N = g["X"].shape[0]
+    free = np.zeros((N, 3), dtype=bool)
+    free[np.unique(g["elems"])] = True
+    free[np.asarray(g["fixed"], dtype=np.int64)] = False
+    ip, ix = O.reduced_pattern_csr([g["elems"]], free, N)
+    np.testing.assert_array_equal(ip, g["indptr"])
+    np.testing.assert_array_equal(ix, g["indices"])
+
+
+@pytest.mark.parametrize("dofs", [(0, 1, 2), (2,), (0, 2)])
+def test_node_level_pattern_matches_oracle_with_partial_bcs(dofs):
+    X, el = O.hex_block(3, jitter=0.1, seed=4)
+    Xt, et = O.tet_block(2)
+    et = et + X.shape[0]                                  # a second group on nodes of its own
+    Xa = torch.cat([X, Xt + 2.0])
+    fixed = np.arange(0, Xa.shape[0], 5)
+    m = O.Model(Xa, [O.Group("C3D8", el, 1.0, 50.0), O.Group("C3D4", et, 1.0, 10.0)], [], [(fixed, dofs)])
+    R, (ip, ix, v) = m.assemble(torch.zeros(int(m.free_mask().sum()), dtype=torch.float64))
+    ip2, ix2 = O.reduced_pattern_csr([el.numpy(), et.numpy()], m.free_mask().numpy(), Xa.shape[0])
+    np.testing.assert_array_equal(ip2, ip.numpy())
+    np.testing.assert_array_equal(ix2, ix.numpy())
