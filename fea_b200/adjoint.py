@@ -43,7 +43,21 @@ def residual_vjp(asm, GC, lam):
         dmu.append(out[0])
     for fi, ld in enumerate(asm._face_loads):
         P.adjoint_hvp_pressure(fi, float(ld.pressure), asm._Xinst, gc, lam_full, dX)
-    return dX, dmu
+    return _to_part_frames(asm, dX), dmu
+
+
+def _to_part_frames(asm, dX):
+    """Coordinate gradients with respect to each part's own nodes: a rotated
+    instance evaluates its elements at X R^T (and its loads at X R^T + t), so
+    the gradient with respect to X is the assembly-frame one times R."""
+    for name, ins in asm._instances.items():
+        R = ins.rotation_matrix.to(torch.float64)
+        if torch.equal(R, torch.eye(3, dtype=torch.float64)):
+            continue
+        o = asm._node_offset[name]
+        n = ins.part.nodes.shape[0]
+        dX[o:o + n] = dX[o:o + n] @ R.to(dX.device)
+    return dX
 
 
 def pressure_hvp(asm, GC, v_full):
@@ -80,7 +94,7 @@ def compliance_gradient(asm, GC, pcg_tol=1e-26, pcg_max_iter=200000, return_lamb
     lam = torch.zeros_like(rhs)
     it, rr, st = P.pcg(K, rhs, lam, pcg_tol, pcg_max_iter, check_every=50)
     dX, dmu = residual_vjp(asm, gc, lam)
-    dCdX = -(dX + Hu)
+    dCdX = -(dX + _to_part_frames(asm, Hu))
     if return_lambda:
         return C, dCdX, [-d for d in dmu], it, lam
     return C, dCdX, [-d for d in dmu], it
@@ -121,5 +135,5 @@ def set_coordinates(asm, X):
     X = torch.as_tensor(X, dtype=torch.float64)
     ins.part.nodes = X.detach().cpu().clone()
     P = asm.plan
-    P.X.copy_(X.detach().to(P.device))
+    P.X.copy_(asm._element_frame_nodes(ins).to(P.device))
     asm._Xinst.copy_(ins.nodes.to(P.device))

@@ -19,8 +19,10 @@ import numpy as np
 import torch
 
 from ._trace import nvtx
-from .boundarys import Boundary_Condition
-from .loads import Pressure
+from .boundarys import Boundary_Condition, Boundary_Condition_RP
+from .constraints import Couple
+from .coupled import CoupledSystem
+from .loads import Concentrate_Force, Moment, Pressure
 from .part import Instance, Part
 from .plan import DevicePlan
 
@@ -115,10 +117,36 @@ class Assembly:
         del self._boundarys[name]
 
     def add_reference_point(self, rp, name: str = None):
-        raise NotImplementedError("reference points (and their couplings) are outside the B200 element path")
+        if name is None:
+            number = len(self._reference_points)
+            while ("rp-%d" % number) in self._reference_points:
+                number += 1
+            name = "rp-%d" % number
+        self._reference_points[name] = rp
+        return name
+
+    def get_reference_point(self, name):
+        if name not in self._reference_points:
+            raise ValueError("Reference point '%s' not found in the model." % name)
+        return self._reference_points[name]
+
+    def delete_reference_point(self, name):
+        self.get_reference_point(name)
+        del self._reference_points[name]
 
     def add_constraint(self, constraint, name: str = None):
-        raise NotImplementedError("constraints are outside the B200 element path")
+        name = name or self._name(self._constraints, constraint, constraint.__class__.__name__)
+        self._constraints[name] = constraint
+        return name
+
+    def get_constraint(self, name):
+        if name not in self._constraints:
+            raise ValueError("Constraint '%s' not found in the model." % name)
+        return self._constraints[name]
+
+    def delete_constraint(self, name):
+        self.get_constraint(name)
+        del self._constraints[name]
 
     # -- initialization (assembly.py:76-185) -----------------------------------
     def _allocate_RGC(self, size):
@@ -132,14 +160,19 @@ class Assembly:
     def initialize(self, *args, **kwargs):
         self._parts = dict(sorted(self._parts.items()))
         self._instances = dict(sorted(self._instances.items()))
+        self._reference_points = dict(sorted(self._reference_points.items()))
         self._loads = dict(sorted(self._loads.items()))
+        self._constraints = dict(sorted(self._constraints.items()))
         self._boundarys = dict(sorted(self._boundarys.items()))
         for name, ld in self._loads.items():
-            if not isinstance(ld, Pressure):
+            if not isinstance(ld, (Pressure, Concentrate_Force, Moment)):
                 raise NotImplementedError("load %r (%s) is outside the B200 path" % (name, type(ld).__name__))
         for name, b in self._boundarys.items():
-            if not isinstance(b, Boundary_Condition):
+            if not isinstance(b, (Boundary_Condition, Boundary_Condition_RP)):
                 raise NotImplementedError("boundary %r (%s) is outside the B200 path" % (name, type(b).__name__))
+        for name, c in self._constraints.items():
+            if not isinstance(c, Couple):
+                raise NotImplementedError("constraint %r (%s) is outside the B200 path" % (name, type(c).__name__))
         if not self._instances:
             raise ValueError("the assembly has no instance")
         self.RGC, self.RGC_remain_index, self.RGC_list_indexStart, self._RGC_size = [], [], [0], []
@@ -147,30 +180,51 @@ class Assembly:
         for ins in self._instances.values():
             idx = self._allocate_RGC(ins._RGC_requirements)
             ins.set_RGC_index(idx)
+        for rp in self._reference_points.values():
+            idx = self._allocate_RGC((rp._RGC_requirements,))
+            rp.set_RGC_index(idx)
         self.RGC[idx][-1] = 1e-5                  # the reference's seed (assembly.py:113)
         for ld in self._loads.values():
             ld.set_RGC_index(self._allocate_RGC(ld._RGC_requirements))
+        for c in self._constraints.values():
+            c.set_RGC_index(self._allocate_RGC(c._RGC_requirements))
         for b in self._boundarys.values():
             b.set_RGC_index(self._allocate_RGC(b._RGC_requirements))
         for part in self._parts.values():
             part.initialize(self)
         for ins in self._instances.values():
             ins.initialize(self)
+        for rp in self._reference_points.values():
+            rp.initialize(self)
         for ld in self._loads.values():
             ld.initialize(self)
+        for c in self._constraints.values():
+            c.initialize(self)
         for b in self._boundarys.values():
             b.initialize(self)
-        # required DOFs: element nodes, pressure face nodes; Dirichlet last
+        # required DOFs: element nodes, pressure face nodes, reference points
+        # carrying loads or ties; tied nodes and Dirichlet DOFs removed
+        # (assembly.py:150-170)
         for ins in self._instances.values():
             rem = self.RGC_remain_index[ins._RGC_index]
             for e in ins.part.elems.values():
                 rem = e.set_required_DoFs(rem)
         for ld in self._loads.values():
-            rem = self.RGC_remain_index[ld._load_index]
-            for s in ld.surface_element:
-                rem[np.unique(s._elems.numpy())] = True
+            if isinstance(ld, Pressure):
+                rem = self.RGC_remain_index[ld._load_index]
+                for s in ld.surface_element:
+                    rem[np.unique(s._elems.numpy())] = True
+            else:
+                ld.set_required_DoFs(self.RGC_remain_index)
+        for c in self._constraints.values():
+            c.set_required_DoFs(self.RGC_remain_index)
         for b in self._boundarys.values():
             rem = self.RGC_remain_index[b._constraint_index]
+            if isinstance(b, Boundary_Condition_RP):
+                for d in b.indexDoF:
+                    rem[d] = False
+                    self.RGC[b._constraint_index][d] = 0.0
+                continue
             for d in b.indexDoF:
                 rem[np.asarray(b.index_nodes, dtype=np.int64), d] = False
                 self.RGC[b._constraint_index][torch.as_tensor(np.asarray(b.index_nodes, dtype=np.int64)), d] = 0.0
@@ -187,12 +241,12 @@ class Assembly:
         off = 0
         for name, ins in self._instances.items():
             self._node_offset[name] = off
-            R = ins.rotation_matrix
-            if not torch.equal(R, torch.eye(3, dtype=torch.float64)):
-                raise NotImplementedError("rotated instances are outside the B200 element path")
-            X.append(ins.part.nodes.to(torch.float64).cpu())
+            X.append(self._element_frame_nodes(ins))
             Xi.append(ins.nodes.to(torch.float64).cpu())
-            rem = self.RGC_remain_index[ins._RGC_index]
+            rem = self.RGC_remain_index[ins._RGC_index].copy()
+            for c in self._constraints.values():      # tied nodes stay rows of the plan
+                if c._couple_index == ins._RGC_index:
+                    rem[c._indexNodes] = True
             masks.append((rem[:, 0] * 1 + rem[:, 1] * 2 + rem[:, 2] * 4).astype(np.uint8))
             for e in ins.part.elems.values():
                 if e.materials is None:
@@ -206,9 +260,38 @@ class Assembly:
                 faces.append((s.kind, s._elems.numpy() + o))
                 self._face_loads.append(ld)
         self._mat_elems = mats
-        self._plan = DevicePlan(torch.cat(X), np.concatenate(masks), groups, faces, device=self.device)
+        plan_mask = np.concatenate(masks)
+        self._plan = DevicePlan(torch.cat(X), plan_mask, groups, faces, device=self.device)
         self._Xinst = torch.cat(Xi).to(self.device).contiguous()
         self._energy_buf = torch.zeros(1, dtype=torch.float64, device=self.device)
+        self._system = None
+        if self._constraints:
+            tied = []
+            for c in self._constraints.values():
+                name = next(k for k, v in self._instances.items() if v._RGC_index == c._couple_index)
+                tied.append((c, c._indexNodes + self._node_offset[name], c.rp_name))
+            self._system = CoupledSystem(self, plan_mask, tied)
+        elif self._reference_points:
+            raise NotImplementedError("reference points without a Couple constraint are outside the B200 path")
+
+    @property
+    def system(self):
+        """The reduced linear system the solvers see (CSR, PCG): the plan
+        itself, or the system condensed onto reference points when nodes are
+        tied to them."""
+        return self._system if self._system is not None else self.plan
+
+    @staticmethod
+    def _element_frame_nodes(ins):
+        """Coordinates the element kernels of an instance use: the part's
+        nodes, rotated by the instance's rotation when it has one.  With the
+        instance's displacement (assembly frame) this gives the reference's
+        rotated element outputs R R_e, R K_e R^T (C3base.py:417-418,
+        441-443) for the isotropic material; translation does not enter the
+        element arithmetic."""
+        X = ins.part.nodes.to(torch.float64).cpu()
+        R = ins.rotation_matrix.to(torch.float64).cpu()
+        return X if torch.equal(R, torch.eye(3, dtype=torch.float64)) else X @ R.T
 
     @property
     def plan(self) -> DevicePlan:
@@ -220,8 +303,11 @@ class Assembly:
     def _GC2RGC(self, GC):
         full = torch.zeros(self.RGC_list_indexStart[-1], dtype=torch.float64, device=self.device)
         full[self._remain_dev] = GC.to(self.device, torch.float64)
-        return [full[self.RGC_list_indexStart[i]:self.RGC_list_indexStart[i + 1]].view(self._RGC_size[i])
-                for i in range(len(self._RGC_size))]
+        RGC = [full[self.RGC_list_indexStart[i]:self.RGC_list_indexStart[i + 1]].view(self._RGC_size[i])
+               for i in range(len(self._RGC_size))]
+        for c in self._constraints.values():      # tied nodes follow their points (couple.py:34-40)
+            RGC = c.modify_RGC(RGC)
+        return RGC
 
     def _RGC2GC(self, RGC):
         return torch.cat([RGC[i].reshape(-1)[torch.from_numpy(self.RGC_remain_index[i].reshape(-1)).to(RGC[i].device)]
@@ -241,8 +327,24 @@ class Assembly:
             return self._assemble_csr(GC, want_K, K, R)
 
     def _assemble_csr(self, GC, want_K, K, R):
+        if self._system is not None:
+            S = self._system
+            gc = self._gc(GC=GC)
+            mot = S.motions(gc)
+            Rp, Kp = self._assemble_plan(S.plan_gc(gc, mot), want_K, None, None)
+            Rr, Kr = S.condense(gc, Rp, Kp, mot)
+            if R is not None:
+                R.copy_(Rr)
+                Rr = R
+            if K is not None and Kr is not None:
+                K.copy_(Kr)
+                Kr = K
+            return Rr, Kr
+        return self._assemble_plan(self._gc(GC=GC), want_K, K, R)
+
+    def _assemble_plan(self, gc, want_K, K, R):
+        """R and K of the plan's rows at the plan displacement gc."""
         P = self.plan
-        gc = self._gc(GC=GC)
         R = P.zeros(P.ndof) if R is None else R
         if want_K and K is None:
             K = torch.empty(P.nnz, dtype=torch.float64, device=P.device)
@@ -265,7 +367,7 @@ class Assembly:
         """(R [n], K_indices int64 [2,nnz], K_values [nnz]) in reduced numbering
         (assembly.py:283-309)."""
         R, K = self.assemble_csr(self._gc(RGC, GC))
-        return R, self.plan.coo_indices(), K
+        return R, self.system.coo_indices(), K
 
     def assemble_force(self, RGC=None, GC=None):
         """Reduced residual R [n] (assembly.py:230-281)."""
@@ -276,6 +378,16 @@ class Assembly:
         P = self.plan
         gc = self._gc(RGC, GC)
         total = torch.zeros((), dtype=torch.float64, device=self.device)
+        if self._system is not None:
+            S = self._system
+            gcr = gc
+            gc = S.plan_gc(gcr)
+            f = S.point_loads()
+            for name, rp, keep, b0 in S.points:
+                if name in f:
+                    q = torch.zeros(6, dtype=torch.float64, device=self.device)
+                    q[torch.as_tensor(keep, device=self.device)] = gcr[b0:b0 + keep.shape[0]]
+                    total = total - (f[name] * q).sum()
         for gi, e in enumerate(self._mat_elems):
             mu, kappa = e.materials.parameters()
             P.energy_volume(gi, mu, kappa, gc, self._energy_buf)
@@ -287,6 +399,8 @@ class Assembly:
 
     # -- dynamics (assembly.py:187-206, 421-443) -----------------------------------
     def initialize_dynamic(self):
+        if self._system is not None:
+            raise NotImplementedError("dynamics with reference points are outside the B200 path")
         rhos = [float(e.density) for e in self._mat_elems]
         self._minv = self.plan.lumped_mass_inv(rhos)
         self._mass_values = self.plan.mass_csr(rhos)

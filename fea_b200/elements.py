@@ -85,6 +85,7 @@ class Element_3D(BaseElement):
     def __init__(self, elems=None, elems_index=None, part=None) -> None:
         super().__init__(elems_index=elems_index, elems=elems, part=part)
         self._plan = None
+        self._frame = None
 
     def initialize(self, *args, **kwargs):
         if self._elems.shape[1] != self.num_nodes_per_elem:
@@ -93,6 +94,7 @@ class Element_3D(BaseElement):
         el = self._elems.T
         self._indices_force_cpu = (3 * el[:, None, :] + torch.arange(3)[None, :, None]).reshape(-1)
         self._plan = None
+        self._frame = None
 
     # -- per-group plan (all DOFs of the group's nodes active) ---------------
     def _group_plan(self):
@@ -102,6 +104,7 @@ class Element_3D(BaseElement):
             mask = np.zeros(N, np.uint8)
             mask[np.unique(self._elems.numpy())] = 7
             self._plan = DevicePlan(self.part.nodes, mask, [(self.kind, self._elems.numpy())])
+            self._frame = None
             free = torch.from_numpy(np.repeat(mask != 0, 3))
             self._free = free.to(self._plan.device)
             self._dof_map = torch.nonzero(free).flatten().to(self._plan.device)
@@ -115,21 +118,44 @@ class Element_3D(BaseElement):
         return U.reshape(-1)[self._free].contiguous()
 
     @staticmethod
-    def _check_rotation(rotation_matrix):
-        if rotation_matrix is not None:
-            R = torch.as_tensor(rotation_matrix, dtype=torch.float64).cpu()
-            if not torch.equal(R, torch.eye(3, dtype=torch.float64)):
-                raise NotImplementedError("rotated instances are outside the B200 element path")
+    def _frame_key(rotation_matrix):
+        """None for the part's own frame (no rotation or the identity), else
+        the rotation as a float64 CPU tensor."""
+        if rotation_matrix is None:
+            return None
+        R = torch.as_tensor(rotation_matrix, dtype=torch.float64).detach().cpu()
+        if tuple(R.shape) != (3, 3):
+            raise ValueError("rotation_matrix must be 3 x 3")
+        return None if torch.equal(R, torch.eye(3, dtype=torch.float64)) else R
+
+    def _framed_plan(self, rotation_matrix=None):
+        """The group plan with its coordinates in the frame of
+        ``rotation_matrix``: the part's nodes X rotated to R X.  An isotropic
+        element evaluated on R X with the instance's (global) displacement
+        gives R R_e and R K_e R^T of the part frame, which is what the
+        reference computes by rotating U in and R_e, K_e out
+        (C3base.py:417-418, 441-443)."""
+        P = self._group_plan()
+        key = self._frame_key(rotation_matrix)
+        cur = self._frame
+        if (cur is None) != (key is None) or (key is not None and not torch.equal(cur, key)):
+            X = self.part.nodes.to(torch.float64).cpu()
+            if key is not None:
+                X = X @ key.T
+            P.X.copy_(X.to(P.device))
+            self._frame = key
+        return P
 
     def structural_Force(self, RGC, rotation_matrix=None, if_onlyforce: bool = False, *args, **kwargs):
         """Element residual (and tangent) of the group (C3base.py:413-452).
 
         Returns (indices_force, R_e[(a,j,e)]) or, with the tangent,
         (indices_force, R_e, indices_matrix [2,nnz_e], values [nnz_e]) where
-        indices_matrix is the sorted unique DOF-pair COO of the group.
+        indices_matrix is the sorted unique DOF-pair COO of the group.  With
+        a rotation matrix R (the instance's), RGC is the displacement in the
+        instance frame and the outputs are R R_e and R K_e R^T.
         """
-        self._check_rotation(rotation_matrix)
-        P = self._group_plan()
+        P = self._framed_plan(rotation_matrix)
         mu, kappa = self.materials.parameters()
         gc = self._gc(RGC)
         elemR = P.zeros(self.num_nodes_per_elem * 3 * self._elems.shape[0])
@@ -141,12 +167,22 @@ class Element_3D(BaseElement):
         return self._indices_force, elemR, self._indices_matrix, K
 
     def potential_Energy(self, RGC):
-        """sum_{g,e} W(F) w  (C3base.py:387-411) as a 0-d device tensor."""
-        P = self._group_plan()
+        """sum_{g,e} W(F) w  (C3base.py:387-411) as a 0-d device tensor;
+        RGC is the displacement in the part's own frame."""
+        P = self._framed_plan(None)
         mu, kappa = self.materials.parameters()
         out = P.zeros(1)
         P.energy_volume(0, mu, kappa, self._gc(RGC), out)
         return out[0]
+
+    def get_mass_matrix(self, rotation_matrix=None):
+        """(indices_matrix [2, nnz_e], values [nnz_e]): the consistent mass
+        rho N_a N_b w times the 3 x 3 identity of every element on the
+        group's pattern (C3base.py:348-384).  R M R^T = M for this isotropic
+        mass, so a rotation leaves the values unchanged."""
+        self._frame_key(rotation_matrix)
+        P = self._framed_plan(None)
+        return self._indices_matrix, P.mass_csr([float(self.density)])
 
     def get_volumn(self, U=None):
         raise NotImplementedError("element volume queries are outside the B200 path")

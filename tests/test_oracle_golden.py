@@ -183,3 +183,75 @@ def test_newmark_run(golden, name):
         assert rel(GC[k], g["GC"][k]) < 1e-10 or np.abs(g["GC"][k]).max() < 1e-15
         assert rel(GV[k], g["GV"][k]) < 1e-10 or np.abs(g["GV"][k]).max() < 1e-15
         assert rel(GA[k], g["GA"][k]) < 1e-10
+
+
+def rotated_model(g):
+    """Two instances of the rot_hex3 part as one oracle model: instance a at
+    the part's nodes, instance b at R X + t (elements and pressure faces of
+    b shifted by the part's node count)."""
+    X = torch.from_numpy(g["X"])
+    el = torch.from_numpy(g["elems"])
+    R = torch.from_numpy(g["rotation_matrix"])
+    Xb = X @ R.T + torch.from_numpy(g["translation"])
+    N = X.shape[0]
+    end = torch.from_numpy(g["end_elems"])
+    fa = el[end][:, [1, 2, 6, 5]]
+    mu, kappa, p = float(g["mu"]), float(g["kappa"]), float(g["p"])
+    return O.Model(torch.cat([X, Xb]), [O.Group("C3D8", el, mu, kappa), O.Group("C3D8", el + N, mu, kappa)],
+                   [O.PressureLoad(fa, p), O.PressureLoad(fa + N, p)],
+                   [(g["fixed"], (0, 1, 2)), (g["fixed"] + N, (0, 1, 2))])
+
+
+def test_rotated_instances_as_assembly_frame_coordinates(golden):
+    """A rotated, translated instance evaluated on R X + t with the
+    assembly-frame displacement gives the reference's rotated element
+    outputs: reduced R, K and energy of the two-instance model."""
+    g = golden("rot_hex3")
+    m = rotated_model(g)
+    state = torch.from_numpy(g["state"])
+    R, (ip, ix, v) = m.assemble(state)
+    np.testing.assert_array_equal(ip.numpy(), g["indptr"])
+    np.testing.assert_array_equal(ix.numpy(), g["indices"])
+    assert rel(R, g["R"]) < 1e-13 and rel(v, g["values"]) < 1e-13
+    assert abs(float(m.energy(state)) - float(g["energy"])) <= 1e-13 * abs(float(g["energy"]))
+    Rc, _ = m.assemble(torch.from_numpy(g["gc_converged"]), want_K=False)
+    assert float(Rc.abs().max()) < 1e-12
+
+
+def test_explicit_with_pressure_and_two_groups(golden):
+    g = golden("explicit_loaded")
+    X = torch.from_numpy(g["X"])
+    (mu0, k0), (mu1, k1) = g["mats"]
+    rho = float(g["rho"])
+    m = O.Model(X, [O.Group("C3D4", torch.from_numpy(g["elems0"]), float(mu0), float(k0), rho),
+                    O.Group("C3D4", torch.from_numpy(g["elems1"]), float(mu1), float(k1), rho)],
+                [O.PressureLoad(torch.from_numpy(g["pressure_faces"]), float(g["p"]))], [(g["fixed"], (0, 1, 2))])
+    assert rel(m.lumped_mass_inv(), g["minv"]) < 1e-14
+    gv0 = torch.from_numpy(g["gv0"])
+    u, v, a = O.explicit_run(m, torch.zeros_like(gv0), gv0, float(g["dt"]), int(g["steps"]))
+    assert rel(u, g["u_final"]) < 1e-12 and rel(v, g["v_final"]) < 1e-12 and rel(a, g["a_final"]) < 1e-12
+
+
+def couple_model(g):
+    X = torch.from_numpy(g["X"])
+    el = torch.from_numpy(g["elems"])
+    base = O.Model(X, [O.Group("C3D8", el, float(g["mu"]), float(g["kappa"]))], [], [(g["fixed"], (0, 1, 2))])
+    return O.CoupledModel(base, g["top"], torch.from_numpy(g["rp"]), torch.from_numpy(g["force"]),
+                          torch.from_numpy(g["moment"]))
+
+
+def test_couple_constraint_vs_reference(golden):
+    """Tied nodes following a reference point (Couple), with a force and a
+    moment on the point: reduced R, K and energy at a state with a finite
+    rotation, and the reference's converged solution in equilibrium."""
+    g = golden("couple_hex3")
+    m = couple_model(g)
+    state = torch.from_numpy(g["state"])
+    np.testing.assert_allclose(m.node_u(state).numpy(), g["rgc_state"][:3 * g["X"].shape[0]], rtol=0, atol=1e-15)
+    R, (ip, ix, v) = m.assemble(state)
+    np.testing.assert_array_equal(ip.numpy(), g["indptr"])
+    np.testing.assert_array_equal(ix.numpy(), g["indices"])
+    assert rel(R, g["R"]) < 1e-13 and rel(v, g["values"]) < 1e-13
+    assert abs(float(m.energy(state)) - float(g["energy"])) <= 1e-13 * abs(float(g["energy"]))
+    Rc, _ = m.assemble(torch.from_numpy(g["gc_converged"]))
+    assert float(Rc.abs().max()) < 1e-12
