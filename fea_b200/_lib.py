@@ -125,6 +125,7 @@ fea_pcgb_iterate = _sig("fea_pcgb_iterate", I32, P, I32, I64, I32, P)
 fea_pcgb_state = _sig("fea_pcgb_state", I32, P, I32, I64, I32, P, P)
 fea_explicit_work_len = _sig("fea_explicit_work_len", I64, I64)
 fea_explicit_run = _sig("fea_explicit_run", I32, NP, GP, D, D, P, D, I64, I32, I32, P, P, P, P, P, I64, P)
+fea_explicit_stage = _sig("fea_explicit_stage", I32, I64, I32, D, P, P, P, P, P, P, P, P)
 fea_adjoint_vjp_volume = _sig("fea_adjoint_vjp_volume", I32, NP, GP, D, D, P, P, P, P, P, I64, P)
 fea_adjoint_hvp_pressure = _sig("fea_adjoint_hvp_pressure", I32, NP, GP, D, P, P, P, P, P)
 fea_version = _sig("fea_version", I32)
@@ -135,5 +136,5 @@ EXPORTED = ["fea_plan_build", "fea_plan_free", "fea_plan_get", "fea_assemble_wor
             "fea_reduce_scratch_len", "fea_energy_volume", "fea_energy_volume_noalloc", "fea_energy_pressure", "fea_lumped_mass",
             "fea_invert_mass", "fea_mass_csr", "fea_axpy", "fea_pcg_work_len", "fea_pcg_solve", "fea_pcg_mixed_work_len",
             "fea_pcg_solve_mixed", "fea_spmv", "fea_spmv_nodes", "fea_pcg_solve_nodes", "fea_pcg_solve_mixed_nodes", "fea_convert_f32", "fea_pcgb_work_len", "fea_pcgb_table_bytes", "fea_pcgb_set", "fea_pcgb_start",
-            "fea_pcgb_iterate", "fea_pcgb_state", "fea_explicit_work_len", "fea_explicit_run",
+            "fea_pcgb_iterate", "fea_pcgb_state", "fea_explicit_work_len", "fea_explicit_run", "fea_explicit_stage",
             "fea_adjoint_vjp_volume", "fea_adjoint_hvp_pressure", "fea_version", "fea_launch_count"]

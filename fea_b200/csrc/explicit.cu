@@ -170,9 +170,51 @@ __global__ void __launch_bounds__(128) k_explicit(ExParams P, int flags) {
   }
 }
 
+// One stage of the central-difference loop around a separately assembled
+// residual (several element groups, loads): see fea_explicit_stage.
+__global__ void __launch_bounds__(256) k_explicit_stage(int64_t n, int32_t stage, double dt,
+                                                        const double* __restrict__ minv,
+                                                        const double* __restrict__ R, double* __restrict__ u,
+                                                        double* __restrict__ vh, double* __restrict__ vhp,
+                                                        double* __restrict__ a, double* __restrict__ v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (stage == 0) {                       // before the force pass
+      const double h = vh[i];
+      const double hn = h + dt * a[i];
+      vhp[i] = h;
+      vh[i] = hn;
+      u[i] = u[i] + dt * hn;
+    } else if (stage == 1) {                // after it
+      a[i] = -minv[i] * R[i];
+      v[i] = 0.5 * (vh[i] + vhp[i]);
+    } else {                                // start: a_0 and vh_{-1/2}
+      const double ai = -minv[i] * R[i];
+      a[i] = ai;
+      vh[i] = v[i] - 0.5 * dt * ai;
+    }
+  }
+}
+
 }  // namespace fea
 
 using namespace fea;
+
+extern "C" int fea_explicit_stage(int64_t n, int32_t stage, double dt, const double* minv, const double* R,
+                                  double* u, double* vh, double* vhp, double* a, double* v, cudaStream_t st) {
+  if (n < 0 || stage < 0 || stage > 2 || !minv || !vh || !a) return FEA_EINVAL;
+  if (stage == 0 && (!u || !vhp)) return FEA_EINVAL;
+  if (stage >= 1 && !R) return FEA_EINVAL;
+  if ((stage == 1 && (!vhp || !v)) || (stage == 2 && !v)) return FEA_EINVAL;
+  if (n == 0) return FEA_OK;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t want = (n + 255) / 256;
+  const int grid = (int)(want < 8LL * sms ? want : 8LL * sms);
+  k_explicit_stage<<<grid, 256, 0, st>>>(n, stage, dt, minv, R, u, vh, vhp, a, v);
+  count_launch();
+  return (int)cudaGetLastError();
+}
 
 extern "C" int64_t fea_explicit_work_len(int64_t ndof) { return ndof; }
 

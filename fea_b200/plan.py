@@ -321,6 +321,12 @@ class DevicePlan:
         L.check(L.fea_convert_f32(values.numel(), vptr(values), vptr(out), stream()), "fea_convert_f32")
         return out
 
+    def explicit_stage(self, stage, dt, minv, R, u, vh, vhp, a, v):
+        """One stage of the central-difference step around an assembled
+        residual R (fea_explicit_stage); unused arguments may be None."""
+        L.check(L.fea_explicit_stage(self.ndof, int(stage), float(dt), vptr(minv), vptr(R), vptr(u), vptr(vh),
+                                     vptr(vhp), vptr(a), vptr(v), stream()), "fea_explicit_stage")
+
     def explicit_run(self, gi, mu, kappa, minv, dt, steps, u, vh, a, v, fp32=False, init=False):
         w = self.scratch(L.fea_explicit_work_len(self.ndof))
         L.check(L.fea_explicit_run(C.byref(self.nodes), C.byref(self.groups[gi].desc), float(mu), float(kappa),

@@ -232,7 +232,7 @@ class StaticImplicitSolver(BaseSolver):
             self._run_linear_inner(req)
 
     def _run_linear_inner(self, req):
-        P = self.assembly.plan
+        P = self.assembly.system
         if self.precision == "mixed":
             v32 = P.to_f32(req.K)
             req.it, outer, req.rr, req.status = P.pcg_mixed(req.K, v32, req.b, req.x, req.tol, 1e-4, req.cap,
@@ -252,12 +252,11 @@ class StaticImplicitSolver(BaseSolver):
         return x
 
     def _scaled_rmax(self, K_values, R):
-        P = self.assembly.plan
         diag = self._diag(K_values)
         return float((R / diag.abs().sqrt().clamp_min(1e-300)).abs().max()) if R.numel() else 0.0
 
     def _diag(self, K_values):
-        P = self.assembly.plan
+        P = self.assembly.system
         if not hasattr(self, "_diag_pos") or self._diag_pos.numel() != P.ndof:
             rows = P.coo_indices()
             self._diag_pos = torch.nonzero(rows[0] == rows[1]).flatten()
@@ -523,22 +522,27 @@ class DynamicExplicitSolver(BaseSolver):
         c = math.sqrt((kappa + 4 * mu / 3) / float(e.density))
         return factor * hmin / c
 
-    def _group(self):
+    def _fused_group(self):
+        """(group, (mu, kappa)) when one fused launch per step covers the
+        model (one element group, no loads), else None."""
         es = self.assembly._mat_elems
         if len(es) != 1 or self.assembly._face_loads:
-            raise NotImplementedError("the fused explicit kernel covers one element group without loads")
+            return None
         return 0, es[0].materials.parameters()
 
     def solve(self, GC0=None, GV0=None, *args, **kwargs):
         A = self.assembly
         P = A.plan
-        gi, (mu, kappa) = self._group()
         dt = float(self._deltaT)
         u = (A.GC.clone() if GC0 is None else A._gc(GC=GC0).clone()).contiguous()
         v = (torch.zeros_like(u) if GV0 is None else A._gc(GC=GV0).clone()).contiguous()
         vh = torch.empty_like(u)
         a = torch.empty_like(u)
         minv = A.lumped_mass_inv()
+        fused = self._fused_group()
+        if fused is None:
+            return self._solve_assembled(u, v, vh, a, minv, dt)
+        gi, (mu, kappa) = fused
         # a_0 and vh_{-1/2} (dynamic_explicit.py:80-91)
         P.explicit_run(gi, mu, kappa, minv, dt, 0, u, vh, a, v, fp32=self.fp32, init=True)
         self._GC_list.append(u.clone())
@@ -560,6 +564,39 @@ class DynamicExplicitSolver(BaseSolver):
                 self._next_storage_time += self._time_per_storage
         if pending:
             P.explicit_run(gi, mu, kappa, minv, dt, pending, u, vh, a, v, fp32=self.fp32, init=False)
+        self.GC = u
+        self.GV, self.GA, self.GV_half = v, a, vh
+        return True
+
+    def _solve_assembled(self, u, v, vh, a, minv, dt):
+        """The reference's loop for several element groups and loads
+        (dynamic_explicit.py:80-134): each step the residual of every group
+        and load is assembled by the residual kernels (assemble_force) between
+        the two stages of fea_explicit_stage."""
+        if self.fp32:
+            raise NotImplementedError("the FP32 element force covers the fused one-group path")
+        A = self.assembly
+        P = A.plan
+        R = torch.empty_like(u)
+        vhp = torch.empty_like(u)
+        A.assemble_csr(u, want_K=False, R=R)
+        P.explicit_stage(2, dt, minv, R, None, vh, None, a, v)
+        self._GC_list.append(u.clone())
+        self._GV_list.append(v.clone())
+        self._GA_list.append(a.clone())
+        self._time_list.append(0.0)
+        current_time = 0.0
+        while current_time < self._time_end:
+            P.explicit_stage(0, dt, minv, None, u, vh, vhp, a, None)
+            A.assemble_csr(u, want_K=False, R=R)
+            P.explicit_stage(1, dt, minv, R, None, vh, vhp, a, v)
+            current_time += dt
+            if current_time >= self._next_storage_time or current_time >= self._time_end:
+                self._GC_list.append(u.clone())
+                self._GV_list.append(v.clone())
+                self._GA_list.append(a.clone())
+                self._time_list.append(current_time)
+                self._next_storage_time += self._time_per_storage
         self.GC = u
         self.GV, self.GA, self.GV_half = v, a, vh
         return True

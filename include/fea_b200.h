@@ -389,6 +389,17 @@ int fea_convert_f32(int64_t nnz, const double* values_dev, float* values32_dev, 
  * work_dev: fea_explicit_work_len(ndof) doubles (second u buffer).
  * ------------------------------------------------------------------------- */
 int64_t fea_explicit_work_len(int64_t ndof);
+
+/* One stage of the same central-difference step around a residual R that
+ * the caller assembles (all element groups and loads: the reference's
+ * assemble_force call inside its loop, dynamic_explicit.py:80-117), n reduced DOFs:
+ *   stage 0 (before the force pass): vhp = vh; vh += dt a; u += dt vh
+ *   stage 1 (R = reduced residual at u): a = -minv R; v = (vh + vhp)/2
+ *   stage 2 (start, R at u_0, v = v_0): a = -minv R; vh = v - dt/2 a
+ * Pointers not used by a stage may be null. */
+int fea_explicit_stage(int64_t n, int32_t stage, double dt, const double* minv_dev, const double* R_dev,
+                       double* u_dev, double* vh_dev, double* vhp_dev, double* a_dev, double* v_dev,
+                       cudaStream_t stream);
 int fea_explicit_run(const fea_nodes_t* nodes, const fea_group_t* group, double mu, double kappa,
                      const double* minv_dev, double dt, int64_t steps, int32_t fp32, int32_t init,
                      double* u_dev, double* vh_dev, double* a_dev, double* v_dev,
