@@ -6,13 +6,14 @@ in-tree by ``python -m fea_b200._build``.  Importing the package loads the
 library and raises ImportError when it is missing; there is no fallback.
 """
 from . import _lib  # noqa: F401  (loads the native library or raises)
-from . import materials, elements, loads, boundarys
+from . import materials, elements, loads, boundarys, constraints
 from .part import Part, Instance
+from .reference_points import ReferencePoint
 from .assembly import Assembly
 from .controller import FEAController
 from . import solver
 from .plan import DevicePlan
 from .inp import FEA_INP, from_inp
 
-__all__ = ["Part", "Instance", "Assembly", "FEAController", "materials", "elements", "loads", "boundarys",
-           "solver", "DevicePlan", "FEA_INP", "from_inp"]
+__all__ = ["Part", "Instance", "ReferencePoint", "Assembly", "FEAController", "materials", "elements", "loads",
+           "boundarys", "constraints", "solver", "DevicePlan", "FEA_INP", "from_inp"]

@@ -28,3 +28,17 @@ class Boundary_Condition(BaseBoundary):
         inst = assembly.get_instance(self.instance_name)
         self.index_nodes = inst.set_nodes[self.set_nodes_name]
         self._constraint_index = inst._RGC_index
+
+
+class Boundary_Condition_RP(BaseBoundary):
+    """Fix DOFs `indexDoF` (0-2 translation, 3-5 rotation) of a reference
+    point to zero (boundary_condition_rp.py:5-32)."""
+
+    def __init__(self, rp_name: str, indexDoF=(0, 1, 2, 3, 4, 5)) -> None:
+        super().__init__()
+        self.rp_name = rp_name
+        self.indexDoF = list(indexDoF)
+
+    def initialize(self, assembly):
+        super().initialize(assembly)
+        self._constraint_index = assembly.get_reference_point(self.rp_name)._RGC_index

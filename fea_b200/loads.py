@@ -1,5 +1,9 @@
-"""Loads on the B200 path: the follower pressure (FEA/assemble/loads/pressure.py)."""
+"""Loads on the B200 path: the follower pressure (FEA/assemble/loads/pressure.py)
+and the concentrated force and moment on a reference point
+(concentrate_force.py, moment.py)."""
 from __future__ import annotations
+
+import torch
 
 
 class BaseLoad:
@@ -36,3 +40,56 @@ class Pressure(BaseLoad):
         inst = assembly.get_instance(self.instance_name)
         self.surface_element = inst.extract_surfaces(self.surface_name)
         self._load_index = inst._RGC_index
+
+
+class _PointLoad(BaseLoad):
+    """A constant generalized force on three DOFs of a reference point."""
+
+    _offset = 0
+
+    def __init__(self, rp_name: str, value) -> None:
+        super().__init__()
+        self.rp_name = rp_name
+        self._value = torch.as_tensor(value, dtype=torch.float64).reshape(3)
+
+    def initialize(self, assembly):
+        super().initialize(assembly)
+        self.rp_index = assembly.get_reference_point(self.rp_name)._RGC_index
+
+    def set_required_DoFs(self, RGC_remain_index):
+        RGC_remain_index[self.rp_index][self._offset:self._offset + 3] = True
+        return RGC_remain_index
+
+
+class Concentrate_Force(_PointLoad):
+    """Force on a reference point's translation DOFs (concentrate_force.py:5-55):
+    it adds -force to their residual and -force . v to the total potential."""
+
+    def __init__(self, rp_name: str, force) -> None:
+        super().__init__(rp_name, force)
+
+    @property
+    def force(self):
+        return self._value
+
+    @force.setter
+    def force(self, value):
+        self._value = torch.as_tensor(value, dtype=torch.float64).reshape(3)
+
+
+class Moment(_PointLoad):
+    """Moment on a reference point's rotation DOFs (moment.py:5-55): it adds
+    -moment to their residual and -moment . z to the total potential."""
+
+    _offset = 3
+
+    def __init__(self, rp_name: str, moment) -> None:
+        super().__init__(rp_name, moment)
+
+    @property
+    def moment(self):
+        return self._value
+
+    @moment.setter
+    def moment(self, value):
+        self._value = torch.as_tensor(value, dtype=torch.float64).reshape(3)
