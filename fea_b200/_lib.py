@@ -126,6 +126,14 @@ fea_pcgb_state = _sig("fea_pcgb_state", I32, P, I32, I64, I32, P, P)
 fea_explicit_work_len = _sig("fea_explicit_work_len", I64, I64)
 fea_explicit_run = _sig("fea_explicit_run", I32, NP, GP, D, D, P, D, I64, I32, I32, P, P, P, P, P, I64, P)
 fea_explicit_stage = _sig("fea_explicit_stage", I32, I64, I32, D, P, P, P, P, P, P, P, P)
+fea_ls_ladder_len = _sig("fea_ls_ladder_len", I32)
+fea_ls_scratch_len = _sig("fea_ls_scratch_len", I64, I64)
+fea_ls_prepare = _sig("fea_ls_prepare", I32, I64, P, P, P, P, P, I64, P)
+fea_ls_energy_volume = _sig("fea_ls_energy_volume", I32, NP, GP, D, D, P, P, P, I32, I32, P, P, I64, P)
+fea_ls_energy_pressure = _sig("fea_ls_energy_pressure", I32, NP, GP, D, P, P, P, P, I32, I32, P, P, I64, P)
+fea_ls_select = _sig("fea_ls_select", I32, I64, P, I32, D, D, P, P, P, P)
+FEA_LS_M, FEA_LS_NSTATE = 8, 8
+(FEA_LS_DE, FEA_LS_E0, FEA_LS_SMAX, FEA_LS_SIGN, FEA_LS_ALPHA, FEA_LS_ENEW, FEA_LS_FOUND, FEA_LS_ROUND) = range(8)
 fea_adjoint_vjp_volume = _sig("fea_adjoint_vjp_volume", I32, NP, GP, D, D, P, P, P, P, P, I64, P)
 fea_adjoint_hvp_pressure = _sig("fea_adjoint_hvp_pressure", I32, NP, GP, D, P, P, P, P, P)
 fea_version = _sig("fea_version", I32)
@@ -137,4 +145,6 @@ EXPORTED = ["fea_plan_build", "fea_plan_free", "fea_plan_get", "fea_assemble_wor
             "fea_invert_mass", "fea_mass_csr", "fea_axpy", "fea_pcg_work_len", "fea_pcg_solve", "fea_pcg_mixed_work_len",
             "fea_pcg_solve_mixed", "fea_spmv", "fea_spmv_nodes", "fea_pcg_solve_nodes", "fea_pcg_solve_mixed_nodes", "fea_convert_f32", "fea_pcgb_work_len", "fea_pcgb_table_bytes", "fea_pcgb_set", "fea_pcgb_start",
             "fea_pcgb_iterate", "fea_pcgb_state", "fea_explicit_work_len", "fea_explicit_run", "fea_explicit_stage",
-            "fea_adjoint_vjp_volume", "fea_adjoint_hvp_pressure", "fea_version", "fea_launch_count"]
+            "fea_adjoint_vjp_volume", "fea_adjoint_hvp_pressure", "fea_version", "fea_launch_count",
+            "fea_ls_ladder_len", "fea_ls_scratch_len", "fea_ls_prepare", "fea_ls_energy_volume",
+            "fea_ls_energy_pressure", "fea_ls_select"]

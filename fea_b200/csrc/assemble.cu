@@ -21,6 +21,7 @@
 // contraction sum_il C_ijkl g_ai g_bl equals
 //   (alpha f_a + beta q_a)_j q_bk + alpha q_aj f_bk + gamma q_ak q_bj
 //   + mu J^-2/3 (g_a . g_b) delta_jk.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -948,6 +949,229 @@ __global__ void __launch_bounds__(256) k_face_volume(FaceParams P, double* parti
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
+// ---- device line search -----------------------------------------------------
+// The Armijo backtracking of the Newton solver (static_implicit.py:97-169)
+// with its trial energies evaluated on the device: a ladder of LS_M trial
+// steps alpha_k = 2^-(k0 + k) per launch, every element (and pressure face)
+// evaluated at all of them in one pass, and the first step that passes the
+// test selected and applied on the device.  The state vector (LS_*) carries
+// the directional derivative, the energy at the current point, the largest
+// step component, the direction's sign and the outcome.
+constexpr int LS_M = 8;
+enum { LS_DE = 0, LS_E0, LS_SMAX, LS_SIGN, LS_ALPHA, LS_ENEW, LS_FOUND, LS_ROUND, LS_NSTATE };
+
+template <int NN>
+__global__ void __launch_bounds__(128) k_vol_energy_ladder(VolParams P, const double* __restrict__ dgc,
+                                                           const double* __restrict__ state, int k0,
+                                                           double* __restrict__ partial, int64_t nb) {
+  __shared__ double sh[128];
+  const int64_t e = (int64_t)blockIdx.x * 128 + threadIdx.x;
+  double acc[LS_M];
+#pragma unroll
+  for (int k = 0; k < LS_M; ++k) acc[k] = 0.0;
+  if (e < P.ne) {
+    int32_t cn[NN];
+    unsigned mk[NN];
+    int32_t rd[NN];
+#pragma unroll
+    for (int b = 0; b < NN; ++b) {
+      cn[b] = P.conn[e * NN + b];
+      mk[b] = P.mask[cn[b]];
+      rd[b] = P.rdof[cn[b]];
+    }
+    const double sgn = state[LS_SIGN];
+#pragma unroll 1
+    for (int g = 0; g < Elem<NN>::NG; ++g) {
+      double J0[9], Ju[9], Jd[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) J0[i] = Ju[i] = Jd[i] = 0.0;
+#pragma unroll
+      for (int b = 0; b < NN; ++b) {
+        const double* xb = P.X + 3 * (int64_t)cn[b];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const double x = __ldg(xb + i), u = node_u(P.gc, rd[b], mk[b], i), du = node_u(dgc, rd[b], mk[b], i);
+#pragma unroll
+          for (int m = 0; m < 3; ++m) {
+            const double d = Elem<NN>::dxi(g, b, m);
+            J0[3 * i + m] += x * d;
+            Ju[3 * i + m] += u * d;
+            Jd[3 * i + m] += du * d;
+          }
+        }
+      }
+      double iJ[9];
+      const double w = inv3(J0, iJ) * Elem<NN>::wq(g);
+      double Gu[9], Gd[9];
+#pragma unroll
+      for (int I = 0; I < 3; ++I)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          Gu[3 * I + i] = (I == i ? 1.0 : 0.0) + Ju[3 * I] * iJ[i] + Ju[3 * I + 1] * iJ[3 + i] + Ju[3 * I + 2] * iJ[6 + i];
+          Gd[3 * I + i] = Jd[3 * I] * iJ[i] + Jd[3 * I + 1] * iJ[3 + i] + Jd[3 * I + 2] * iJ[6 + i];
+        }
+#pragma unroll
+      for (int k = 0; k < LS_M; ++k) {
+        const double a = sgn * ldexp(1.0, -(k0 + k));
+        double F[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) F[i] = Gu[i] + a * Gd[i];
+        const double J = det3(F);
+        double sF2 = 0.0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];
+        const double I1 = sF2 * jm23(J);
+        acc[k] += (P.mu / 2.0 * (I1 - 3.0) + P.kappa / 2.0 * (J - 1.0) * (J - 1.0)) * w;
+      }
+    }
+  }
+#pragma unroll 1
+  for (int k = 0; k < LS_M; ++k) {
+    const double s = block_sum<128>(acc[k], sh);
+    if (threadIdx.x == 0) partial[k * nb + blockIdx.x] = s;
+  }
+}
+
+template <int NF>
+__global__ void __launch_bounds__(128) k_face_volume_ladder(FaceParams P, const double* __restrict__ dgc,
+                                                            const double* __restrict__ state, int k0,
+                                                            double* __restrict__ partial, int64_t nb) {
+  __shared__ double sh[128];
+  const int64_t f = (int64_t)blockIdx.x * 128 + threadIdx.x;
+  double acc[LS_M];
+#pragma unroll
+  for (int k = 0; k < LS_M; ++k) acc[k] = 0.0;
+  if (f < P.nf) {
+    int32_t cn[NF];
+#pragma unroll
+    for (int b = 0; b < NF; ++b) cn[b] = P.conn[f * NF + b];
+    double x[NF][3], d[NF][3];
+    face_nodes<NF>(P, cn, x);
+#pragma unroll
+    for (int b = 0; b < NF; ++b) {
+      const unsigned m = P.mask[cn[b]];
+      const int32_t rd = P.rdof[cn[b]];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) d[b][i] = node_u(dgc, rd, m, i);
+    }
+    const double sgn = state[LS_SIGN];
+#pragma unroll
+    for (int g = 0; g < Face<NF>::NG; ++g) {
+      double rx[9], rd[9];
+      face_frame<NF>(x, g, rx);
+      face_frame<NF>(d, g, rd);
+#pragma unroll
+      for (int k = 0; k < LS_M; ++k) {
+        const double a = sgn * ldexp(1.0, -(k0 + k));
+        double r[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) r[i] = rx[i] + a * rd[i];
+        acc[k] += Face<NF>::w(g) * det3(r) / 3.0;
+      }
+    }
+  }
+#pragma unroll 1
+  for (int k = 0; k < LS_M; ++k) {
+    const double s = block_sum<128>(acc[k], sh);
+    if (threadIdx.x == 0) partial[k * nb + blockIdx.x] = s;
+  }
+}
+
+// out[k] (+)= scale * sum_i partial[k * nb + i], fixed order; one block per k
+__global__ void __launch_bounds__(256) k_sum_ladder(const double* __restrict__ partial, int64_t nb, double scale,
+                                                    double* out, int accumulate) {
+  __shared__ double sh[256];
+  const int k = blockIdx.x;
+  double acc = 0.0;
+  for (int64_t i = threadIdx.x; i < nb; i += 256) acc += partial[k * nb + i];
+  const double s = block_sum<256>(acc, sh);
+  if (threadIdx.x == 0) out[k] = (accumulate ? out[k] : 0.0) + scale * s;
+}
+
+// per-block sum of dgc.R and max |dgc|
+__global__ void __launch_bounds__(256) k_ls_partial(int64_t n, const double* __restrict__ dgc,
+                                                    const double* __restrict__ R, double* partial, int64_t nb) {
+  __shared__ double sh[256];
+  double dot = 0.0, mx = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+    const double d = dgc[i];
+    dot += d * R[i];
+    mx = fmax(mx, fabs(d));
+  }
+  const double s = block_sum<256>(dot, sh);
+  sh[threadIdx.x] = mx;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = s;
+    partial[nb + blockIdx.x] = sh[0];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_ls_prepare(const double* __restrict__ partial, int64_t nb,
+                                                    const double* __restrict__ e0, double* state) {
+  __shared__ double sh[256];
+  double dot = 0.0, mx = 0.0;
+  for (int64_t i = threadIdx.x; i < nb; i += 256) {
+    dot += partial[i];
+    mx = fmax(mx, partial[nb + i]);
+  }
+  const double de = block_sum<256>(dot, sh);
+  sh[threadIdx.x] = mx;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double E0 = e0[0];
+    state[LS_SIGN] = de > 0.0 ? -1.0 : 1.0;      // the reference turns an ascent direction around
+    state[LS_DE] = de > 0.0 ? -de : de;
+    state[LS_E0] = E0;
+    state[LS_SMAX] = sh[0];
+    state[LS_ALPHA] = 0.0;
+    state[LS_ENEW] = E0;
+    state[LS_FOUND] = 0.0;
+    // the predicted decrease is below the energy's own round-off: the
+    // energy comparison carries no information (the host decides instead)
+    state[LS_ROUND] = fabs(de) <= 1e-10 * fabs(E0) ? 1.0 : 0.0;
+  }
+}
+
+// first accepted step of the ladder [k0, k0 + LS_M): Armijo with c1 and the
+// step-length cap; alpha below 1e-12 ends the search without a step
+__global__ void k_ls_select(const double* __restrict__ E, int k0, double c1, double max_step, double* state) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (state[LS_FOUND] != 0.0 || state[LS_ROUND] != 0.0) return;
+  for (int k = 0; k < LS_M; ++k) {
+    const double a = ldexp(1.0, -(k0 + k));
+    if (a < 1e-12) {
+      state[LS_FOUND] = -1.0;
+      return;
+    }
+    const double e = E[k];
+    const bool ok = isfinite(e) && e <= state[LS_E0] + c1 * state[LS_DE] * a && a * state[LS_SMAX] <= max_step;
+    if (ok) {
+      state[LS_ALPHA] = state[LS_SIGN] * a;
+      state[LS_ENEW] = e;
+      state[LS_FOUND] = 1.0;
+      return;
+    }
+  }
+}
+
+// gc += alpha dgc once a step has been accepted
+__global__ void __launch_bounds__(256) k_ls_apply(int64_t n, const double* __restrict__ state,
+                                                  const double* __restrict__ dgc, double* gc) {
+  if (state[LS_FOUND] != 1.0) return;
+  const double a = state[LS_ALPHA];
+  for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256)
+    gc[i] += a * dgc[i];
+}
+
 // ---- lumped mass: thread per node ------------------------------------------
 // m[(n,d)] += sum_{e,b} rho w N_a N_b over free (conn[e][b], d), the row sum
 // of the reduced consistent mass (C3base.py:348-384, assembly.py:421-443,
@@ -1387,5 +1611,71 @@ extern "C" int fea_energy_volume_noalloc(const fea_nodes_t* N, const fea_group_t
   }
   k_sum_partials<<<1, 256, 0, st>>>(part, nb, out, 0);
   count_launch();
+  return (int)cudaGetLastError();
+}
+
+// ---- device line search entry points ------------------------------------------
+extern "C" int32_t fea_ls_ladder_len() { return LS_M; }
+
+extern "C" int64_t fea_ls_scratch_len(int64_t n_items) { return (int64_t)LS_M * ((n_items + 127) / 128) + 16; }
+
+extern "C" int fea_ls_energy_volume(const fea_nodes_t* N, const fea_group_t* G, double mu, double kappa,
+                                    const double* gc, const double* dgc, const double* state, int32_t k0,
+                                    int32_t accumulate, double* out, double* scratch, int64_t scratch_len,
+                                    cudaStream_t st) {
+  if (!N || !G || !gc || !dgc || !state || !out || !scratch || k0 < 0) return FEA_EINVAL;
+  if (G->kind != FEA_C3D4 && G->kind != FEA_C3D8) return FEA_EINVAL;
+  if (scratch_len < fea_ls_scratch_len(G->ne)) return FEA_EWORK;
+  if (int r = ensure_tables()) return r;
+  VolParams P = vol_params(N, G, mu, kappa, gc);
+  const int64_t nb = (G->ne + 127) / 128;
+  if (nb > 0) {
+    if (G->kind == FEA_C3D8) k_vol_energy_ladder<8><<<(unsigned)nb, 128, 0, st>>>(P, dgc, state, k0, scratch, nb);
+    else k_vol_energy_ladder<4><<<(unsigned)nb, 128, 0, st>>>(P, dgc, state, k0, scratch, nb);
+    count_launch();
+  }
+  k_sum_ladder<<<LS_M, 256, 0, st>>>(scratch, nb, 1.0, out, accumulate);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+extern "C" int fea_ls_energy_pressure(const fea_nodes_t* N, const fea_group_t* G, double p, const double* Xi,
+                                      const double* gc, const double* dgc, const double* state, int32_t k0,
+                                      int32_t accumulate, double* out, double* scratch, int64_t scratch_len,
+                                      cudaStream_t st) {
+  if (!N || !G || !Xi || !gc || !dgc || !state || !out || !scratch || k0 < 0) return FEA_EINVAL;
+  if (G->kind != FEA_T3 && G->kind != FEA_Q4) return FEA_EINVAL;
+  if (scratch_len < fea_ls_scratch_len(G->ne)) return FEA_EWORK;
+  if (int r = ensure_tables()) return r;
+  FaceParams P = face_params(N, G, p, Xi, gc);
+  const int64_t nb = (G->ne + 127) / 128;
+  if (nb > 0) {
+    if (G->kind == FEA_T3) k_face_volume_ladder<3><<<(unsigned)nb, 128, 0, st>>>(P, dgc, state, k0, scratch, nb);
+    else k_face_volume_ladder<4><<<(unsigned)nb, 128, 0, st>>>(P, dgc, state, k0, scratch, nb);
+    count_launch();
+  }
+  k_sum_ladder<<<LS_M, 256, 0, st>>>(scratch, nb, p, out, accumulate);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+extern "C" int fea_ls_prepare(int64_t n, const double* dgc, const double* R, const double* e0, double* state,
+                              double* scratch, int64_t scratch_len, cudaStream_t st) {
+  if (n < 0 || !dgc || !R || !e0 || !state || !scratch) return FEA_EINVAL;
+  const int64_t nb = n > 0 ? std::min<int64_t>((n + 255) / 256, 1024) : 1;
+  if (scratch_len < 2 * nb) return FEA_EWORK;
+  k_ls_partial<<<(unsigned)nb, 256, 0, st>>>(n, dgc, R, scratch, nb);
+  k_ls_prepare<<<1, 256, 0, st>>>(scratch, nb, e0, state);
+  count_launch(2);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int fea_ls_select(int64_t n, const double* E, int32_t k0, double c1, double max_step, double* state,
+                             const double* dgc, double* gc, cudaStream_t st) {
+  if (n < 0 || !E || !state || !dgc || !gc || k0 < 0) return FEA_EINVAL;
+  k_ls_select<<<1, 32, 0, st>>>(E, k0, c1, max_step, state);
+  const int64_t nb = n > 0 ? std::min<int64_t>((n + 255) / 256, 4096) : 1;
+  k_ls_apply<<<(unsigned)nb, 256, 0, st>>>(n, state, dgc, gc);
+  count_launch(2);
   return (int)cudaGetLastError();
 }

@@ -225,6 +225,31 @@ class DevicePlan:
         L.check(L.fea_energy_pressure(C.byref(self.nodes), C.byref(f.desc), vptr(Xinst), vptr(gc), vptr(out),
                                       vptr(s), s.numel(), stream()), "fea_energy_pressure")
 
+    # -- device line search (fea_ls_*) --------------------------------------------
+    def ls_prepare(self, dgc, R, e0, state):
+        nb = min((self.ndof + 255) // 256, 1024) if self.ndof else 1
+        s = self.scratch(2 * nb)
+        L.check(L.fea_ls_prepare(self.ndof, vptr(dgc), vptr(R), vptr(e0), vptr(state), vptr(s), s.numel(),
+                                 stream()), "fea_ls_prepare")
+
+    def ls_energy_volume(self, gi, mu, kappa, gc, dgc, state, k0, out, accumulate):
+        g = self.groups[gi]
+        s = self.scratch(L.fea_ls_scratch_len(g.ne))
+        L.check(L.fea_ls_energy_volume(C.byref(self.nodes), C.byref(g.desc), float(mu), float(kappa), vptr(gc),
+                                       vptr(dgc), vptr(state), int(k0), int(bool(accumulate)), vptr(out), vptr(s),
+                                       s.numel(), stream()), "fea_ls_energy_volume")
+
+    def ls_energy_pressure(self, fi, p, Xinst, gc, dgc, state, k0, out, accumulate):
+        f = self.faces[fi]
+        s = self.scratch(L.fea_ls_scratch_len(f.ne))
+        L.check(L.fea_ls_energy_pressure(C.byref(self.nodes), C.byref(f.desc), float(p), vptr(Xinst), vptr(gc),
+                                         vptr(dgc), vptr(state), int(k0), int(bool(accumulate)), vptr(out), vptr(s),
+                                         s.numel(), stream()), "fea_ls_energy_pressure")
+
+    def ls_select(self, E, k0, c1, max_step, state, dgc, gc):
+        L.check(L.fea_ls_select(self.ndof, vptr(E), int(k0), float(c1), float(max_step), vptr(state), vptr(dgc),
+                                vptr(gc), stream()), "fea_ls_select")
+
     def adjoint_vjp_volume(self, gi, mu, kappa, gc, lam_full, dX, dmu):
         """dX += d(lam . R_e)/dX (all nodes); dmu[0] = d(lam . R_e)/dmu."""
         g = self.groups[gi]

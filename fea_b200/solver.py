@@ -59,8 +59,10 @@ class BaseSolver:
 class StaticImplicitSolver(BaseSolver):
     def __init__(self, maximum_iteration: int = 10000, tol_error: float = 1e-5, rtol: float = None,
                  pcg_tol: float = 1e-5, pcg_max_iter: int = 1500, tight_pcg_tol: float = 1e-22,
-                 tight_pcg_max_iter: int = 20000, precision: str = "fp64", verbose: bool = False) -> None:
+                 tight_pcg_max_iter: int = 20000, precision: str = "fp64", verbose: bool = False,
+                 device_line_search: bool = True) -> None:
         super().__init__()
+        self.device_line_search = device_line_search
         self.maximum_iteration = maximum_iteration
         self.tol_error = tol_error
         self.rtol = rtol
@@ -99,7 +101,52 @@ class StaticImplicitSolver(BaseSolver):
         return self.assembly.assemble_Stiffness_Matrix(GC=GC_now)
 
     def _line_search(self, GC0, dGC, R, energy0):
-        """Armijo backtracking, c1 = 0.3, halving, alpha < 1e-12 -> 0 (static_implicit.py:153-232).
+        """Armijo backtracking, c1 = 0.3, halving, alpha < 1e-12 -> 0
+        (static_implicit.py:97-169): on the device (a ladder of trial steps
+        per launch, one host read per ladder) unless the assembly has
+        reference points or the predicted decrease is at round-off level."""
+        self._last_smax = None
+        if self.device_line_search and getattr(self.assembly, "_system", None) is None:
+            res = self._line_search_device(GC0, dGC, R, energy0)
+            if res is not None:
+                return res
+        return self._line_search_host(GC0, dGC, R, energy0)
+
+    def _line_search_device(self, GC0, dGC, R, energy0):
+        A = self.assembly
+        P = A.plan
+        dev = GC0.device
+        e0 = torch.as_tensor(energy0, dtype=torch.float64, device=dev).reshape(1).contiguous()
+        st = torch.empty(L.FEA_LS_NSTATE, dtype=torch.float64, device=dev)
+        dGC = dGC.contiguous()
+        P.ls_prepare(dGC, R.contiguous(), e0, st)
+        gc = GC0.clone().contiguous()
+        E = torch.empty(L.FEA_LS_M, dtype=torch.float64, device=dev)
+        for k0 in range(0, 40, L.FEA_LS_M):
+            acc = False
+            for gi, e in enumerate(A._mat_elems):
+                mu, kappa = e.materials.parameters()
+                P.ls_energy_volume(gi, mu, kappa, GC0, dGC, st, k0, E, acc)
+                acc = True
+            for fi, ld in enumerate(A._face_loads):
+                P.ls_energy_pressure(fi, float(ld.pressure), A._Xinst, GC0, dGC, st, k0, E, acc)
+                acc = True
+            P.ls_select(E, k0, 0.3, self._maximum_step_length, st, dGC, gc)
+            h = st.tolist()
+            if not (math.isfinite(h[L.FEA_LS_DE]) and math.isfinite(h[L.FEA_LS_SMAX])):
+                raise ValueError("dGC has nan or inf")
+            if h[L.FEA_LS_ROUND] != 0.0:
+                return None
+            self._last_smax = h[L.FEA_LS_SMAX]
+            if h[L.FEA_LS_FOUND] == 1.0:
+                return abs(h[L.FEA_LS_ALPHA]), gc, st[L.FEA_LS_ENEW].clone()
+            if h[L.FEA_LS_FOUND] != 0.0:
+                break
+        return 0.0, GC0.clone(), energy0
+
+    def _line_search_host(self, GC0, dGC, R, energy0):
+        """The line search on the host: one energy (or, at round-off level,
+        one residual norm) per trial step.
 
         When the predicted energy decrease is below the round-off of the
         energy itself (|dGC . R| <= 1e-10 |E|), the energy comparison carries
@@ -149,6 +196,7 @@ class StaticImplicitSolver(BaseSolver):
         (``_run_linear`` here; the batched engine of ``fea_b200.serving``
         when many solves share the device).  Returns GC or False."""
         self._iter_now = 0
+        self._last_smax = None
         energy = self.get_total_energy(GC)
         dGC = torch.zeros_like(GC)
         low_alpha, alpha = 0, 0.0
@@ -159,8 +207,11 @@ class StaticImplicitSolver(BaseSolver):
                 return False
             R, Kv = self.assembly.assemble_csr(GC)
             self._iter_now += 1
-            rmax = float(R.abs().max()) if R.numel() else 0.0
-            rnorm = float(R.norm())
+            if R.numel():
+                # one host read for the residual statistics of this iteration
+                rmax, rnorm, srmax = torch.stack([R.abs().max(), R.norm(), self._scaled_rmax_dev(Kv, R)]).tolist()
+            else:
+                rmax, rnorm, srmax = 0.0, 0.0, 0.0
             if r_first is None:
                 r_first = rnorm
             self.history.append(dict(iter=self._iter_now, rmax=rmax, rnorm=rnorm))
@@ -168,7 +219,7 @@ class StaticImplicitSolver(BaseSolver):
                 break
             if self._at_floor(r_first):
                 break
-            req = self._linear_request(Kv, -R, self._iter_now, alpha, dGC)
+            req = self._linear_request(Kv, -R, self._iter_now, alpha, dGC, srmax=srmax)
             yield req
             dGC = self._linear_finish(req, Kv, -R)
             alpha, GCnew, energynew = self._line_search(GC, dGC, R, energy)
@@ -189,8 +240,10 @@ class StaticImplicitSolver(BaseSolver):
             energy = self.get_total_energy(GC)
             if self.verbose:
                 print("iter %3d  alpha %.2f  energy %.10e  max|R| %.4e" % (self._iter_now, alpha, float(energy), rmax))
-            if self.rtol is None and ((float(dGC.abs().max()) < tol_error and rmax < tol_error) or rmax < 1e-6):
-                break
+            if self.rtol is None:
+                dmax = self._last_smax if self._last_smax is not None else float(dGC.abs().max())
+                if (dmax < tol_error and rmax < tol_error) or rmax < 1e-6:
+                    break
         return GC
 
     def _at_floor(self, r_first):
@@ -210,7 +263,7 @@ class StaticImplicitSolver(BaseSolver):
         self._run_linear(req)
         return self._linear_finish(req, K_values, R)
 
-    def _linear_request(self, K_values, R, iter_now=0, alpha0=None, dGC0=None):
+    def _linear_request(self, K_values, R, iter_now=0, alpha0=None, dGC0=None, srmax=None):
         """The PCG tolerance and cap for this Newton iteration: loose solves
         far from equilibrium, a tight solve where the reference switches to
         its exact solver (scaled residual below 1e-3, or repeated small
@@ -218,7 +271,9 @@ class StaticImplicitSolver(BaseSolver):
         x = (torch.zeros_like(R) if dGC0 is None else dGC0.clone()).contiguous()
         alpha0 = 1e-10 if alpha0 is None else alpha0
         self._low_alpha_count = self._low_alpha_count + 1 if alpha0 < 1e-1 else 0
-        tight = self._low_alpha_count > 3 or self._scaled_rmax(K_values, R) < 1e-3
+        if srmax is None:
+            srmax = self._scaled_rmax(K_values, R)
+        tight = self._low_alpha_count > 3 or srmax < 1e-3
         if tight:
             tol, cap = self.tight_pcg_tol, self.tight_pcg_max_iter
             self._low_alpha_count = 0
@@ -252,8 +307,12 @@ class StaticImplicitSolver(BaseSolver):
         return x
 
     def _scaled_rmax(self, K_values, R):
+        return float(self._scaled_rmax_dev(K_values, R)) if R.numel() else 0.0
+
+    def _scaled_rmax_dev(self, K_values, R):
+        """max |R_i| / sqrt|K_ii| as a device scalar (static_implicit.py:384-388 test)."""
         diag = self._diag(K_values)
-        return float((R / diag.abs().sqrt().clamp_min(1e-300)).abs().max()) if R.numel() else 0.0
+        return (R / diag.abs().sqrt().clamp_min(1e-300)).abs().max()
 
     def _diag(self, K_values):
         P = self.assembly.system
@@ -285,6 +344,9 @@ class DynamicImplicitSolver(StaticImplicitSolver):
         super().__init__(maximum_iteration=maximum_iteration, tol_error=tol_error, pcg_tol=pcg_tol,
                          pcg_max_iter=pcg_max_iter, tight_pcg_tol=tight_pcg_tol,
                          tight_pcg_max_iter=tight_pcg_max_iter, verbose=verbose)
+        # the step's incremental potential includes the inertia term, which
+        # the device ladder does not evaluate: the host line search serves
+        self.device_line_search = False
         self._deltaT = deltaT
         self._time_end = time_end
         self._gamma = 0.5
@@ -444,7 +506,7 @@ class DynamicImplicitSolver(StaticImplicitSolver):
             self._iter_now += 1
             rmax = float(R.abs().max()) if R.numel() else 0.0
             self.history.append(dict(iter=self._iter_now, rmax=rmax, rnorm=float(R.norm())))
-            req = self._linear_request(Kv, -R, self._iter_now, alpha, dGC)
+            req = self._linear_request(Kv, -R, self._iter_now, alpha, dGC, srmax=srmax)
             self._run_linear(req)
             dGC = self._linear_finish(req, Kv, -R)
             alpha, GCnew, energy_new = self._dyn_line_search(GC_now, GC_pre, dGC, R, energy, deltaT)

@@ -378,6 +378,51 @@ int fea_pcgb_state(void* table_dev, int32_t max_slots, int64_t max_items, int32_
 int fea_convert_f32(int64_t nnz, const double* values_dev, float* values32_dev, cudaStream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Device line search of the Newton solver.  Replaces the host loop of
+ * StaticImplicitSolver._line_search (static_implicit.py:97-169: Armijo with
+ * c1, step halving from 1, no step below 1e-12, step-length cap) by trial
+ * energies evaluated on the device a ladder at a time.
+ *   state_dev: FEA_LS_NSTATE doubles.  fea_ls_prepare writes
+ *     [DE] = -|dgc.R|, [E0] = *e0_dev (energy at gc), [SMAX] = max|dgc|,
+ *     [SIGN] = -1 when dgc.R > 0 (the direction is turned around, as the
+ *     reference does), +1 otherwise; [FOUND] = 0; [ROUND] = 1 when
+ *     |dgc.R| <= 1e-10 |E0| (the energy test carries no information; the
+ *     caller decides that step itself).  scratch: 2 * min(ceil(n/256), 1024).
+ *   fea_ls_energy_volume / _pressure: out[k] (+)= the group's energy (or
+ *     p V of the face group) at gc + SIGN 2^-(k0+k) dgc, k < FEA_LS_M;
+ *     scratch: fea_ls_scratch_len(ne).
+ *   fea_ls_select: the first k of the ladder with
+ *     E[k] <= E0 + c1 DE 2^-(k0+k) and 2^-(k0+k) SMAX <= max_step sets
+ *     [ALPHA] = SIGN 2^-(k0+k), [ENEW] = E[k], [FOUND] = 1 and adds
+ *     ALPHA dgc to gc; a step below 1e-12 sets [FOUND] = -1.  Nothing
+ *     happens once FOUND != 0 or ROUND != 0.
+ * ------------------------------------------------------------------------- */
+#define FEA_LS_M 8
+#define FEA_LS_DE 0
+#define FEA_LS_E0 1
+#define FEA_LS_SMAX 2
+#define FEA_LS_SIGN 3
+#define FEA_LS_ALPHA 4
+#define FEA_LS_ENEW 5
+#define FEA_LS_FOUND 6
+#define FEA_LS_ROUND 7
+#define FEA_LS_NSTATE 8
+int32_t fea_ls_ladder_len(void);
+int64_t fea_ls_scratch_len(int64_t n_items);
+int fea_ls_prepare(int64_t n, const double* dgc_dev, const double* R_dev, const double* e0_dev,
+                   double* state_dev, double* scratch_dev, int64_t scratch_len, cudaStream_t stream);
+int fea_ls_energy_volume(const fea_nodes_t* nodes, const fea_group_t* group, double mu, double kappa,
+                         const double* gc_dev, const double* dgc_dev, const double* state_dev, int32_t k0,
+                         int32_t accumulate, double* out_dev, double* scratch_dev, int64_t scratch_len,
+                         cudaStream_t stream);
+int fea_ls_energy_pressure(const fea_nodes_t* nodes, const fea_group_t* faces, double p, const double* Xi_dev,
+                           const double* gc_dev, const double* dgc_dev, const double* state_dev, int32_t k0,
+                           int32_t accumulate, double* out_dev, double* scratch_dev, int64_t scratch_len,
+                           cudaStream_t stream);
+int fea_ls_select(int64_t n, const double* E_dev, int32_t k0, double c1, double max_step, double* state_dev,
+                  const double* dgc_dev, double* gc_dev, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Explicit central difference (lumped mass), one element group, no loads.
  * One reference time step (dynamic_explicit.py:103-117) is
  *   vh += dt a;  u += dt vh;  a = minv * (-f_int(u));  v = (vh_new + vh_old)/2.
