@@ -72,6 +72,8 @@ def args_():
     ap.add_argument("--serve-slots", type=int, default=48)
     ap.add_argument("--serve-round", type=int, default=32, help="PCG iterations per captured round")
     ap.add_argument("--serve-plain", type=int, default=1, help="also time the one-at-a-time path")
+    ap.add_argument("--serve-sample", type=int, default=48,
+                    help="requests of the serving record in the default line (0: none)")
     return ap.parse_args()
 
 
@@ -709,45 +711,48 @@ def run_adjoint(a):
     print(json.dumps(line), flush=True)
 
 
-def run_serving(a):
-    """Stream of seeded cantilever static solves (C3D4, Newton to 1e-8):
-    solves/s and p50/p99 latency of the continuous-batching server against
-    solving the same requests one at a time through StaticImplicitSolver."""
+def serving_run(n_requests, rate, slots, round_iters, min_elems, max_elems, plain=True, seed=0):
+    """One stream of seeded cantilever static solves (C3D4, Newton to 1e-8):
+    solves/s and p50/p99 latency of the continuous-batching server, and of
+    the same requests solved one at a time through StaticImplicitSolver."""
     import torch
     from fea_b200 import serving
-    out = []
-    for rate in [float(x) for x in a.serve_rates.split(",")]:
-        reqs = serving.make_requests(a.serve_requests, rate, seed=0, min_elems=a.serve_min_elems,
-                                     max_elems=a.serve_max_elems)
-        if not math.isfinite(rate):
-            for r in reqs:
-                r.arrival = 0.0
+    reqs = serving.make_requests(n_requests, rate, seed=seed, min_elems=min_elems, max_elems=max_elems)
+    if not math.isfinite(rate):
+        for r in reqs:
+            r.arrival = 0.0
 
-        def summary(res, wall):
-            ok = [r for r in res if r.error is None]
-            lat = np.array([r.latency for r in ok])
-            span = max(r.done for r in res) - min(r.arrival for r in res)
-            return {"solves_per_s": len(ok) / span, "rejected": len(res) - len(ok), "p50_s": float(np.percentile(lat, 50)),
-                    "p99_s": float(np.percentile(lat, 99)), "makespan_s": span, "wall_s": wall,
-                    "newton_iters": int(sum(r.newton_iters for r in res)), "pcg_iters": int(sum(r.pcg_iters for r in res))}
-        # warm-up: one small request through both paths
-        w = serving.make_requests(1, float("inf"), seed=99, min_elems=2000, max_elems=2000)
-        w[0].arrival = 0.0
-        serving.serve(w, max_slots=a.serve_slots, round_iters=a.serve_round, keep=False)
-        serving.solve_plain(w, keep=False)
-        torch.cuda.synchronize()
+    def summary(res, wall):
+        ok = [r for r in res if r.error is None]
+        lat = np.array([r.latency for r in ok])
+        span = max(r.done for r in res) - min(r.arrival for r in res)
+        return {"solves_per_s": len(ok) / span, "rejected": len(res) - len(ok), "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)), "makespan_s": span, "wall_s": wall,
+                "newton_iters": int(sum(r.newton_iters for r in res)), "pcg_iters": int(sum(r.pcg_iters for r in res))}
+    # warm-up: one small request through both paths
+    w = serving.make_requests(1, float("inf"), seed=99, min_elems=2000, max_elems=2000)
+    w[0].arrival = 0.0
+    serving.serve(w, max_slots=slots, round_iters=round_iters, keep=False)
+    serving.solve_plain(w, keep=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    served, stats = serving.serve(reqs, max_slots=slots, round_iters=round_iters)
+    rec = {"rate_per_s": rate, "served": summary(served, time.perf_counter() - t0), "server": stats}
+    if plain:
         t0 = time.perf_counter()
-        served, stats = serving.serve(reqs, max_slots=a.serve_slots, round_iters=a.serve_round)
-        rec = {"rate_per_s": rate, "served": summary(served, time.perf_counter() - t0), "server": stats}
-        if a.serve_plain:
-            t0 = time.perf_counter()
-            plain = serving.solve_plain(reqs)
-            rec["plain"] = summary(plain, time.perf_counter() - t0)
-            rec["speedup_solves_per_s"] = rec["served"]["solves_per_s"] / rec["plain"]["solves_per_s"]
-            rec["max_rel_diff_served_vs_plain"] = max(float((x.gc - y.gc).norm() / y.gc.norm())
-                                                      for x, y in zip(served, plain)
-                                                      if x.gc is not None and y.gc is not None)
-        out.append(rec)
+        plain_res = serving.solve_plain(reqs)
+        rec["plain"] = summary(plain_res, time.perf_counter() - t0)
+        rec["speedup_solves_per_s"] = rec["served"]["solves_per_s"] / rec["plain"]["solves_per_s"]
+        rec["max_rel_diff_served_vs_plain"] = max(float((x.gc - y.gc).norm() / y.gc.norm())
+                                                  for x, y in zip(served, plain_res)
+                                                  if x.gc is not None and y.gc is not None)
+    return rec
+
+
+def run_serving(a):
+    """The serving workload at every rate of --serve-rates."""
+    out = [serving_run(a.serve_requests, float(x), a.serve_slots, a.serve_round, a.serve_min_elems,
+                       a.serve_max_elems, plain=bool(a.serve_plain)) for x in a.serve_rates.split(",")]
     line = {"metric": "served static solves/s (C3D4 cantilevers, Newton to 1e-8)", "unit": "solves/s",
             "value": out[0]["served"]["solves_per_s"], "higher_is_better": True, "workload": "serving",
             "requests": a.serve_requests, "elems": [a.serve_min_elems, a.serve_max_elems], "runs": out}
@@ -930,6 +935,14 @@ def main():
     }
     if world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(n)
+    if world == 1 and a.serve_sample > 0:
+        # the serving form on a seeded sample of the cantilever stream (all
+        # requests at t = 0), served against one at a time on this GPU
+        rec = serving_run(a.serve_sample, float("inf"), a.serve_slots, a.serve_round, a.serve_min_elems,
+                          a.serve_max_elems)
+        line["serving"] = {"requests": a.serve_sample, "arrivals": "all at t = 0", "elems": [a.serve_min_elems,
+                           a.serve_max_elems], "sample": "first %d requests of the seeded 512-request stream "
+                           "(seed 0)" % a.serve_sample, **rec}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -5,7 +5,8 @@ with seeded dimensions, size and material, clamped at x = 1 - length and
 loaded by a follower pressure on its free end x = 1).  The server
 
 - prepares arriving requests on host threads (mesh, plan, device upload) as
-  long as their estimated device memory fits the budget;
+  long as their estimated device memory fits the budget (by default a share
+  of the device memory free when serving starts, torch.cuda.mem_get_info);
 - keeps every admitted request's mesh, CSR pattern and Newton state resident
   and runs its Newton iteration as a generator
   (``StaticImplicitSolver._newton``), which stops at each tangent solve;
@@ -300,11 +301,23 @@ def _prepare(req, stream_):
     return asm, sol
 
 
-def serve(requests, max_slots=48, round_iters=32, mem_budget=32 << 30, use_graph=True, prep_threads=2,
+def admission_budget(fraction=0.8, reserve=2 << 30, device=None):
+    """Bytes the server may hand to admitted requests: ``fraction`` of the
+    device memory free now (torch.cuda.mem_get_info), less ``reserve`` for
+    the batched-PCG table, graphs and the allocator's slack."""
+    free, _ = torch.cuda.mem_get_info(device)
+    return max(0, int(fraction * free) - int(reserve))
+
+
+def serve(requests, max_slots=48, round_iters=32, mem_budget=None, use_graph=True, prep_threads=2,
           keep=True):
     """Serve `requests` (arrival times honoured) with continuous batching.
-    Returns (results in request order, server statistics)."""
+    ``mem_budget`` (bytes) defaults to ``admission_budget()``, measured on
+    the device when serving starts.  Returns (results in request order,
+    server statistics)."""
     dev = torch.device("cuda")
+    if mem_budget is None:
+        mem_budget = admission_budget(device=dev)
     # items of the largest admissible batch: SpMV items of 16 nodes (3 rows
     # per node at most) outnumber update items of 256 rows
     max_chunks = max_slots * (max((request_rows(r) // 3 + 15) // 16 + 1 for r in requests) if requests else 1)
@@ -444,6 +457,7 @@ def serve(requests, max_slots=48, round_iters=32, mem_budget=32 << 30, use_graph
         in_flight = True
     pool.shutdown()
     stats = {"rounds": busy_rounds, "graph": eng.graph is not None, "max_slots": max_slots,
-             "round_iters": round_iters, "wall_s": time.perf_counter() - t0, **timing}
+             "round_iters": round_iters, "mem_budget": int(mem_budget), "wall_s": time.perf_counter() - t0,
+             **timing}
     return [results[r.rid] for r in sorted(requests, key=lambda r: r.rid)], stats
 
