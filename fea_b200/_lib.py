@@ -117,6 +117,16 @@ fea_pcg_solve_nodes = _sig("fea_pcg_solve_nodes", I32, NP, P, P, P, P, D, I32, I
 fea_pcg_solve_mixed_nodes = _sig("fea_pcg_solve_mixed_nodes", I32, NP, P, P, P, P, P, D, D, I32, I32, P, I64,
                                  C.POINTER(I32), C.POINTER(I32), C.POINTER(D), P)
 fea_convert_f32 = _sig("fea_convert_f32", I32, I64, P, P, P)
+
+
+class F32Layout(C.Structure):
+    _fields_ = [("cbase_dev", C.c_void_p), ("qbase_dev", C.c_void_p), ("cols_dev", C.c_void_p),
+                ("vals_dev", C.c_void_p)]
+
+
+fea_f32_layout_fill = _sig("fea_f32_layout_fill", I32, NP, P, P, C.POINTER(F32Layout), I32, P)
+fea_pcg_solve_mixed_nodes32 = _sig("fea_pcg_solve_mixed_nodes32", I32, NP, P, P, C.POINTER(F32Layout), P, P, D, D,
+                                   I32, I32, P, I64, C.POINTER(I32), C.POINTER(I32), C.POINTER(D), P)
 fea_pcgb_work_len = _sig("fea_pcgb_work_len", I64, I64, I64)
 fea_pcgb_table_bytes = _sig("fea_pcgb_table_bytes", I64, I32, I64)
 fea_pcgb_set = _sig("fea_pcgb_set", I32, P, I32, I64, I32, C.POINTER(PcgbSlot), P)
@@ -143,7 +153,7 @@ fea_launch_count = _sig("fea_launch_count", I64)
 EXPORTED = ["fea_plan_build", "fea_plan_free", "fea_plan_get", "fea_assemble_work_len", "fea_assemble_volume", "fea_assemble_pressure",
             "fea_reduce_scratch_len", "fea_energy_volume", "fea_energy_volume_noalloc", "fea_energy_pressure", "fea_lumped_mass",
             "fea_invert_mass", "fea_mass_csr", "fea_axpy", "fea_pcg_work_len", "fea_pcg_solve", "fea_pcg_mixed_work_len",
-            "fea_pcg_solve_mixed", "fea_spmv", "fea_spmv_nodes", "fea_pcg_solve_nodes", "fea_pcg_solve_mixed_nodes", "fea_convert_f32", "fea_pcgb_work_len", "fea_pcgb_table_bytes", "fea_pcgb_set", "fea_pcgb_start",
+            "fea_pcg_solve_mixed", "fea_spmv", "fea_spmv_nodes", "fea_pcg_solve_nodes", "fea_pcg_solve_mixed_nodes", "fea_convert_f32", "fea_f32_layout_fill", "fea_pcg_solve_mixed_nodes32", "fea_pcgb_work_len", "fea_pcgb_table_bytes", "fea_pcgb_set", "fea_pcgb_start",
             "fea_pcgb_iterate", "fea_pcgb_state", "fea_explicit_work_len", "fea_explicit_run", "fea_explicit_stage",
             "fea_adjoint_vjp_volume", "fea_adjoint_hvp_pressure", "fea_version", "fea_launch_count",
             "fea_ls_ladder_len", "fea_ls_scratch_len", "fea_ls_prepare", "fea_ls_energy_volume",

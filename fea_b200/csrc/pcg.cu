@@ -356,6 +356,115 @@ __global__ void __launch_bounds__(PCG_TPB) k_spmv_node_sub(NodeOp<V> A, const X*
   if (mode == 1) finish_pq(contrib, st, part, counter);
 }
 
+// FP32 copy of the node-row matrix in a padded layout: every node's column
+// list and each of its rows start on a 16-byte boundary and are padded to a
+// multiple of 4 entries (column 0, value 0), so that a lane reads 4 columns
+// and the 4 values of each row with 128-bit loads.  One warp per node, 128
+// columns per pass (one pass for a solid interior node).
+struct NodeOp32q {
+  const int64_t* __restrict__ cbase;   // [N+1] first padded column of node n
+  const int64_t* __restrict__ qbase;   // [N+1] first value of node n's rows
+  const int32_t* __restrict__ cols;
+  const float* __restrict__ vals;
+  const uint8_t* __restrict__ mask;
+  const int32_t* __restrict__ dbase;
+  int64_t n_nodes;
+  int64_t n;
+};
+
+template <class X>
+__global__ void __launch_bounds__(PCG_TPB) k_spmv_node32q(NodeOp32q A, const X* __restrict__ x, X* __restrict__ y,
+                                                          double* st, double* part, unsigned* counter, int mode) {
+  if (mode == 1 && st[S_DONE] != 0.0) return;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int64_t step = (int64_t)gridDim.x * PCG_WARPS;
+  double contrib = 0.0;
+  int64_t nd = (int64_t)blockIdx.x * PCG_WARPS + warp;
+  unsigned m = 0;
+  int64_t cb = 0, ce = 0, qb = 0;
+  if (nd < A.n_nodes) {
+    m = A.mask[nd];
+    cb = A.cbase[nd];
+    ce = A.cbase[nd + 1];
+    qb = A.qbase[nd];
+  }
+  while (nd < A.n_nodes) {                       // warp-uniform
+    const int64_t nx = nd + step;
+    unsigned m2 = 0;
+    int64_t cb2 = 0, ce2 = 0, qb2 = 0;
+    if (nx < A.n_nodes) {                        // the next node's metadata, loaded ahead
+      m2 = A.mask[nx];
+      cb2 = A.cbase[nx];
+      ce2 = A.cbase[nx + 1];
+      qb2 = A.qbase[nx];
+    }
+    if (m) {
+      const int f = popc3(m);
+      const int L4 = (int)(ce - cb);
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+      for (int q0 = 0; q0 < L4; q0 += 128) {
+        const int q = q0 + 4 * lane;
+        const bool h = q < L4;
+        const int4 c = h ? __ldg(reinterpret_cast<const int4*>(A.cols + cb + q)) : make_int4(0, 0, 0, 0);
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 v0 = h ? __ldcs(reinterpret_cast<const float4*>(A.vals + qb + q)) : z4;
+        const float4 v1 = (h && f > 1) ? __ldcs(reinterpret_cast<const float4*>(A.vals + qb + L4 + q)) : z4;
+        const float4 v2 = (h && f > 2) ? __ldcs(reinterpret_cast<const float4*>(A.vals + qb + 2 * L4 + q)) : z4;
+        double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
+        if (h) {
+          x0 = (double)x[c.x];
+          x1 = (double)x[c.y];
+          x2 = (double)x[c.z];
+          x3 = (double)x[c.w];
+        }
+        s0 += (double)v0.x * x0 + (double)v0.y * x1 + (double)v0.z * x2 + (double)v0.w * x3;
+        s1 += (double)v1.x * x0 + (double)v1.y * x1 + (double)v1.z * x2 + (double)v1.w * x3;
+        s2 += (double)v2.x * x0 + (double)v2.y * x1 + (double)v2.z * x2 + (double)v2.w * x3;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      }
+      if (lane == 0) {
+        const int64_t r = A.dbase[nd];
+        y[r] = (X)s0;
+        contrib += s0 * (double)x[r];
+        if (f > 1) { y[r + 1] = (X)s1; contrib += s1 * (double)x[r + 1]; }
+        if (f > 2) { y[r + 2] = (X)s2; contrib += s2 * (double)x[r + 2]; }
+      }
+    }
+    nd = nx;
+    m = m2;
+    cb = cb2;
+    ce = ce2;
+    qb = qb2;
+  }
+  if (mode == 1) finish_pq(contrib, st, part, counter);
+}
+
+// Fill the padded FP32 layout from the FP64 node-row values (and, when
+// cols != nullptr, the padded column lists): one warp per node.
+__global__ void __launch_bounds__(256) k_fill_node32q(NodeOp<double> A, const int64_t* __restrict__ cbase,
+                                                      const int64_t* __restrict__ qbase, int32_t* cols,
+                                                      float* __restrict__ vals) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nd = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (nd >= A.n_nodes) return;
+  const unsigned m = A.mask[nd];
+  if (!m) return;
+  const int f = popc3(m);
+  const int L = A.rowlen[nd];
+  const int64_t vb = A.vbase[nd], cb = cbase[nd], qb = qbase[nd];
+  const int L4 = (int)(cbase[nd + 1] - cb);
+  for (int q = lane; q < L4; q += 32) {
+    if (cols) cols[cb + q] = q < L ? A.idx[vb + q] : 0;
+    for (int r = 0; r < f; ++r) vals[qb + (int64_t)r * L4 + q] = q < L ? (float)A.val[vb + (int64_t)r * L + q] : 0.f;
+  }
+}
+
 // 1/|K_jj| of the node rows (0 -> 1): the diagonal entry of row (n, j) is the
 // column dbase[n] + j of the shared column list (sorted), found by bisection
 template <class V>
@@ -655,6 +764,14 @@ static void spmv(const NodeOp<V>& A, const X* x, X* y, double* st, double* part,
   count_launch();
 }
 
+template <class X>
+static void spmv(const NodeOp32q& A, const X* x, X* y, double* st, double* part, unsigned* counter, int mode,
+                 cudaStream_t s) {
+  k_spmv_node32q<X><<<occ_grid(k_spmv_node32q<X>, A.n_nodes, PCG_WARPS), PCG_TPB, 0, s>>>(A, x, y, st, part,
+                                                                                        counter, mode);
+  count_launch();
+}
+
 template <class V>
 static void diag_inv(const CsrOp<V>& A, double* dinv, int jacobi, cudaStream_t s) {
   k_dinv_csr<V><<<fixed_grid(A.n, 256), 256, 0, s>>>(A, dinv, jacobi ? 0 : 1);
@@ -755,7 +872,11 @@ static int pcg_mixed(const Op64& A, const Op32& A32, int64_t n, const double* b,
   // x64 += x32, the true residual b - A x64 is formed in FP64 and replaces
   // the FP32 one, and the recurrence continues with the same search
   // direction.  The stop test is the FP64 one, on the true residual.
-  (void)inner_tol;
+  // inner_tol > 0: a batch ends in a replacement only once the FP32
+  // recurrence's r.z has fallen below inner_tol times its value at the last
+  // replacement (or the FP64 stop test may pass, or it broke down, or the
+  // cap is reached); otherwise the FP32 recurrence continues.  inner_tol <= 0
+  // replaces after every batch.
   PcgWork W = carve(work, n);                 // st64 and r64 (FP64 residual), dinv
   double* st2 = work + S_LEN + 2 + 5 * n + part_len(n);
   unsigned* counter2 = (unsigned*)(st2 + S_LEN);
@@ -786,6 +907,7 @@ static int pcg_mixed(const Op64& A, const Op32& A32, int64_t n, const double* b,
     count_launch();
     cudaMemcpyAsync(st2 + S_RZ0, W.st + S_RZ0, sizeof(double), cudaMemcpyDeviceToDevice, s);
     const int ce = std::max(1, check_every);
+    double rz_last = h64[S_RZ];
     while (total < max_iter) {
       const int batch = std::min(ce, max_iter - total);
       for (int k = 0; k < batch; ++k) {
@@ -799,6 +921,18 @@ static int pcg_mixed(const Op64& A, const Op32& A32, int64_t n, const double* b,
         }
       }
       total += batch;
+      if (inner_tol > 0.0 && total < max_iter) {
+        double h32[S_LEN];
+        cudaMemcpyAsync(h32, st2, sizeof(h32), cudaMemcpyDeviceToHost, s);
+        if (cudaError_t e = cudaStreamSynchronize(s)) return (int)e;
+        const double rz32 = h32[S_RZ];
+        if (h32[S_STATUS] != (double)FEA_EBREAKDOWN && rz32 > inner_tol * rz_last &&
+            rz32 / h64[S_RZ0] >= tol) {
+          k_pcg_p<float><<<vgf, PCG_TPB, 0, s>>>(n, pf, zf, st2);
+          count_launch();
+          continue;
+        }
+      }
       // replacement: x64 += x32, r64 = b - A x64, r32 / z32 / rho / beta from it
       k_axpy_f32<<<grid_for(n, 256), 256, 0, s>>>(n, x, xf);
       cudaMemsetAsync(xf, 0, sizeof(float) * n, s);
@@ -812,6 +946,7 @@ static int pcg_mixed(const Op64& A, const Op32& A32, int64_t n, const double* b,
       cudaMemcpyAsync(h32, st2, sizeof(h32), cudaMemcpyDeviceToHost, s);
       if (cudaError_t e = cudaStreamSynchronize(s)) return (int)e;
       rel = h64[S_RZ] / h64[S_RZ0];
+      rz_last = h64[S_RZ];
       if (rel < tol) { status = FEA_OK; break; }
       if (h32[S_STATUS] == (double)FEA_EBREAKDOWN) { status = FEA_EBREAKDOWN; break; }
     }
@@ -1397,6 +1532,39 @@ extern "C" int fea_pcg_solve_mixed_nodes(const fea_nodes_t* N, const int32_t* ix
   if (n == 0) return FEA_OK;
   return pcg_mixed(node_op<double>(N, ix, v), node_op<float>(N, ix, v32), n, b, x, tol, inner_tol, max_iter,
                    check_every, work, iters, outer, relres, s);
+}
+
+static bool layout_ok(const fea_f32_layout_t* Q) {
+  return Q && Q->cbase_dev && Q->qbase_dev && Q->cols_dev && Q->vals_dev;
+}
+
+extern "C" int fea_f32_layout_fill(const fea_nodes_t* N, const int32_t* ix, const double* v, fea_f32_layout_t* Q,
+                                   int32_t with_cols, cudaStream_t s) {
+  if (!nodes_ok(N) || !ix || !v || !layout_ok(Q)) return FEA_EINVAL;
+  if (N->n_nodes == 0) return FEA_OK;
+  const unsigned grid = (unsigned)((N->n_nodes * 32 + 255) / 256);
+  k_fill_node32q<<<grid, 256, 0, s>>>(node_op<double>(N, ix, v), Q->cbase_dev, Q->qbase_dev,
+                                      with_cols ? Q->cols_dev : nullptr, Q->vals_dev);
+  count_launch();
+  return (int)cudaGetLastError();
+}
+
+extern "C" int fea_pcg_solve_mixed_nodes32(const fea_nodes_t* N, const int32_t* ix, const double* v,
+                                           const fea_f32_layout_t* Q, const double* b, double* x, double tol,
+                                           double inner_tol, int32_t max_iter, int32_t check_every, double* work,
+                                           int64_t work_len, int32_t* iters, int32_t* outer, double* relres,
+                                           cudaStream_t s) {
+  if (!nodes_ok(N) || !ix || !v || !layout_ok(Q) || !b || !x || !work || max_iter < 0) return FEA_EINVAL;
+  const int64_t n = N->ndof;
+  if (work_len < fea_pcg_mixed_work_len(n)) return FEA_EWORK;
+  if (iters) *iters = 0;
+  if (outer) *outer = 0;
+  if (relres) *relres = 0.0;
+  if (n == 0) return FEA_OK;
+  const NodeOp32q A32{Q->cbase_dev, Q->qbase_dev, Q->cols_dev, Q->vals_dev, N->mask_dev, N->dbase_dev,
+                      N->n_nodes, n};
+  return pcg_mixed(node_op<double>(N, ix, v), A32, n, b, x, tol, inner_tol, max_iter, check_every, work, iters,
+                   outer, relres, s);
 }
 
 // ---- batched PCG C ABI ------------------------------------------------------

@@ -320,13 +320,48 @@ class DevicePlan:
             L.check(st, "fea_pcg_solve")
         return int(it.value), float(rr.value), st
 
+    def f32_layout(self):
+        """The padded FP32 copy of this plan's matrix (fea_f32_layout_t):
+        per node, its column list and rows on 16-byte boundaries, padded to
+        multiples of 4.  Built once; fill_f32 writes the values."""
+        if getattr(self, "_f32q", None) is None:
+            mask = self.mask.cpu().numpy()
+            f = np.array([bin(int(m) & 7).count("1") for m in range(8)], np.int64)[mask]
+            L4 = np.where(mask != 0, (self.rowlen.cpu().numpy().astype(np.int64) + 3) & ~3, 0)
+            cbase = torch.from_numpy(np.concatenate([[0], np.cumsum(L4)])).to(self.device)
+            qbase = torch.from_numpy(np.concatenate([[0], np.cumsum(f * L4)])).to(self.device)
+            cols = torch.zeros(max(int(cbase[-1]), 4), dtype=torch.int32, device=self.device)
+            vals = torch.zeros(max(int(qbase[-1]), 4), dtype=torch.float32, device=self.device)
+            desc = L.F32Layout(cbase.data_ptr(), qbase.data_ptr(), cols.data_ptr(), vals.data_ptr())
+            self._f32q = (desc, cbase, qbase, cols, vals)
+            self._f32q_cols = False
+        return self._f32q
+
+    def fill_f32(self, values):
+        """FP32 values (and, the first time, the column lists) of the padded layout."""
+        desc = self.f32_layout()[0]
+        L.check(L.fea_f32_layout_fill(C.byref(self.nodes), vptr(self.indices), vptr(values), C.byref(desc),
+                                      int(not self._f32q_cols), stream()), "fea_f32_layout_fill")
+        self._f32q_cols = True
+        return desc
+
     def pcg_mixed(self, values, values32, b, x, tol, inner_tol, max_iter, check_every=20, raise_on_breakdown=True,
                   generic=False):
+        """FP32 inner CG with FP64 residual replacement, in place on x.
+        values32 None: the padded FP32 node layout, filled from values here
+        (128-bit loads); a float tensor: the plan's own layout (or CSR with
+        generic).  Returns (iterations, replacements, relres, status)."""
         n = self.ndof
         wl = L.fea_pcg_mixed_work_len(n)
         w = self.scratch(wl)
         it, outer, rr = C.c_int32(0), C.c_int32(0), C.c_double(0.0)
-        if generic:
+        if values32 is None and not generic:
+            desc = self.fill_f32(values)
+            st = L.fea_pcg_solve_mixed_nodes32(C.byref(self.nodes), vptr(self.indices), vptr(values), C.byref(desc),
+                                               vptr(b), vptr(x), float(tol), float(inner_tol), int(max_iter),
+                                               int(check_every), vptr(w), w.numel(), C.byref(it), C.byref(outer),
+                                               C.byref(rr), stream())
+        elif generic:
             st = L.fea_pcg_solve_mixed(n, vptr(self.indptr), vptr(self.indices), vptr(values), vptr(values32),
                                        vptr(b), vptr(x), float(tol), float(inner_tol), int(max_iter),
                                        int(check_every), vptr(w), w.numel(), C.byref(it), C.byref(outer),

@@ -63,6 +63,9 @@ class StaticImplicitSolver(BaseSolver):
                  device_line_search: bool = True) -> None:
         super().__init__()
         self.device_line_search = device_line_search
+        # FP32 inner solves: a residual replacement after every batch of
+        # iterations (0) or once the FP32 residual fell by this factor
+        self.inner_tol = 0.0
         self.maximum_iteration = maximum_iteration
         self.tol_error = tol_error
         self.rtol = rtol
@@ -289,9 +292,8 @@ class StaticImplicitSolver(BaseSolver):
     def _run_linear_inner(self, req):
         P = self.assembly.system
         if self.precision == "mixed":
-            v32 = P.to_f32(req.K)
-            req.it, outer, req.rr, req.status = P.pcg_mixed(req.K, v32, req.b, req.x, req.tol, 1e-4, req.cap,
-                                                            raise_on_breakdown=False)
+            req.it, outer, req.rr, req.status = P.pcg_mixed(req.K, None, req.b, req.x, req.tol, self.inner_tol,
+                                                            req.cap, raise_on_breakdown=False)
         else:
             req.it, req.rr, req.status = P.pcg(req.K, req.b, req.x, req.tol, req.cap, raise_on_breakdown=False)
 

@@ -285,7 +285,11 @@ int fea_pcg_solve(int64_t n, const int64_t* indptr_dev, const int32_t* indices_d
  * b - A x is formed in FP64 and replaces the FP32 one, and the recurrence
  * continues with the same search direction (residual replacement, no
  * restart).  The stop test is fea_pcg_solve's, on the FP64 residual.
- * values32_dev: float copy of values.  inner_tol: unused.  outer: number of
+ * values32_dev: float copy of values.  inner_tol > 0: a batch of
+ * check_every iterations ends in a replacement only once the FP32 r.D^-1 r
+ * has fallen below inner_tol times its value at the last replacement (or
+ * the stop test may pass, the FP32 recurrence broke down, or the cap is
+ * reached); inner_tol <= 0 replaces after every batch.  outer: number of
  * refinements.  work: fea_pcg_mixed_work_len(n) doubles. */
 int64_t fea_pcg_mixed_work_len(int64_t n);
 int fea_pcg_solve_mixed(int64_t n, const int64_t* indptr_dev, const int32_t* indices_dev,
@@ -317,6 +321,29 @@ int fea_pcg_solve_mixed_nodes(const fea_nodes_t* nodes, const int32_t* indices_d
                               double inner_tol, int32_t max_iter, int32_t check_every, double* work_dev,
                               int64_t work_len, int32_t* iters, int32_t* outer, double* relres,
                               cudaStream_t stream);
+/* The mixed solver on an FP32 copy of the plan's matrix in a padded layout:
+ * node n's column list starts at cbase[n] and its row j at qbase[n] + j *
+ * (cbase[n+1] - cbase[n]); both are multiples of 4 and every list is padded
+ * to a multiple of 4 entries (column 0, value 0), so that the FP32 SpMV
+ * reads 4 columns and 4 values of each row with 128-bit loads, one warp per
+ * node.  cbase / qbase are prefix sums over the nodes of L4 = rowlen rounded
+ * up to 4 (0 for a node without free DOFs) and of popcount(mask) * L4.
+ * fea_f32_layout_fill writes vals_dev (and cols_dev when with_cols != 0)
+ * from the FP64 values in the plan's layout.  No counterpart in the
+ * reference (its solves are FP64 throughout). */
+typedef struct {
+  const int64_t* cbase_dev;   /* [N+1] */
+  const int64_t* qbase_dev;   /* [N+1] */
+  int32_t* cols_dev;          /* [cbase[N]] */
+  float* vals_dev;            /* [qbase[N]] */
+} fea_f32_layout_t;
+int fea_f32_layout_fill(const fea_nodes_t* nodes, const int32_t* indices_dev, const double* values_dev,
+                        fea_f32_layout_t* layout, int32_t with_cols, cudaStream_t stream);
+int fea_pcg_solve_mixed_nodes32(const fea_nodes_t* nodes, const int32_t* indices_dev, const double* values_dev,
+                                const fea_f32_layout_t* layout, const double* b_dev, double* x_dev, double tol,
+                                double inner_tol, int32_t max_iter, int32_t check_every, double* work_dev,
+                                int64_t work_len, int32_t* iters, int32_t* outer, double* relres,
+                                cudaStream_t stream);
 /* ---------------------------------------------------------------------------
  * Batched Jacobi-PCG over independent systems ("slots"), for serving many
  * static solves at once (no counterpart in the reference, which solves one
