@@ -255,6 +255,8 @@ class Assembly:
                 mats.append(e)
             off += ins.part.nodes.shape[0]
         for ld in self._loads.values():
+            if not isinstance(ld, Pressure):              # point loads act on reference points only
+                continue
             o = self._node_offset[ld.instance_name]
             for s in ld.surface_element:
                 faces.append((s.kind, s._elems.numpy() + o))

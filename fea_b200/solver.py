@@ -508,7 +508,7 @@ class DynamicImplicitSolver(StaticImplicitSolver):
             self._iter_now += 1
             rmax = float(R.abs().max()) if R.numel() else 0.0
             self.history.append(dict(iter=self._iter_now, rmax=rmax, rnorm=float(R.norm())))
-            req = self._linear_request(Kv, -R, self._iter_now, alpha, dGC, srmax=srmax)
+            req = self._linear_request(Kv, -R, self._iter_now, alpha, dGC)
             self._run_linear(req)
             dGC = self._linear_finish(req, Kv, -R)
             alpha, GCnew, energy_new = self._dyn_line_search(GC_now, GC_pre, dGC, R, energy, deltaT)

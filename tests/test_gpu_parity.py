@@ -131,7 +131,9 @@ def test_explicit_fp32_variant_close(golden):
     c.initialize()
     c.solver._deltaT = dt
     c.solver.solve(GC0=torch.zeros_like(c.assembly.GC), GV0=torch.from_numpy(g["gv0"]).cuda())
-    assert rel(c.solver._GC_list[-1], g["u_final"]) < 1e-3
+    # FP32 element force with FP64 nodal sums: 1.35e-5 of the FP64 reference
+    # run after the fixture's 40 steps (measured on a B200)
+    assert rel(c.solver._GC_list[-1], g["u_final"]) < 3e-5
 
 
 @pytest.mark.parametrize("kind,dofs", [("C3D8", (0, 1, 2)), ("C3D4", (2,)), ("C3D8", (0, 2))])

@@ -9,8 +9,8 @@
   oracle's loop, within 1e-12.
 - The 40^3 compliance block: the residual VJP (lam . dR/dX, lam . dR/dmu)
   against torch autograd of the oracle's residual, within 1e-12.
-- A C3D8 fan whose axis nodes have 75 neighbours: rows longer than the
-  32-block pass of the node-row gather, against the oracle.
+- A C3D8 fan whose middle axis node has 50 active neighbours: rows longer
+  than the 32-block pass of the node-row gather, against the oracle.
 """
 import math
 
@@ -185,7 +185,8 @@ def test_config5_residual_vjp_40cube():
 def fan_mesh(M=12, layers=2):
     """C3D8 fan around the z axis: M kite-shaped sectors (axis node, ring
     node, outer node, next ring node) extruded over ``layers`` layers; the
-    inner axis node is shared by 2M hexes and has 3 + 6M neighbours."""
+    inner axis node is shared by 2M hexes and has 3 + 6M neighbours, 2 + 4M
+    of them active when the bottom plane is clamped."""
     th = 2 * math.pi * np.arange(M) / M
     ring = np.stack([np.cos(th), np.sin(th)], 1)
     outer = 1.6 * np.stack([np.cos(th + math.pi / M), np.sin(th + math.pi / M)], 1)
@@ -219,7 +220,7 @@ def test_high_valence_c3d8_node_rows():
     P = asm.plan
     adj = P.adjptr.cpu().numpy() if hasattr(P, "adjptr") else None
     if adj is not None:
-        assert int(np.diff(adj).max()) == 3 + 6 * M              # the middle axis node: rows of 75 blocks
+        assert int(np.diff(adj).max()) == 2 + 4 * M              # the middle axis node: rows of 50 blocks
     m = O.Model(X, [O.Group("C3D8", el, 1.0, 50.0)], [], [(fixed, (0, 1, 2))])
     gc = 1e-2 * torch.randn(int(m.free_mask().sum()), generator=torch.Generator().manual_seed(7),
                             dtype=torch.float64)
