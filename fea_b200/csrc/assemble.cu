@@ -319,12 +319,16 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
 // node's region to shared memory with coalesced loads, sums it per upper
 // column block and writes each block into the node's rows and its transpose
 // into the column node's rows: every CSR value written once.
+// Five CTAs per SM: 45,568 bytes of shared memory (plus the 1 KB the
+// driver reserves per CTA) five times fit the SM's 228 KB, and the launch
+// bound holds the kernel to 168 registers (64 threads x 5 CTAs x 168 <= 64K):
+// 10 warps per SM instead of 8 (k_hex_elem 683.6 -> 589.6 us at 64^3).
 constexpr int HX_EPB = 8;                 // elements per CTA
 constexpr int HX_TPB = 8 * HX_EPB;        // threads per CTA
 constexpr int HX_VB = 10;                 // doubles per (gp, node) vector slot: q, f, g + pad
 constexpr int HX_VG = 82;                 // doubles per Gauss point (8 slots + 2 pad, 16-byte rows)
-constexpr int HX_SC = 8 * HX_VG;          // offset of the per-Gauss-point scalars (8 each)
-constexpr int HX_EL = HX_SC + 64;         // doubles per element (16-byte aligned)
+constexpr int HX_SC = 8 * HX_VG;          // offset of the per-Gauss-point scalars (7 each)
+constexpr int HX_EL = HX_SC + 56;         // doubles per element (7 scalars per Gauss point)
 constexpr int HX_GW = 4;                  // warps (row nodes) per gather CTA
 
 // Offset of the residual slots in the C3D8 scratch: after the staged blocks,
@@ -337,7 +341,7 @@ __device__ __forceinline__ double csx(int c) { return (((c + 1) >> 1) & 1) ? 1.0
 __device__ __forceinline__ double csy(int c) { return ((c >> 1) & 1) ? 1.0 : -1.0; }
 __device__ __forceinline__ double csz(int c) { return (c >> 2) ? 1.0 : -1.0; }
 template <bool ER>
-__global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __restrict__ stage,
+__global__ void __launch_bounds__(HX_TPB, 5) k_hex_elem(VolParams P, double* __restrict__ stage,
                                                      double* __restrict__ rslot) {
   __shared__ __align__(16) double sv[HX_EPB * HX_EL];
   const double q3 = 0.57735026918962576451;   // 1/sqrt(3)
@@ -383,7 +387,7 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
 #pragma unroll
     for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];
     const double I1 = Jm * sF2, muJm = mu * Jm;
-    double* S = V + HX_SC + lane * 8;
+    double* S = V + HX_SC + lane * 7;
     S[0] = w * (-2.0 / 3.0 * muJm);                                 // w alpha
     S[1] = w * (kappa * J * (2.0 * J - 1.0) + 2.0 / 9.0 * mu * I1);  // w beta
     S[2] = w * (mu * I1 / 3.0 - kappa * J * (J - 1.0));              // w gamma
@@ -436,7 +440,7 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
     for (int i = 0; i < 9; ++i) acc[d][i] = 0.0;
 #pragma unroll 1
   for (int g = 0; g < (act ? 8 : 0); ++g) {
-    const double* S = V + HX_SC + g * 8;
+    const double* S = V + HX_SC + g * 7;
     const double wa = S[0], wb = S[1], wg = S[2], wc = S[3], wc2 = S[4];
     const double* Va = V + g * HX_VG + a * HX_VB;
     double qa[3], fa[3], ga[3], A[3], B[3], Cc[3];
@@ -494,11 +498,11 @@ __global__ void __launch_bounds__(HX_TPB) k_hex_elem(VolParams P, double* __rest
   if (act) {
     const int32_t rb = P.recbase[e * 8 + a];
     if (rb >= 0) {
-      const double na = V[HX_SC + a * 8 + 5];
+      const double na = V[HX_SC + a * 7 + 5];
       double* out = stage + (int64_t)rb * 9;
 #pragma unroll
       for (int b = 0; b < 8; ++b) {
-        const double* Sb = V + HX_SC + b * 8;
+        const double* Sb = V + HX_SC + b * 7;
         if (Sb[6] == 0.0 || Sb[5] < na) continue;
         const int d = (b - a) & 7;
         if (d < 4 || (d == 4 && a < 4)) {

@@ -359,8 +359,7 @@ __global__ void __launch_bounds__(PCG_TPB) k_spmv_node_sub(NodeOp<V> A, const X*
 // FP32 copy of the node-row matrix in a padded layout: every node's column
 // list and each of its rows start on a 16-byte boundary and are padded to a
 // multiple of 4 entries (column 0, value 0), so that a lane reads 4 columns
-// and the 4 values of each row with 128-bit loads.  One warp per node, 128
-// columns per pass (one pass for a solid interior node).
+// and the 4 values of each row with 128-bit loads.
 struct NodeOp32q {
   const int64_t* __restrict__ cbase;   // [N+1] first padded column of node n
   const int64_t* __restrict__ qbase;   // [N+1] first value of node n's rows
@@ -372,75 +371,89 @@ struct NodeOp32q {
   int64_t n;
 };
 
-template <class X>
+// LPN lanes per node (32 / LPN nodes per warp), 4 columns per lane per
+// pass: the next nodes' metadata are loaded while the current ones are
+// processed; loops and shuffles warp-uniform.
+#ifndef FEA_F32Q_LPN
+#define FEA_F32Q_LPN 8
+#endif
+template <int LPN, class X>
 __global__ void __launch_bounds__(PCG_TPB) k_spmv_node32q(NodeOp32q A, const X* __restrict__ x, X* __restrict__ y,
                                                           double* st, double* part, unsigned* counter, int mode) {
   if (mode == 1 && st[S_DONE] != 0.0) return;
+  constexpr int NPW = 32 / LPN;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const int64_t step = (int64_t)gridDim.x * PCG_WARPS;
+  const int sub = lane / LPN, hl = lane % LPN;
+  const int64_t step = (int64_t)gridDim.x * PCG_WARPS * NPW;
   double contrib = 0.0;
-  int64_t nd = (int64_t)blockIdx.x * PCG_WARPS + warp;
+  int64_t base = ((int64_t)blockIdx.x * PCG_WARPS + warp) * NPW;
+  int64_t nd = base + sub;
   unsigned m = 0;
   int64_t cb = 0, ce = 0, qb = 0;
+  int32_t db = 0;
   if (nd < A.n_nodes) {
     m = A.mask[nd];
     cb = A.cbase[nd];
     ce = A.cbase[nd + 1];
     qb = A.qbase[nd];
+    db = A.dbase[nd];
   }
-  while (nd < A.n_nodes) {                       // warp-uniform
+  for (; base < A.n_nodes; base += step) {       // warp-uniform
     const int64_t nx = nd + step;
     unsigned m2 = 0;
     int64_t cb2 = 0, ce2 = 0, qb2 = 0;
-    if (nx < A.n_nodes) {                        // the next node's metadata, loaded ahead
+    int32_t db2 = 0;
+    if (nx < A.n_nodes) {                        // the next nodes' metadata, loaded ahead
       m2 = A.mask[nx];
       cb2 = A.cbase[nx];
       ce2 = A.cbase[nx + 1];
       qb2 = A.qbase[nx];
+      db2 = A.dbase[nx];
     }
-    if (m) {
-      const int f = popc3(m);
-      const int L4 = (int)(ce - cb);
-      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-      for (int q0 = 0; q0 < L4; q0 += 128) {
-        const int q = q0 + 4 * lane;
-        const bool h = q < L4;
-        const int4 c = h ? __ldg(reinterpret_cast<const int4*>(A.cols + cb + q)) : make_int4(0, 0, 0, 0);
-        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 v0 = h ? __ldcs(reinterpret_cast<const float4*>(A.vals + qb + q)) : z4;
-        const float4 v1 = (h && f > 1) ? __ldcs(reinterpret_cast<const float4*>(A.vals + qb + L4 + q)) : z4;
-        const float4 v2 = (h && f > 2) ? __ldcs(reinterpret_cast<const float4*>(A.vals + qb + 2 * L4 + q)) : z4;
-        double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
-        if (h) {
-          x0 = (double)x[c.x];
-          x1 = (double)x[c.y];
-          x2 = (double)x[c.z];
-          x3 = (double)x[c.w];
-        }
-        s0 += (double)v0.x * x0 + (double)v0.y * x1 + (double)v0.z * x2 + (double)v0.w * x3;
-        s1 += (double)v1.x * x0 + (double)v1.y * x1 + (double)v1.z * x2 + (double)v1.w * x3;
-        s2 += (double)v2.x * x0 + (double)v2.y * x1 + (double)v2.z * x2 + (double)v2.w * x3;
-      }
+    const int f = popc3(m);
+    const int L4 = m ? (int)(ce - cb) : 0;
+    int Lmax = L4;
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    for (int o = 16; o >= LPN; o >>= 1) Lmax = max(Lmax, __shfl_xor_sync(0xffffffffu, Lmax, o));
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int q0 = 0; q0 < Lmax; q0 += 4 * LPN) {
+      const int q = q0 + 4 * hl;
+      const bool h = q < L4;
+      const int4 c = h ? __ldg(reinterpret_cast<const int4*>(A.cols + cb + q)) : make_int4(0, 0, 0, 0);
+      const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 v0 = h ? __ldcs(reinterpret_cast<const float4*>(A.vals + qb + q)) : z4;
+      const float4 v1 = (h && f > 1) ? __ldcs(reinterpret_cast<const float4*>(A.vals + qb + L4 + q)) : z4;
+      const float4 v2 = (h && f > 2) ? __ldcs(reinterpret_cast<const float4*>(A.vals + qb + 2 * L4 + q)) : z4;
+      double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
+      if (h) {
+        x0 = (double)x[c.x];
+        x1 = (double)x[c.y];
+        x2 = (double)x[c.z];
+        x3 = (double)x[c.w];
       }
-      if (lane == 0) {
-        const int64_t r = A.dbase[nd];
-        y[r] = (X)s0;
-        contrib += s0 * (double)x[r];
-        if (f > 1) { y[r + 1] = (X)s1; contrib += s1 * (double)x[r + 1]; }
-        if (f > 2) { y[r + 2] = (X)s2; contrib += s2 * (double)x[r + 2]; }
-      }
+      s0 += (double)v0.x * x0 + (double)v0.y * x1 + (double)v0.z * x2 + (double)v0.w * x3;
+      s1 += (double)v1.x * x0 + (double)v1.y * x1 + (double)v1.z * x2 + (double)v1.w * x3;
+      s2 += (double)v2.x * x0 + (double)v2.y * x1 + (double)v2.z * x2 + (double)v2.w * x3;
+    }
+#pragma unroll
+    for (int o = LPN / 2; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o, LPN);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o, LPN);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o, LPN);
+    }
+    if (m && hl < f) {
+      const int64_t r = db + hl;
+      const double sr = hl == 0 ? s0 : (hl == 1 ? s1 : s2);
+      y[r] = (X)sr;
+      contrib += sr * (double)x[r];
     }
     nd = nx;
     m = m2;
     cb = cb2;
     ce = ce2;
     qb = qb2;
+    db = db2;
   }
   if (mode == 1) finish_pq(contrib, st, part, counter);
 }
@@ -767,8 +780,9 @@ static void spmv(const NodeOp<V>& A, const X* x, X* y, double* st, double* part,
 template <class X>
 static void spmv(const NodeOp32q& A, const X* x, X* y, double* st, double* part, unsigned* counter, int mode,
                  cudaStream_t s) {
-  k_spmv_node32q<X><<<occ_grid(k_spmv_node32q<X>, A.n_nodes, PCG_WARPS), PCG_TPB, 0, s>>>(A, x, y, st, part,
-                                                                                        counter, mode);
+  constexpr int LPN = FEA_F32Q_LPN;
+  k_spmv_node32q<LPN, X><<<occ_grid(k_spmv_node32q<LPN, X>, A.n_nodes, PCG_WARPS * (32 / LPN)), PCG_TPB, 0, s>>>(
+      A, x, y, st, part, counter, mode);
   count_launch();
 }
 
