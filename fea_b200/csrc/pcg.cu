@@ -378,8 +378,8 @@ struct NodeOp32q {
 #define FEA_F32Q_LPN 8
 #endif
 template <int LPN, class X>
-__global__ void __launch_bounds__(PCG_TPB) k_spmv_node32q(NodeOp32q A, const X* __restrict__ x, X* __restrict__ y,
-                                                          double* st, double* part, unsigned* counter, int mode) {
+__global__ void __launch_bounds__(PCG_TPB, 4) k_spmv_node32q(NodeOp32q A, const X* __restrict__ x, X* __restrict__ y,
+                                                             double* st, double* part, unsigned* counter, int mode) {
   if (mode == 1 && st[S_DONE] != 0.0) return;
   constexpr int NPW = 32 / LPN;
   const int lane = threadIdx.x & 31;
@@ -416,7 +416,9 @@ __global__ void __launch_bounds__(PCG_TPB) k_spmv_node32q(NodeOp32q A, const X* 
     int Lmax = L4;
 #pragma unroll
     for (int o = 16; o >= LPN; o >>= 1) Lmax = max(Lmax, __shfl_xor_sync(0xffffffffu, Lmax, o));
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    // FP32 products and row sums (the inner solve is FP32; its residual is
+    // refined in FP64), FP64 for the p.q contribution
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
     for (int q0 = 0; q0 < Lmax; q0 += 4 * LPN) {
       const int q = q0 + 4 * hl;
       const bool h = q < L4;
@@ -425,16 +427,16 @@ __global__ void __launch_bounds__(PCG_TPB) k_spmv_node32q(NodeOp32q A, const X* 
       const float4 v0 = h ? __ldcs(reinterpret_cast<const float4*>(A.vals + qb + q)) : z4;
       const float4 v1 = (h && f > 1) ? __ldcs(reinterpret_cast<const float4*>(A.vals + qb + L4 + q)) : z4;
       const float4 v2 = (h && f > 2) ? __ldcs(reinterpret_cast<const float4*>(A.vals + qb + 2 * L4 + q)) : z4;
-      double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
+      float x0 = 0.f, x1 = 0.f, x2 = 0.f, x3 = 0.f;
       if (h) {
-        x0 = (double)x[c.x];
-        x1 = (double)x[c.y];
-        x2 = (double)x[c.z];
-        x3 = (double)x[c.w];
+        x0 = (float)x[c.x];
+        x1 = (float)x[c.y];
+        x2 = (float)x[c.z];
+        x3 = (float)x[c.w];
       }
-      s0 += (double)v0.x * x0 + (double)v0.y * x1 + (double)v0.z * x2 + (double)v0.w * x3;
-      s1 += (double)v1.x * x0 + (double)v1.y * x1 + (double)v1.z * x2 + (double)v1.w * x3;
-      s2 += (double)v2.x * x0 + (double)v2.y * x1 + (double)v2.z * x2 + (double)v2.w * x3;
+      s0 += v0.x * x0 + v0.y * x1 + v0.z * x2 + v0.w * x3;
+      s1 += v1.x * x0 + v1.y * x1 + v1.z * x2 + v1.w * x3;
+      s2 += v2.x * x0 + v2.y * x1 + v2.z * x2 + v2.w * x3;
     }
 #pragma unroll
     for (int o = LPN / 2; o > 0; o >>= 1) {
@@ -444,7 +446,7 @@ __global__ void __launch_bounds__(PCG_TPB) k_spmv_node32q(NodeOp32q A, const X* 
     }
     if (m && hl < f) {
       const int64_t r = db + hl;
-      const double sr = hl == 0 ? s0 : (hl == 1 ? s1 : s2);
+      const double sr = (double)(hl == 0 ? s0 : (hl == 1 ? s1 : s2));
       y[r] = (X)sr;
       contrib += sr * (double)x[r];
     }
