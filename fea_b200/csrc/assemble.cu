@@ -95,7 +95,7 @@ __device__ __forceinline__ void gauss_kin(const VolParams& P, const int32_t* cn,
   for (int I = 0; I < 3; ++I)
 #pragma unroll
     for (int i = 0; i < 3; ++i)
-      F[3 * I + i] = (I == i ? 1.0 : 0.0) + Ju[3 * I] * iJ[i] + Ju[3 * I + 1] * iJ[3 + i] + Ju[3 * I + 2] * iJ[6 + i];
+      F[3 * I + i] = fma(Ju[3 * I], iJ[i], fma(Ju[3 * I + 1], iJ[3 + i], fma(Ju[3 * I + 2], iJ[6 + i], I == i ? 1.0 : 0.0)));
   J = inv3(F, iF);
 }
 
@@ -165,18 +165,27 @@ __device__ __forceinline__ void element_strip(const VolParams& P, const int32_t*
       double wc = w * muJm;
 #pragma unroll
       for (int m = 0; m < 3; ++m) gm[m] = wc * (iJ[3 * m] * gav[0] + iJ[3 * m + 1] * gav[1] + iJ[3 * m + 2] * gav[2]);
+      // fused multiply-add chains; the delta term only on the diagonal
 #pragma unroll
       for (int j = 0; j < 3; ++j)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
           double h[3];
 #pragma unroll
-          for (int m = 0; m < 3; ++m)
-            h[m] = va[j] * Mq[3 * m + k] + ua[j] * Mf[3 * m + k] + ga[k] * Mq[3 * m + j] + (j == k ? gm[m] : 0.0);
+          for (int m = 0; m < 3; ++m) {
+            double t = ga[k] * Mq[3 * m + j];
+            t = fma(ua[j], Mf[3 * m + k], t);
+            t = fma(va[j], Mq[3 * m + k], t);
+            h[m] = j == k ? t + gm[m] : t;
+          }
 #pragma unroll
-          for (int b = 0; b < NN; ++b)
-            acc[b][3 * j + k] += Elem<NN>::dxi(g, b, 0) * h[0] + Elem<NN>::dxi(g, b, 1) * h[1] +
-                                 Elem<NN>::dxi(g, b, 2) * h[2];
+          for (int b = 0; b < NN; ++b) {
+            double t = acc[b][3 * j + k];
+            t = fma(Elem<NN>::dxi(g, b, 0), h[0], t);
+            t = fma(Elem<NN>::dxi(g, b, 1), h[1], t);
+            t = fma(Elem<NN>::dxi(g, b, 2), h[2], t);
+            acc[b][3 * j + k] = t;
+          }
         }
     }
   }
@@ -303,7 +312,7 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
 // ---- C3D8 R + K: element kernel + staged-block gather -----------------------
 // k_hex_elem evaluates every element ONCE: 8 lanes per element, lane g
 // computes the kinematics of Gauss point g and the vectors q_b = F^-T g_b,
-// f_b = F g_b, g_b of all 8 nodes into shared memory; then lane a builds the
+// f_b = F g_b of all 8 nodes into shared memory; then lane a builds the
 // upper-triangular blocks K_ab it owns (circulant assignment: b = a + d mod 8,
 // d = 0..3, plus d = 4 for a < 4 — 36 blocks over 8 lanes) with its own row
 // vectors in registers,
@@ -319,17 +328,24 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
 // node's region to shared memory with coalesced loads, sums it per upper
 // column block and writes each block into the node's rows and its transpose
 // into the column node's rows: every CSR value written once.
-// Five CTAs per SM: 45,568 bytes of shared memory (plus the 1 KB the
-// driver reserves per CTA) five times fit the SM's 228 KB, and the launch
-// bound holds the kernel to 168 registers (64 threads x 5 CTAs x 168 <= 64K):
-// 10 warps per SM instead of 8 (k_hex_elem 683.6 -> 589.6 us at 64^3).
+// g_b itself is not staged: g_a . g_b = (F^-1 f_a) . (F^T q_b) = f_a . q_b,
+// so a (Gauss point, node) slot holds 6 doubles and an element 456: 29,184
+// bytes of shared memory per CTA.  Six CTAs per SM: the launch bound holds
+// the kernel to 168 registers (64 threads x 6 CTAs x 168 <= 64K), 12 warps
+// per SM (k_hex_elem 544.3 -> 474.6 us at 64^3 against 45,568 bytes and five
+// CTAs).
+constexpr int HX_CTAS = 6;                // resident CTAs per SM the launch bound asks for
 constexpr int HX_EPB = 8;                 // elements per CTA
 constexpr int HX_TPB = 8 * HX_EPB;        // threads per CTA
-constexpr int HX_VB = 10;                 // doubles per (gp, node) vector slot: q, f, g + pad
-constexpr int HX_VG = 82;                 // doubles per Gauss point (8 slots + 2 pad, 16-byte rows)
+constexpr int HX_VB = 6;                  // doubles per (gp, node) vector slot: q, f (16-byte aligned)
+constexpr int HX_VG = 50;                 // doubles per Gauss point (8 slots + 2 pad: conflict-free rows)
 constexpr int HX_SC = 8 * HX_VG;          // offset of the per-Gauss-point scalars (7 each)
 constexpr int HX_EL = HX_SC + 56;         // doubles per element (7 scalars per Gauss point)
-constexpr int HX_GW = 4;                  // warps (row nodes) per gather CTA
+constexpr int HX_GW = 4;                  // warps per gather CTA
+// Gather lanes per row node: 16 (two nodes per warp: 397.0 against 461.4 us
+// with 32 lanes per node at 64^3, where rows hold 27 blocks and regions 36),
+// 32 when two regions per warp would not fit the shared memory.
+constexpr int HX_LPN = 16;
 
 // Offset of the residual slots in the C3D8 scratch: after the staged blocks,
 // rounded to 16 bytes.
@@ -341,7 +357,7 @@ __device__ __forceinline__ double csx(int c) { return (((c + 1) >> 1) & 1) ? 1.0
 __device__ __forceinline__ double csy(int c) { return ((c >> 1) & 1) ? 1.0 : -1.0; }
 __device__ __forceinline__ double csz(int c) { return (c >> 2) ? 1.0 : -1.0; }
 template <bool ER>
-__global__ void __launch_bounds__(HX_TPB, 5) k_hex_elem(VolParams P, double* __restrict__ stage,
+__global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, double* __restrict__ stage,
                                                      double* __restrict__ rslot) {
   __shared__ __align__(16) double sv[HX_EPB * HX_EL];
   const double q3 = 0.57735026918962576451;   // 1/sqrt(3)
@@ -379,7 +395,7 @@ __global__ void __launch_bounds__(HX_TPB, 5) k_hex_elem(VolParams P, double* __r
     for (int I = 0; I < 3; ++I)
 #pragma unroll
       for (int i = 0; i < 3; ++i)
-        F[3 * I + i] = (I == i ? 1.0 : 0.0) + Ju[3 * I] * iJ[i] + Ju[3 * I + 1] * iJ[3 + i] + Ju[3 * I + 2] * iJ[6 + i];
+        F[3 * I + i] = fma(Ju[3 * I], iJ[i], fma(Ju[3 * I + 1], iJ[3 + i], fma(Ju[3 * I + 2], iJ[6 + i], I == i ? 1.0 : 0.0)));
     const double J = inv3(F, iF);
     const double mu = P.mu, kappa = P.kappa;
     const double Jm = jm23(J);
@@ -413,19 +429,16 @@ __global__ void __launch_bounds__(HX_TPB, 5) k_hex_elem(VolParams P, double* __r
       const double sx = (((b + 1) >> 1) & 1) ? 1.0 : -1.0, sy = ((b >> 1) & 1) ? 1.0 : -1.0, sz = (b >> 2) ? 1.0 : -1.0;
       const double fx = sx > 0 ? fxp : fxm, fy = sy > 0 ? fyp : fym, fz = sz > 0 ? fzp : fzm;
       const double d0 = 0.125 * sx * fy * fz, d1 = 0.125 * sy * fx * fz, d2 = 0.125 * sz * fx * fy;
-      double v[9];
+      double v[6];
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         v[k] = d0 * Mq[k] + d1 * Mq[3 + k] + d2 * Mq[6 + k];
         v[3 + k] = d0 * Mf[k] + d1 * Mf[3 + k] + d2 * Mf[6 + k];
-        v[6 + k] = d0 * iJ[k] + d1 * iJ[3 + k] + d2 * iJ[6 + k];
       }
       double2* o = reinterpret_cast<double2*>(Vg + b * HX_VB);   // 16-byte aligned slot
       o[0] = make_double2(v[0], v[1]);
       o[1] = make_double2(v[2], v[3]);
       o[2] = make_double2(v[4], v[5]);
-      o[3] = make_double2(v[6], v[7]);
-      Vg[b * HX_VB + 8] = v[8];
     }
   }
   __syncwarp();
@@ -443,37 +456,47 @@ __global__ void __launch_bounds__(HX_TPB, 5) k_hex_elem(VolParams P, double* __r
     const double* S = V + HX_SC + g * 7;
     const double wa = S[0], wb = S[1], wg = S[2], wc = S[3], wc2 = S[4];
     const double* Va = V + g * HX_VG + a * HX_VB;
-    double qa[3], fa[3], ga[3], A[3], B[3], Cc[3];
+    double qa[3], fa[3], gm[3], A[3], B[3], Cc[3];
     {
       const double2* v2 = reinterpret_cast<const double2*>(Va);
-      const double2 x0 = v2[0], x1 = v2[1], x2 = v2[2], x3 = v2[3];
+      const double2 x0 = v2[0], x1 = v2[1], x2 = v2[2];
       qa[0] = x0.x; qa[1] = x0.y; qa[2] = x1.x; fa[0] = x1.y; fa[1] = x2.x; fa[2] = x2.y;
-      ga[0] = x3.x; ga[1] = x3.y; ga[2] = Va[8];
+      gm[0] = wc * fa[0]; gm[1] = wc * fa[1]; gm[2] = wc * fa[2];       // w mu J^-2/3 f_a
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       A[k] = wa * fa[k] + wb * qa[k];
       B[k] = wa * qa[k];
       Cc[k] = wg * qa[k];
-      racc[k] += wc * fa[k] + wc2 * qa[k];
+      racc[k] = fma(wc, fa[k], racc[k]);
+      racc[k] = fma(wc2, qa[k], racc[k]);
     }
 #pragma unroll
     for (int d = 0; d < 5; ++d) {
       if (d == 4 && nb == 4) break;
       const double* Vb = V + g * HX_VG + ((a + d) & 7) * HX_VB;
-      double qb[3], fb[3], gb[3];
+      double qb[3], fb[3];
       {
         const double2* v2 = reinterpret_cast<const double2*>(Vb);
-        const double2 x0 = v2[0], x1 = v2[1], x2 = v2[2], x3 = v2[3];
+        const double2 x0 = v2[0], x1 = v2[1], x2 = v2[2];
         qb[0] = x0.x; qb[1] = x0.y; qb[2] = x1.x; fb[0] = x1.y; fb[1] = x2.x; fb[2] = x2.y;
-        gb[0] = x3.x; gb[1] = x3.y; gb[2] = Vb[8];
       }
-      const double dg = wc * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
+      const double dg = gm[0] * qb[0] + gm[1] * qb[1] + gm[2] * qb[2];    // w mu J^-2/3 g_a . g_b
+      // three fused multiply-adds into each accumulator, the delta term on
+      // the diagonal alone: 33 FP64 operations per block and Gauss point
 #pragma unroll
       for (int j = 0; j < 3; ++j)
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
-          acc[d][3 * j + k] += A[j] * qb[k] + B[j] * fb[k] + qb[j] * Cc[k] + (j == k ? dg : 0.0);
+        for (int k = 0; k < 3; ++k) {
+          double t = acc[d][3 * j + k];
+          t = fma(A[j], qb[k], t);
+          t = fma(B[j], fb[k], t);
+          t = fma(qb[j], Cc[k], t);
+          acc[d][3 * j + k] = t;
+        }
+      acc[d][0] += dg;
+      acc[d][4] += dg;
+      acc[d][8] += dg;
     }
   }
   // ---- phase 3: upper block row a to the incidence record --------------------
@@ -540,13 +563,17 @@ __global__ void __launch_bounds__(HX_TPB, 5) k_hex_elem(VolParams P, double* __r
 // lanes' block metadata and residual slots are loaded before the region
 // copy.  capb = the most staged blocks of one node (shared memory per warp:
 // capb blocks).
-template <bool WR, bool ACC>
+template <bool WR, bool ACC, int LPN>
 __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const double* __restrict__ stage,
                                                         const double* __restrict__ rslot, int capb) {
   extern __shared__ __align__(16) double gsm[];
+  static_assert(LPN == 8 || LPN == 16 || LPN == 32, "lanes per node");
+  constexpr int NPW = 32 / LPN;                   // nodes per warp
   const int warp = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
-  const int64_t n = (int64_t)blockIdx.x * HX_GW + warp;
+  const int sub = (threadIdx.x & 31) / LPN;
+  const int lane = (threadIdx.x & 31) % LPN;      // lane within the node's group
+  const unsigned gmask = LPN == 32 ? 0xffffffffu : (((1u << LPN) - 1u) << (sub * LPN));
+  const int64_t n = ((int64_t)blockIdx.x * HX_GW + warp) * NPW + sub;
   if (n >= P.n_nodes) return;
   const unsigned mn = P.mask[n];
   if (!mn) return;
@@ -577,14 +604,14 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
 #pragma unroll
     for (int j = 0; j < 3; ++j) rq[j] = sr[j];
   }
-  double* S = gsm + (int64_t)warp * capb * 9;
+  double* S = gsm + (int64_t)(warp * NPW + sub) * capb * 9;
   {
     // the region copy as asynchronous 8-byte global-to-shared copies (no
     // register round trip; 461.8 against 472.3 us for load-and-store at 64^3)
     const double* src = stage + b0 * 9;
     const int nd = nbk * 9;
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(S);
-    for (int i = lane; i < nd; i += 32)
+    for (int i = lane; i < nd; i += LPN)
       asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sbase + 8u * (unsigned)i), "l"(src + i)
                    : "memory");
     asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -592,7 +619,7 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
   }
   double r[3] = {0.0, 0.0, 0.0};
   if (WR) {                                      // warp-uniform: incidences in order
-    for (int qb = 0; qb < nq; qb += 32) {
+    for (int qb = 0; qb < nq; qb += LPN) {
       if (qb > 0) {
         rq[0] = rq[1] = rq[2] = 0.0;
         if (qb + lane < nq) {
@@ -601,14 +628,14 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
           for (int j = 0; j < 3; ++j) rq[j] = sr[j];
         }
       }
-      const int m = min(32, nq - qb);
+      const int m = min(LPN, nq - qb);
       for (int i = 0; i < m; ++i) {
 #pragma unroll
-        for (int j = 0; j < 3; ++j) r[j] += __shfl_sync(0xffffffffu, rq[j], i);
+        for (int j = 0; j < 3; ++j) r[j] += __shfl_sync(gmask, rq[j], i, LPN);
       }
     }
   }
-  __syncwarp();
+  __syncwarp(gmask);
   const int L = P.rowlen[n];
   const int64_t vb = P.vbase[n];
   while (p < p1) {
@@ -663,7 +690,7 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
           }
       }
     }
-    p += 32;                                     // rows of more than 32 blocks
+    p += LPN;                                 // rows of more blocks than the group has lanes
     c = -1;
     if (p < p1) {
       c = P.adjcol[p];
@@ -1418,7 +1445,10 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
     const bool acc = accumulate != 0, wr = R != nullptr, er = elemR != nullptr;
     if (hex) {
       const int capb = std::max<int>(G->maxblk, 1);
-      const size_t gbytes = (size_t)HX_GW * capb * 9 * sizeof(double);
+      const size_t region = (size_t)capb * 9 * sizeof(double);
+      const bool two = (size_t)HX_GW * (32 / HX_LPN) * region <= (size_t)smem_limit();
+      const int lpn = two ? HX_LPN : 32;
+      const size_t gbytes = (size_t)HX_GW * (32 / lpn) * region;
       if (gbytes > (size_t)smem_limit()) return FEA_ESMEM;
       double* rslot = work + hx_rslot_base(G->nblk);
       const unsigned grid = (unsigned)((G->ne + HX_EPB - 1) / HX_EPB);
@@ -1428,11 +1458,14 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
         count_launch();
         if (cudaError_t ce = cudaGetLastError()) return (int)ce;
       }
-      const unsigned g2 = (unsigned)((N->n_nodes + HX_GW - 1) / HX_GW);
+      const int per_cta = HX_GW * (32 / lpn);
+      const unsigned g2 = (unsigned)((N->n_nodes + per_cta - 1) / per_cta);
       if (g2) {
         void (*gk)(VolParams, const double*, const double*, int) =
-            wr ? (acc ? k_hex_gat<true, true> : k_hex_gat<true, false>)
-               : (acc ? k_hex_gat<false, true> : k_hex_gat<false, false>);
+            two ? (wr ? (acc ? k_hex_gat<true, true, HX_LPN> : k_hex_gat<true, false, HX_LPN>)
+                      : (acc ? k_hex_gat<false, true, HX_LPN> : k_hex_gat<false, false, HX_LPN>))
+                : (wr ? (acc ? k_hex_gat<true, true, 32> : k_hex_gat<true, false, 32>)
+                      : (acc ? k_hex_gat<false, true, 32> : k_hex_gat<false, false, 32>));
         if (cudaError_t ce = cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gbytes))
           return (int)ce;
         gk<<<g2, HX_GW * 32, gbytes, st>>>(P, work, rslot, capb);

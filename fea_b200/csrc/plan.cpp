@@ -194,7 +194,10 @@ int build_gather(const fea_plan& P, int kind, int64_t ne, const int32_t* conn, c
     if (ni == 0) continue;
     int64_t f = popc3(P.mask[n]);
     int64_t v = f * (int64_t)P.rowlen[n];
-    if (ni > threads || v + f > smem_budget) return FEA_ECHUNK;
+    // the C3D8 kernels read no chunks (staged blocks and a node-row gather
+    // instead): a node of more incidences than a chunk takes gets a chunk of
+    // its own there, and only the C3D4 and face lists are bounded
+    if (kind != FEA_C3D8 && (ni > threads || v + f > smem_budget)) return FEA_ECHUNK;
     if (cur_inc + ni > threads || cur_v + v + cur_r + f > smem_budget) close();
     if (!cur.empty() && G.nodeinc[cur.back() + 1] != G.nodeinc[n]) close();
     G.soff[n] = (int32_t)cur_v;

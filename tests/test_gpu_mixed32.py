@@ -1,7 +1,7 @@
 """The FP32 inner solver on the padded node layout (fea_f32_layout_fill,
 fea_pcg_solve_mixed_nodes32): the layout holds the plan's FP32 values and
-columns (padding zeros), the mixed solve reaches the FP64 direct solution
-to 1e-9 with and without inner_tol, and the Newton solver's mixed mode uses
+columns (padding zeros), the mixed solve meets its FP64 stop test and the
+direct solution to 1e-8 with and without inner_tol, and the Newton solver's mixed mode uses
 it."""
 import numpy as np
 import pytest
@@ -52,8 +52,16 @@ def test_mixed_padded_layout_solve_matches_direct(golden, inner_tol):
     x = torch.zeros_like(b)
     it, outer, rr, st = P.pcg_mixed(K, None, b, x, 1e-22, inner_tol, 20000, check_every=20)
     assert st == 0 and outer >= 1
-    xd = O.direct_solve(P.indptr.cpu(), P.indices.cpu().long(), K.cpu(), b.cpu())
-    assert rel(x, xd) < 1e-9
+    ip, ix, Kc = P.indptr.cpu(), P.indices.cpu().long(), K.cpu()
+    xd = O.direct_solve(ip, ix, Kc, b.cpu())
+    # the true FP64 residual meets the stop test (r.D^-1 r)/(b.D^-1 b) < tol,
+    # and the displacements are within the 1e-8 of the solver contract
+    A = torch.sparse_csr_tensor(ip, ix, Kc, (b.numel(), b.numel()))
+    rows = torch.repeat_interleave(torch.arange(b.numel()), ip[1:] - ip[:-1])
+    dinv = 1.0 / Kc[ix == rows]
+    r = b.cpu() - A @ x.cpu()
+    assert float((r * dinv * r).sum() / (b.cpu() * dinv * b.cpu()).sum()) < 1e-20
+    assert rel(x, xd) < 1e-8
     if inner_tol > 0:
         x0 = torch.zeros_like(b)
         it0, outer0, _, st0 = P.pcg_mixed(K, None, b, x0, 1e-22, 0.0, 20000, check_every=20)

@@ -9,8 +9,9 @@
   oracle's loop, within 1e-12.
 - The 40^3 compliance block: the residual VJP (lam . dR/dX, lam . dR/dmu)
   against torch autograd of the oracle's residual, within 1e-12.
-- A C3D8 fan whose middle axis node has 50 active neighbours: rows longer
-  than the 32-block pass of the node-row gather, against the oracle.
+- C3D8 fans whose middle axis node has 50 and 162 active neighbours: rows
+  longer than one pass of the node-row gather, and (162) staged regions too
+  large for two nodes per warp, against the oracle.
 """
 import math
 
@@ -199,12 +200,16 @@ def fan_mesh(M=12, layers=2):
     return torch.from_numpy(X), torch.from_numpy(el.astype(np.int64))
 
 
-def test_high_valence_c3d8_node_rows():
+@pytest.mark.parametrize("M", [12, 40])
+def test_high_valence_c3d8_node_rows(M):
+    """M = 12: rows of 50 blocks, more than one pass of a 16- or 32-lane
+    node group.  M = 40: the middle axis node stages 12 M = 480 blocks, two
+    such regions per warp exceed the 227 KB of shared memory of a CTA and the
+    gather falls back to one node per warp."""
     import fea_b200 as F
-    X, el = fan_mesh()
+    X, el = fan_mesh(M)
     dNdX, w, _ = O.preload_gaussian("C3D8", X, el)
     assert bool((w > 0).all())                               # valid hexes at every Gauss point
-    M = 12
     P2 = 1 + 2 * M
     part = F.Part(X)
     e = F.elements.C3D8(elems=el, elems_index=torch.arange(el.shape[0]), part=part)
@@ -220,7 +225,10 @@ def test_high_valence_c3d8_node_rows():
     P = asm.plan
     adj = P.adjptr.cpu().numpy() if hasattr(P, "adjptr") else None
     if adj is not None:
-        assert int(np.diff(adj).max()) == 2 + 4 * M              # the middle axis node: rows of 50 blocks
+        assert int(np.diff(adj).max()) == 2 + 4 * M              # the middle axis node's row
+    maxblk = int(P.groups[0].desc.maxblk)
+    assert maxblk == 12 * M
+    assert (8 * maxblk * 72 > 227 * 1024) == (M == 40)        # two regions per warp do not fit
     m = O.Model(X, [O.Group("C3D8", el, 1.0, 50.0)], [], [(fixed, (0, 1, 2))])
     gc = 1e-2 * torch.randn(int(m.free_mask().sum()), generator=torch.Generator().manual_seed(7),
                             dtype=torch.float64)
