@@ -34,7 +34,7 @@ FEA_C3D4, FEA_C3D8, FEA_T3, FEA_Q4 = 4, 8, 3, 40
  FEA_A_ADJPTR, FEA_A_ADJCOL, FEA_A_ADJOFF, FEA_A_MOFF) = range(10, 21)
 G_BASE, F_BASE = 30, 50
 (A_INC, A_BOFF, A_NODEINC, A_CHUNKPTR, A_CHUNKINC, S_NCHUNK, S_MAXVAL, S_THREADS, S_SMEM, A_CHUNKLIST,
- A_CHUNKDIM, A_SOFF, A_ROFF, A_BLKPTR, A_BLKCON, A_ALLPTR, A_ALLINC, A_INCPOS, A_RECBASE, A_NODEBLK) = range(20)
+ A_CHUNKDIM, A_SOFF, A_ROFF, A_UPTR, A_UBLK, A_ALLPTR, A_ALLINC, A_INCPOS, A_STAGEPOS, A_REGION) = range(20)
 
 
 class FeaError(RuntimeError):
@@ -63,11 +63,11 @@ class Group(C.Structure):
                 ("conn_dev", C.c_void_p), ("inc_dev", C.c_void_p), ("boff_dev", C.c_void_p),
                 ("nodeinc_dev", C.c_void_p), ("chunkptr_dev", C.c_void_p), ("chunkinc_dev", C.c_void_p),
                 ("chunklist_dev", C.c_void_p), ("chunkdim_dev", C.c_void_p), ("soff_dev", C.c_void_p),
-                ("roff_dev", C.c_void_p), ("blkptr_dev", C.c_void_p), ("blkcon_dev", C.c_void_p),
+                ("roff_dev", C.c_void_p), ("uptr_dev", C.c_void_p), ("ublk_dev", C.c_void_p),
                 ("allptr_dev", C.c_void_p), ("allinc_dev", C.c_void_p),
                 ("nchunk", C.c_int64), ("maxval", C.c_int32), ("threads", C.c_int32),
-                ("smem_doubles", C.c_int64), ("incpos_dev", C.c_void_p), ("recbase_dev", C.c_void_p),
-                ("nodeblk_dev", C.c_void_p), ("nblk", C.c_int64), ("maxblk", C.c_int32), ("reserved", C.c_int32)]
+                ("smem_doubles", C.c_int64), ("incpos_dev", C.c_void_p), ("stagepos_dev", C.c_void_p),
+                ("region_dev", C.c_void_p), ("nblk", C.c_int64), ("maxblk", C.c_int32), ("reserved", C.c_int32)]
 
 
 class PcgbSlot(C.Structure):

@@ -50,11 +50,11 @@ struct VolParams {
   const int64_t* __restrict__ adjptr;
   const int32_t* __restrict__ adjcol;
   const int32_t* __restrict__ adjoff;
-  const int64_t* __restrict__ blkptr;
-  const int32_t* __restrict__ blkcon;
+  const int64_t* __restrict__ uptr;
+  const fea_ublk_t* __restrict__ ublk;
   const int32_t* __restrict__ incpos;
-  const int32_t* __restrict__ recbase;
-  const int64_t* __restrict__ nodeblk;
+  const int32_t* __restrict__ stagepos;
+  const int64_t* __restrict__ region;
   const int32_t* __restrict__ moff;
   const double* __restrict__ gc;
   double* K;
@@ -318,16 +318,15 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
 // vectors in registers,
 //   K_ab = sum_g (A_a q_b^T + B_a f_b^T + q_b C_a^T + wc (g_a . g_b) I),
 //   A_a = w(alpha f_a + beta q_a), B_a = w alpha q_a, C_a = w gamma q_a,
-// and the element residual R_a = sum_g w(mu J^-2/3 f_a + c2 q_a).  The
-// lanes then exchange their blocks through shared memory and lane a writes
-// the upper part of the element's block row a — the blocks (a, b) whose
-// column node is active and numbered >= row node, transposing the blocks
-// another lane computed — as the record of incidence (e, a): the records of
-// a node are contiguous in HBM, in element order (its record region); R_a
-// goes to the incidence's slot of a separate array.  k_hex_gat copies a
-// node's region to shared memory with coalesced loads, sums it per upper
-// column block and writes each block into the node's rows and its transpose
-// into the column node's rows: every CSR value written once.
+// and the element residual R_a = sum_g w(mu J^-2/3 f_a + c2 q_a).  Each lane
+// then writes its blocks from registers to their staged positions (the
+// plan's STAGEPOS), oriented to the upper node block (row node numbered
+// lower), and R_a to the incidence's slot of a separate array.  A node's
+// staged region lists, block-major, the contributions to each of its upper
+// blocks in element order; k_hex_gat copies the region to shared memory with
+// coalesced 16-byte copies, sums each upper block's contiguous contributions
+// and writes the block into the node's rows and its transpose into the
+// column node's rows: every CSR value written once.
 // g_b itself is not staged: g_a . g_b = (F^-1 f_a) . (F^T q_b) = f_a . q_b,
 // so a (Gauss point, node) slot holds 6 doubles and an element 456: 29,184
 // bytes of shared memory per CTA.  Six CTAs per SM: the launch bound holds
@@ -339,8 +338,8 @@ constexpr int HX_EPB = 8;                 // elements per CTA
 constexpr int HX_TPB = 8 * HX_EPB;        // threads per CTA
 constexpr int HX_VB = 6;                  // doubles per (gp, node) vector slot: q, f (16-byte aligned)
 constexpr int HX_VG = 50;                 // doubles per Gauss point (8 slots + 2 pad: conflict-free rows)
-constexpr int HX_SC = 8 * HX_VG;          // offset of the per-Gauss-point scalars (7 each)
-constexpr int HX_EL = HX_SC + 56;         // doubles per element (7 scalars per Gauss point)
+constexpr int HX_SC = 8 * HX_VG;          // offset of the per-Gauss-point scalars (6 each)
+constexpr int HX_EL = HX_SC + 48;         // doubles per element (6 scalars per Gauss point)
 constexpr int HX_GW = 4;                  // warps per gather CTA
 // Gather lanes per row node: 16 (two nodes per warp: 397.0 against 461.4 us
 // with 32 lanes per node at 64^3, where rows hold 27 blocks and regions 36),
@@ -403,17 +402,13 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
 #pragma unroll
     for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];
     const double I1 = Jm * sF2, muJm = mu * Jm;
-    double* S = V + HX_SC + lane * 7;
+    double* S = V + HX_SC + lane * 6;
     S[0] = w * (-2.0 / 3.0 * muJm);                                 // w alpha
     S[1] = w * (kappa * J * (2.0 * J - 1.0) + 2.0 / 9.0 * mu * I1);  // w beta
     S[2] = w * (mu * I1 / 3.0 - kappa * J * (J - 1.0));              // w gamma
     S[3] = w * muJm;                                                 // w c (delta term, residual)
     S[4] = w * (kappa * J * (J - 1.0) - mu * I1 / 3.0);              // w c2 (residual)
-    {
-      const int32_t cg = P.conn[e * 8 + lane];                       // node `lane` of the element, for phase 3
-      S[5] = (double)cg;
-      S[6] = (double)P.mask[cg];
-    }
+    S[5] = (double)P.conn[e * 8 + lane];                             // node `lane`, for phase 3
     // Mq = J0^-1 F^-1, Mf = J0^-1 F^T: q_b = Mq^T dxi_b, f_b = Mf^T dxi_b, g_b = J0^-T dxi_b
     double Mq[9], Mf[9];
 #pragma unroll
@@ -445,6 +440,15 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
   // ---- phase 2: row node a = lane (lanes of an inactive element idle) --------
   const int a = lane;
   const int nb = a < 4 ? 5 : 4;
+  int32_t spos[5] = {-1, -1, -1, -1, -1};      // staged positions of the lane's blocks, loaded early
+  int32_t ipos = -1;
+  if (act) {
+    const int32_t* sp = P.stagepos + e * 36 + (a < 4 ? 5 * a : 20 + 4 * (a - 4));
+#pragma unroll
+    for (int d = 0; d < 5; ++d)
+      if (d < nb) spos[d] = sp[d];
+    ipos = P.incpos[e * 8 + a];
+  }
   double acc[5][9];
   double racc[3] = {0.0, 0.0, 0.0};
 #pragma unroll
@@ -453,7 +457,7 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
     for (int i = 0; i < 9; ++i) acc[d][i] = 0.0;
 #pragma unroll 1
   for (int g = 0; g < (act ? 8 : 0); ++g) {
-    const double* S = V + HX_SC + g * 7;
+    const double* S = V + HX_SC + g * 6;
     const double wa = S[0], wb = S[1], wg = S[2], wc = S[3], wc2 = S[4];
     const double* Va = V + g * HX_VG + a * HX_VB;
     double qa[3], fa[3], gm[3], A[3], B[3], Cc[3];
@@ -499,49 +503,35 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
       acc[d][8] += dg;
     }
   }
-  // ---- phase 3: upper block row a to the incidence record --------------------
-  // The blocks go to an exchange area in V (slot 8d + a, 10 doubles each:
-  // 128-bit stores, conflict-free within an element's 8 lanes); lane a then
-  // writes the blocks (a, b) of active column nodes numbered >= its own node,
-  // in ascending b, taking the transpose of a block another lane owns.
-  __syncwarp();                                          // V is no longer read
+  // ---- phase 3: every block from registers to its staged position ------------
+  // K_ab as computed when the column node is numbered above the row node (or
+  // b = a), transposed when below, K_ab + K_ab^T when the element repeats
+  // the node (a != b); R_a to the incidence's residual slot.
   if (act) {
+    const double na = V[HX_SC + a * 6 + 5];
 #pragma unroll
     for (int d = 0; d < 5; ++d) {
       if (d == 4 && nb == 4) break;
-      double2* o = reinterpret_cast<double2*>(V + (8 * d + a) * 10);
-      o[0] = make_double2(acc[d][0], acc[d][1]);
-      o[1] = make_double2(acc[d][2], acc[d][3]);
-      o[2] = make_double2(acc[d][4], acc[d][5]);
-      o[3] = make_double2(acc[d][6], acc[d][7]);
-      o[4] = make_double2(acc[d][8], 0.0);
-    }
-  }
-  __syncwarp();
-  if (act) {
-    const int32_t rb = P.recbase[e * 8 + a];
-    if (rb >= 0) {
-      const double na = V[HX_SC + a * 7 + 5];
-      double* out = stage + (int64_t)rb * 9;
+      if (spos[d] < 0) continue;
+      const double nc = V[HX_SC + ((a + d) & 7) * 6 + 5];
+      double* out = stage + (int64_t)spos[d] * 9;
+      if (d == 0 || nc > na) {
 #pragma unroll
-      for (int b = 0; b < 8; ++b) {
-        const double* Sb = V + HX_SC + b * 7;
-        if (Sb[6] == 0.0 || Sb[5] < na) continue;
-        const int d = (b - a) & 7;
-        if (d < 4 || (d == 4 && a < 4)) {
-          const double* sb = V + (8 * d + a) * 10;
+        for (int i = 0; i < 9; ++i) out[i] = acc[d][i];
+      } else if (nc < na) {
 #pragma unroll
-          for (int i = 0; i < 9; ++i) out[i] = sb[i];
-        } else {
-          const double* sb = V + (8 * ((a - b) & 7) + b) * 10;
+        for (int j = 0; j < 3; ++j)
 #pragma unroll
-          for (int j = 0; j < 3; ++j)
+          for (int k = 0; k < 3; ++k) out[3 * j + k] = acc[d][3 * k + j];
+      } else {
 #pragma unroll
-            for (int k = 0; k < 3; ++k) out[3 * j + k] = sb[3 * k + j];
-        }
-        out += 9;
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+          for (int k = 0; k < 3; ++k) out[3 * j + k] = acc[d][3 * j + k] + acc[d][3 * k + j];
       }
-      double2* ro = reinterpret_cast<double2*>(rslot + (int64_t)P.incpos[e * 8 + a] * 4);
+    }
+    if (ipos >= 0) {
+      double2* ro = reinterpret_cast<double2*>(rslot + (int64_t)ipos * 4);
       ro[0] = make_double2(racc[0], racc[1]);
       ro[1] = make_double2(racc[2], 0.0);
     }
@@ -552,17 +542,16 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
   }
 }
 
-// Per node row: one warp per row node n.  The warp copies the node's record
-// region (its staged upper blocks, element order) to shared memory with
-// coalesced loads; then one lane per upper node block (n, c >= n) sums the
-// blocks of the block's contributors (element order, fixed), writes its 3x3
-// (free DOFs only) into the node's contiguous CSR rows and, for c != n, the
-// transpose into c's rows at n's column offset there; the diagonal lane
-// writes the node's residual, the sum over its incidences in element order
-// (lane i loads incidence i's slot; the sum runs through shuffles).  The
-// lanes' block metadata and residual slots are loaded before the region
-// copy.  capb = the most staged blocks of one node (shared memory per warp:
-// capb blocks).
+// Per node row: a group of LPN lanes per row node n.  The group copies the
+// node's region (its staged contributions, block-major) to shared memory
+// with 16-byte asynchronous copies; then one lane per upper node block (n,
+// c >= n), from the block's record, sums its contributions (element order,
+// fixed), writes the 3x3 (free DOFs only) into the node's contiguous CSR
+// rows and, for c != n, the transpose into c's rows; the diagonal lane writes
+// the node's residual, the sum over its incidences in element order (lane i
+// loads incidence i's slot; the sum runs through shuffles).  The records and
+// residual slots are loaded before the region copy completes.  capb = the
+// largest region (shared memory per group: capb blocks).
 template <bool WR, bool ACC, int LPN>
 __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const double* __restrict__ stage,
                                                         const double* __restrict__ rslot, int capb) {
@@ -577,26 +566,19 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
   if (n >= P.n_nodes) return;
   const unsigned mn = P.mask[n];
   if (!mn) return;
-  const int64_t b0 = P.nodeblk[n];
-  const int64_t nbk_all = P.nodeblk[n + 1] - b0;
+  const int64_t b0 = P.region[n];
+  const int64_t nbk_all = P.region[n + 1] - b0;
   const int nbk = nbk_all < capb ? (int)nbk_all : capb;
-  const int64_t p0 = P.adjptr[n], p1 = P.adjptr[n + 1];
+  const int64_t u0 = P.uptr[n], nu = P.uptr[n + 1] - u0;
   const int q0 = P.nodeinc[n], nq = P.nodeinc[n + 1] - q0;
-  // the lane's first block and its metadata
-  int64_t p = p0 + lane;
-  int32_t c = -1;
-  if (p < p1) c = P.adjcol[p];
-  int64_t t0 = 0, t1 = 0, vbc = 0;
-  int off = 0, om = 0, Lc = 0;
-  unsigned mc = 0;
-  if (c >= n) {
-    t0 = P.blkptr[p];
-    t1 = P.blkptr[p + 1];
-    off = P.adjoff[p];
-    om = P.moff[p];
-    mc = P.mask[c];
-    vbc = P.vbase[c];
-    Lc = P.rowlen[c];
+  // the lane's first record: targets (row, transpose) and (rowlen_c, mask_c, first, count)
+  int64_t u = lane;
+  longlong2 tg = make_longlong2(0, 0);
+  int4 mt = make_int4(0, 0, 0, 0);
+  if (u < nu) {
+    const longlong2* r = reinterpret_cast<const longlong2*>(P.ublk + u0 + u);
+    tg = r[0];
+    mt = *reinterpret_cast<const int4*>(r + 1);
   }
   double rq[3] = {0.0, 0.0, 0.0};
   if (WR && lane < nq) {
@@ -606,19 +588,19 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
   }
   double* S = gsm + (int64_t)(warp * NPW + sub) * capb * 9;
   {
-    // the region copy as asynchronous 8-byte global-to-shared copies (no
-    // register round trip; 461.8 against 472.3 us for load-and-store at 64^3)
+    // regions start at even blocks and hold an even number: whole 16-byte
+    // pieces, copied through L2 only (cg)
     const double* src = stage + b0 * 9;
-    const int nd = nbk * 9;
+    const int nd2 = (nbk * 9) >> 1;
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(S);
-    for (int i = lane; i < nd; i += LPN)
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sbase + 8u * (unsigned)i), "l"(src + i)
+    for (int i = lane; i < nd2; i += LPN)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sbase + 16u * (unsigned)i), "l"(src + 2 * i)
                    : "memory");
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   }
   double r[3] = {0.0, 0.0, 0.0};
-  if (WR) {                                      // warp-uniform: incidences in order
+  if (WR) {                                      // group-uniform: incidences in order
     for (int qb = 0; qb < nq; qb += LPN) {
       if (qb > 0) {
         rq[0] = rq[1] = rq[2] = 0.0;
@@ -637,72 +619,61 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
   }
   __syncwarp(gmask);
   const int L = P.rowlen[n];
-  const int64_t vb = P.vbase[n];
-  while (p < p1) {
-    if (c >= n) {                                // lower blocks: the transposes of c's upper blocks
-      double blk[9];
+  while (u < nu) {
+    double blk[9];
 #pragma unroll
-      for (int i = 0; i < 9; ++i) blk[i] = 0.0;
-      for (int64_t t = t0; t < t1; ++t) {
-        const int32_t code = P.blkcon[t];
-        if (code >= nbk) continue;               // never taken: codes index the node's region
-        const double* sb = S + code * 9;
+    for (int i = 0; i < 9; ++i) blk[i] = 0.0;
+    const int k1 = min(mt.z + mt.w, nbk);        // contributions lie inside the region
+    for (int k = mt.z; k < k1; ++k) {
+      const double* sb = S + k * 9;
 #pragma unroll
-        for (int i = 0; i < 9; ++i) blk[i] += sb[i];
-      }
-      int rj = 0;
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        if (!(mn >> j & 1u)) continue;
-        double* row = P.K + vb + (int64_t)rj * L + off;
-        int rk = 0;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          if (!(mc >> k & 1u)) continue;
-          row[rk] = ACC ? row[rk] + blk[3 * j + k] : blk[3 * j + k];
-          ++rk;
-        }
-        ++rj;
-      }
-      if (c != n) {
-        int rk = 0;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          if (!(mc >> k & 1u)) continue;
-          double* row = P.K + vbc + (int64_t)rk * Lc + om;
-          int cj = 0;
-#pragma unroll
-          for (int j = 0; j < 3; ++j) {
-            if (!(mn >> j & 1u)) continue;
-            row[cj] = ACC ? row[cj] + blk[3 * j + k] : blk[3 * j + k];
-            ++cj;
-          }
-          ++rk;
-        }
-      } else if (WR) {
-        double* Rout = P.R + P.rdof[n];
-        int rr = 0;
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-          if (mn >> j & 1u) {
-            Rout[rr] = ACC ? Rout[rr] + r[j] : r[j];
-            ++rr;
-          }
-      }
+      for (int i = 0; i < 9; ++i) blk[i] += sb[i];
     }
-    p += LPN;                                 // rows of more blocks than the group has lanes
-    c = -1;
-    if (p < p1) {
-      c = P.adjcol[p];
-      if (c >= n) {
-        t0 = P.blkptr[p];
-        t1 = P.blkptr[p + 1];
-        off = P.adjoff[p];
-        om = P.moff[p];
-        mc = P.mask[c];
-        vbc = P.vbase[c];
-        Lc = P.rowlen[c];
+    const unsigned mc = (unsigned)mt.y;
+    int rj = 0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      if (!(mn >> j & 1u)) continue;
+      double* row = P.K + tg.x + (int64_t)rj * L;
+      int rk = 0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (!(mc >> k & 1u)) continue;
+        row[rk] = ACC ? row[rk] + blk[3 * j + k] : blk[3 * j + k];
+        ++rk;
       }
+      ++rj;
+    }
+    if (tg.y >= 0) {                             // the transpose into c's rows
+      int rk = 0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (!(mc >> k & 1u)) continue;
+        double* row = P.K + tg.y + (int64_t)rk * mt.x;
+        int cj = 0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          if (!(mn >> j & 1u)) continue;
+          row[cj] = ACC ? row[cj] + blk[3 * j + k] : blk[3 * j + k];
+          ++cj;
+        }
+        ++rk;
+      }
+    } else if (WR) {
+      double* Rout = P.R + P.rdof[n];
+      int rr = 0;
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        if (mn >> j & 1u) {
+          Rout[rr] = ACC ? Rout[rr] + r[j] : r[j];
+          ++rr;
+        }
+    }
+    u += LPN;                                    // rows of more upper blocks than the group has lanes
+    if (u < nu) {
+      const longlong2* rp = reinterpret_cast<const longlong2*>(P.ublk + u0 + u);
+      tg = rp[0];
+      mt = *reinterpret_cast<const int4*>(rp + 1);
     }
   }
 }
@@ -1355,11 +1326,11 @@ static VolParams vol_params(const fea_nodes_t* N, const fea_group_t* G, double m
   P.adjptr = N->adjptr_dev;
   P.adjcol = N->adjcol_dev;
   P.adjoff = N->adjoff_dev;
-  P.blkptr = G->blkptr_dev;
-  P.blkcon = G->blkcon_dev;
+  P.uptr = G->uptr_dev;
+  P.ublk = G->ublk_dev;
   P.incpos = G->incpos_dev;
-  P.recbase = G->recbase_dev;
-  P.nodeblk = G->nodeblk_dev;
+  P.stagepos = G->stagepos_dev;
+  P.region = G->region_dev;
   P.moff = N->moff_dev;
   P.gc = gc;
   P.K = P.R = P.elemR = nullptr;
@@ -1427,8 +1398,8 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
   if (K && hex) {
     if (!work || work_len < fea_assemble_work_len(G)) return FEA_EWORK;
     if (((uintptr_t)work & 15) != 0) return FEA_EINVAL;
-    if (!G->incpos_dev || !G->recbase_dev || !G->nodeblk_dev || !G->blkptr_dev || !G->blkcon_dev ||
-        !N->adjptr_dev || !N->adjcol_dev || !N->adjoff_dev || !N->moff_dev || G->nblk < 0 || G->maxblk < 0)
+    if (!G->incpos_dev || !G->stagepos_dev || !G->region_dev || !G->uptr_dev || !G->ublk_dev ||
+        G->nblk < 0 || G->maxblk < 0)
       return FEA_EINVAL;
   }
   if (!K) {
@@ -1444,7 +1415,7 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
     int64_t smem = G->smem_doubles;
     const bool acc = accumulate != 0, wr = R != nullptr, er = elemR != nullptr;
     if (hex) {
-      const int capb = std::max<int>(G->maxblk, 1);
+      const int capb = std::max<int>(G->maxblk, 2);   // regions hold even block counts
       const size_t region = (size_t)capb * 9 * sizeof(double);
       const bool two = (size_t)HX_GW * (32 / HX_LPN) * region <= (size_t)smem_limit();
       const int lpn = two ? HX_LPN : 32;

@@ -49,11 +49,11 @@ struct GatherList {            // one element group or one face group
   std::vector<int32_t> chunkdim;   // [nchunk*3]: values, residual entries, contiguous flag
   std::vector<int32_t> soff;       // [N] shared-memory offset of the node's values in its chunk
   std::vector<int32_t> roff;       // [N] offset of its residual entries (after the chunk's values)
-  std::vector<int64_t> blkptr;     // [nnzb+1] contributors of every upper (row node n, column node c >= n) block
-  std::vector<int32_t> blkcon;     // block index of each contributor within the row node's record region
+  std::vector<int64_t> uptr;       // [N+1] first upper-block record of each node (C3D8)
+  std::vector<int64_t> ublk;       // [nu*4] upper-block records, fea_ublk_t layout
   std::vector<int32_t> incpos;     // [ne*nn] incidence index of (e, a), -1 for a node without rows
-  std::vector<int32_t> recbase;    // [ne*nn] first staged block of (e, a)'s record, -1 for a node without rows
-  std::vector<int64_t> nodeblk;    // [N+1] first staged block of each node's record region
+  std::vector<int32_t> stagepos;   // [ne*36] staged block of each element block (lane slot order), -1: none
+  std::vector<int64_t> region;     // [N+1] first staged block of each node's region (even)
   std::vector<int32_t> allptr;     // [N+1] incidences of every node (constrained ones included)
   std::vector<int32_t> allinc;     // e*16 + a, element order ascending
   int64_t maxval = 0, threads = 0, smem = 0;
@@ -210,55 +210,48 @@ int build_gather(const fea_plan& P, int kind, int64_t ne, const int32_t* conn, c
   return FEA_OK;
 }
 
-// Upper-block records of a C3D8 group.  The record of incidence (e, a) of
-// node n = conn[e][a] holds the blocks (a, b) whose column node c =
-// conn[e][b] is active and c >= n, in ascending b; the records of a node are
-// contiguous and in element order (its record region).  Every upper block
-// (n, c >= n) lists its contributors' positions in n's region, in ascending
-// element order; lower blocks have none (they are the transposes of upper
-// ones, written by the column node's gather).
+// Staging of a C3D8 group.  An element block couples the unordered local
+// pair {i, j} (36 per element: 8 diagonal, 28 off-diagonal) and belongs to
+// the upper node block (r, c), r = min(n_i, n_j), c = max(n_i, n_j), when both
+// nodes are active.  The element kernel's lane a computes K_ab for b = (a +
+// d) & 7, d = 0..3 and d = 4 for a < 4: the owner slot of {i, j}.  A node's
+// region lists, block-major, the contributions to each of its upper blocks
+// (adjacency order, c >= r; a block may have none), each block's in ascending
+// element order (then ascending slot, for an element that repeats a node);
+// regions start at even block indices (16-byte aligned).  stagepos maps
+// (e, slot) to the contribution's staged block; the upper-block records give
+// the gather its targets and contributor range.
+int owner_slot(int i, int j) {
+  int a = i, d = (j - i) & 7;
+  if (!(d < 4 || (d == 4 && i < 4))) {
+    a = j;
+    d = (i - j) & 7;
+  }
+  return (a < 4 ? 5 * a : 20 + 4 * (a - 4)) + d;
+}
+
 int build_blocks(const fea_plan& P, int nn, const int32_t* conn, const Incidence& I, GatherList& G) {
   const int64_t N = P.N;
-  auto included = [&](int64_t e, int a, int b) {
-    const int32_t na = conn[e * nn + a], nb = conn[e * nn + b];
-    return P.mask[na] && P.mask[nb] && nb >= na;
+  // contribution of incidence (e, i) of node r with local node j: the pair
+  // {i, j} counted once, from its lower-numbered node (from i <= j when the
+  // element repeats the node)
+  auto contributes = [&](int64_t e, int i, int j, int32_t r) {
+    const int32_t c = conn[e * nn + j];
+    return P.mask[c] && (c > r || (c == r && j >= i));
   };
-  G.nodeblk.assign(N + 1, 0);
-  for (int64_t n = 0; n < N; ++n) {
-    int64_t c = 0;
-    if (P.mask[n])
-      for (int64_t q = I.ptr[n]; q < I.ptr[n + 1]; ++q) {
-        const int64_t e = I.ent[q] >> 4;
-        const int a = (int)(I.ent[q] & 15);
-        for (int b = 0; b < nn; ++b) c += included(e, a, b);
-      }
-    G.nodeblk[n + 1] = G.nodeblk[n] + c;
-  }
-  if (G.nodeblk[N] >= INT32_MAX) return FEA_ERANGE;
-  G.recbase.assign((size_t)G.ne * nn, -1);
-  for (int64_t n = 0; n < N; ++n) {
-    if (!P.mask[n]) continue;
-    int64_t off = G.nodeblk[n];
-    for (int64_t q = I.ptr[n]; q < I.ptr[n + 1]; ++q) {
-      const int64_t e = I.ent[q] >> 4;
-      const int a = (int)(I.ent[q] & 15);
-      G.recbase[e * nn + a] = (int32_t)off;
-      for (int b = 0; b < nn; ++b) off += included(e, a, b);
-    }
-  }
   std::vector<int32_t> cnt(P.nnzb, 0);
   int err = FEA_OK;
   parallel_for(N, [&](int64_t a0, int64_t a1) {
     for (int64_t n = a0; n < a1; ++n) {
       if (!P.mask[n]) continue;
       const int32_t* col = P.adjcol.data() + P.adjptr[n];
-      int64_t ncol = P.adjptr[n + 1] - P.adjptr[n];
+      const int64_t ncol = P.adjptr[n + 1] - P.adjptr[n];
       for (int64_t q = I.ptr[n]; q < I.ptr[n + 1]; ++q) {
         const int64_t e = I.ent[q] >> 4;
-        const int a = (int)(I.ent[q] & 15);
-        for (int b = 0; b < nn; ++b) {
-          if (!included(e, a, b)) continue;
-          const int32_t c = conn[e * nn + b];
+        const int i = (int)(I.ent[q] & 15);
+        for (int j = 0; j < nn; ++j) {
+          if (!contributes(e, i, j, (int32_t)n)) continue;
+          const int32_t c = conn[e * nn + j];
           const int32_t* it = std::lower_bound(col, col + ncol, c);
           if (it == col + ncol || *it != c) { err = FEA_ERANGE; continue; }
           cnt[P.adjptr[n] + (it - col)]++;
@@ -267,25 +260,48 @@ int build_blocks(const fea_plan& P, int nn, const int32_t* conn, const Incidence
     }
   });
   if (err) return err;
-  G.blkptr.assign(P.nnzb + 1, 0);
-  for (int64_t p = 0; p < P.nnzb; ++p) G.blkptr[p + 1] = G.blkptr[p] + cnt[p];
-  G.blkcon.resize(G.blkptr[P.nnzb]);
+  G.region.assign(N + 1, 0);
+  G.uptr.assign(N + 1, 0);
+  for (int64_t n = 0; n < N; ++n) {
+    int64_t nb = 0, nu = 0;
+    if (P.mask[n])
+      for (int64_t p = P.adjptr[n]; p < P.adjptr[n + 1]; ++p)
+        if (P.adjcol[p] >= n) {
+          nb += cnt[p];
+          ++nu;
+        }
+    G.region[n + 1] = G.region[n] + ((nb + 1) & ~(int64_t)1);
+    G.uptr[n + 1] = G.uptr[n] + nu;
+  }
+  if (G.region[N] >= INT32_MAX) return FEA_ERANGE;
+  G.ublk.assign((size_t)G.uptr[N] * 4, 0);
+  G.stagepos.assign((size_t)G.ne * 36, -1);
   parallel_for(N, [&](int64_t a0, int64_t a1) {
     std::vector<int64_t> fill;
     for (int64_t n = a0; n < a1; ++n) {
       if (!P.mask[n]) continue;
-      const int32_t* col = P.adjcol.data() + P.adjptr[n];
-      int64_t ncol = P.adjptr[n + 1] - P.adjptr[n];
-      fill.assign(G.blkptr.begin() + P.adjptr[n], G.blkptr.begin() + P.adjptr[n + 1]);
+      const int64_t p0 = P.adjptr[n], np = P.adjptr[n + 1] - p0;
+      const int32_t* col = P.adjcol.data() + p0;
+      fill.assign(np, -1);
+      int64_t t = 0, u = G.uptr[n];
+      for (int64_t k = 0; k < np; ++k) {
+        const int32_t c = col[k];
+        if (c < n) continue;
+        fill[k] = t;
+        int64_t* rec = G.ublk.data() + 4 * u++;
+        rec[0] = P.vbase[n] + P.adjoff[p0 + k];
+        rec[1] = c != n ? P.vbase[c] + P.moff[p0 + k] : -1;
+        rec[2] = (int64_t)(uint32_t)P.rowlen[c] | ((int64_t)P.mask[c] << 32);
+        rec[3] = (int64_t)(uint32_t)t | ((int64_t)cnt[p0 + k] << 32);
+        t += cnt[p0 + k];
+      }
       for (int64_t q = I.ptr[n]; q < I.ptr[n + 1]; ++q) {
         const int64_t e = I.ent[q] >> 4;
-        const int a = (int)(I.ent[q] & 15);
-        int32_t pos = (int32_t)(G.recbase[e * nn + a] - G.nodeblk[n]);
-        for (int b = 0; b < nn; ++b) {
-          if (!included(e, a, b)) continue;
-          const int32_t c = conn[e * nn + b];
-          int64_t k = std::lower_bound(col, col + ncol, c) - col;
-          G.blkcon[fill[k]++] = pos++;
+        const int i = (int)(I.ent[q] & 15);
+        for (int j = 0; j < nn; ++j) {
+          if (!contributes(e, i, j, (int32_t)n)) continue;
+          const int64_t k = std::lower_bound(col, col + np, conn[e * nn + j]) - col;
+          G.stagepos[e * 36 + owner_slot(i, j)] = (int32_t)(G.region[n] + fill[k]++);
         }
       }
     }
@@ -480,13 +496,13 @@ extern "C" int fea_plan_get(const fea_plan* P, int32_t id, int32_t group, void* 
       case 10: return put(G->chunkdim, dst, count);
       case 11: return put(G->soff, dst, count);
       case 12: return put(G->roff, dst, count);
-      case 13: return put(G->blkptr, dst, count);
-      case 14: return put(G->blkcon, dst, count);
+      case 13: return put(G->uptr, dst, count);
+      case 14: return put(G->ublk, dst, count);
       case 15: return put(G->allptr, dst, count);
       case 16: return put(G->allinc, dst, count);
       case 17: return put(G->incpos, dst, count);
-      case 18: return put(G->recbase, dst, count);
-      case 19: return put(G->nodeblk, dst, count);
+      case 18: return put(G->stagepos, dst, count);
+      case 19: return put(G->region, dst, count);
       default: return FEA_EINVAL;
     }
   }

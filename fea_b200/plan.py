@@ -36,8 +36,8 @@ class HostPlan:
            L.FEA_A_MOFF: np.int32}
     _GDT = {L.A_INC: np.int32, L.A_BOFF: np.uint16, L.A_NODEINC: np.int32, L.A_CHUNKPTR: np.int32,
             L.A_CHUNKINC: np.int32, L.A_CHUNKLIST: np.int32, L.A_CHUNKDIM: np.int32, L.A_SOFF: np.int32,
-            L.A_ROFF: np.int32, L.A_BLKPTR: np.int64, L.A_BLKCON: np.int32, L.A_ALLPTR: np.int32,
-            L.A_ALLINC: np.int32, L.A_INCPOS: np.int32, L.A_RECBASE: np.int32, L.A_NODEBLK: np.int64}
+            L.A_ROFF: np.int32, L.A_UPTR: np.int64, L.A_UBLK: np.int64, L.A_ALLPTR: np.int32,
+            L.A_ALLINC: np.int32, L.A_INCPOS: np.int32, L.A_STAGEPOS: np.int32, L.A_REGION: np.int64}
 
     def __init__(self, n_nodes, free_mask, groups, faces, vol_threads=0, smem_doubles=0):
         self._h = None
@@ -100,15 +100,15 @@ class GatherGroup:
         self.chunkdim = dev(hp.array(base + L.A_CHUNKDIM, index))
         self.soff = dev(hp.array(base + L.A_SOFF, index))
         self.roff = dev(hp.array(base + L.A_ROFF, index))
-        blkptr = hp.array(base + L.A_BLKPTR, index) if base == L.G_BASE else np.zeros(0, np.int64)
-        self.blkptr = dev(blkptr) if blkptr.size else None
-        self.blkcon = dev(hp.array(base + L.A_BLKCON, index)) if blkptr.size else None
-        self.incpos = dev(hp.array(base + L.A_INCPOS, index)) if blkptr.size else None
-        self.recbase = dev(hp.array(base + L.A_RECBASE, index)) if blkptr.size else None
-        nodeblk = hp.array(base + L.A_NODEBLK, index) if blkptr.size else np.zeros(1, np.int64)
-        self.nodeblk = dev(nodeblk) if blkptr.size else None
-        nblk = int(nodeblk[-1])
-        maxblk = int(np.diff(nodeblk).max()) if nodeblk.size > 1 else 0
+        uptr = hp.array(base + L.A_UPTR, index) if base == L.G_BASE else np.zeros(0, np.int64)
+        self.uptr = dev(uptr) if uptr.size else None
+        self.ublk = dev(hp.array(base + L.A_UBLK, index)) if uptr.size else None
+        self.incpos = dev(hp.array(base + L.A_INCPOS, index)) if uptr.size else None
+        self.stagepos = dev(hp.array(base + L.A_STAGEPOS, index)) if uptr.size else None
+        region = hp.array(base + L.A_REGION, index) if uptr.size else np.zeros(1, np.int64)
+        self.region = dev(region) if uptr.size else None
+        nblk = int(region[-1])
+        maxblk = int(np.diff(region).max()) if region.size > 1 else 0
         self.allptr = dev(hp.array(base + L.A_ALLPTR, index))
         self.allinc = dev(hp.array(base + L.A_ALLINC, index))
         self.ne = int(self.conn.shape[0])
@@ -117,15 +117,15 @@ class GatherGroup:
         self.desc = L.Group(kind, self.nn, self.ne, self.conn.data_ptr(), self.inc.data_ptr(), self.boff.data_ptr(),
                             self.nodeinc.data_ptr(), self.chunkptr.data_ptr(), self.chunkinc.data_ptr(),
                             self.chunklist.data_ptr(), self.chunkdim.data_ptr(), self.soff.data_ptr(),
-                            self.roff.data_ptr(), self.blkptr.data_ptr() if self.blkptr is not None else None,
-                            self.blkcon.data_ptr() if self.blkcon is not None else None,
+                            self.roff.data_ptr(), self.uptr.data_ptr() if self.uptr is not None else None,
+                            self.ublk.data_ptr() if self.ublk is not None else None,
                             self.allptr.data_ptr(), self.allinc.data_ptr(),
                             hp.scalar(base + L.S_NCHUNK, index),
                             hp.scalar(base + L.S_MAXVAL, index), hp.scalar(base + L.S_THREADS, index),
                             hp.scalar(base + L.S_SMEM, index),
                             self.incpos.data_ptr() if self.incpos is not None else None,
-                            self.recbase.data_ptr() if self.recbase is not None else None,
-                            self.nodeblk.data_ptr() if self.nodeblk is not None else None, nblk, maxblk, 0)
+                            self.stagepos.data_ptr() if self.stagepos is not None else None,
+                            self.region.data_ptr() if self.region is not None else None, nblk, maxblk, 0)
         self.nchunk = int(self.desc.nchunk)
 
 

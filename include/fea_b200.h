@@ -114,13 +114,13 @@ enum {
   FEA_A_G_CHUNKDIM = 40, /* int32 [nchunk,3] values, residual entries, contiguous */
   FEA_A_G_SOFF = 41,     /* int32 [N] shared offset of the node's values   */
   FEA_A_G_ROFF = 42,     /* int32 [N] offset of its residual entries       */
-  FEA_A_G_BLKPTR = 43,   /* int64 [nnzb+1] contributors of each upper node block (c >= n; C3D8) */
-  FEA_A_G_BLKCON = 44,   /* int32 staged block index within the row node's record region */
+  FEA_A_G_UPTR = 43,     /* int64 [N+1] first upper-block record of each node (C3D8)      */
+  FEA_A_G_UBLK = 44,     /* int64 [nu, 4] upper-block records (fea_ublk_t layout, C3D8)   */
   FEA_A_G_ALLPTR = 45,   /* int32 [N+1] incidences of every node (all nodes) */
   FEA_A_G_ALLINC = 46,   /* int32 element*16 + a                           */
   FEA_A_G_INCPOS = 47,   /* int32 [ne, nn] incidence index of (e, a), -1: node without rows */
-  FEA_A_G_RECBASE = 48,  /* int32 [ne, nn] first staged block of (e, a)'s record, -1: none */
-  FEA_A_G_NODEBLK = 49,  /* int64 [N+1] first staged block of each node's record region */
+  FEA_A_G_STAGEPOS = 48, /* int32 [ne, 36] staged block of each element block, -1: none  */
+  FEA_A_G_REGION = 49,   /* int64 [N+1] first staged block of each node's region (even)   */
   FEA_A_F_INC = 50,      /* the same arrays / scalars for face groups      */
   FEA_A_F_BOFF = 51,
   FEA_A_F_NODEINC = 52,
@@ -162,6 +162,23 @@ typedef struct {
   const int32_t* moff_dev;    /* FEA_A_MOFF   */
 } fea_nodes_t;
 
+/* C3D8 staging.  Element block {i, j} of element e (the 36 unordered local
+ * pairs, in the slot order of the element kernel's lanes: lane a < 4 holds
+ * (a, a + d mod 8) for d = 0..4 at slots 5a + d, lane a >= 4 holds d = 0..3 at
+ * 20 + 4(a - 4) + d) is staged at block STAGEPOS[e, slot], oriented as the
+ * upper node block (row node min(n_i, n_j), column node max): a node's
+ * region REGION[n] .. REGION[n+1] holds, block-major, the contributions to
+ * its upper blocks in adjacency order, each block's in ascending element
+ * order.  One record per upper block (row n, column c >= n): */
+typedef struct {
+  int64_t row;                /* value index of (first free row of n, first free column of c)  */
+  int64_t col;                /* value index of the transpose in c's rows; -1 on the diagonal  */
+  int32_t rowlen_c;           /* values per row of c                                           */
+  int32_t mask_c;             /* free-DOF mask of c                                            */
+  int32_t first;              /* first contribution, relative to REGION[n]                     */
+  int32_t count;              /* contributions (0: the block is written as zero)               */
+} fea_ublk_t;
+
 typedef struct {
   int32_t kind;               /* FEA_C3D4 / FEA_C3D8, or FEA_T3 / FEA_Q4      */
   int32_t nn;                 /* nodes per element / face                     */
@@ -176,8 +193,8 @@ typedef struct {
   const int32_t* chunkdim_dev;
   const int32_t* soff_dev;
   const int32_t* roff_dev;
-  const int64_t* blkptr_dev;  /* C3D8 only */
-  const int32_t* blkcon_dev;
+  const int64_t* uptr_dev;    /* FEA_A_G_UPTR (C3D8 only) */
+  const fea_ublk_t* ublk_dev; /* FEA_A_G_UBLK (C3D8 only) */
   const int32_t* allptr_dev;  /* FEA_A_*_ALLPTR (adjoint kernels) */
   const int32_t* allinc_dev;
   int64_t nchunk;
@@ -185,10 +202,10 @@ typedef struct {
   int32_t threads;
   int64_t smem_doubles;
   const int32_t* incpos_dev;  /* FEA_A_G_INCPOS (C3D8 only) */
-  const int32_t* recbase_dev; /* FEA_A_G_RECBASE (C3D8 only) */
-  const int64_t* nodeblk_dev; /* FEA_A_G_NODEBLK (C3D8 only) */
-  int64_t nblk;               /* staged blocks: NODEBLK[N] (C3D8 only)        */
-  int32_t maxblk;             /* most staged blocks of one node (C3D8 only)   */
+  const int32_t* stagepos_dev;/* FEA_A_G_STAGEPOS (C3D8 only) */
+  const int64_t* region_dev;  /* FEA_A_G_REGION (C3D8 only) */
+  int64_t nblk;               /* staged blocks: REGION[N] (C3D8 only)         */
+  int32_t maxblk;             /* largest region, in blocks (C3D8 only)        */
   int32_t reserved;
 } fea_group_t;
 

@@ -75,14 +75,10 @@ def test_volume_entry_points_check_arguments_first():
     assert vol(hexg, work=None) == EWORK
     assert vol(hexg, work_len=wl - 1) == EWORK
     assert vol(hexg, work=C.c_void_p(FAKE + 8)) == EINVAL           # not 16-byte aligned
-    for f in ("incpos_dev", "recbase_dev", "nodeblk_dev", "blkptr_dev", "blkcon_dev"):
+    for f in ("incpos_dev", "stagepos_dev", "region_dev", "uptr_dev", "ublk_dev"):
         g = _group(L.FEA_C3D8, 8, 32)
         setattr(g, f, None)
         assert vol(g) == EINVAL, f
-    for f in ("adjptr_dev", "adjcol_dev", "adjoff_dev", "moff_dev"):
-        nd = _nodes()
-        setattr(nd, f, None)
-        assert vol(hexg, nodes=nd) == EINVAL, f
     g = _group(L.FEA_C3D8, 8, 32)
     g.maxblk = -1
     assert vol(g) == EINVAL

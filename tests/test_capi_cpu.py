@@ -180,57 +180,92 @@ def test_product_meshes_match_oracle_meshes():
 
 
 def _upper_staging(hp, el, mask):
-    """The C3D8 staging arrays of a plan and the rule they follow: the record
-    of incidence (e, a) holds the blocks (a, b) of active column nodes
-    numbered >= the row node, in ascending b; a node's records are
-    contiguous, in element order."""
+    """The C3D8 staging arrays of a plan, the upper-block records decoded."""
     from fea_b200 import _lib as L
     arr = lambda i: hp.array(L.G_BASE + i)
+    ub = arr(L.A_UBLK).reshape(-1, 4)
     return dict(nodeinc=arr(L.A_NODEINC), inc=arr(L.A_INC), incpos=arr(L.A_INCPOS).reshape(-1, 8),
-                recbase=arr(L.A_RECBASE).reshape(-1, 8), nodeblk=arr(L.A_NODEBLK), bp=arr(L.A_BLKPTR),
-                bc=arr(L.A_BLKCON), adjptr=hp.array(L.FEA_A_ADJPTR), adjcol=hp.array(L.FEA_A_ADJCOL),
+                stagepos=arr(L.A_STAGEPOS).reshape(-1, 36), region=arr(L.A_REGION), uptr=arr(L.A_UPTR),
+                row=ub[:, 0], col=ub[:, 1], lc=ub[:, 2] & 0xFFFFFFFF, mc=ub[:, 2] >> 32,
+                first=ub[:, 3] & 0xFFFFFFFF, count=ub[:, 3] >> 32,
+                adjptr=hp.array(L.FEA_A_ADJPTR), adjcol=hp.array(L.FEA_A_ADJCOL),
                 adjoff=hp.array(L.FEA_A_ADJOFF), moff=hp.array(L.FEA_A_MOFF))
 
 
-def _included(el, mask, e, a):
-    na = el[e, a]
-    return [b for b in range(8) if mask[el[e, b]] and el[e, b] >= na] if mask[na] else []
+def _slots():
+    """(lane a, distance d, slot) of the element kernel: lane a computes K_ab,
+    b = (a + d) mod 8, for d = 0..3 and d = 4 when a < 4."""
+    out = []
+    for a in range(8):
+        for d in range(5 if a < 4 else 4):
+            out.append((a, d, len(out)))
+    return out
+
+
+def _expected_contributions(el, mask):
+    """Upper block (r, c) -> [(e, slot)] in staging order: the pair {i, j} of
+    element e is counted once, from the incidence (e, i) of its lower node r
+    (from i <= j when the element repeats the node), in ascending e, i, j."""
+    slot = {}
+    for a, d, s in _slots():
+        slot[(a, (a + d) % 8)] = s
+        slot[((a + d) % 8, a)] = s
+    expect = {}
+    for e in range(el.shape[0]):
+        for i in range(8):
+            r = el[e, i]
+            if not mask[r]:
+                continue
+            for j in range(8):
+                c = el[e, j]
+                if mask[c] and (c > r or (c == r and j >= i)):
+                    expect.setdefault((r, c), []).append((e, slot[(i, j)]))
+    return expect
 
 
 def test_block_contributor_lists(golden):
-    """Records, regions and contributor lists of the C3D8 staging: every upper
-    block (n, c >= n) lists the positions, in n's record region, of the (e, a,
-    b) that couple the two nodes, in ascending element order; lower blocks
-    list none; MOFF is n's value offset in row c."""
+    """Regions and upper-block records of the C3D8 staging: each node's
+    region holds, block-major in adjacency order, the contributions to its
+    upper blocks (n, c >= n) in ascending element order, regions start at
+    even blocks; every element block of two active nodes has one staged
+    position and the others none; the records carry the row and transpose
+    targets (MOFF: n's value offset in row c)."""
     g = golden("hex5")
     N, el = g["X"].shape[0], g["elems"]
     mask = np.full(N, 7, np.uint8)
     mask[g["fixed"]] = 0
     mask[g["fixed"][:3]] = 5                          # partial masks too
-    st = _upper_staging(_plan(N, mask, [("C3D8", el)]), el, mask)
-    nodeblk, recbase = st["nodeblk"], st["recbase"]
-    assert st["bp"].size == st["adjcol"].size + 1
-    pos = {n: int(nodeblk[n]) for n in range(N)}
-    expect = {}
-    for e in range(el.shape[0]):                       # element order = incidence order per node
-        for a in range(8):
-            n = el[e, a]
-            if not mask[n]:
-                assert recbase[e, a] == -1 and st["incpos"][e, a] == -1
-                continue
-            assert recbase[e, a] == pos[n]
-            for b in _included(el, mask, e, a):
-                expect.setdefault((n, el[e, b]), []).append(pos[n] - nodeblk[n])
-                pos[n] += 1
+    hp = _plan(N, mask, [("C3D8", el)])
+    from fea_b200 import _lib as L
+    vbase, rowlen = hp.array(L.FEA_A_VBASE), hp.array(L.FEA_A_ROWLEN)
+    st = _upper_staging(hp, el, mask)
+    expect = _expected_contributions(el, mask)
+    sp, region, uptr = st["stagepos"], st["region"], st["uptr"]
+    seen = np.zeros(sp.shape, bool)
     for n in range(N):
-        assert pos[n] == nodeblk[n + 1]
+        assert region[n] % 2 == 0
+        u = uptr[n]
+        t = 0
         for p in range(st["adjptr"][n], st["adjptr"][n + 1]):
             c = st["adjcol"][p]
-            assert list(st["bc"][st["bp"][p]:st["bp"][p + 1]]) == expect.get((n, c), [])
             if c < n:
-                assert st["bp"][p] == st["bp"][p + 1]
+                continue
+            assert st["row"][u] == vbase[n] + st["adjoff"][p]
             q = np.nonzero(st["adjcol"][st["adjptr"][c]:st["adjptr"][c + 1]] == n)[0][0] + st["adjptr"][c]
             assert st["moff"][p] == st["adjoff"][q]
+            assert st["col"][u] == (vbase[c] + st["moff"][p] if c != n else -1)
+            assert st["lc"][u] == rowlen[c] and st["mc"][u] == mask[c]
+            lst = expect.get((n, c), [])
+            assert st["first"][u] == t and st["count"][u] == len(lst)
+            for k, (e, s) in enumerate(lst):
+                assert sp[e, s] == region[n] + t + k
+                seen[e, s] = True
+            t += len(lst)
+            u += 1
+        assert u == uptr[n + 1]
+        assert region[n + 1] - region[n] == (t + 1) // 2 * 2
+    assert np.all(sp[~seen] == -1) and np.all(sp[seen] >= 0)
+    assert np.unique(sp[seen]).size == int(seen.sum())
 
 
 def test_serving_requests_are_seeded_and_bounded():
@@ -304,9 +339,10 @@ def test_csr_of_eight_hex_mesh_by_hand(clamp):
 @pytest.mark.parametrize("dofs,collapse", [((0, 1, 2), False), ((1,), False), ((0, 1, 2), True)])
 def test_upper_staging_emulated_gives_reference_K(dofs, collapse):
     """The C3D8 assembly as the kernels perform it, emulated on the CPU with
-    the oracle's element blocks: upper records written per incidence, then
-    per node the upper block sums into the node's rows and their transposes
-    into the column nodes' rows.  The CSR values equal the oracle's reduced K
+    the oracle's element blocks: each element block written to its staged
+    position, oriented to its upper node block, then per node the upper
+    block sums into the node's rows and their transposes into the column
+    nodes' rows.  The CSR values equal the oracle's reduced K
     and R; also with a collapsed element (two of its corners one node), whose
     repeated node puts two blocks of the element on the diagonal."""
     from fea_b200 import _lib as L
@@ -329,38 +365,43 @@ def test_upper_staging_emulated_gives_reference_K(dofs, collapse):
     vbase, rowlen, rdof = hp.array(L.FEA_A_VBASE), hp.array(L.FEA_A_ROWLEN), hp.array(L.FEA_A_RDOF)
     Re, Ke = O.element_residual_tangent("C3D8", X, torch.from_numpy(el), m.gc_to_u(gc), 1.0, 10.0)
     Re, Ke = Re.numpy(), Ke.numpy()                    # [a,j,e], [a,j,b,k,e]
-    blocks = np.full((int(st["nodeblk"][-1]), 3, 3), np.nan)
+    blocks = np.full((int(st["region"][-1]), 3, 3), np.nan)
     rslot = np.full((int(st["nodeinc"][-1]), 3), np.nan)
     for e in range(el.shape[0]):                       # element kernel, phase 3
-        for a in range(8):
-            rb = st["recbase"][e, a]
-            if rb < 0:
+        for a, d, s in _slots():
+            pos = st["stagepos"][e, s]
+            if pos < 0:
                 continue
-            for b in _included(el, mask, e, a):
-                blocks[rb] = Ke[a, :, b, :, e]
-                rb += 1
-            rslot[st["incpos"][e, a]] = Re[a, :, e]
+            b = (a + d) % 8
+            Kab = Ke[a, :, b, :, e]
+            if d == 0 or el[e, b] > el[e, a]:
+                blocks[pos] = Kab
+            elif el[e, b] < el[e, a]:
+                blocks[pos] = Kab.T
+            else:
+                blocks[pos] = Kab + Kab.T
+        for a in range(8):
+            if st["incpos"][e, a] >= 0:
+                rslot[st["incpos"][e, a]] = Re[a, :, e]
     K = np.full(int(vbase[-1]), np.nan)
     R = np.full(nfree, np.nan)
     free = lambda mk: [j for j in range(3) if mk >> j & 1]
-    for n in range(N):                                  # gather, one warp per node
+    for n in range(N):                                  # gather, one lane group per node
         if not mask[n]:
             continue
-        S = blocks[st["nodeblk"][n]:st["nodeblk"][n + 1]]
-        for p in range(st["adjptr"][n], st["adjptr"][n + 1]):
-            c = st["adjcol"][p]
-            if c < n:
-                continue
+        S = blocks[st["region"][n]:st["region"][n + 1]]
+        for u in range(st["uptr"][n], st["uptr"][n + 1]):
+            f, cnt, mc = st["first"][u], st["count"][u], st["mc"][u]
             blk = np.zeros((3, 3))
-            for t in range(st["bp"][p], st["bp"][p + 1]):
-                blk = blk + S[st["bc"][t]]
+            for t in range(f, f + cnt):
+                blk = blk + S[t]
             for rj, j in enumerate(free(mask[n])):
-                for rk, k in enumerate(free(mask[c])):
-                    K[vbase[n] + rj * rowlen[n] + st["adjoff"][p] + rk] = blk[j, k]
-            if c != n:
-                for rk, k in enumerate(free(mask[c])):
+                for rk, k in enumerate(free(mc)):
+                    K[st["row"][u] + rj * rowlen[n] + rk] = blk[j, k]
+            if st["col"][u] >= 0:
+                for rk, k in enumerate(free(mc)):
                     for cj, j in enumerate(free(mask[n])):
-                        K[vbase[c] + rk * rowlen[c] + st["moff"][p] + cj] = blk[j, k]
+                        K[st["col"][u] + rk * st["lc"][u] + cj] = blk[j, k]
             else:
                 r = rslot[st["nodeinc"][n]:st["nodeinc"][n + 1]].sum(0)
                 for rr, j in enumerate(free(mask[n])):
