@@ -365,29 +365,45 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
   const int64_t e = (int64_t)blockIdx.x * HX_EPB + le;
   const bool act = e < P.ne;
   double* V = sv + le * HX_EL;
+  // ---- phase 0: node `lane`'s coordinates and displacement, once per element,
+  // to the scalar area of V (48 doubles: 6 per node) for all 8 lanes --------
+  int32_t cl = 0;
   if (act) {
-    // ---- phase 1: Gauss point g = lane --------------------------------------
-    const double px = csx(lane) * q3, py = csy(lane) * q3, pz = csz(lane) * q3;
-    const double fxp = 1.0 + px, fxm = 1.0 - px, fyp = 1.0 + py, fym = 1.0 - py, fzp = 1.0 + pz, fzm = 1.0 - pz;
-    double J0[9], Ju[9];
+    cl = P.conn[e * 8 + lane];
+    const double* xb = P.X + 3 * (int64_t)cl;
+    const unsigned mb = P.mask[cl];
+    const int32_t rb = P.rdof[cl];
+    double2* o = reinterpret_cast<double2*>(V + HX_SC + lane * 6);
+    o[0] = make_double2(__ldg(xb), __ldg(xb + 1));
+    o[1] = make_double2(__ldg(xb + 2), node_u(P.gc, rb, mb, 0));
+    o[2] = make_double2(node_u(P.gc, rb, mb, 1), node_u(P.gc, rb, mb, 2));
+  }
+  __syncwarp();
+  // ---- phase 1: Gauss point g = lane ----------------------------------------
+  const double px = csx(lane) * q3, py = csy(lane) * q3, pz = csz(lane) * q3;
+  const double fxp = 1.0 + px, fxm = 1.0 - px, fyp = 1.0 + py, fym = 1.0 - py, fzp = 1.0 + pz, fzm = 1.0 - pz;
+  double J0[9], Ju[9];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) J0[i] = Ju[i] = 0.0;
+  for (int i = 0; i < 9; ++i) J0[i] = Ju[i] = 0.0;
+  if (act) {
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
       const double sx = (((b + 1) >> 1) & 1) ? 1.0 : -1.0, sy = ((b >> 1) & 1) ? 1.0 : -1.0, sz = (b >> 2) ? 1.0 : -1.0;
       const double fx = sx > 0 ? fxp : fxm, fy = sy > 0 ? fyp : fym, fz = sz > 0 ? fzp : fzm;
       const double d0 = 0.125 * sx * fy * fz, d1 = 0.125 * sy * fx * fz, d2 = 0.125 * sz * fx * fy;
-      const int32_t c = P.conn[e * 8 + b];
-      const double* xb = P.X + 3 * (int64_t)c;
-      const unsigned mb = P.mask[c];
-      const int32_t rb = P.rdof[c];
+      const double2* xs = reinterpret_cast<const double2*>(V + HX_SC + b * 6);
+      const double2 v0 = xs[0], v1 = xs[1], v2 = xs[2];
+      const double xv[3] = {v0.x, v0.y, v1.x}, uv[3] = {v1.y, v2.x, v2.y};
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
-        const double x = __ldg(xb + i), u = node_u(P.gc, rb, mb, i);
+        const double x = xv[i], u = uv[i];
         J0[3 * i] += x * d0; J0[3 * i + 1] += x * d1; J0[3 * i + 2] += x * d2;
         Ju[3 * i] += u * d0; Ju[3 * i + 1] += u * d1; Ju[3 * i + 2] += u * d2;
       }
     }
+  }
+  __syncwarp();                                  // the node data are read: the area takes the scalars
+  if (act) {
     double iJ[9], F[9], iF[9];
     const double w = inv3(J0, iJ);             // Gauss weight 1
 #pragma unroll
@@ -395,9 +411,9 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
 #pragma unroll
       for (int i = 0; i < 3; ++i)
         F[3 * I + i] = fma(Ju[3 * I], iJ[i], fma(Ju[3 * I + 1], iJ[3 + i], fma(Ju[3 * I + 2], iJ[6 + i], I == i ? 1.0 : 0.0)));
-    const double J = inv3(F, iF);
+    double Jm;
+    const double J = inv3_jm(F, iF, &Jm);      // F^-1 and J^-2/3 from one reciprocal cube root
     const double mu = P.mu, kappa = P.kappa;
-    const double Jm = jm23(J);
     double sF2 = 0.0;
 #pragma unroll
     for (int i = 0; i < 9; ++i) sF2 += F[i] * F[i];
@@ -408,7 +424,7 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
     S[2] = w * (mu * I1 / 3.0 - kappa * J * (J - 1.0));              // w gamma
     S[3] = w * muJm;                                                 // w c (delta term, residual)
     S[4] = w * (kappa * J * (J - 1.0) - mu * I1 / 3.0);              // w c2 (residual)
-    S[5] = (double)P.conn[e * 8 + lane];                             // node `lane`, for phase 3
+    S[5] = (double)cl;                                               // node `lane`, for phase 3
     // Mq = J0^-1 F^-1, Mf = J0^-1 F^T: q_b = Mq^T dxi_b, f_b = Mf^T dxi_b, g_b = J0^-T dxi_b
     double Mq[9], Mf[9];
 #pragma unroll
@@ -457,8 +473,9 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
     for (int i = 0; i < 9; ++i) acc[d][i] = 0.0;
 #pragma unroll 1
   for (int g = 0; g < (act ? 8 : 0); ++g) {
-    const double* S = V + HX_SC + g * 6;
-    const double wa = S[0], wb = S[1], wg = S[2], wc = S[3], wc2 = S[4];
+    const double2* S2 = reinterpret_cast<const double2*>(V + HX_SC + g * 6);   // 16-byte aligned
+    const double2 s01 = S2[0], s23 = S2[1], s45 = S2[2];
+    const double wa = s01.x, wb = s01.y, wg = s23.x, wc = s23.y, wc2 = s45.x;
     const double* Va = V + g * HX_VG + a * HX_VB;
     double qa[3], fa[3], gm[3], A[3], B[3], Cc[3];
     {
@@ -1496,14 +1513,14 @@ static FaceParams face_params(const fea_nodes_t* N, const fea_group_t* G, double
 extern "C" int fea_assemble_pressure(const fea_nodes_t* N, const fea_group_t* G, double p, const double* Xi,
                                      const double* gc, double* K, double* R, cudaStream_t st) {
   if (!N || !G || !Xi || !gc || (G->kind != FEA_T3 && G->kind != FEA_Q4)) return FEA_EINVAL;
-  if (G->nn != (G->kind == FEA_T3 ? 3 : 4) || G->threads != 128) return FEA_EINVAL;
+  if (G->nn != (G->kind == FEA_T3 ? 3 : 4) || (G->threads != 32 && G->threads != 128)) return FEA_EINVAL;
   if (!K && !R) return FEA_OK;
   if (int r = ensure_tables()) return r;
   FaceParams P = face_params(N, G, p, Xi, gc);
   P.K = K;
   P.R = R;
-  if (G->kind == FEA_T3) return launch_chunked(k_face_rk<3>, G->nchunk, 128, G->smem_doubles, st, P);
-  return launch_chunked(k_face_rk<4>, G->nchunk, 128, G->smem_doubles, st, P);
+  if (G->kind == FEA_T3) return launch_chunked(k_face_rk<3>, G->nchunk, G->threads, G->smem_doubles, st, P);
+  return launch_chunked(k_face_rk<4>, G->nchunk, G->threads, G->smem_doubles, st, P);
 }
 
 extern "C" int fea_energy_volume(const fea_nodes_t* N, const fea_group_t* G, double mu, double kappa,

@@ -446,7 +446,12 @@ extern "C" int fea_plan_build(int64_t n_nodes, const uint8_t* free_mask, int32_t
     if (group_kind[g] == FEA_C3D8 && (r = build_blocks(*P, 8, group_conn[g], ginc[g], P->groups[g]))) return r;
   }
   for (int g = 0; g < n_faces; ++g) {
-    int r = build_gather(*P, face_kind[g], face_nf[g], face_conn[g], finc[g], 128, budget, P->faces[g]);
+    // chunks of 32 face incidences (one warp per CTA: many small CTAs for the
+    // few thousand faces of a loaded surface), 128 when a node has more
+    int64_t most = 0;
+    for (int64_t n = 0; n < N; ++n) most = std::max<int64_t>(most, finc[g].ptr[n + 1] - finc[g].ptr[n]);
+    const int th = most <= 32 ? 32 : 128;
+    int r = build_gather(*P, face_kind[g], face_nf[g], face_conn[g], finc[g], th, budget, P->faces[g]);
     if (r) return r;
   }
   *out = P.release();

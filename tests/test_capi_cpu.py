@@ -268,6 +268,26 @@ def test_block_contributor_lists(golden):
     assert np.unique(sp[seen]).size == int(seen.sum())
 
 
+def test_face_chunks_take_one_warp_unless_a_node_has_more_faces():
+    """Face lists are chunked by 32 incidences (one-warp CTAs), by 128 when a
+    node lies on more than 32 faces: a fan of 40 triangles around one apex
+    node of a tet fan."""
+    from fea_b200 import _lib as L
+    X, el = O.hex_block(2)
+    N = X.shape[0]
+    mask = np.full(N, 7, np.uint8)
+    quads = el.numpy()[:, :4].astype(np.int32)                  # bottom faces of the elements
+    hp = _plan(N, mask, [("C3D8", el.numpy())], [("Q4", quads)])
+    assert hp.scalar(L.F_BASE + L.S_THREADS, 0) == 32
+    M = 40
+    apex, ring = 0, np.arange(1, M + 1)
+    tets = np.stack([np.full(M, apex), ring, np.roll(ring, -1), np.full(M, M + 1)], 1).astype(np.int32)
+    tris = tets[:, :3].copy()
+    mask = np.full(M + 2, 7, np.uint8)
+    hp = _plan(M + 2, mask, [("C3D4", tets)], [("T3", tris)])
+    assert hp.scalar(L.F_BASE + L.S_THREADS, 0) == 128
+
+
 def test_serving_requests_are_seeded_and_bounded():
     from fea_b200 import meshes, serving
     a = serving.make_requests(20, 5.0, seed=3)
