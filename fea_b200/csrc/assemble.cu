@@ -191,6 +191,28 @@ __device__ __forceinline__ void element_strip(const VolParams& P, const int32_t*
   }
 }
 
+// out[i] (+)= src[i] for i = threadIdx.x, + blockDim.x, ... < len: the global
+// reads of eight strides issued together (one round trip per eight values
+// instead of one per value: the read-modify-write of the accumulate mode was
+// latency-serial)
+template <bool ACC>
+__device__ __forceinline__ void add_rows(double* __restrict__ out, const double* __restrict__ src, int len) {
+  constexpr int U = 8;
+  for (int i0 = threadIdx.x; i0 < len; i0 += U * (int)blockDim.x) {
+    double v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * (int)blockDim.x;
+      v[u] = (ACC && i < len) ? out[i] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * (int)blockDim.x;
+      if (i < len) out[i] = ACC ? v[u] + src[i] : src[i];
+    }
+  }
+}
+
 // Copy a chunk's shared-memory rows to the reduced K values and R: one flat
 // copy when the chunk's node rows are contiguous in HBM, else node by node.
 template <bool ACC>
@@ -204,22 +226,15 @@ __device__ __forceinline__ void write_back(const int32_t* __restrict__ chunkptr,
   if (chunkdim[3 * ch + 2]) {
     const int n0 = chunklist[l0];
     if (K) {
-      double* out = K + vbase[n0];
-      for (int i = threadIdx.x; i < nv; i += blockDim.x) out[i] = ACC ? out[i] + sm[i] : sm[i];
+      add_rows<ACC>(K + vbase[n0], sm, nv);
     }
-    if (R) {
-      double* out = R + dbase[n0];
-      for (int i = threadIdx.x; i < nr; i += blockDim.x) out[i] = ACC ? out[i] + sm[nv + i] : sm[nv + i];
-    }
+    if (R) add_rows<ACC>(R + dbase[n0], sm + nv, nr);
     return;
   }
   for (int l = l0; l < l1; ++l) {
     const int n = chunklist[l];
     if (K) {
-      const int len = (int)(vbase[n + 1] - vbase[n]);
-      double* out = K + vbase[n];
-      const double* src = sm + soff[n];
-      for (int i = threadIdx.x; i < len; i += blockDim.x) out[i] = ACC ? out[i] + src[i] : src[i];
+      add_rows<ACC>(K + vbase[n], sm + soff[n], (int)(vbase[n + 1] - vbase[n]));
     }
     if (R) {
       const int f = popc3(mask[n]);
@@ -494,7 +509,6 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
     }
 #pragma unroll
     for (int d = 0; d < 5; ++d) {
-      if (d == 4 && nb == 4) break;
       const double* Vb = V + g * HX_VG + ((a + d) & 7) * HX_VB;
       double qb[3], fb[3];
       {
@@ -504,11 +518,16 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
       }
       const double dg = gm[0] * qb[0] + gm[1] * qb[1] + gm[2] * qb[2];    // w mu J^-2/3 g_a . g_b
       // three fused multiply-adds into each accumulator, the delta term on
-      // the diagonal alone: 33 FP64 operations per block and Gauss point
+      // the diagonal alone: 33 FP64 operations per block and Gauss point.
+      // d = 0 (K_aa, symmetric) and d = 4 take the upper triangle only (24):
+      // at d = 4 every lane computes one, lane a < 4 that of K_a,a+4 and
+      // lane a + 4 that of K_a+4,a, whose strict part is the strict lower
+      // triangle of K_a,a+4 transposed (the two lanes share the block)
 #pragma unroll
       for (int j = 0; j < 3; ++j)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
+          if ((d == 0 || d == 4) && k < j) continue;
           double t = acc[d][3 * j + k];
           t = fma(A[j], qb[k], t);
           t = fma(B[j], fb[k], t);
@@ -520,6 +539,17 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
       acc[d][8] += dg;
     }
   }
+  // the strict lower triangle of K_a,a+4 from lane a + 4 (all lanes shuffle)
+  const int partner = (lane + 4) & 7;
+  const double l10 = __shfl_sync(0xffffffffu, acc[4][1], partner, 8);
+  const double l20 = __shfl_sync(0xffffffffu, acc[4][2], partner, 8);
+  const double l21 = __shfl_sync(0xffffffffu, acc[4][5], partner, 8);
+  acc[0][3] = acc[0][1];
+  acc[0][6] = acc[0][2];
+  acc[0][7] = acc[0][5];
+  acc[4][3] = l10;
+  acc[4][6] = l20;
+  acc[4][7] = l21;
   // ---- phase 3: every block from registers to its staged position ------------
   // K_ab as computed when the column node is numbered above the row node (or
   // b = a), transposed when below, K_ab + K_ab^T when the element repeats
@@ -571,7 +601,7 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
 // largest region (shared memory per group: capb blocks).
 template <bool WR, bool ACC, int LPN>
 __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const double* __restrict__ stage,
-                                                        const double* __restrict__ rslot, int capb) {
+                                                        const double* __restrict__ rslot, int capb, int capq) {
   extern __shared__ __align__(16) double gsm[];
   static_assert(LPN == 8 || LPN == 16 || LPN == 32, "lanes per node");
   constexpr int NPW = 32 / LPN;                   // nodes per warp
@@ -581,13 +611,15 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
   const unsigned gmask = LPN == 32 ? 0xffffffffu : (((1u << LPN) - 1u) << (sub * LPN));
   const int64_t n = ((int64_t)blockIdx.x * HX_GW + warp) * NPW + sub;
   if (n >= P.n_nodes) return;
+  // the node's metadata issued together, before the mask decides
   const unsigned mn = P.mask[n];
+  const int64_t b0 = P.region[n], b1 = P.region[n + 1];
+  const int64_t u0 = P.uptr[n], u1 = P.uptr[n + 1];
+  const int q0 = P.nodeinc[n], q1 = P.nodeinc[n + 1];
   if (!mn) return;
-  const int64_t b0 = P.region[n];
-  const int64_t nbk_all = P.region[n + 1] - b0;
-  const int nbk = nbk_all < capb ? (int)nbk_all : capb;
-  const int64_t u0 = P.uptr[n], nu = P.uptr[n + 1] - u0;
-  const int q0 = P.nodeinc[n], nq = P.nodeinc[n + 1] - q0;
+  const int nbk = b1 - b0 < capb ? (int)(b1 - b0) : capb;
+  const int64_t nu = u1 - u0;
+  const int nq = q1 - q0 < capq ? q1 - q0 : capq;
   // the lane's first record: targets (row, transpose) and (rowlen_c, mask_c, first, count)
   int64_t u = lane;
   longlong2 tg = make_longlong2(0, 0);
@@ -597,42 +629,29 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
     tg = r[0];
     mt = *reinterpret_cast<const int4*>(r + 1);
   }
-  double rq[3] = {0.0, 0.0, 0.0};
-  if (WR && lane < nq) {
-    const double* sr = rslot + (int64_t)(q0 + lane) * 4;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) rq[j] = sr[j];
-  }
-  double* S = gsm + (int64_t)(warp * NPW + sub) * capb * 9;
+  // the group's shared area: the region (capb blocks), then the node's
+  // residual slots (capq x 4 doubles) when R is written
+  double* S = gsm + (int64_t)(warp * NPW + sub) * (capb * 9 + (WR ? capq * 4 : 0));
+  double* SR = S + capb * 9;
   {
-    // regions start at even blocks and hold an even number: whole 16-byte
-    // pieces, copied through L2 only (cg)
+    // regions start at even blocks and hold an even number, residual slots
+    // are 32 bytes: whole 16-byte pieces, copied through L2 only (cg)
     const double* src = stage + b0 * 9;
     const int nd2 = (nbk * 9) >> 1;
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(S);
     for (int i = lane; i < nd2; i += LPN)
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sbase + 16u * (unsigned)i), "l"(src + 2 * i)
                    : "memory");
+    if (WR) {
+      const double* rsrc = rslot + (int64_t)q0 * 4;
+      const unsigned rbase = (unsigned)__cvta_generic_to_shared(SR);
+      for (int i = lane; i < 2 * nq; i += LPN)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(rbase + 16u * (unsigned)i),
+                     "l"(rsrc + 2 * i)
+                     : "memory");
+    }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-  }
-  double r[3] = {0.0, 0.0, 0.0};
-  if (WR) {                                      // group-uniform: incidences in order
-    for (int qb = 0; qb < nq; qb += LPN) {
-      if (qb > 0) {
-        rq[0] = rq[1] = rq[2] = 0.0;
-        if (qb + lane < nq) {
-          const double* sr = rslot + (int64_t)(q0 + qb + lane) * 4;
-#pragma unroll
-          for (int j = 0; j < 3; ++j) rq[j] = sr[j];
-        }
-      }
-      const int m = min(LPN, nq - qb);
-      for (int i = 0; i < m; ++i) {
-#pragma unroll
-        for (int j = 0; j < 3; ++j) r[j] += __shfl_sync(gmask, rq[j], i, LPN);
-      }
-    }
   }
   __syncwarp(gmask);
   const int L = P.rowlen[n];
@@ -676,7 +695,12 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
         }
         ++rk;
       }
-    } else if (WR) {
+    } else if (WR) {                             // the residual, incidences in element order
+      double r[3] = {0.0, 0.0, 0.0};
+      for (int q = 0; q < nq; ++q) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r[j] += SR[q * 4 + j];
+      }
       double* Rout = P.R + P.rdof[n];
       int rr = 0;
 #pragma unroll
@@ -1433,7 +1457,8 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
     const bool acc = accumulate != 0, wr = R != nullptr, er = elemR != nullptr;
     if (hex) {
       const int capb = std::max<int>(G->maxblk, 2);   // regions hold even block counts
-      const size_t region = (size_t)capb * 9 * sizeof(double);
+      const int capq = std::max<int>(G->maxval, 1);   // most incidences of one node
+      const size_t region = ((size_t)capb * 9 + (wr ? (size_t)capq * 4 : 0)) * sizeof(double);
       const bool two = (size_t)HX_GW * (32 / HX_LPN) * region <= (size_t)smem_limit();
       const int lpn = two ? HX_LPN : 32;
       const size_t gbytes = (size_t)HX_GW * (32 / lpn) * region;
@@ -1449,14 +1474,14 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
       const int per_cta = HX_GW * (32 / lpn);
       const unsigned g2 = (unsigned)((N->n_nodes + per_cta - 1) / per_cta);
       if (g2) {
-        void (*gk)(VolParams, const double*, const double*, int) =
+        void (*gk)(VolParams, const double*, const double*, int, int) =
             two ? (wr ? (acc ? k_hex_gat<true, true, HX_LPN> : k_hex_gat<true, false, HX_LPN>)
                       : (acc ? k_hex_gat<false, true, HX_LPN> : k_hex_gat<false, false, HX_LPN>))
                 : (wr ? (acc ? k_hex_gat<true, true, 32> : k_hex_gat<true, false, 32>)
                       : (acc ? k_hex_gat<false, true, 32> : k_hex_gat<false, false, 32>));
         if (cudaError_t ce = cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gbytes))
           return (int)ce;
-        gk<<<g2, HX_GW * 32, gbytes, st>>>(P, work, rslot, capb);
+        gk<<<g2, HX_GW * 32, gbytes, st>>>(P, work, rslot, capb, capq);
         count_launch();
       }
       return (int)cudaGetLastError();
