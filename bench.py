@@ -927,7 +927,7 @@ def main():
         "config": bench_config(n, E, N, ndof, nnz, world),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "algorithmic_bytes": B, "kernel_ms": kern_ms,
-                     "kernel": "k_hex_elem + k_hex_gat (C3D8 upper block rows staged node by node, then node-row gather with transposed writes into CSR)",
+                     "kernel": "k_hex_elem + k_hex_gat (C3D8 element blocks staged block-major in per-node regions, then a node-row gather with transposed writes into CSR)",
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650"},
         "roofline_fp64": fp64_roofline(E, B, hbm, kern_ms),
         "e2e": {"value": job_rate(world, E, e2e_ms), "unit": UNIT, "ms_per_step": e2e_ms,
