@@ -133,7 +133,7 @@ fea_pcgb_set = _sig("fea_pcgb_set", I32, P, I32, I64, I32, C.POINTER(PcgbSlot), 
 fea_pcgb_start = _sig("fea_pcgb_start", I32, P, I32, I64, I32, I64, I64, P)
 fea_pcgb_iterate = _sig("fea_pcgb_iterate", I32, P, I32, I64, I32, P)
 fea_pcgb_state = _sig("fea_pcgb_state", I32, P, I32, I64, I32, P, P)
-fea_explicit_work_len = _sig("fea_explicit_work_len", I64, I64)
+fea_explicit_work_len = _sig("fea_explicit_work_len", I64, NP)
 fea_explicit_run = _sig("fea_explicit_run", I32, NP, GP, D, D, P, D, I64, I32, I32, P, P, P, P, P, I64, P)
 fea_explicit_stage = _sig("fea_explicit_stage", I32, I64, I32, D, P, P, P, P, P, P, P, P)
 fea_ls_ladder_len = _sig("fea_ls_ladder_len", I32)

@@ -10,6 +10,10 @@
 // One thread per node evaluates the internal force of the node from its
 // incident elements (gather, no atomics) and immediately advances that node's
 // state; u is double-buffered so every thread reads a consistent u_k.  The
+// element nodes' coordinates and displacements are read from a node-major
+// copy (x, y, z, ux, uy, uz per node: three 16-byte loads instead of eight
+// scalar loads through the mask and the reduced DOF numbering), double-
+// buffered with u and written by each node's thread as it advances.  The
 // element math runs in T (double, or float for the FP32 variant) and the
 // nodal sums in double.
 #include <cmath>
@@ -31,6 +35,8 @@ struct ExParams {
   double* vh;                     // in: vh_{k-1/2} (or v0 when init), out: vh_{k+1/2}
   double* v;                      // out: v_{k+1}
   double* a;                      // in/out
+  const double* __restrict__ xu;  // [N, 6] coordinates and u_k of every node
+  double* xunext;                 // [N, 6] the same at u_{k+1}
   double mu, kappa, dt;
   int32_t n_nodes;
 };
@@ -38,13 +44,6 @@ struct ExParams {
 // residual contribution of local node a of one element, computed in T
 template <int NN, class T>
 __device__ __forceinline__ void elem_force(const ExParams& P, const int32_t* cn, int a, double r[3]) {
-  unsigned mk[NN];
-  int32_t rd[NN];
-#pragma unroll
-  for (int b = 0; b < NN; ++b) {
-    mk[b] = P.mask[cn[b]];
-    rd[b] = P.rdof[cn[b]];
-  }
   const T mu = (T)P.mu, kappa = (T)P.kappa;
 #pragma unroll
   for (int g = 0; g < Elem<NN>::NG; ++g) {
@@ -53,13 +52,9 @@ __device__ __forceinline__ void elem_force(const ExParams& P, const int32_t* cn,
     for (int i = 0; i < 9; ++i) J0[i] = Ju[i] = T(0);
 #pragma unroll
     for (int b = 0; b < NN; ++b) {
-      const double* xb = P.X + 3 * (int64_t)cn[b];
-      T x[3], uu[3];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        x[i] = (T)__ldg(xb + i);
-        uu[i] = (T)node_u(P.u, rd[b], mk[b], i);
-      }
+      const double2* xb = reinterpret_cast<const double2*>(P.xu + 6 * (int64_t)cn[b]);
+      const double2 v0 = xb[0], v1 = xb[1], v2 = xb[2];
+      const T x[3] = {(T)v0.x, (T)v0.y, (T)v1.x}, uu[3] = {(T)v1.y, (T)v2.x, (T)v2.y};
 #pragma unroll
       for (int m = 0; m < 3; ++m) {
         T d = (T)Elem<NN>::dxi(g, b, m);
@@ -110,7 +105,7 @@ __device__ __forceinline__ void elem_force(const ExParams& P, const int32_t* cn,
 // flags: bit0 compute the force (else use a), bit1 init (vh = v0 - dt/2 a),
 //        bit2 advance (vh, v, u_next)
 template <int NN, class T>
-__global__ void __launch_bounds__(128) k_explicit(ExParams P, int flags) {
+__global__ void __launch_bounds__(128, NN == 4 ? 5 : 1) k_explicit(ExParams P, int flags) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= P.n_nodes) return;
   const unsigned mn = P.mask[n];
@@ -152,6 +147,7 @@ __global__ void __launch_bounds__(128) k_explicit(ExParams P, int flags) {
   }
   const int32_t base = P.rdof[n];
   int rj = 0;
+  double un[3] = {0.0, 0.0, 0.0};
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     if (!(mn >> d & 1u)) continue;
@@ -163,11 +159,33 @@ __global__ void __launch_bounds__(128) k_explicit(ExParams P, int flags) {
       double vhn = vh + P.dt * acc;
       P.v[i] = 0.5 * (vhn + vh);
       P.vh[i] = vhn;
-      P.unext[i] = P.u[i] + P.dt * vhn;
+      un[d] = P.u[i] + P.dt * vhn;
+      P.unext[i] = un[d];
     } else if (flags & 2) {
       P.vh[i] = P.vh[i] - 0.5 * P.dt * acc;
     }
   }
+  if (flags & 4) {                               // the node's copy at u_{k+1} (fixed components 0)
+    double* o = P.xunext + 6 * (int64_t)n;
+    o[3] = un[0];
+    reinterpret_cast<double2*>(o)[2] = make_double2(un[1], un[2]);
+  }
+}
+
+// The node-major copy of coordinates and u (both buffers): x, y, z, then
+// the displacement (0 for fixed components).
+__global__ void __launch_bounds__(256) k_xu_init(ExParams P, double* __restrict__ xu0, double* __restrict__ xu1) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= P.n_nodes) return;
+  const unsigned m = P.mask[n];
+  const int32_t rd = P.rdof[n];
+  const double* x = P.X + 3 * (int64_t)n;
+  const double2 a = make_double2(x[0], x[1]), b = make_double2(x[2], node_u(P.u, rd, m, 0)),
+                c = make_double2(node_u(P.u, rd, m, 1), node_u(P.u, rd, m, 2));
+  double2* o0 = reinterpret_cast<double2*>(xu0 + 6 * (int64_t)n);
+  double2* o1 = reinterpret_cast<double2*>(xu1 + 6 * (int64_t)n);
+  o0[0] = a; o0[1] = b; o0[2] = c;
+  o1[0] = a; o1[1] = b; o1[2] = c;
 }
 
 // One stage of the central-difference loop around a separately assembled
@@ -216,7 +234,12 @@ extern "C" int fea_explicit_stage(int64_t n, int32_t stage, double dt, const dou
   return (int)cudaGetLastError();
 }
 
-extern "C" int64_t fea_explicit_work_len(int64_t ndof) { return ndof; }
+// second u buffer (ndof doubles, rounded to 16 bytes), then the two
+// node-major copies of coordinates and u (6 doubles per node each)
+extern "C" int64_t fea_explicit_work_len(const fea_nodes_t* N) {
+  if (!N || N->ndof < 0 || N->n_nodes < 0) return 0;
+  return ((N->ndof + 1) & ~(int64_t)1) + 12 * N->n_nodes;
+}
 
 // state on entry: u = u_k, vh = vh_{k-1/2}, a = a_k   (init == 0), or
 //                 u = u_0, v = v_0 (a, vh are outputs)  (init != 0)
@@ -226,7 +249,8 @@ extern "C" int fea_explicit_run(const fea_nodes_t* N, const fea_group_t* G, doub
                                    cudaStream_t st) {
   if (!N || !G || !minv || !u || !vh || !a || !v || !work || steps < 0) return FEA_EINVAL;
   if (G->kind != FEA_C3D4 && G->kind != FEA_C3D8) return FEA_EINVAL;
-  if (work_len < fea_explicit_work_len(N->ndof)) return FEA_EWORK;
+  if (work_len < fea_explicit_work_len(N)) return FEA_EWORK;
+  if (((uintptr_t)work & 15) != 0) return FEA_EINVAL;
   if (int r = ensure_tables()) return r;
   if (N->n_nodes == 0 || N->ndof == 0) return FEA_OK;
   ExParams P;
@@ -244,11 +268,17 @@ extern "C" int fea_explicit_run(const fea_nodes_t* N, const fea_group_t* G, doub
   P.kappa = kappa;
   P.dt = dt;
   P.n_nodes = (int32_t)N->n_nodes;
+  double* xub[2] = {work + ((N->ndof + 1) & ~(int64_t)1), work + ((N->ndof + 1) & ~(int64_t)1) + 6 * N->n_nodes};
+  P.u = u;
+  k_xu_init<<<grid_for(N->n_nodes, 256), 256, 0, st>>>(P, xub[0], xub[1]);
+  count_launch();
   const int grid = grid_for(N->n_nodes, 128);
   const bool hex = G->kind == FEA_C3D8;
   auto launch = [&](const double* ucur, double* unext, int flags) {
     P.u = ucur;
     P.unext = unext;
+    P.xu = xub[ucur == u ? 0 : 1];
+    P.xunext = xub[ucur == u ? 1 : 0];
     if (hex) {
       if (fp32) k_explicit<8, float><<<grid, 128, 0, st>>>(P, flags);
       else k_explicit<8, double><<<grid, 128, 0, st>>>(P, flags);

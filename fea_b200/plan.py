@@ -388,7 +388,7 @@ class DevicePlan:
                                      vptr(vhp), vptr(a), vptr(v), stream()), "fea_explicit_stage")
 
     def explicit_run(self, gi, mu, kappa, minv, dt, steps, u, vh, a, v, fp32=False, init=False):
-        w = self.scratch(L.fea_explicit_work_len(self.ndof))
+        w = self.scratch(L.fea_explicit_work_len(C.byref(self.nodes)))
         L.check(L.fea_explicit_run(C.byref(self.nodes), C.byref(self.groups[gi].desc), float(mu), float(kappa),
                                    vptr(minv), float(dt), int(steps), int(bool(fp32)), int(bool(init)), vptr(u),
                                    vptr(vh), vptr(a), vptr(v), vptr(w), w.numel(), stream()), "fea_explicit_run")

@@ -475,9 +475,11 @@ int fea_ls_select(int64_t n, const double* E_dev, int32_t k0, double c1, double 
  * init == 0: on entry u = u_k, vh = vh_{k-1/2}, a = a_k.
  * Runs `steps` steps and leaves u, vh, a, v at the final step.
  * fp32 != 0 evaluates the element force in FP32 with FP64 nodal sums.
- * work_dev: fea_explicit_work_len(ndof) doubles (second u buffer).
+ * work_dev: fea_explicit_work_len(nodes) doubles, 16-byte aligned (a second
+ * u buffer and two node-major copies of the coordinates and u, which the
+ * element math reads with 16-byte loads).
  * ------------------------------------------------------------------------- */
-int64_t fea_explicit_work_len(int64_t ndof);
+int64_t fea_explicit_work_len(const fea_nodes_t* nodes);
 
 /* One stage of the same central-difference step around a residual R that
  * the caller assembles (all element groups and loads: the reference's

@@ -116,12 +116,16 @@ def test_volume_entry_points_check_arguments_first():
     assert L.fea_invert_mass(-1, _p(1), None) == EINVAL
     assert L.fea_invert_mass(0, _p(1), None) == 0
 
-    assert L.fea_explicit_work_len(30) == 30
-    ex = lambda G, steps=3, wlen=30: L.fea_explicit_run(C.byref(N), C.byref(G), 1.0, 10.0, _p(1), 1e-4, steps, 0,
-                                                        0, _p(2), _p(3), _p(4), _p(5), _p(6), wlen, None)
+    ewl = int(L.fea_explicit_work_len(C.byref(N)))
+    assert ewl == 30 + 12 * 10                                      # u buffer + two node-major copies
+    assert L.fea_explicit_work_len(None) == 0
+    ex = lambda G, steps=3, wlen=ewl, w=_p(6): L.fea_explicit_run(C.byref(N), C.byref(G), 1.0, 10.0, _p(1), 1e-4,
+                                                                  steps, 0, 0, _p(2), _p(3), _p(4), _p(5), w, wlen,
+                                                                  None)
     assert ex(tetg, steps=-1) == EINVAL
     assert ex(face) == EINVAL
-    assert ex(tetg, wlen=29) == EWORK
+    assert ex(tetg, wlen=ewl - 1) == EWORK
+    assert ex(tetg, w=C.c_void_p(FAKE + 8)) == EINVAL               # not 16-byte aligned
     assert L.fea_adjoint_vjp_volume(C.byref(N), C.byref(tetg), 1.0, 10.0, _p(1), _p(2), _p(3), _p(4), _p(5),
                                     ns - 1, None) == EWORK
     noall = _group(L.FEA_C3D4, 4, 128)

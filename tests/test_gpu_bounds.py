@@ -130,7 +130,7 @@ def test_explicit_and_adjoint_stay_in_bounds(golden, name, kind):
     a.zero_()
     vb, v = guarded(n)
     v.zero_()
-    wl = int(L.fea_explicit_work_len(n))
+    wl = int(L.fea_explicit_work_len(C.byref(P.nodes)))
     wb, w = guarded(wl)
     L.check(L.fea_explicit_run(C.byref(P.nodes), C.byref(g.desc), float(mu), float(kappa), ptr(minv), 1e-4, 7, 0, 1,
                                ptr(u), ptr(vh), ptr(a), ptr(v), ptr(w), wl, st), "explicit")
