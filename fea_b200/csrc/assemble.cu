@@ -364,7 +364,7 @@ constexpr int HX_LPN = 16;
 // Offset of the residual slots in the C3D8 scratch: after the staged blocks,
 // rounded to 16 bytes.
 __host__ __device__ inline int64_t hx_rslot_base(int64_t nblk) { return (nblk * 9 + 1) & ~(int64_t)1; }
-constexpr int HX_GINC = 32;               // incidences per gather chunk (8 lanes each)
+constexpr int HX_GINC = 32;               // chunk capacity of C3D8 plans (the C3D8 kernels read no chunks)
 
 // corner signs of hex node / Gauss point c (brick.py:15-25, 151-160)
 __device__ __forceinline__ double csx(int c) { return (((c + 1) >> 1) & 1) ? 1.0 : -1.0; }
