@@ -266,6 +266,10 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
   double racc[3];
   int32_t cn[NN];
   int rank = -1, a = 0, n = 0;
+  // the row metadata and column offsets of the incidence, issued before the
+  // element math so that their loads overlap it
+  unsigned mn = 0, mcb[NN], bob[NN];
+  int rowoff = 0, L = 0, dr = 0;
   if (act) {
     const int ea = P.inc[q];
     const int64_t e = ea >> 4;
@@ -274,6 +278,15 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
     for (int b = 0; b < NN; ++b) cn[b] = P.conn[e * NN + b];
     n = cn[a];
     rank = q - P.nodeinc[n];
+    mn = P.mask[n];
+    rowoff = P.soff[n];
+    L = P.rowlen[n];
+    dr = P.roff[n];
+#pragma unroll
+    for (int b = 0; b < NN; ++b) {
+      bob[b] = P.boff[(int64_t)q * NN + b];
+      mcb[b] = P.mask[cn[b]];
+    }
     element_strip<NN, true>(P, cn, a, acc, racc);
     if (ER) {
 #pragma unroll
@@ -281,21 +294,13 @@ __global__ void __launch_bounds__(VolTPB<NN>::v) k_vol_rk(VolParams P) {
     }
   }
   // per-node sums in incidence order (one thread per node per round)
-  unsigned mn = 0;
-  int rowoff = 0, L = 0, dr = 0;
-  if (act) {
-    mn = P.mask[n];
-    rowoff = P.soff[n];
-    L = P.rowlen[n];
-    dr = P.roff[n];
-  }
   for (int k = 0; k < P.maxval; ++k) {
     if (rank == k) {
 #pragma unroll
       for (int b = 0; b < NN; ++b) {
-        const unsigned bo = P.boff[(int64_t)q * NN + b];
+        const unsigned bo = bob[b];
         if (bo == 0xFFFFu) continue;
-        const unsigned mc = P.mask[cn[b]];
+        const unsigned mc = mcb[b];
         int rj = 0;
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
@@ -616,6 +621,8 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
   const int64_t b0 = P.region[n], b1 = P.region[n + 1];
   const int64_t u0 = P.uptr[n], u1 = P.uptr[n + 1];
   const int q0 = P.nodeinc[n], q1 = P.nodeinc[n + 1];
+  const int L = P.rowlen[n];                     // before the copy: no load waits behind its barrier
+  const int32_t rdn = P.rdof[n];
   if (!mn) return;
   const int nbk = b1 - b0 < capb ? (int)(b1 - b0) : capb;
   const int64_t nu = u1 - u0;
@@ -654,7 +661,6 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   }
   __syncwarp(gmask);
-  const int L = P.rowlen[n];
   while (u < nu) {
     double blk[9];
 #pragma unroll
@@ -701,7 +707,7 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
 #pragma unroll
         for (int j = 0; j < 3; ++j) r[j] += SR[q * 4 + j];
       }
-      double* Rout = P.R + P.rdof[n];
+      double* Rout = P.R + rdn;
       int rr = 0;
 #pragma unroll
       for (int j = 0; j < 3; ++j)
@@ -881,6 +887,8 @@ __global__ void __launch_bounds__(128) k_face_rk(FaceParams P) {
   double racc[3] = {0.0, 0.0, 0.0};
   int32_t cn[NF];
   int rank = -1, n = 0;
+  unsigned mn = 0;
+  int rowoff = 0, L = 0, dr = 0;
   if (act) {
     const int ea = P.inc[q];
     const int64_t f = ea >> 4;
@@ -889,6 +897,10 @@ __global__ void __launch_bounds__(128) k_face_rk(FaceParams P) {
     for (int b = 0; b < NF; ++b) cn[b] = P.conn[f * NF + b];
     n = cn[a];
     rank = q - P.nodeinc[n];
+    mn = P.mask[n];                              // the row metadata, issued before the face math
+    rowoff = P.soff[n];
+    L = P.rowlen[n];
+    dr = P.roff[n];
     double x[NF][3];
     face_nodes<NF>(P, cn, x);
 #pragma unroll
@@ -932,14 +944,6 @@ __global__ void __launch_bounds__(128) k_face_rk(FaceParams P) {
           for (int j = 0; j < 3; ++j) kacc[b][3 * i + j] += w3 * (A[i] * C[j] - D[i] * B[j]);
       }
     }
-  }
-  unsigned mn = 0;
-  int rowoff = 0, L = 0, dr = 0;
-  if (act) {
-    mn = P.mask[n];
-    rowoff = P.soff[n];
-    L = P.rowlen[n];
-    dr = P.roff[n];
   }
   for (int k = 0; k < P.maxval; ++k) {
     if (rank == k) {
