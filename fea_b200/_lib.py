@@ -33,6 +33,7 @@ FEA_C3D4, FEA_C3D8, FEA_T3, FEA_Q4 = 4, 8, 3, 40
 (FEA_A_RDOF, FEA_A_MASK, FEA_A_DBASE, FEA_A_VBASE, FEA_A_ROWLEN, FEA_A_INDPTR, FEA_A_INDICES,
  FEA_A_ADJPTR, FEA_A_ADJCOL, FEA_A_ADJOFF, FEA_A_MOFF) = range(10, 21)
 G_BASE, F_BASE = 30, 50
+FEA_S_G_HXSTRIDE = 70     # element-group scalar past the face id range
 (A_INC, A_BOFF, A_NODEINC, A_CHUNKPTR, A_CHUNKINC, S_NCHUNK, S_MAXVAL, S_THREADS, S_SMEM, A_CHUNKLIST,
  A_CHUNKDIM, A_SOFF, A_ROFF, A_UPTR, A_UBLK, A_ALLPTR, A_ALLINC, A_INCPOS, A_STAGEPOS, A_REGION) = range(20)
 
@@ -67,7 +68,7 @@ class Group(C.Structure):
                 ("allptr_dev", C.c_void_p), ("allinc_dev", C.c_void_p),
                 ("nchunk", C.c_int64), ("maxval", C.c_int32), ("threads", C.c_int32),
                 ("smem_doubles", C.c_int64), ("incpos_dev", C.c_void_p), ("stagepos_dev", C.c_void_p),
-                ("region_dev", C.c_void_p), ("nblk", C.c_int64), ("maxblk", C.c_int32), ("reserved", C.c_int32)]
+                ("region_dev", C.c_void_p), ("nblk", C.c_int64), ("maxblk", C.c_int32), ("hx_stride", C.c_int32)]
 
 
 class PcgbSlot(C.Structure):

@@ -604,7 +604,7 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
 // loads incidence i's slot; the sum runs through shuffles).  The records and
 // residual slots are loaded before the region copy completes.  capb = the
 // largest region (shared memory per group: capb blocks).
-template <bool WR, bool ACC, int LPN>
+template <bool WR, bool ACC, int LPN, bool FIXED>
 __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const double* __restrict__ stage,
                                                         const double* __restrict__ rslot, int capb, int capq) {
   extern __shared__ __align__(16) double gsm[];
@@ -616,17 +616,20 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
   const unsigned gmask = LPN == 32 ? 0xffffffffu : (((1u << LPN) - 1u) << (sub * LPN));
   const int64_t n = ((int64_t)blockIdx.x * HX_GW + warp) * NPW + sub;
   if (n >= P.n_nodes) return;
-  // the node's metadata issued together, before the mask decides
+  // the node's metadata issued together, before the mask decides; in the
+  // fixed layout the region, record and residual-slot addresses follow from
+  // n alone, so their copies start without waiting for these loads
   const unsigned mn = P.mask[n];
-  const int64_t b0 = P.region[n], b1 = P.region[n + 1];
-  const int64_t u0 = P.uptr[n], u1 = P.uptr[n + 1];
+  const int64_t b0 = FIXED ? n * capb : P.region[n], b1 = FIXED ? b0 + capb : P.region[n + 1];
+  const int64_t u0 = FIXED ? n * 16 : P.uptr[n], u1 = FIXED ? u0 + 16 : P.uptr[n + 1];
   const int q0 = P.nodeinc[n], q1 = P.nodeinc[n + 1];
   const int L = P.rowlen[n];                     // before the copy: no load waits behind its barrier
   const int32_t rdn = P.rdof[n];
-  if (!mn) return;
+  if (!FIXED && !mn) return;
   const int nbk = b1 - b0 < capb ? (int)(b1 - b0) : capb;
   const int64_t nu = u1 - u0;
-  const int nq = q1 - q0 < capq ? q1 - q0 : capq;
+  const int64_t rs0 = FIXED ? n * capq : q0;     // the node's first residual slot
+  const int nqc = FIXED ? capq : (q1 - q0 < capq ? q1 - q0 : capq);   // slots copied
   // the lane's first record: targets (row, transpose) and (rowlen_c, mask_c, first, count)
   int64_t u = lane;
   longlong2 tg = make_longlong2(0, 0);
@@ -650,9 +653,9 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sbase + 16u * (unsigned)i), "l"(src + 2 * i)
                    : "memory");
     if (WR) {
-      const double* rsrc = rslot + (int64_t)q0 * 4;
+      const double* rsrc = rslot + rs0 * 4;
       const unsigned rbase = (unsigned)__cvta_generic_to_shared(SR);
-      for (int i = lane; i < 2 * nq; i += LPN)
+      for (int i = lane; i < 2 * nqc; i += LPN)
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(rbase + 16u * (unsigned)i),
                      "l"(rsrc + 2 * i)
                      : "memory");
@@ -661,7 +664,10 @@ __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const do
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   }
   __syncwarp(gmask);
+  if (FIXED && !mn) return;                      // (the whole group: mn is the group's node's)
+  const int nq = q1 - q0 < capq ? q1 - q0 : capq;
   while (u < nu) {
+    if (FIXED && tg.x < 0) break;                // the node's records are first in its 16 slots
     double blk[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) blk[i] = 0.0;
@@ -1428,7 +1434,9 @@ extern "C" int64_t fea_reduce_scratch_len(int64_t n_items) { return (n_items + 2
 
 extern "C" int64_t fea_assemble_work_len(const fea_group_t* G) {
   if (!G || G->kind != FEA_C3D8) return 0;
-  return hx_rslot_base(G->nblk) + G->ne * 8 * 4;
+  // residual slots: one per incidence, or maxval per node in the fixed layout
+  const int64_t slots = G->hx_stride > 0 ? (G->nblk / G->hx_stride) * (int64_t)G->maxval : G->ne * 8;
+  return hx_rslot_base(G->nblk) + slots * 4;
 }
 
 extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, double mu, double kappa,
@@ -1460,6 +1468,8 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
     int64_t smem = G->smem_doubles;
     const bool acc = accumulate != 0, wr = R != nullptr, er = elemR != nullptr;
     if (hex) {
+      const bool fixed = G->hx_stride > 0;
+      if (fixed && G->hx_stride != G->maxblk) return FEA_EINVAL;
       const int capb = std::max<int>(G->maxblk, 2);   // regions hold even block counts
       const int capq = std::max<int>(G->maxval, 1);   // most incidences of one node
       const size_t region = ((size_t)capb * 9 + (wr ? (size_t)capq * 4 : 0)) * sizeof(double);
@@ -1479,10 +1489,14 @@ extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, d
       const unsigned g2 = (unsigned)((N->n_nodes + per_cta - 1) / per_cta);
       if (g2) {
         void (*gk)(VolParams, const double*, const double*, int, int) =
-            two ? (wr ? (acc ? k_hex_gat<true, true, HX_LPN> : k_hex_gat<true, false, HX_LPN>)
-                      : (acc ? k_hex_gat<false, true, HX_LPN> : k_hex_gat<false, false, HX_LPN>))
-                : (wr ? (acc ? k_hex_gat<true, true, 32> : k_hex_gat<true, false, 32>)
-                      : (acc ? k_hex_gat<false, true, 32> : k_hex_gat<false, false, 32>));
+            fixed ? (two ? (wr ? (acc ? k_hex_gat<true, true, HX_LPN, true> : k_hex_gat<true, false, HX_LPN, true>)
+                               : (acc ? k_hex_gat<false, true, HX_LPN, true> : k_hex_gat<false, false, HX_LPN, true>))
+                         : (wr ? (acc ? k_hex_gat<true, true, 32, true> : k_hex_gat<true, false, 32, true>)
+                               : (acc ? k_hex_gat<false, true, 32, true> : k_hex_gat<false, false, 32, true>)))
+                  : (two ? (wr ? (acc ? k_hex_gat<true, true, HX_LPN, false> : k_hex_gat<true, false, HX_LPN, false>)
+                               : (acc ? k_hex_gat<false, true, HX_LPN, false> : k_hex_gat<false, false, HX_LPN, false>))
+                         : (wr ? (acc ? k_hex_gat<true, true, 32, false> : k_hex_gat<true, false, 32, false>)
+                               : (acc ? k_hex_gat<false, true, 32, false> : k_hex_gat<false, false, 32, false>)));
         if (cudaError_t ce = cudaFuncSetAttribute(gk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gbytes))
           return (int)ce;
         gk<<<g2, HX_GW * 32, gbytes, st>>>(P, work, rslot, capb, capq);

@@ -54,6 +54,7 @@ struct GatherList {            // one element group or one face group
   std::vector<int32_t> incpos;     // [ne*nn] incidence index of (e, a), -1 for a node without rows
   std::vector<int32_t> stagepos;   // [ne*36] staged block of each element block (lane slot order), -1: none
   std::vector<int64_t> region;     // [N+1] first staged block of each node's region (even)
+  int32_t hx_stride = 0;           // C3D8: regions at n * hx_stride, 16 records per node (0: by region / uptr)
   std::vector<int32_t> allptr;     // [N+1] incidences of every node (constrained ones included)
   std::vector<int32_t> allinc;     // e*16 + a, element order ascending
   int64_t maxval = 0, threads = 0, smem = 0;
@@ -262,6 +263,7 @@ int build_blocks(const fea_plan& P, int nn, const int32_t* conn, const Incidence
   if (err) return err;
   G.region.assign(N + 1, 0);
   G.uptr.assign(N + 1, 0);
+  int64_t smax = 0, umax = 0;
   for (int64_t n = 0; n < N; ++n) {
     int64_t nb = 0, nu = 0;
     if (P.mask[n])
@@ -270,11 +272,30 @@ int build_blocks(const fea_plan& P, int nn, const int32_t* conn, const Incidence
           nb += cnt[p];
           ++nu;
         }
-    G.region[n + 1] = G.region[n] + ((nb + 1) & ~(int64_t)1);
+    nb = (nb + 1) & ~(int64_t)1;
+    smax = std::max(smax, nb);
+    umax = std::max(umax, nu);
+    G.region[n + 1] = G.region[n] + nb;
     G.uptr[n + 1] = G.uptr[n] + nu;
+  }
+  // Regular meshes (a structured block: 36 blocks in an interior region)
+  // take a fixed stride, so that the gather can start a node's region copy
+  // and record loads without first loading where they are: regions at
+  // n * smax, 16 record slots per node (unused ones with row = -1), the
+  // residual slots of node n at n * maxval.  Chosen when it costs at most a
+  // quarter more staging than the packed layout.
+  G.hx_stride = 0;
+  if (smax > 0 && umax <= 16 && smax <= 96 && N * smax <= G.region[N] + G.region[N] / 4) {
+    G.hx_stride = (int32_t)smax;
+    for (int64_t n = 0; n <= N; ++n) {
+      G.region[n] = n * smax;
+      G.uptr[n] = n * 16;
+    }
   }
   if (G.region[N] >= INT32_MAX) return FEA_ERANGE;
   G.ublk.assign((size_t)G.uptr[N] * 4, 0);
+  if (G.hx_stride)
+    for (int64_t u = 0; u < G.uptr[N]; ++u) G.ublk[4 * u] = G.ublk[4 * u + 1] = -1;   // unused slots
   G.stagepos.assign((size_t)G.ne * 36, -1);
   parallel_for(N, [&](int64_t a0, int64_t a1) {
     std::vector<int64_t> fill;
@@ -306,6 +327,14 @@ int build_blocks(const fea_plan& P, int nn, const int32_t* conn, const Incidence
       }
     }
   });
+  if (G.hx_stride) {
+    // residual slot of incidence (e, a) of node n: n * maxval + its rank
+    for (int64_t n = 0; n < N; ++n)
+      for (int32_t q = G.nodeinc[n]; q < G.nodeinc[n + 1]; ++q) {
+        const int32_t ea = G.inc[q];
+        G.incpos[(size_t)(ea >> 4) * nn + (ea & 15)] = (int32_t)(n * G.maxval + (q - G.nodeinc[n]));
+      }
+  }
   return FEA_OK;
 }
 
@@ -485,6 +514,10 @@ extern "C" int fea_plan_get(const fea_plan* P, int32_t id, int32_t group, void* 
     if (group < 0 || group >= (int)P->faces.size()) return FEA_EINVAL;
     G = &P->faces[group];
     id -= 50;
+  } else if (id >= 70 && id < 80) {               // element-group ids, continued
+    if (group < 0 || group >= (int)P->groups.size()) return FEA_EINVAL;
+    G = &P->groups[group];
+    id -= 50;
   }
   if (G) {
     switch (id) {
@@ -508,6 +541,7 @@ extern "C" int fea_plan_get(const fea_plan* P, int32_t id, int32_t group, void* 
       case 17: return put(G->incpos, dst, count);
       case 18: return put(G->stagepos, dst, count);
       case 19: return put(G->region, dst, count);
+      case 20: return scalar(G->hx_stride, count);
       default: return FEA_EINVAL;
     }
   }

@@ -125,7 +125,8 @@ class GatherGroup:
                             hp.scalar(base + L.S_SMEM, index),
                             self.incpos.data_ptr() if self.incpos is not None else None,
                             self.stagepos.data_ptr() if self.stagepos is not None else None,
-                            self.region.data_ptr() if self.region is not None else None, nblk, maxblk, 0)
+                            self.region.data_ptr() if self.region is not None else None, nblk, maxblk,
+                            hp.scalar(L.FEA_S_G_HXSTRIDE, index) if uptr.size else 0)
         self.nchunk = int(self.desc.nchunk)
 
 

@@ -121,6 +121,7 @@ enum {
   FEA_A_G_INCPOS = 47,   /* int32 [ne, nn] incidence index of (e, a), -1: node without rows */
   FEA_A_G_STAGEPOS = 48, /* int32 [ne, 36] staged block of each element block, -1: none  */
   FEA_A_G_REGION = 49,   /* int64 [N+1] first staged block of each node's region (even)   */
+  FEA_S_G_HXSTRIDE = 70, /* int64 scalar: C3D8 fixed region stride in blocks, 0 = packed  */
   FEA_A_F_INC = 50,      /* the same arrays / scalars for face groups      */
   FEA_A_F_BOFF = 51,
   FEA_A_F_NODEINC = 52,
@@ -169,7 +170,11 @@ typedef struct {
  * upper node block (row node min(n_i, n_j), column node max): a node's
  * region REGION[n] .. REGION[n+1] holds, block-major, the contributions to
  * its upper blocks in adjacency order, each block's in ascending element
- * order.  One record per upper block (row n, column c >= n): */
+ * order.  One record per upper block (row n, column c >= n), from UPTR[n].
+ * In the fixed layout of a regular mesh (FEA_S_G_HXSTRIDE > 0) REGION[n] =
+ * n * stride, UPTR[n] = 16 n (record slots past the node's own hold row =
+ * col = -1) and the residual slot of incidence (e, a) (INCPOS) is n * maxval
+ * + its rank among the node's incidences: */
 typedef struct {
   int64_t row;                /* value index of (first free row of n, first free column of c)  */
   int64_t col;                /* value index of the transpose in c's rows; -1 on the diagonal  */
@@ -206,7 +211,10 @@ typedef struct {
   const int64_t* region_dev;  /* FEA_A_G_REGION (C3D8 only) */
   int64_t nblk;               /* staged blocks: REGION[N] (C3D8 only)         */
   int32_t maxblk;             /* largest region, in blocks (C3D8 only)        */
-  int32_t reserved;
+  int32_t hx_stride;          /* FEA_S_G_HXSTRIDE: > 0 when the C3D8 staging has
+                                 the fixed layout (regions at n * hx_stride =
+                                 n * maxblk, records at 16 n, residual slots at
+                                 n * maxval); 0: packed (REGION, UPTR, NODEINC) */
 } fea_group_t;
 
 /* Element residual and tangent of one Neo-Hookean group, gathered per node

@@ -186,6 +186,7 @@ def _upper_staging(hp, el, mask):
     ub = arr(L.A_UBLK).reshape(-1, 4)
     return dict(nodeinc=arr(L.A_NODEINC), inc=arr(L.A_INC), incpos=arr(L.A_INCPOS).reshape(-1, 8),
                 stagepos=arr(L.A_STAGEPOS).reshape(-1, 36), region=arr(L.A_REGION), uptr=arr(L.A_UPTR),
+                stride=hp.scalar(L.FEA_S_G_HXSTRIDE, 0), maxval=hp.scalar(L.G_BASE + L.S_MAXVAL, 0),
                 row=ub[:, 0], col=ub[:, 1], lc=ub[:, 2] & 0xFFFFFFFF, mc=ub[:, 2] >> 32,
                 first=ub[:, 3] & 0xFFFFFFFF, count=ub[:, 3] >> 32,
                 adjptr=hp.array(L.FEA_A_ADJPTR), adjcol=hp.array(L.FEA_A_ADJCOL),
@@ -223,27 +224,46 @@ def _expected_contributions(el, mask):
     return expect
 
 
-def test_block_contributor_lists(golden):
+def _staging_case(golden, case):
+    """(N, el, mask) of the packed-layout case (the hex5 fixture, partial
+    masks) or of a fixed-layout case (a 16^3 structured block, one face
+    clamped, part of it in x only)."""
+    if case == "packed":
+        g = golden("hex5")
+        N, el = g["X"].shape[0], g["elems"]
+        fixed = g["fixed"]
+    else:
+        X, el = O.hex_block(16, jitter=0.1, seed=3)
+        N, el = X.shape[0], el.numpy()
+        fixed = np.nonzero(X[:, 0].numpy() < 1e-9)[0]
+    mask = np.full(N, 7, np.uint8)
+    mask[fixed] = 0
+    mask[fixed[:3]] = 5                               # partial masks too
+    return N, el, mask
+
+
+@pytest.mark.parametrize("case", ["packed", "fixed"])
+def test_block_contributor_lists(golden, case):
     """Regions and upper-block records of the C3D8 staging: each node's
     region holds, block-major in adjacency order, the contributions to its
     upper blocks (n, c >= n) in ascending element order, regions start at
-    even blocks; every element block of two active nodes has one staged
-    position and the others none; the records carry the row and transpose
-    targets (MOFF: n's value offset in row c)."""
-    g = golden("hex5")
-    N, el = g["X"].shape[0], g["elems"]
-    mask = np.full(N, 7, np.uint8)
-    mask[g["fixed"]] = 0
-    mask[g["fixed"][:3]] = 5                          # partial masks too
+    even blocks (packed) or at n * stride (fixed, with 16 record slots per
+    node and the residual slots at n * maxval); every element block of two
+    active nodes has one staged position and the others none; the records
+    carry the row and transpose targets (MOFF: n's value offset in row c)."""
+    N, el, mask = _staging_case(golden, case)
     hp = _plan(N, mask, [("C3D8", el)])
     from fea_b200 import _lib as L
     vbase, rowlen = hp.array(L.FEA_A_VBASE), hp.array(L.FEA_A_ROWLEN)
     st = _upper_staging(hp, el, mask)
     expect = _expected_contributions(el, mask)
-    sp, region, uptr = st["stagepos"], st["region"], st["uptr"]
+    sp, region, uptr, S = st["stagepos"], st["region"], st["uptr"], st["stride"]
+    assert (S > 0) == (case == "fixed")
     seen = np.zeros(sp.shape, bool)
     for n in range(N):
         assert region[n] % 2 == 0
+        if S:
+            assert region[n] == n * S and uptr[n] == 16 * n
         u = uptr[n]
         t = 0
         for p in range(st["adjptr"][n], st["adjptr"][n + 1]):
@@ -262,10 +282,20 @@ def test_block_contributor_lists(golden):
                 seen[e, s] = True
             t += len(lst)
             u += 1
-        assert u == uptr[n + 1]
-        assert region[n + 1] - region[n] == (t + 1) // 2 * 2
+        if S:
+            assert t <= S and u <= uptr[n] + 16
+            assert np.all(st["row"][u:uptr[n] + 16] == -1) and np.all(st["col"][u:uptr[n] + 16] == -1)
+        else:
+            assert u == uptr[n + 1]
+            assert region[n + 1] - region[n] == (t + 1) // 2 * 2
     assert np.all(sp[~seen] == -1) and np.all(sp[seen] >= 0)
     assert np.unique(sp[seen]).size == int(seen.sum())
+    # residual slots: one per incidence of an active node, node by node
+    inc, nodeinc, ip = st["inc"], st["nodeinc"], st["incpos"]
+    for n in range(N):
+        for k, q in enumerate(range(nodeinc[n], nodeinc[n + 1])):
+            e, a = inc[q] >> 4, inc[q] & 15
+            assert ip[e, a] == (n * st["maxval"] + k if S else q)
 
 
 def test_face_chunks_take_one_warp_unless_a_node_has_more_faces():
@@ -356,17 +386,19 @@ def test_csr_of_eight_hex_mesh_by_hand(clamp):
     np.testing.assert_array_equal(oix.numpy(), ix)
 
 
-@pytest.mark.parametrize("dofs,collapse", [((0, 1, 2), False), ((1,), False), ((0, 1, 2), True)])
-def test_upper_staging_emulated_gives_reference_K(dofs, collapse):
+@pytest.mark.parametrize("n,dofs,collapse", [(3, (0, 1, 2), False), (3, (1,), False), (3, (0, 1, 2), True),
+                                             (14, (0, 2), False)])
+def test_upper_staging_emulated_gives_reference_K(n, dofs, collapse):
     """The C3D8 assembly as the kernels perform it, emulated on the CPU with
     the oracle's element blocks: each element block written to its staged
     position, oriented to its upper node block, then per node the upper
     block sums into the node's rows and their transposes into the column
     nodes' rows.  The CSR values equal the oracle's reduced K
     and R; also with a collapsed element (two of its corners one node), whose
-    repeated node puts two blocks of the element on the diagonal."""
+    repeated node puts two blocks of the element on the diagonal, and on a
+    14^3 block, which takes the fixed layout."""
     from fea_b200 import _lib as L
-    X, el = O.hex_block(3, jitter=0.1, seed=5)
+    X, el = O.hex_block(n, jitter=0.1, seed=5)
     if collapse:
         el = el.clone()
         el[13, 6] = el[13, 7]                   # the centre element's top edge 6-7 collapsed
@@ -385,8 +417,10 @@ def test_upper_staging_emulated_gives_reference_K(dofs, collapse):
     vbase, rowlen, rdof = hp.array(L.FEA_A_VBASE), hp.array(L.FEA_A_ROWLEN), hp.array(L.FEA_A_RDOF)
     Re, Ke = O.element_residual_tangent("C3D8", X, torch.from_numpy(el), m.gc_to_u(gc), 1.0, 10.0)
     Re, Ke = Re.numpy(), Ke.numpy()                    # [a,j,e], [a,j,b,k,e]
+    S, Q = st["stride"], st["maxval"]
+    assert (S > 0) == (n == 14)
     blocks = np.full((int(st["region"][-1]), 3, 3), np.nan)
-    rslot = np.full((int(st["nodeinc"][-1]), 3), np.nan)
+    rslot = np.full((N * Q if S else int(st["nodeinc"][-1]), 3), np.nan)
     for e in range(el.shape[0]):                       # element kernel, phase 3
         for a, d, s in _slots():
             pos = st["stagepos"][e, s]
@@ -409,12 +443,14 @@ def test_upper_staging_emulated_gives_reference_K(dofs, collapse):
     for n in range(N):                                  # gather, one lane group per node
         if not mask[n]:
             continue
-        S = blocks[st["region"][n]:st["region"][n + 1]]
+        Sn = blocks[st["region"][n]:st["region"][n + 1]]
         for u in range(st["uptr"][n], st["uptr"][n + 1]):
+            if st["row"][u] < 0:                        # unused record slot (fixed layout)
+                break
             f, cnt, mc = st["first"][u], st["count"][u], st["mc"][u]
             blk = np.zeros((3, 3))
             for t in range(f, f + cnt):
-                blk = blk + S[t]
+                blk = blk + Sn[t]
             for rj, j in enumerate(free(mask[n])):
                 for rk, k in enumerate(free(mc)):
                     K[st["row"][u] + rj * rowlen[n] + rk] = blk[j, k]
@@ -423,7 +459,9 @@ def test_upper_staging_emulated_gives_reference_K(dofs, collapse):
                     for cj, j in enumerate(free(mask[n])):
                         K[st["col"][u] + rk * st["lc"][u] + cj] = blk[j, k]
             else:
-                r = rslot[st["nodeinc"][n]:st["nodeinc"][n + 1]].sum(0)
+                nq = st["nodeinc"][n + 1] - st["nodeinc"][n]
+                r0 = n * Q if S else st["nodeinc"][n]
+                r = rslot[r0:r0 + nq].sum(0)
                 for rr, j in enumerate(free(mask[n])):
                     R[rdof[n] + rr] = r[j]
     assert not np.isnan(K).any() and not np.isnan(R).any()
