@@ -405,12 +405,26 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
   double J0[9], Ju[9];
 #pragma unroll
   for (int i = 0; i < 9; ++i) J0[i] = Ju[i] = 0.0;
+  // dN_b/dxi at this Gauss point, once for both node loops: 12 products of
+  // two shape factors (with the 1/8), signed per node (the same bits as
+  // 0.125 * s * f * f')
+  double dxs[8][3];
+  {
+    const double yz[4] = {0.125 * fym * fzm, 0.125 * fyp * fzm, 0.125 * fym * fzp, 0.125 * fyp * fzp};
+    const double xz[4] = {0.125 * fxm * fzm, 0.125 * fxp * fzm, 0.125 * fxm * fzp, 0.125 * fxp * fzp};
+    const double xy[4] = {0.125 * fxm * fym, 0.125 * fxp * fym, 0.125 * fxm * fyp, 0.125 * fxp * fyp};
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int ix = ((b + 1) >> 1) & 1, iy = (b >> 1) & 1, iz = b >> 2;
+      dxs[b][0] = ix ? yz[iy + 2 * iz] : -yz[iy + 2 * iz];
+      dxs[b][1] = iy ? xz[ix + 2 * iz] : -xz[ix + 2 * iz];
+      dxs[b][2] = iz ? xy[ix + 2 * iy] : -xy[ix + 2 * iy];
+    }
+  }
   if (act) {
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
-      const double sx = (((b + 1) >> 1) & 1) ? 1.0 : -1.0, sy = ((b >> 1) & 1) ? 1.0 : -1.0, sz = (b >> 2) ? 1.0 : -1.0;
-      const double fx = sx > 0 ? fxp : fxm, fy = sy > 0 ? fyp : fym, fz = sz > 0 ? fzp : fzm;
-      const double d0 = 0.125 * sx * fy * fz, d1 = 0.125 * sy * fx * fz, d2 = 0.125 * sz * fx * fy;
+      const double d0 = dxs[b][0], d1 = dxs[b][1], d2 = dxs[b][2];
       const double2* xs = reinterpret_cast<const double2*>(V + HX_SC + b * 6);
       const double2 v0 = xs[0], v1 = xs[1], v2 = xs[2];
       const double xv[3] = {v0.x, v0.y, v1.x}, uv[3] = {v1.y, v2.x, v2.y};
@@ -457,9 +471,7 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
     double* Vg = V + lane * HX_VG;
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
-      const double sx = (((b + 1) >> 1) & 1) ? 1.0 : -1.0, sy = ((b >> 1) & 1) ? 1.0 : -1.0, sz = (b >> 2) ? 1.0 : -1.0;
-      const double fx = sx > 0 ? fxp : fxm, fy = sy > 0 ? fyp : fym, fz = sz > 0 ? fzp : fzm;
-      const double d0 = 0.125 * sx * fy * fz, d1 = 0.125 * sy * fx * fz, d2 = 0.125 * sz * fx * fy;
+      const double d0 = dxs[b][0], d1 = dxs[b][1], d2 = dxs[b][2];
       double v[6];
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
@@ -505,10 +517,12 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
       gm[0] = wc * fa[0]; gm[1] = wc * fa[1]; gm[2] = wc * fa[2];       // w mu J^-2/3 f_a
     }
 #pragma unroll
+    double AC[3];
     for (int k = 0; k < 3; ++k) {
       A[k] = wa * fa[k] + wb * qa[k];
       B[k] = wa * qa[k];
       Cc[k] = wg * qa[k];
+      AC[k] = A[k] + Cc[k];
       racc[k] = fma(wc, fa[k], racc[k]);
       racc[k] = fma(wc2, qa[k], racc[k]);
     }
@@ -524,8 +538,9 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
       const double dg = gm[0] * qb[0] + gm[1] * qb[1] + gm[2] * qb[2];    // w mu J^-2/3 g_a . g_b
       // three fused multiply-adds into each accumulator, the delta term on
       // the diagonal alone: 33 FP64 operations per block and Gauss point.
-      // d = 0 (K_aa, symmetric) and d = 4 take the upper triangle only (24):
-      // at d = 4 every lane computes one, lane a < 4 that of K_a,a+4 and
+      // d = 0 (K_aa = wa (f q^T + q f^T) + (wb + wg) q q^T + dg I, symmetric)
+      // takes the upper triangle with two FMAs an entry (18), d = 4 the upper
+      // triangle (24): at d = 4 every lane computes one, lane a < 4 that of K_a,a+4 and
       // lane a + 4 that of K_a+4,a, whose strict part is the strict lower
       // triangle of K_a,a+4 transposed (the two lanes share the block)
 #pragma unroll
@@ -534,9 +549,14 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
         for (int k = 0; k < 3; ++k) {
           if ((d == 0 || d == 4) && k < j) continue;
           double t = acc[d][3 * j + k];
-          t = fma(A[j], qb[k], t);
-          t = fma(B[j], fb[k], t);
-          t = fma(qb[j], Cc[k], t);
+          if (d == 0) {                          // K_aa: fa_j B_k + qa_j (A_k + C_k), two FMAs
+            t = fma(fa[j], B[k], t);
+            t = fma(qa[j], AC[k], t);
+          } else {
+            t = fma(A[j], qb[k], t);
+            t = fma(B[j], fb[k], t);
+            t = fma(qb[j], Cc[k], t);
+          }
           acc[d][3 * j + k] = t;
         }
       acc[d][0] += dg;
