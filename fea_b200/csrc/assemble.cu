@@ -615,15 +615,18 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
 }
 
 // Per node row: a group of LPN lanes per row node n.  The group copies the
-// node's region (its staged contributions, block-major) to shared memory
-// with 16-byte asynchronous copies; then one lane per upper node block (n,
-// c >= n), from the block's record, sums its contributions (element order,
-// fixed), writes the 3x3 (free DOFs only) into the node's contiguous CSR
-// rows and, for c != n, the transpose into c's rows; the diagonal lane writes
-// the node's residual, the sum over its incidences in element order (lane i
-// loads incidence i's slot; the sum runs through shuffles).  The records and
-// residual slots are loaded before the region copy completes.  capb = the
-// largest region (shared memory per group: capb blocks).
+// node's region (its staged contributions, block-major) and its residual
+// slots to shared memory with 16-byte asynchronous copies; then one lane per
+// upper node block (n, c >= n), from the block's record, sums its
+// contributions (element order, fixed), writes the 3x3 (free DOFs only)
+// into the node's contiguous CSR rows and, for c != n, the transpose into
+// c's rows; the diagonal lane writes the node's residual, the sum of its
+// slots in incidence (element) order.  The records are loaded while the
+// copies are in flight.  FIXED (regular meshes): region, records and slots
+// sit at n * capb, 16 n and n * capq, so the copies and record loads do not
+// wait for the node's metadata.  capb = the largest region, capq = the most
+// incidences of a node (shared memory per group: capb blocks and capq
+// slots).
 template <bool WR, bool ACC, int LPN, bool FIXED>
 __global__ void __launch_bounds__(HX_GW * 32, 8) k_hex_gat(VolParams P, const double* __restrict__ stage,
                                                         const double* __restrict__ rslot, int capb, int capq) {
