@@ -516,8 +516,8 @@ __global__ void __launch_bounds__(HX_TPB, HX_CTAS) k_hex_elem(VolParams P, doubl
       qa[0] = x0.x; qa[1] = x0.y; qa[2] = x1.x; fa[0] = x1.y; fa[1] = x2.x; fa[2] = x2.y;
       gm[0] = wc * fa[0]; gm[1] = wc * fa[1]; gm[2] = wc * fa[2];       // w mu J^-2/3 f_a
     }
-#pragma unroll
     double AC[3];
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
       A[k] = wa * fa[k] + wb * qa[k];
       B[k] = wa * qa[k];
