@@ -2,7 +2,7 @@
 sssnnn7119/FEA as hand-written sm_100a kernels behind the reference's API.
 
 The kernels live in ``libfea_b200.so`` (C ABI: include/fea_b200.h), built
-in-tree by ``python -m fea_b200._build``.  Importing the package loads the
+in-tree by ``python fea_b200/_build.py``.  Importing the package loads the
 library and raises ImportError when it is missing; there is no fallback.
 """
 from . import _lib  # noqa: F401  (loads the native library or raises)

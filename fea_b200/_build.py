@@ -1,6 +1,9 @@
 """Build the fea_b200 native library in-tree with nvcc (sm_100a only).
 
-    python -m fea_b200._build [--verbose]
+    python fea_b200/_build.py [--verbose]
+
+(run by path: ``python -m`` would import the package first, and the
+package raises ImportError while the library is missing)
 
 Produces ``fea_b200/libfea_b200.so`` (static CUDA runtime, no torch
 dependency).  Objects go to ``fea_b200/_build/``.

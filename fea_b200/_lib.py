@@ -1,6 +1,6 @@
 """ctypes binding of libfea_b200.so (the C ABI declared in include/fea_b200.h).
 
-The library is built in-tree (``python -m fea_b200._build``).  Importing this
+The library is built in-tree (``python fea_b200/_build.py``).  Importing this
 module loads it; a missing library raises ImportError — there is no fallback
 implementation of any kernel.
 """
@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libfea_b200.so")
 
 if not os.path.exists(LIB_PATH):
     raise ImportError("fea_b200: native library %s is missing; build it with "
-                      "`python -m fea_b200._build` (nvcc, sm_100a)" % LIB_PATH)
+                      "`python %s` (nvcc, sm_100a)" % (LIB_PATH, os.path.join(HERE, "_build.py")))
 lib = C.CDLL(LIB_PATH)
 
 FEA_OK = 0

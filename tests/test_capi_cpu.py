@@ -485,3 +485,21 @@ def test_nvtx_ranges_are_opt_in():
     off = subprocess.run([sys.executable, "-c", code], env=env, cwd=ROOT, capture_output=True, text=True)
     assert on.returncode == 0 and on.stdout.strip() == "1"
     assert off.returncode == 0 and off.stdout.strip() == "0"
+
+
+def test_missing_library_fails_loudly_with_the_build_command(tmp_path):
+    """Without libfea_b200.so the package import raises ImportError (no
+    fallback), naming the build script to run by path."""
+    import shutil
+    import subprocess
+    import sys
+    pkg = tmp_path / "fea_b200"
+    pkg.mkdir()
+    for f in os.listdir(os.path.join(ROOT, "fea_b200")):
+        if f.endswith(".py"):
+            shutil.copy(os.path.join(ROOT, "fea_b200", f), pkg / f)
+    r = subprocess.run([sys.executable, "-c", "import fea_b200"], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode != 0
+    last = r.stderr.strip().splitlines()[-1]
+    assert last.startswith("ImportError: fea_b200: native library")
+    assert "python " + str(pkg / "_build.py") in last
