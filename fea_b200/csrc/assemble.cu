@@ -1465,17 +1465,21 @@ extern "C" int64_t fea_assemble_work_len(const fea_group_t* G) {
 extern "C" int fea_assemble_volume(const fea_nodes_t* N, const fea_group_t* G, double mu, double kappa,
                                    const double* gc, double* K, double* R, double* elemR, int32_t accumulate,
                                    double* work, int64_t work_len, cudaStream_t st) {
-  if (!N || !G || !gc || (G->kind != FEA_C3D4 && G->kind != FEA_C3D8)) return FEA_EINVAL;
+  // gc may be NULL when no DOF is free (the kernels read it for free DOFs only)
+  if (!N || !G || (!gc && N->ndof > 0) || (G->kind != FEA_C3D4 && G->kind != FEA_C3D8)) return FEA_EINVAL;
   if (G->nn != (G->kind == FEA_C3D8 ? 8 : 4)) return FEA_EINVAL;
   const bool hex = G->kind == FEA_C3D8;
   const int tpb = hex ? HX_GINC : VolTPB<4>::v;
   if (G->threads != tpb) return FEA_ECHUNK;
   // every argument check comes before the first device call
   if (K && hex) {
-    if (!work || work_len < fea_assemble_work_len(G)) return FEA_EWORK;
+    // an empty group stages nothing (work length 0): its gather writes zero
+    // blocks, or adds them, and reads neither work nor the element arrays
+    const int64_t wneed = fea_assemble_work_len(G);
+    if ((wneed > 0 && !work) || work_len < wneed) return FEA_EWORK;
     if (((uintptr_t)work & 15) != 0) return FEA_EINVAL;
-    if (!G->incpos_dev || !G->stagepos_dev || !G->region_dev || !G->uptr_dev || !G->ublk_dev ||
-        G->nblk < 0 || G->maxblk < 0)
+    if (G->ne < 0 || (G->ne > 0 && (!G->incpos_dev || !G->stagepos_dev)) || !G->region_dev || !G->uptr_dev ||
+        !G->ublk_dev || G->nblk < 0 || G->maxblk < 0)
       return FEA_EINVAL;
   }
   if (!K) {
@@ -1578,7 +1582,7 @@ static FaceParams face_params(const fea_nodes_t* N, const fea_group_t* G, double
 
 extern "C" int fea_assemble_pressure(const fea_nodes_t* N, const fea_group_t* G, double p, const double* Xi,
                                      const double* gc, double* K, double* R, cudaStream_t st) {
-  if (!N || !G || !Xi || !gc || (G->kind != FEA_T3 && G->kind != FEA_Q4)) return FEA_EINVAL;
+  if (!N || !G || !Xi || (!gc && N->ndof > 0) || (G->kind != FEA_T3 && G->kind != FEA_Q4)) return FEA_EINVAL;
   if (G->nn != (G->kind == FEA_T3 ? 3 : 4) || (G->threads != 32 && G->threads != 128)) return FEA_EINVAL;
   if (!K && !R) return FEA_OK;
   if (int r = ensure_tables()) return r;
@@ -1592,7 +1596,7 @@ extern "C" int fea_assemble_pressure(const fea_nodes_t* N, const fea_group_t* G,
 extern "C" int fea_energy_volume(const fea_nodes_t* N, const fea_group_t* G, double mu, double kappa,
                                  const double* gc, double* out, double* scratch, int64_t scratch_len,
                                  cudaStream_t st) {
-  if (!N || !G || !gc || !out || !scratch) return FEA_EINVAL;
+  if (!N || !G || (!gc && N->ndof > 0) || !out || !scratch) return FEA_EINVAL;
   if (G->kind != FEA_C3D4 && G->kind != FEA_C3D8) return FEA_EINVAL;
   if (scratch_len < fea_reduce_scratch_len(G->ne)) return FEA_EWORK;
   if (int r = ensure_tables()) return r;
@@ -1611,7 +1615,7 @@ extern "C" int fea_energy_volume(const fea_nodes_t* N, const fea_group_t* G, dou
 extern "C" int fea_energy_pressure(const fea_nodes_t* N, const fea_group_t* G, const double* Xi,
                                    const double* gc, double* out, double* scratch, int64_t scratch_len,
                                    cudaStream_t st) {
-  if (!N || !G || !Xi || !gc || !out || !scratch) return FEA_EINVAL;
+  if (!N || !G || !Xi || (!gc && N->ndof > 0) || !out || !scratch) return FEA_EINVAL;
   if (G->kind != FEA_T3 && G->kind != FEA_Q4) return FEA_EINVAL;
   if (scratch_len < fea_reduce_scratch_len(G->ne)) return FEA_EWORK;
   if (int r = ensure_tables()) return r;

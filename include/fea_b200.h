@@ -219,8 +219,10 @@ typedef struct {
 
 /* Element residual and tangent of one Neo-Hookean group, gathered per node
  * row and written once into the reduced CSR values (store mode) or added to
- * them (accumulate != 0).  gc_dev: reduced displacement [ndof].  Any of
- * K_dev / R_dev / elemR_dev may be NULL.  elemR_dev receives the unassembled
+ * them (accumulate != 0).  gc_dev: reduced displacement [ndof] (NULL allowed
+ * when ndof == 0).  Any of K_dev / R_dev / elemR_dev may be NULL.  A group
+ * without elements writes nothing in either mode and needs no work (its
+ * INCPOS and STAGEPOS may be NULL).  elemR_dev receives the unassembled
  * element residual in the reference's (a, j, e) order [nn*3*ne]; it is only
  * meaningful for a plan whose every element node is active.
  * work_dev: fea_assemble_work_len(group) doubles of scratch, 16-byte

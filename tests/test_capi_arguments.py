@@ -85,6 +85,20 @@ def test_volume_entry_points_check_arguments_first():
     assert vol(hexg, K=None, R=None) == 0                           # nothing to compute
     assert vol(tetg, K=None, R=None) == 0
     assert vol(hexg, K=None, R=None, elemR=_p(5)) == EINVAL         # the R-only path writes R
+    # gc may be NULL only when no DOF is free
+    assert L.fea_assemble_volume(C.byref(N), C.byref(hexg), 1.0, 10.0, None, _p(1), _p(2), None, 0, _p(3), wl,
+                                 None) == EINVAL
+    N0 = _nodes(ndof=0)
+    assert L.fea_assemble_volume(C.byref(N0), C.byref(hexg), 1.0, 10.0, None, None, None, None, 0, None, 0,
+                                 None) == 0
+    # an element group without elements needs no staging scratch, but the
+    # node-side arrays its gather reads
+    e0 = _group(L.FEA_C3D8, 8, 32, ne=0)
+    e0.nblk, e0.maxval = 0, 0
+    assert L.fea_assemble_work_len(C.byref(e0)) == 0
+    e0.region_dev = None
+    assert L.fea_assemble_volume(C.byref(N), C.byref(e0), 1.0, 10.0, _p(4), _p(1), _p(2), None, 0, None, 0,
+                                 None) == EINVAL
 
     face = _group(L.FEA_Q4, 4, 128)
     assert L.fea_assemble_pressure(C.byref(N), C.byref(face), 1.0, _p(1), _p(2), None, None, None) == 0
