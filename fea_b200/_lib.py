@@ -26,6 +26,7 @@ FEA_ENOTCONV = -6
 FEA_EBREAKDOWN = -7
 FEA_ETOOBIG = -8
 FEA_NOALLOC_MAX_ELEMS = 4194304
+FEA_PLAN_MAX_ELEMS = 134217727      # elements (faces) per group: incidences e * 16 + a in 32 bits
 
 FEA_C3D4, FEA_C3D8, FEA_T3, FEA_Q4 = 4, 8, 3, 40
 

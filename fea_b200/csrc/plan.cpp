@@ -285,7 +285,9 @@ int build_blocks(const fea_plan& P, int nn, const int32_t* conn, const Incidence
   // residual slots of node n at n * maxval.  Chosen when it costs at most a
   // quarter more staging than the packed layout.
   G.hx_stride = 0;
-  if (smax > 0 && umax <= 16 && smax <= 96 && N * smax <= G.region[N] + G.region[N] / 4) {
+  // (residual slots are addressed n * maxval in 32 bits)
+  if (smax > 0 && umax <= 16 && smax <= 96 && N * smax <= G.region[N] + G.region[N] / 4 &&
+      N * (int64_t)G.maxval < INT32_MAX) {
     G.hx_stride = (int32_t)smax;
     for (int64_t n = 0; n <= N; ++n) {
       G.region[n] = n * smax;
@@ -358,6 +360,11 @@ extern "C" int fea_plan_build(int64_t n_nodes, const uint8_t* free_mask, int32_t
     int k = face_kind[g];
     if ((k != FEA_T3 && k != FEA_Q4) || face_nf[g] < 0 || (face_nf[g] > 0 && !face_conn[g])) return FEA_EINVAL;
   }
+  // incidences are coded e * 16 + a in 32 bits
+  for (int g = 0; g < n_groups; ++g)
+    if (group_ne[g] > FEA_PLAN_MAX_ELEMS) return FEA_ETOOBIG;
+  for (int g = 0; g < n_faces; ++g)
+    if (face_nf[g] > FEA_PLAN_MAX_ELEMS) return FEA_ETOOBIG;
   std::unique_ptr<fea_plan> P(new fea_plan);
   const int64_t N = n_nodes;
   P->N = N;

@@ -48,7 +48,8 @@ extern "C" {
 #define FEA_EWORK -5       /* caller-provided work buffer too small */
 #define FEA_ENOTCONV -6    /* iterative solver hit its iteration cap */
 #define FEA_EBREAKDOWN -7  /* PCG breakdown (p.Ap <= 0 or non-finite) */
-#define FEA_ETOOBIG -8     /* size beyond the fixed limit of an allocation-free entry point */
+#define FEA_ETOOBIG -8     /* size beyond a fixed limit: of an allocation-free entry point, or a
+                              group of more than FEA_PLAN_MAX_ELEMS elements or faces */
 
 /* element kinds (reference class names) */
 #define FEA_C3D4 4
@@ -75,7 +76,10 @@ typedef struct fea_plan fea_plan;
  *   smem_doubles     per-chunk shared-memory budget in doubles (0 = default)
  * The reduced DOF numbering is node-major over free DOFs, as GC in the
  * reference (assembly.py:170-183); the CSR pattern equals the reference's
- * coalesced reduced K pattern. */
+ * coalesced reduced K pattern.  A group of more than FEA_PLAN_MAX_ELEMS
+ * elements (faces) returns FEA_ETOOBIG: incidences are coded e * 16 + a in
+ * 32 bits; split larger meshes into several groups. */
+#define FEA_PLAN_MAX_ELEMS 134217727
 int fea_plan_build(int64_t n_nodes, const uint8_t* free_mask,
                    int32_t n_groups, const int32_t* group_kind, const int64_t* group_ne,
                    const int32_t* const* group_conn,

@@ -152,6 +152,34 @@ def test_plan_errors():
     assert ex.value.status == -3
 
 
+def test_header_constants_match_the_binding():
+    """Every integer #define of the header has the same value in the binding."""
+    from fea_b200 import _lib as L
+    src = open(os.path.join(ROOT, "include", "fea_b200.h")).read()
+    defs = dict(re.findall(r"^#define\s+(FEA_[A-Z0-9_]+)\s+(-?\d+)\b", src, flags=re.M))
+    assert "FEA_PLAN_MAX_ELEMS" in defs and "FEA_ETOOBIG" in defs
+    bound = {k: v for k, v in defs.items() if hasattr(L, k)}
+    assert len(bound) >= 10
+    assert all(getattr(L, k) == int(v) for k, v in bound.items()), \
+        {k: (getattr(L, k), v) for k, v in bound.items() if getattr(L, k) != int(v)}
+
+
+def test_plan_rejects_groups_beyond_the_incidence_code():
+    """More than FEA_PLAN_MAX_ELEMS elements (faces) in one group: FEA_ETOOBIG
+    before the connectivity is read (incidences e * 16 + a fit 32 bits)."""
+    from fea_b200 import _lib as L
+    conn = np.zeros(8, np.int32)
+    mask = np.full(8, 7, np.uint8)
+    h = ctypes.c_void_p()
+    one = lambda t, *v: (t * 1)(*v)
+    for ne, nf in ((L.FEA_PLAN_MAX_ELEMS + 1, 0), (1, L.FEA_PLAN_MAX_ELEMS + 1)):
+        st = L.fea_plan_build(8, mask.ctypes.data, 1, one(ctypes.c_int32, L.FEA_C3D8), one(ctypes.c_int64, ne),
+                              one(ctypes.c_void_p, conn.ctypes.data), 1, one(ctypes.c_int32, L.FEA_Q4),
+                              one(ctypes.c_int64, nf), one(ctypes.c_void_p, conn.ctypes.data), 0, 0, ctypes.byref(h))
+        assert st == L.FEA_ETOOBIG and not h.value
+    assert (L.FEA_PLAN_MAX_ELEMS - 1) * 16 + 15 <= 2 ** 31 - 1 < L.FEA_PLAN_MAX_ELEMS * 16 + 16
+
+
 def test_empty_group_and_fully_fixed_mesh():
     from fea_b200 import _lib as L
     hp = _plan(5, np.zeros(5, np.uint8), [("C3D4", np.zeros((0, 4), np.int32))])
