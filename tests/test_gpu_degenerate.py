@@ -4,7 +4,7 @@
   C3D4): the same reduced pattern as the populated group alone; the empty
   group's assembly, residual-only pass and energy add nothing, so both
   groups accumulated into zeroed buffers give the populated group's values
-  bit for bit.
+  bit for bit; a pressure load on an empty face group adds nothing either.
 - A mesh whose every DOF is fixed: an empty reduced system; the entry points
   take NULL for the (empty) solution, residual and matrix and the energy of
   the undeformed mesh is zero.
@@ -34,7 +34,8 @@ def test_empty_group_beside_a_populated_one(kind, n):
     free[:(n + 1) ** 2] = 0                                   # the plane x = 0 clamped
     empty = np.zeros((0, el.shape[1]), np.int32)
     P1 = DevicePlan(X, free, [(kind, el)])
-    P2 = DevicePlan(X, free, [(kind, empty), (kind, el)])
+    no_faces = ("Q4", np.zeros((0, 4), np.int32)) if kind == "C3D8" else ("T3", np.zeros((0, 3), np.int32))
+    P2 = DevicePlan(X, free, [(kind, empty), (kind, el)], faces=[no_faces])
     assert P2.groups[0].ne == 0 and not P2.groups[0].covers_active
     assert P1.nnz == P2.nnz and P1.ndof == P2.ndof
     assert torch.equal(P1.indptr, P2.indptr) and torch.equal(P1.indices, P2.indices)
@@ -47,6 +48,12 @@ def test_empty_group_beside_a_populated_one(kind, n):
     assert not K2.any() and not R2.any()                      # the empty group adds nothing
     P2.assemble_volume(1, MU, KAPPA, gc, K=K2, R=R2, accumulate=True)
     assert torch.equal(K1, K2) and torch.equal(R1, R2)
+    # a pressure load on no face adds nothing and encloses no volume
+    P2.assemble_pressure(0, 0.1, P2.X, gc, K=K2, R=R2)
+    vol = P2.zeros(1)
+    vol.fill_(7.0)
+    P2.pressure_volume(0, P2.X, gc, vol)
+    assert torch.equal(K1, K2) and torch.equal(R1, R2) and float(vol) == 0.0
     # the residual-only pass (its own kernel: the same bits as the populated
     # group's R-only pass alone, the K pass's residual to rounding)
     Rr1, Rr = P1.zeros(P1.ndof), P2.zeros(P2.ndof)
