@@ -21,7 +21,8 @@ FEA_OK = 0
 ERRORS = {-1: "invalid argument", -2: "index out of range", -3: "a node does not fit one gather chunk",
           -4: "shared memory request exceeds the device limit", -5: "work buffer too small",
           -6: "iteration cap reached", -7: "PCG breakdown (p.Ap <= 0 or non-finite)",
-          -8: "size beyond the fixed limit of an allocation-free entry point"}
+          -8: "size beyond a fixed limit (an allocation-free entry point, or FEA_PLAN_MAX_ELEMS per group)"}
+FEA_EINVAL, FEA_ERANGE, FEA_ECHUNK, FEA_ESMEM, FEA_EWORK = -1, -2, -3, -4, -5
 FEA_ENOTCONV = -6
 FEA_EBREAKDOWN = -7
 FEA_ETOOBIG = -8

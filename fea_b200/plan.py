@@ -42,6 +42,12 @@ class HostPlan:
     def __init__(self, n_nodes, free_mask, groups, faces, vol_threads=0, smem_doubles=0):
         self._h = None
         mask = np.ascontiguousarray(free_mask, dtype=np.uint8)
+        for _, c in list(groups) + list(faces):
+            # node ids are checked before the int32 cast, which would wrap
+            # an id of 2^32 + k onto node k
+            c = np.asarray(c)
+            if c.size and (c.min() < 0 or c.max() >= n_nodes):
+                L.check(L.FEA_ERANGE, "fea_plan_build")
         gconn = [np.ascontiguousarray(c, dtype=np.int32) for _, c in groups]
         fconn = [np.ascontiguousarray(c, dtype=np.int32) for _, c in faces]
         self._keep = (mask, gconn, fconn)

@@ -150,6 +150,14 @@ def test_plan_errors():
     with pytest.raises(L.FeaError) as ex:
         _plan(8, np.full(8, 7, np.uint8), [("C3D4", hub)])
     assert ex.value.status == -3
+    # 64-bit node ids beyond int32 are out of range, not wrapped onto small ids
+    wide = np.array([[0, 1, 2, 2 ** 32 + 3]], np.int64)
+    with pytest.raises(L.FeaError) as ex:
+        _plan(4, np.full(4, 7, np.uint8), [("C3D4", wide)])
+    assert ex.value.status == -2
+    with pytest.raises(L.FeaError) as ex:
+        _plan(4, np.full(4, 7, np.uint8), [("C3D4", np.array([[0, 1, 2, 3]]))], [("T3", np.array([[0, 1, -1]]))])
+    assert ex.value.status == -2
 
 
 def test_header_constants_match_the_binding():
