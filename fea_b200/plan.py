@@ -27,6 +27,21 @@ def stream():
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
+def need(t, n, device, what):
+    """A caller's buffer handed to a kernel as a raw pointer: float64,
+    contiguous, on the plan's device, at least n entries (else ValueError,
+    before any launch)."""
+    if t is None:
+        return
+    idx = device.index if device.index is not None else torch.cuda.current_device()
+    if (not isinstance(t, torch.Tensor) or t.dtype != torch.float64 or t.device.type != device.type
+            or t.device.index != idx or not t.is_contiguous() or t.numel() < n):
+        raise ValueError("%s: expected a contiguous float64 tensor of at least %d entries on %s, got %s" %
+                         (what, n, device, "%s %s %s%s" % (tuple(t.shape), t.dtype, t.device,
+                                                          "" if t.is_contiguous() else " (strided)")
+                          if isinstance(t, torch.Tensor) else type(t).__name__))
+
+
 class HostPlan:
     """Result of ``fea_plan_build`` (host memory)."""
 
@@ -208,6 +223,10 @@ class DevicePlan:
 
     def assemble_volume(self, gi, mu, kappa, gc, K=None, R=None, elemR=None, accumulate=False):
         g = self.groups[gi]
+        need(gc, self.ndof, self.device, "gc")
+        need(K, self.nnz, self.device, "K")
+        need(R, self.ndof, self.device, "R")
+        need(elemR, g.nn * 3 * g.ne, self.device, "elemR")
         w, wn = self.stage(gi) if K is not None else (None, 0)
         L.check(L.fea_assemble_volume(C.byref(self.nodes), C.byref(g.desc), float(mu), float(kappa), vptr(gc),
                                       vptr(K), vptr(R), vptr(elemR), int(bool(accumulate)), vptr(w), int(wn),
@@ -215,6 +234,10 @@ class DevicePlan:
 
     def assemble_pressure(self, fi, p, Xinst, gc, K=None, R=None):
         f = self.faces[fi]
+        need(Xinst, 3 * self.n_nodes, self.device, "Xinst")
+        need(gc, self.ndof, self.device, "gc")
+        need(K, self.nnz, self.device, "K")
+        need(R, self.ndof, self.device, "R")
         L.check(L.fea_assemble_pressure(C.byref(self.nodes), C.byref(f.desc), float(p), vptr(Xinst), vptr(gc),
                                         vptr(K), vptr(R), stream()), "fea_assemble_pressure")
 

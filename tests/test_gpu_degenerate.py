@@ -93,3 +93,26 @@ def test_fully_fixed_mesh_has_an_empty_system():
     out.fill_(7.0)
     P.energy_volume(0, MU, KAPPA, gc, out)                    # the undeformed mesh
     assert abs(float(out)) < 1e-14
+
+
+def test_bad_buffers_are_refused_before_any_launch():
+    """A caller's K / R / gc that is on the host, of another dtype, too short
+    or strided raises ValueError and launches nothing."""
+    from fea_b200 import _lib as L
+    from fea_b200.plan import DevicePlan
+    X, el = _mesh("C3D8", 2)
+    N = X.shape[0]
+    P = DevicePlan(X, np.full(N, 7, np.uint8), [("C3D8", el)])
+    gc = P.zeros(P.ndof)
+    K, R = P.zeros(P.nnz), P.zeros(P.ndof)
+    P.assemble_volume(0, MU, KAPPA, gc, K=K, R=R)
+    torch.cuda.synchronize()
+    n0 = L.fea_launch_count()
+    bad = [dict(K=K.cpu()), dict(K=K.float()), dict(K=K[:-1]), dict(R=P.zeros(2 * P.ndof)[::2]),
+           dict(gc=gc[:-1])]
+    for b in bad:
+        args = dict(gc=gc, K=K, R=R)
+        args.update(b)
+        with pytest.raises(ValueError):
+            P.assemble_volume(0, MU, KAPPA, args.pop("gc"), **args)
+    assert L.fea_launch_count() == n0
